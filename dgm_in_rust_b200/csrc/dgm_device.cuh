@@ -1,0 +1,883 @@
+// dgm_device.cuh -- device code of the B200 DG residual + SSP-RK3 path (FP64).
+//
+// Data layout in HBM (one solver instance):
+//   state      U[v*NB + b][ld]        SoA, v = conserved variable, b = Dubiner mode, ld = padded
+//                                      element count; a warp's 32 consecutive elements read one
+//                                      256-byte segment per (v, b).
+//   geometry   jac[ne], dinv[4][ld]   (dxi/dx, dxi/dy, deta/dx, deta/dy), hmin[ne], h15[ne]
+//   faces      face[3][ld]            (edge slot << 1) | side, side 1 = element is the edge's
+//                                      right element; slots [0, n_int) are internal edges,
+//                                      [n_int, n_int + n_bnd) boundary edges
+//   edge flux  F[slot][NG][4]          HLLC / boundary flux at the edge Gauss points, already
+//                                      multiplied by half the edge length; written by the edge
+//                                      pass, gathered by the element pass (no atomics).
+// Tables (basis, quadrature) travel in the kernel parameter block (constant bank), so every
+// compile-time-indexed table read is a broadcast operand.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dgm {
+
+constexpr int NEQ = 4;
+constexpr double F64_EPS = 2.220446049250313e-16;  // f64::EPSILON, weno.rs:1
+
+// Status codes (mirrors include/dgm_b200.h).
+enum : int {
+  ST_OK = 0,
+  ST_NEG_DENSITY = 1,
+  ST_NEG_PRESSURE = 2,
+  ST_NONFINITE = 3,
+  ST_TOO_MANY_BOUNDARY_EDGES = 4,
+  ST_TIMEOUT = 6,
+};
+
+// Supported discretisations: (order, triangle rule, edge rule, derivative keys used by WENO).
+template <int P> struct Variant;
+template <> struct Variant<1> { static constexpr int NB = 3, NQ = 3, NG = 2, NK = 2; };
+template <> struct Variant<2> { static constexpr int NB = 6, NQ = 6, NG = 3, NK = 5; };
+template <> struct Variant<3> { static constexpr int NB = 10, NQ = 12, NG = 4, NK = 9; };
+
+template <int P>
+struct Tables {
+  using V = Variant<P>;
+  double phi_cell[V::NQ][V::NB];          // phis_cell_gps
+  double dxi[V::NQ][V::NB];               // d/dxi  at cell points
+  double deta[V::NQ][V::NB];              // d/deta at cell points
+  double dref[V::NQ][V::NB][V::NK];       // all reference derivatives up to order P
+  double phi_edge[3][V::NG][V::NB];       // phis_edge_gps
+  double cell_w[V::NQ];
+  double edge_w[V::NG];
+  double mass[V::NB];
+};
+
+struct MeshDev {
+  int ne, ld, n_int, n_bnd;
+  const double* __restrict__ jac;     // [ne]
+  const double* __restrict__ dinv;    // [4][ld]
+  const double* __restrict__ hmin;    // [ne]
+  const double* __restrict__ h15;     // [ne] circumradius^1.5
+  const int* __restrict__ face;       // [3][ld]
+  const int* __restrict__ nbr;        // [3][ld]  -1 on the boundary
+  const int2* __restrict__ ie_lr;     // [n_int] left, right element
+  const int* __restrict__ ie_ic;      // [n_int] ilic | iric << 2
+  const double4* __restrict__ ie_geo; // [n_int] nx, ny, half length, length
+  const int* __restrict__ be_elem;    // [n_bnd]
+  const int* __restrict__ be_info;    // [n_bnd] ic | type << 2 | patch << 3
+  const double4* __restrict__ be_geo; // [n_bnd] outward nx, ny, half length, length
+  const double4* __restrict__ patch_q;// [np] conserved far-field state
+  const int64_t* __restrict__ slot_ref;  // [n_int + n_bnd] reference edge id of each slot
+};
+
+// Per-context control block in device memory: the time-march loop state lives here so the
+// whole loop can run from CUDA graphs without host round trips.
+struct Control {
+  double t, dt, final_time, cfl;
+  long long step, final_step;
+  unsigned long long dt_bits;  // atomicMin target for the global time step
+  int active;                  // this step runs (loop condition of temporal_disc.rs:22)
+  int status;                  // first error raised on the device
+  long long err_where;         // edge / element of that error
+  int t0_count;                // cells flagged by the parallel KXRCF pass
+  int troubled;                // cells limited by the last limiter pass
+  int waves;                   // limiter waves of the last pass
+  int unknown[2];              // per-wave count of unsettled cells (double-buffered)
+  unsigned int bar_count, bar_gen;  // grid barrier of the limiter kernel
+};
+
+template <int P>
+struct KParams {
+  Tables<P> tab;
+  MeshDev m;
+  double hcr;
+  Control* ctl;
+};
+
+__device__ __forceinline__ void raise_status(Control* ctl, int code, long long where) {
+  if (atomicCAS(&ctl->status, 0, code) == 0) ctl->err_where = where;
+}
+
+// flux::flux, flux.rs:154-169
+__device__ __forceinline__ void euler_flux(const double q[4], double hcr, double f[4], double g[4]) {
+  const double u = q[1] / q[0];
+  const double v = q[2] / q[0];
+  const double p = (hcr - 1.0) * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+  f[0] = q[1];
+  f[1] = q[1] * u + p;
+  f[2] = q[2] * u;
+  f[3] = u * (q[3] + p);
+  g[0] = q[2];
+  g[1] = q[1] * v;
+  g[2] = q[2] * v + p;
+  g[3] = v * (q[3] + p);
+}
+
+// flux::hllc, flux.rs:28-153.  Returns ST_NEG_DENSITY / ST_NEG_PRESSURE like the reference's Err.
+__device__ __forceinline__ int hllc(const double lv[4], const double rv[4], double nx, double ny,
+                                    double hcr, double flux[4]) {
+  const double ql0 = lv[0], ql1 = lv[1] * nx + lv[2] * ny, ql2 = -lv[1] * ny + lv[2] * nx, ql3 = lv[3];
+  const double qr0 = rv[0], qr1 = rv[1] * nx + rv[2] * ny, qr2 = -rv[1] * ny + rv[2] * nx, qr3 = rv[3];
+  const double ul = ql1 / ql0, ur = qr1 / qr0, vl = ql2 / ql0, vr = qr2 / qr0;
+  const double pl = (hcr - 1.0) * (ql3 - 0.5 * (ql1 * ql1 + ql2 * ql2) / ql0);
+  const double pr = (hcr - 1.0) * (qr3 - 0.5 * (qr1 * qr1 + qr2 * qr2) / qr0);
+  if (ql0 < 0.0 || qr0 < 0.0) return ST_NEG_DENSITY;
+  if (pl < 0.0 || pr < 0.0) return ST_NEG_PRESSURE;
+  const double cl = sqrt(hcr * pl / ql0);
+  const double cr = sqrt(hcr * pr / qr0);
+  const double fl0 = ql1, fl1 = ql1 * ul + pl, fl2 = ql2 * ul, fl3 = ul * (ql3 + pl);
+  const double fr0 = qr1, fr1 = qr1 * ur + pr, fr2 = qr2 * ur, fr3 = ur * (qr3 + pr);
+  const double zeta = (hcr - 1.0) / (2.0 * hcr);
+  const double p_star = pow((cl + cr - (zeta - 1.0) / 2.0 * (ur - ul)) / (cl / pow(pl, zeta) + cr / pow(pr, zeta)),
+                            1.0 / zeta);
+  const double ql_lower = (p_star <= pl) ? 1.0 : sqrt(1.0 + (hcr + 1.0) / (2.0 * hcr) * (p_star / pl - 1.0));
+  const double sl = ul - cl * ql_lower;
+  const double qr_lower = (p_star <= pr) ? 1.0 : sqrt(1.0 + (hcr + 1.0) / (2.0 * hcr) * (p_star / pr - 1.0));
+  const double sr = ur + cr * qr_lower;
+  double f0, fn, ft, f3;
+  if (sl >= 0.0) {
+    f0 = fl0; fn = fl1; ft = fl2; f3 = fl3;
+  } else if (sr <= 0.0) {
+    f0 = fr0; fn = fr1; ft = fr2; f3 = fr3;
+  } else {
+    const double s_star = (pr - pl + ql0 * ul * (sl - ul) - qr0 * ur * (sr - ur)) / (ql0 * (sl - ul) - qr0 * (sr - ur));
+    if (s_star >= 0.0) {
+      const double m = ql0 * (sl - ul) / (sl - s_star);
+      const double qs0 = m, qs1 = m * s_star, qs2 = m * vl;
+      const double qs3 = m * (ql3 / ql0 + (s_star - ul) * (s_star + pl / (ql0 * (sl - ul))));
+      f0 = fl0 + sl * (qs0 - ql0);
+      fn = fl1 + sl * (qs1 - ql1);
+      ft = fl2 + sl * (qs2 - ql2);
+      f3 = fl3 + sl * (qs3 - ql3);
+    } else {
+      const double m = qr0 * (sr - ur) / (sr - s_star);
+      const double qs0 = m, qs1 = m * s_star, qs2 = m * vr;
+      const double qs3 = m * (qr3 / qr0 + (s_star - ur) * (s_star + pr / (qr0 * (sr - ur))));
+      f0 = fr0 + sr * (qs0 - qr0);
+      fn = fr1 + sr * (qs1 - qr1);
+      ft = fr2 + sr * (qs2 - qr2);
+      f3 = fr3 + sr * (qs3 - qr3);
+    }
+  }
+  flux[0] = f0;
+  flux[1] = fn * nx - ft * ny;
+  flux[2] = fn * ny + ft * nx;
+  flux[3] = f3;
+  return ST_OK;
+}
+
+// compute_eigenmatrix, local_characteristics.rs:4-50
+__device__ __forceinline__ void eigenmatrix(const double q[4], double nx, double ny, double hcr,
+                                            double L[4][4], double R[4][4]) {
+  const double u = q[1] / q[0];
+  const double v = q[2] / q[0];
+  const double p = (hcr - 1.0) * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+  const double c = sqrt(hcr * p / q[0]);
+  const double h = (q[3] + p) / q[0];
+  const double b1 = (hcr - 1.0) / (c * c);
+  const double b2 = b1 * (u * u + v * v) / 2.0;
+  const double vn = u * nx + v * ny;
+  L[0][0] = (b2 + vn / c) / 2.0;
+  L[0][1] = -(b1 * u + nx / c) / 2.0;
+  L[0][2] = -(b1 * v + ny / c) / 2.0;
+  L[0][3] = b1 / 2.0;
+  L[1][0] = ny * u - nx * v;
+  L[1][1] = -ny;
+  L[1][2] = nx;
+  L[1][3] = 0.0;
+  L[2][0] = 1.0 - b2;
+  L[2][1] = b1 * u;
+  L[2][2] = b1 * v;
+  L[2][3] = -b1;
+  L[3][0] = (b2 - vn / c) / 2.0;
+  L[3][1] = -(b1 * u - nx / c) / 2.0;
+  L[3][2] = -(b1 * v - ny / c) / 2.0;
+  L[3][3] = b1 / 2.0;
+  R[0][0] = 1.0;
+  R[0][1] = 0.0;
+  R[0][2] = 1.0;
+  R[0][3] = 1.0;
+  R[1][0] = u - c * nx;
+  R[1][1] = -ny;
+  R[1][2] = u;
+  R[1][3] = u + c * nx;
+  R[2][0] = v - c * ny;
+  R[2][1] = nx;
+  R[2][2] = v;
+  R[2][3] = v + c * ny;
+  R[3][0] = h - c * vn;
+  R[3][1] = -u * ny + v * nx;
+  R[3][2] = (u * u + v * v) / 2.0;
+  R[3][3] = h + c * vn;
+}
+
+// Physical derivative of a mode for key kk from reference derivatives r[] (mesh.rs:101-114;
+// third order: the same chain rule expanded, p=3 extension).
+template <int NK>
+__device__ __forceinline__ double phys_deriv(const double (&r)[NK], double xx, double xy, double ex,
+                                             double ey, int kk) {
+  switch (kk) {
+    case 0: return xx * r[0] + ex * r[1];
+    case 1: return xy * r[0] + ey * r[1];
+  }
+  if constexpr (NK >= 5) {
+    switch (kk) {
+      case 2: return (xx * xx) * r[2] + 2.0 * xx * ex * r[3] + (ex * ex) * r[4];
+      case 3: return xx * xy * r[2] + (xx * ey + ex * xy) * r[3] + ex * ey * r[4];
+      case 4: return (xy * xy) * r[2] + 2.0 * xy * ey * r[3] + (ey * ey) * r[4];
+    }
+  }
+  if constexpr (NK >= 9) {
+    // (xx Dxi + ex Deta)^a (xy Dxi + ey Deta)^c, a + c = 3, c = kk - 5
+    switch (kk) {
+      case 5: return xx * xx * xx * r[5] + 3.0 * xx * xx * ex * r[6] + 3.0 * xx * ex * ex * r[7] + ex * ex * ex * r[8];
+      case 6: return xx * xx * xy * r[5] + (xx * xx * ey + 2.0 * xx * ex * xy) * r[6] +
+                     (2.0 * xx * ex * ey + ex * ex * xy) * r[7] + ex * ex * ey * r[8];
+      case 7: return xx * xy * xy * r[5] + (2.0 * xx * xy * ey + ex * xy * xy) * r[6] +
+                     (xx * ey * ey + 2.0 * ex * xy * ey) * r[7] + ex * ey * ey * r[8];
+      case 8: return xy * xy * xy * r[5] + 3.0 * xy * xy * ey * r[6] + 3.0 * xy * ey * ey * r[7] + ey * ey * ey * r[8];
+    }
+  }
+  return 0.0;
+}
+
+__device__ __forceinline__ double ld_state(const double* p) { return __ldcg(p); }
+
+// ------------------------------------------------------------------------------------------
+// Edge pass: one thread per (edge slot, Gauss point).  Internal slots: traces of both
+// elements + HLLC (integrate_over_edges_euler, spatial_disc.rs:161-211).  Boundary slots:
+// slip-wall pressure flux or characteristic far-field flux (apply_bc_euler,
+// boundary_condition.rs:19-97).  Writes F[slot][g][v] * half length.
+// ------------------------------------------------------------------------------------------
+template <int P>
+__global__ void __launch_bounds__(256) k_edge_flux(const __grid_constant__ KParams<P> kp,
+                                                   const double* __restrict__ U, double* __restrict__ F) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NG = V::NG;
+  __shared__ double s_pe[3 * NG * NB];
+  for (int i = threadIdx.x; i < 3 * NG * NB; i += blockDim.x) s_pe[i] = (&kp.tab.phi_edge[0][0][0])[i];
+  __syncthreads();
+  if (!kp.ctl->active) return;
+  const MeshDev& m = kp.m;
+  const double hcr = kp.hcr;
+  const int total = (m.n_int + m.n_bnd) * NG;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int s = t / NG, g = t - s * NG;
+    double out[4];
+    if (s < m.n_int) {
+      const int2 lr = m.ie_lr[s];
+      const int ic = m.ie_ic[s];
+      const double* pl = &s_pe[((ic & 3) * NG + g) * NB];
+      const double* pr = &s_pe[((ic >> 2) * NG + (NG - 1 - g)) * NB];
+      double lv[4], rv[4];
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) {
+        double a = 0.0, c = 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          a += ld_state(&U[(size_t)(v * NB + b) * m.ld + lr.x]) * pl[b];
+          c += ld_state(&U[(size_t)(v * NB + b) * m.ld + lr.y]) * pr[b];
+        }
+        lv[v] = a;
+        rv[v] = c;
+      }
+      const double4 geo = m.ie_geo[s];
+      const int st = hllc(lv, rv, geo.x, geo.y, hcr, out);
+      if (st != ST_OK) raise_status(kp.ctl, st, m.slot_ref[s]);
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) out[v] *= geo.z;
+    } else {
+      const int sb = s - m.n_int;
+      const int e = m.be_elem[sb];
+      const int info = m.be_info[sb];
+      const double* pe = &s_pe[((info & 3) * NG + g) * NB];
+      double lv[4];
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) {
+        double a = 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) a += ld_state(&U[(size_t)(v * NB + b) * m.ld + e]) * pe[b];
+        lv[v] = a;
+      }
+      const double4 geo = m.be_geo[sb];
+      const double nx = geo.x, ny = geo.y;
+      if (((info >> 2) & 1) == 0) {
+        // slip wall, boundary_condition.rs:31-47
+        const double pressure = (hcr - 1.0) * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+        out[0] = 0.0;
+        out[1] = pressure * nx;
+        out[2] = pressure * ny;
+        out[3] = 0.0;
+      } else {
+        // characteristic far field, boundary_condition.rs:48-94
+        const double4 bq = m.patch_q[info >> 3];
+        const double bc[4] = {bq.x, bq.y, bq.z, bq.w};
+        const double u = lv[1] / lv[0];
+        const double v = lv[2] / lv[0];
+        const double p = (hcr - 1.0) * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+        const double c = sqrt(hcr * p / lv[0]);
+        const double vn = u * nx + v * ny;
+        double Lm[4][4], Rm[4][4];
+        eigenmatrix(lv, nx, ny, hcr, Lm, Rm);
+        const double lam[4] = {vn - c, vn, vn, vn + c};
+        double mix[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          double alpha = 0.0, beta = 0.0;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            alpha += Lm[i][j] * lv[j];
+            beta += Lm[i][j] * bc[j];
+          }
+          mix[i] = lam[i] >= 0.0 ? alpha : beta;
+        }
+        double q[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          double sum = 0.0;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) sum += Rm[i][j] * mix[j];
+          q[i] = sum;
+        }
+        const double un = q[1] / q[0];
+        const double vv = q[2] / q[0];
+        const double vn_new = un * nx + vv * ny;
+        const double p_new = (hcr - 1.0) * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+        const double h_new = q[3] + p_new;
+        out[0] = q[0] * vn_new;
+        out[1] = q[1] * vn_new + p_new * nx;
+        out[2] = q[2] * vn_new + p_new * ny;
+        out[3] = h_new * vn_new;
+      }
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) out[v] *= geo.z;
+    }
+    double2* dst = reinterpret_cast<double2*>(&F[((size_t)s * NG + g) * 4]);
+    dst[0] = make_double2(out[0], out[1]);
+    dst[1] = make_double2(out[2], out[3]);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Element pass: one thread per element.  Volume integral (integrate_over_cell_euler,
+// spatial_disc.rs:40-69, and boundary_condition.rs:98-117 for boundary elements), gather of
+// the three faces' edge fluxes with the left/right sign and Gauss-point reversal of
+// spatial_disc.rs:202-206, inverse mass (spatial_disc.rs:349-357), then the SSP-RK3 stage
+// combination of rk3.rs:10,16,22.
+//   MODE 0: out = (Rin + terms) / mass            (compute_residuals semantics)
+//   MODE 1: out = Uin + dt R
+//   MODE 2: out = 0.75 Ubase + 0.25 (Uin + dt R)
+//   MODE 3: out = 1/3 Ubase + 2/3 (Uin + dt R)
+// ------------------------------------------------------------------------------------------
+template <int P, int MODE>
+__global__ void __launch_bounds__(128) k_element(const __grid_constant__ KParams<P> kp,
+                                                 const double* __restrict__ Uin,
+                                                 const double* Ubase,
+                                                 const double* __restrict__ F,
+                                                 double* Uout,
+                                                 const double* Rin,
+                                                 double* Rout) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NQ = V::NQ, NG = V::NG;
+  Control* ctl = kp.ctl;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl->t0_count = 0;
+    ctl->unknown[0] = 0;
+    ctl->unknown[1] = 0;
+  }
+  if (!ctl->active) return;
+  const MeshDev& m = kp.m;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.ne) return;
+  const size_t ld = m.ld;
+  double u[NEQ][NB], r[NEQ][NB];
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v)
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      u[v][b] = ld_state(&Uin[(v * NB + b) * ld + e]);
+      r[v][b] = 0.0;
+    }
+  const double J = m.jac[e];
+  const double xx = m.dinv[0 * ld + e], xy = m.dinv[1 * ld + e], ex = m.dinv[2 * ld + e], ey = m.dinv[3 * ld + e];
+  const double hcr = kp.hcr;
+  // volume term
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double uq[NEQ];
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) {
+      double a = 0.0;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) a += u[v][b] * kp.tab.phi_cell[q][b];
+      uq[v] = a;
+    }
+    double f[NEQ], g[NEQ];
+    euler_flux(uq, hcr, f, g);
+    const double sc = kp.tab.cell_w[q] * 0.5 * J;
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) {
+      const double fx = sc * (f[v] * xx + g[v] * xy);
+      const double fe = sc * (f[v] * ex + g[v] * ey);
+#pragma unroll
+      for (int b = 0; b < NB; ++b) r[v][b] += fx * kp.tab.dxi[q][b] + fe * kp.tab.deta[q][b];
+    }
+  }
+  // face terms
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int fw = m.face[k * ld + e];
+    const int slot = fw >> 1;
+    const bool right = fw & 1;
+    const double* Fs = &F[(size_t)slot * NG * 4];
+#pragma unroll
+    for (int gp = 0; gp < NG; ++gp) {
+      const int src = right ? (NG - 1 - gp) : gp;
+      const double2 a = __ldcg(reinterpret_cast<const double2*>(&Fs[src * 4]));
+      const double2 c = __ldcg(reinterpret_cast<const double2*>(&Fs[src * 4 + 2]));
+      const double coef = right ? kp.tab.edge_w[gp] : -kp.tab.edge_w[gp];
+      const double fv[4] = {coef * a.x, coef * a.y, coef * c.x, coef * c.y};
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) r[v][b] += fv[v] * kp.tab.phi_edge[k][gp][b];
+    }
+  }
+  const double dt = ctl->dt;
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v)
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const size_t idx = (v * NB + b) * ld + e;
+      double rr = r[v][b];
+      if constexpr (MODE == 0) rr = Rin[idx] + rr;
+      rr = rr / (kp.tab.mass[b] * 0.5 * J);
+      if (Rout) Rout[idx] = rr;
+      if constexpr (MODE == 1) {
+        Uout[idx] = u[v][b] + dt * rr;
+      } else if constexpr (MODE == 2) {
+        Uout[idx] = 0.75 * Ubase[idx] + 0.25 * (u[v][b] + dt * rr);
+      } else if constexpr (MODE == 3) {
+        Uout[idx] = (1.0 / 3.0) * Ubase[idx] + (2.0 / 3.0) * (u[v][b] + dt * rr);
+      }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// modified_kxrcf, weno.rs:7-85, for element e on state U.  Keeps the reference's exterior-trace
+// indexing: the neighbour's modes are evaluated with this element's own local edge index k
+// (weno.rs:21-27 pick in_cell_indices[side], which is always this element's index).
+// ------------------------------------------------------------------------------------------
+template <int P>
+__device__ __forceinline__ bool kxrcf(const KParams<P>& kp, const double* __restrict__ U, int e) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NG = V::NG;
+  const MeshDev& m = kp.m;
+  const size_t ld = m.ld;
+  double density_jump = 0.0, total_energy_jump = 0.0, surface = 0.0;
+  double min_density = 1.0e10, min_total_energy = 1.0e10;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int fw = m.face[k * ld + e];
+    const int slot = fw >> 1;
+    if (slot >= m.n_int) continue;
+    const int nb = m.nbr[k * ld + e];
+    const double4 geo = m.ie_geo[slot];
+    const double nx = (fw & 1) ? -geo.x : geo.x;
+    const double ny = (fw & 1) ? -geo.y : geo.y;
+    double own_rho[NG], own_rhoe[NG];
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+      double rho = 0.0, rho_e = 0.0;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        rho += ld_state(&U[(0 * NB + b) * ld + e]) * kp.tab.phi_edge[k][g][b];
+        rho_e += ld_state(&U[(3 * NB + b) * ld + e]) * kp.tab.phi_edge[k][g][b];
+      }
+      own_rho[g] = rho;
+      own_rhoe[g] = rho_e;
+      if (rho < min_density) min_density = rho;
+      if (rho_e < min_total_energy) min_total_energy = rho_e;
+    }
+    constexpr int cg = NG / 2;
+    double rho_u = 0.0, rho_v = 0.0;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      rho_u += ld_state(&U[(1 * NB + b) * ld + e]) * kp.tab.phi_edge[k][cg][b];
+      rho_v += ld_state(&U[(2 * NB + b) * ld + e]) * kp.tab.phi_edge[k][cg][b];
+    }
+    if (rho_u * nx + rho_v * ny < 0.0) {
+      double rho_jump = 0.0, rho_e_jump = 0.0;
+      const double jd = geo.w;
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        double er = 0.0, ere = 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          er += ld_state(&U[(0 * NB + b) * ld + nb]) * kp.tab.phi_edge[k][NG - 1 - g][b];
+          ere += ld_state(&U[(3 * NB + b) * ld + nb]) * kp.tab.phi_edge[k][NG - 1 - g][b];
+        }
+        rho_jump += 0.5 * jd * kp.tab.edge_w[g] * (own_rho[g] - er);
+        rho_e_jump += 0.5 * jd * kp.tab.edge_w[g] * (own_rhoe[g] - ere);
+      }
+      density_jump += rho_jump;
+      total_energy_jump += rho_e_jump;
+      surface += jd;
+    }
+  }
+  const double h15 = m.h15[e];
+  const double ind_d = fabs(density_jump) / (h15 * surface * min_density);
+  const double ind_e = fabs(total_energy_jump) / (h15 * surface * min_total_energy);
+  return (ind_d >= 1.0) || (ind_e >= 1.0);
+}
+
+// Parallel KXRCF pass on the unlimited stage state: flags t0[e], resets the limiter status.
+template <int P>
+__global__ void __launch_bounds__(256) k_detect(const __grid_constant__ KParams<P> kp,
+                                                const double* __restrict__ U,
+                                                unsigned char* __restrict__ t0,
+                                                unsigned int* __restrict__ status) {
+  Control* ctl = kp.ctl;
+  if (!ctl->active) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  int flag = 0;
+  if (e < kp.m.ne) {
+    flag = kxrcf<P>(kp, U, e) ? 1 : 0;
+    t0[e] = (unsigned char)flag;
+    status[e] = 0u;
+  }
+  const unsigned int ballot = __ballot_sync(0xffffffffu, flag);
+  if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(&ctl->t0_count, __popc(ballot));
+}
+
+// ------------------------------------------------------------------------------------------
+// weno, weno.rs:86-269: characteristic WENO reconstruction of element e, one warp per element.
+// Lanes split the projections (lane -> (r, b)), the smoothness indicators (lane -> (j, v)) and
+// the recombination (lane -> (r, b)); sums run in the reference's order within each lane.
+// ------------------------------------------------------------------------------------------
+template <int P>
+struct WenoScratch {
+  using V = Variant<P>;
+  double tgt[NEQ][V::NB];
+  double nbp[3][NEQ][V::NB];
+  double proj[4][NEQ][V::NB];
+  double pol_new[NEQ][V::NB];
+  double recon[NEQ][V::NB];
+  double L[4][4], R[4][4];
+  double nlw[4][NEQ];
+};
+
+template <int P>
+__device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __restrict__ U, int e, int lane,
+                                WenoScratch<P>& S) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NQ = V::NQ, NK = V::NK;
+  const MeshDev& m = kp.m;
+  const size_t ld = m.ld;
+  int faces[3], nbrs[3];
+  bool interior[3];
+  int nbd = 0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    faces[k] = m.face[k * ld + e];
+    interior[k] = (faces[k] >> 1) < m.n_int;
+    nbrs[k] = m.nbr[k * ld + e];
+    if (!interior[k]) ++nbd;
+  }
+  if (nbd > 2) return ST_TOO_MANY_BOUNDARY_EDGES;
+  // linear weights with the reference's indexing (weno.rs:93-110)
+  double lw[4] = {0.997, 0.001, 0.001, 0.001};
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    if (!interior[k]) lw[k] = 0.0;
+  if (nbd == 0) lw[0] = 0.997;
+  else if (nbd == 1) lw[1] = 0.998;
+  else lw[2] = 0.999;
+  for (int i = lane; i < NEQ * NB; i += 32) {
+    const int v = i / NB, b = i - v * NB;
+    S.tgt[v][b] = ld_state(&U[(v * NB + b) * ld + e]);
+    S.recon[v][b] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) S.nbp[k][v][b] = interior[k] ? ld_state(&U[(v * NB + b) * ld + nbrs[k]]) : 0.0;
+  }
+  __syncwarp();
+  const double J = m.jac[e];
+  const double xx = m.dinv[0 * ld + e], xy = m.dinv[1 * ld + e], ex = m.dinv[2 * ld + e], ey = m.dinv[3 * ld + e];
+  double neighbour_area = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    if (!interior[i]) continue;
+    const double Jnb = m.jac[nbrs[i]];
+    neighbour_area += Jnb * 0.5;
+    const double4 geo = m.ie_geo[faces[i] >> 1];
+    if (lane == 0) {
+      double mean[4];
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) mean[v] = S.tgt[v][0];
+      eigenmatrix(mean, geo.x, geo.y, kp.hcr, S.L, S.R);
+    }
+    __syncwarp();
+    // projections: proj[0] = L tgt, proj[j+1] = L (nb_j with mode 0 <- tgt mode 0)
+    for (int idx = lane; idx < 4 * NEQ * NB; idx += 32) {
+      const int j = idx / (NEQ * NB), rem = idx - j * NEQ * NB, r = rem / NB, b = rem - r * NB;
+      double sum = 0.0;
+      if (j == 0) {
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) sum += S.L[r][k] * S.tgt[k][b];
+      } else if (interior[j - 1]) {
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) sum += S.L[r][k] * (b == 0 ? S.tgt[k][0] : S.nbp[j - 1][k][b]);
+      }
+      S.proj[j][r][b] = sum;
+    }
+    __syncwarp();
+    // smoothness indicators (weno.rs:125-143, 156-174)
+    if (lane < 4 * NEQ) {
+      const int j = lane >> 2, v = lane & 3;
+      double w = 0.0;
+      if (j == 0 || interior[j - 1]) {
+        double beta = 0.0;
+#pragma unroll
+        for (int l = 1; l <= P; ++l) {
+#pragma unroll
+          for (int l1 = 0; l1 <= l; ++l1) {
+            const int l2 = l - l1;
+            const int kk = l * (l + 1) / 2 - 1 + l2;  // key (l1, l2)
+            double integral = 0.0;
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+              double value = 0.0;
+#pragma unroll
+              for (int b = 0; b < NB; ++b)
+                value += S.proj[j][v][b] * phys_deriv<NK>(kp.tab.dref[q][b], xx, xy, ex, ey, kk);
+              integral += 0.5 * J * kp.tab.cell_w[q] * (value * value);
+            }
+            const double jp = (l == 1) ? 1.0 : (l == 2 ? J : J * J);
+            beta += jp * integral;
+          }
+        }
+        w = lw[j] / ((beta + F64_EPS) * (beta + F64_EPS));
+      }
+      S.nlw[j][v] = w;
+    }
+    __syncwarp();
+    // normalise and combine (weno.rs:180-194)
+    for (int idx = lane; idx < NEQ * NB; idx += 32) {
+      const int v = idx / NB, b = idx - v * NB;
+      const double den = ((S.nlw[0][v] + S.nlw[1][v]) + S.nlw[2][v]) + S.nlw[3][v];
+      double acc = 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc += (S.nlw[j][v] / den) * S.proj[j][v][b];
+      S.pol_new[v][b] = acc;
+    }
+    __syncwarp();
+    // back to conserved variables and area weighting (weno.rs:195-196)
+    for (int idx = lane; idx < NEQ * NB; idx += 32) {
+      const int r = idx / NB, b = idx - r * NB;
+      double sum = 0.0;
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) sum += S.R[r][k] * S.pol_new[k][b];
+      S.recon[r][b] = S.recon[r][b] + sum * Jnb * 0.5;
+    }
+    __syncwarp();
+  }
+  for (int idx = lane; idx < NEQ * NB; idx += 32) {
+    const int v = idx / NB, b = idx - v * NB;
+    U[(v * NB + b) * ld + e] = S.recon[v][b] / neighbour_area;
+  }
+  __syncwarp();
+  return ST_OK;
+}
+
+// Bounded grid barrier for the co-resident (cooperative) limiter kernel.
+__device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int nblocks) {
+  __syncthreads();
+  __shared__ int s_fail;
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    volatile unsigned int* gen = &ctl->bar_gen;
+    const unsigned int g = *gen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(&ctl->bar_count, 1u);
+    if (arrived == nblocks - 1) {
+      ctl->bar_count = 0u;
+      __threadfence();
+      atomicAdd(&ctl->bar_gen, 1u);
+    } else {
+      long long it = 0;
+      while (*gen == g) {
+        if (++it > (1ll << 25)) {  // ~ seconds: co-residency is guaranteed, so this is a fault
+          raise_status(ctl, ST_TIMEOUT, -1);
+          s_fail = 1;
+          break;
+        }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_fail == 0;
+}
+
+// Limiter waves.  Reproduces the reference's sequential, in-place limiter (weno.rs:90-263,
+// element order) exactly, in parallel: an element settles in wave w once every lower-index
+// neighbour settled in an earlier wave.  Its KXRCF flag is recomputed when such a neighbour
+// was rewritten (else the parallel flag t0 stands); a troubled element is reconstructed from
+// final lower neighbours and untouched higher neighbours, exactly the values the sequential
+// loop sees.  Elements settled in one wave are never neighbours with one reading the other,
+// so in-place writes are race free.  Status word: (wave << 2) | kind, kind 1 clean, 2 limited.
+template <int P>
+__global__ void __launch_bounds__(256) k_limiter_waves(const __grid_constant__ KParams<P> kp,
+                                                       double* __restrict__ U,
+                                                       const unsigned char* __restrict__ t0,
+                                                       unsigned int* __restrict__ status) {
+  Control* ctl = kp.ctl;
+  if (!ctl->active) return;
+  if (ctl->t0_count == 0) {  // nothing flagged: the sequential loop changes nothing
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctl->troubled = 0;
+      ctl->waves = 0;
+    }
+    return;
+  }
+  const MeshDev& m = kp.m;
+  __shared__ WenoScratch<P> scratch[8];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int gwarp = blockIdx.x * (blockDim.x >> 5) + wib;
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  int troubled_local = 0;
+  int wave = 1;
+  for (;; ++wave) {
+    int unknown_local = 0;
+    for (int e = gwarp; e < m.ne; e += nwarps) {
+      const unsigned int st = __ldcg(&status[e]);
+      if (st & 3u) continue;
+      bool ready = true, any_mod = false;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int nb = m.nbr[k * m.ld + e];
+        if (nb >= 0 && nb < e) {
+          const unsigned int sn = __ldcg(&status[nb]);
+          if ((sn & 3u) == 0u || (int)(sn >> 2) >= wave) ready = false;
+          else if ((sn & 3u) == 2u) any_mod = true;
+        }
+      }
+      if (!ready) {
+        ++unknown_local;
+        continue;
+      }
+      bool trouble = t0[e] != 0;
+      if (any_mod) trouble = kxrcf<P>(kp, U, e);
+      if (trouble) {
+        const int rs = weno_reconstruct<P>(kp, U, e, lane, scratch[wib]);
+        if (rs != ST_OK && lane == 0) raise_status(ctl, rs, e);
+        ++troubled_local;
+      }
+      __threadfence();
+      if (lane == 0) status[e] = ((unsigned int)wave << 2) | (trouble ? 2u : 1u);
+    }
+    if (lane == 0 && unknown_local) atomicAdd(&ctl->unknown[wave & 1], unknown_local);
+    if (!grid_barrier(ctl, gridDim.x)) break;
+    const int remaining = *((volatile int*)&ctl->unknown[wave & 1]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->unknown[(wave + 1) & 1] = 0;
+    if (remaining == 0 || wave > m.ne + 2) break;
+    if (!grid_barrier(ctl, gridDim.x)) break;
+  }
+  if (lane == 0 && troubled_local) atomicAdd(&ctl->troubled, troubled_local);
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->waves = wave;
+}
+
+// compute_time_step, temporal_disc.rs:58-88: global minimum over elements (deterministic).
+template <int P>
+__global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KParams<P> kp,
+                                                   const double* __restrict__ U) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB;
+  Control* ctl = kp.ctl;
+  if (!ctl->active) return;
+  const MeshDev& m = kp.m;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long bits = 0x7ff0000000000000ull;  // +inf never wins against 1e10
+  if (e < m.ne) {
+    double s[NEQ];
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) {
+      double a = 0.0;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) a += ld_state(&U[(size_t)(v * NB + b) * m.ld + e]);
+      s[v] = a;
+    }
+    const double hcr = kp.hcr;
+    const double rho = s[0];
+    const double u = s[1] / rho;
+    const double v = s[2] / rho;
+    const double p = (hcr - 1.0) * (s[3] - 0.5 * rho * (u * u + v * v));
+    const double c = sqrt(hcr * p / rho);
+    const double speed = sqrt(u * u + v * v) + c;
+    const double dt = ctl->cfl * m.hmin[e] / speed;
+    if (dt < 1.0e10) bits = (unsigned long long)__double_as_longlong(dt);  // NaN never passes
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+    bits = other < bits ? other : bits;
+  }
+  __shared__ unsigned long long s_min[8];
+  if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = bits;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long b = s_min[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) b = s_min[i] < b ? s_min[i] : b;
+    atomicMin(&ctl->dt_bits, b);
+  }
+}
+
+// Loop head of time_march (temporal_disc.rs:22): decide whether this step runs.
+__global__ void k_step_begin(Control* ctl) {
+  const bool run = ctl->status == 0 && ctl->step < ctl->final_step && ctl->t < ctl->final_time;
+  ctl->active = run ? 1 : 0;
+  ctl->dt_bits = (unsigned long long)__double_as_longlong(1.0e10);
+  ctl->troubled = 0;
+}
+// temporal_disc.rs:23-26: the step's dt, clamped to reach final_time exactly.
+__global__ void k_step_dt(Control* ctl) {
+  if (!ctl->active) return;
+  double dt = __longlong_as_double((long long)ctl->dt_bits);
+  if (ctl->t + dt > ctl->final_time) dt = ctl->final_time - ctl->t;
+  ctl->dt = dt;
+}
+// temporal_disc.rs:32-33
+__global__ void k_step_end(Control* ctl) {
+  if (!ctl->active) return;
+  ctl->t += ctl->dt;
+  ctl->step += 1;
+}
+// Host-driven calls (compute_residuals / apply_limiter / rk3 with a given dt).
+__global__ void k_set_active(Control* ctl, double dt, int reset_dt) {
+  ctl->active = 1;
+  if (reset_dt) {
+    ctl->dt = dt;
+  }
+  ctl->dt_bits = (unsigned long long)__double_as_longlong(1.0e10);
+  ctl->troubled = 0;
+  ctl->t0_count = 0;
+}
+
+// Layout transposes between the reference's [element][variable][basis] and the SoA state.
+template <int NB>
+__global__ void k_aos_to_soa(const double* __restrict__ src, double* __restrict__ dst, int ne, int ld) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)ne * NEQ * NB) return;
+  const int e = (int)(i / (NEQ * NB));
+  const int c = (int)(i - (long long)e * NEQ * NB);
+  dst[(size_t)c * ld + e] = src[i];
+}
+template <int NB>
+__global__ void k_soa_to_aos(const double* __restrict__ src, double* __restrict__ dst, int ne, int ld) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)ne * NEQ * NB) return;
+  const int e = (int)(i / (NEQ * NB));
+  const int c = (int)(i - (long long)e * NEQ * NB);
+  dst[i] = src[(size_t)c * ld + e];
+}
+
+}  // namespace dgm

@@ -1,0 +1,331 @@
+"""Host-side mirror of DGM_in_rust's solver objects, backed by the CUDA library.
+
+Names, argument meaning and error behaviour follow the reference:
+
+* :class:`SpatialDisc` -- ``compute_residuals(residuals, solutions)`` (src/spatial_disc.rs:27)
+  and ``apply_limiter(solutions)`` (src/spatial_disc/limiter.rs:7);
+* :class:`TemperalDisc` -- ``rk3(spatial_disc, residuals, solutions, time_step)``
+  (src/temporal_disc/rk3.rs:7), ``time_march(spatial_disc, residuals, solutions)``
+  (src/temporal_disc.rs:21), ``compute_time_step(solutions)`` (src/temporal_disc.rs:58);
+* :class:`Solver` -- ``set_initial_solution()`` (src/solver.rs:45) and ``solve()``
+  (src/solver.rs:80).
+
+States are numpy float64 arrays shaped like the reference's ``Array<f64, Ix3>``
+``[element][variable][basis]``.  Where the reference panics (negative density/pressure in
+HLLC, an element with three boundary edges in WENO) these raise :class:`DgmError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+
+import numpy as np
+
+from . import _native
+from ._native import DgmError
+from .basis_function import DubinerBasis, GaussPoints, default_rules
+from .mesh import Mesh
+
+__all__ = [
+    "SolverParameters",
+    "FlowParameters",
+    "MeshParameters",
+    "InitialSolution",
+    "SpatialDisc",
+    "TemperalDisc",
+    "Solver",
+    "reference_cfl",
+    "initial_state",
+]
+
+
+def reference_cfl(order: int) -> float:
+    """CFL formula of initialization.rs:29-33 (overrides the JSON value in the reference)."""
+    p = float(order)
+    return 1.0 * 1.0 / ((2.0 * p + 1.0) * (1.0 + 4.0 / (p + 2.0) ** 2.0))
+
+
+@dataclasses.dataclass
+class SolverParameters:
+    """SolverParameters (src/solver.rs:10-20)."""
+
+    cfl: float
+    final_time: float
+    final_step: int
+    order_of_polynomials: int = 2
+    number_of_cell_gp: int = 6
+    number_of_edge_gp: int = 3
+    number_of_equations: int = 4
+    inviscid_flux_scheme: str = "hllc"
+
+    @property
+    def number_of_basis_functions(self) -> int:
+        p = self.order_of_polynomials
+        return (p + 1) * (p + 2) // 2
+
+    def __post_init__(self):
+        if self.inviscid_flux_scheme.lower() != "hllc":
+            raise ValueError("Inviscid flux scheme not implemented")
+        if self.number_of_equations != 4:
+            raise ValueError("the Euler system has 4 equations")
+
+
+@dataclasses.dataclass
+class FlowParameters:
+    """FlowParameters (src/solver.rs:27-31)."""
+
+    hcr: float = 1.4
+    gas_constant: float = 287.0
+    prandtl_number: float = 0.72
+
+
+@dataclasses.dataclass
+class MeshParameters:
+    """MeshParameters (src/solver.rs:21-26)."""
+
+    number_of_elements: int
+    number_of_edges: int
+    number_of_vertices: int
+    number_of_patches: int
+
+    @staticmethod
+    def of(mesh: Mesh) -> "MeshParameters":
+        return MeshParameters(mesh.n_elements, mesh.n_edges, int(mesh.vertices.shape[0]),
+                              int(mesh.patch_type.shape[0]))
+
+
+@dataclasses.dataclass
+class InitialSolution:
+    """InitialSolution (src/io/initial_solution_parser.rs:4-10)."""
+
+    density: float
+    angle_of_attack: float
+    mach_number: float
+    pressure: float
+
+
+def initial_state(mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints, hcr: float,
+                  init: InitialSolution) -> np.ndarray:
+    """L2 projection of a uniform state onto the basis (Solver::set_initial_solution,
+    src/solver.rs:45-79), same summation order as the reference."""
+    rho, p = init.density, init.pressure
+    c = math.sqrt(hcr * p / rho)
+    a = init.angle_of_attack * (math.pi / 180.0)
+    xv = init.mach_number * math.cos(a) * c
+    yv = init.mach_number * math.sin(a) * c
+    te = p / (hcr - 1.0) + 0.5 * rho * (xv * xv + yv * yv)
+    q = np.array([rho, rho * xv, rho * yv, te])
+    J = mesh.elem_jacob_det
+    nb = basis.dof
+    U = np.zeros((mesh.n_elements, 4, nb))
+    for g in range(gauss_points.cell_gp_number):
+        U += ((0.5 * J)[:, None, None] * gauss_points.cell_weights[g] * q[None, :, None]
+              * basis.phis_cell_gps[g][None, None, :])
+    U /= basis.mass_mat_diag[None, None, :] * 0.5 * J[:, None, None]
+    return U
+
+
+def _check_state(a: np.ndarray, ne: int, nb: int, name: str) -> None:
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or a.shape != (ne, 4, nb) or not a.flags.c_contiguous:
+        raise ValueError(f"{name} must be a C-contiguous float64 array of shape ({ne}, 4, {nb})")
+
+
+class SpatialDisc:
+    """GPU-resident SpatialDisc (src/spatial_disc.rs:17-25).  Owns the device context."""
+
+    def __init__(self, mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints,
+                 flow_param: FlowParameters, mesh_param: MeshParameters, solver_param: SolverParameters,
+                 limiter: bool = True, device: int = 0):
+        self.mesh = mesh
+        self.basis = basis
+        self.gauss_points = gauss_points
+        self.flow_param = flow_param
+        self.mesh_param = mesh_param
+        self.solver_param = solver_param
+        self.limiter = bool(limiter)
+        L = _native.lib()
+        keep = []
+
+        def f64(a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            return _native.dptr(a)
+
+        def i64(a):
+            a = np.ascontiguousarray(a, dtype=np.int64)
+            keep.append(a)
+            return _native.iptr(a)
+
+        def i32(a):
+            a = np.ascontiguousarray(a, dtype=np.int32)
+            keep.append(a)
+            return _native.i32ptr(a)
+
+        m = mesh
+        md = _native.MeshDesc(
+            n_vertices=m.vertices.shape[0], n_elements=m.n_elements, n_edges=m.n_edges,
+            n_patches=m.patch_type.shape[0], vertex_xy=f64(m.vertices), elem_vertices=i64(m.elem_vertices),
+            elem_edges=i64(m.elem_edges), elem_neighbours=i64(m.elem_neighbours),
+            elem_jacob_det=f64(m.elem_jacob_det), elem_circumradius=f64(m.elem_circumradius),
+            elem_minimum_height=f64(m.elem_minimum_height), edge_elements=i64(m.edge_elements),
+            edge_vertices=i64(m.edge_vertices), edge_in_cell=i64(m.edge_in_cell),
+            edge_jacob_det=f64(m.edge_jacob_det), edge_normal=f64(m.edge_normal), edge_patch=i64(m.edge_patch),
+            patch_type=i32(m.patch_type), patch_quantity=f64(m.patch_quantity),
+            n_internal_edges=m.internal_edge_indices.shape[0], internal_edges=i64(m.internal_edge_indices),
+            n_boundary_elements=m.boundary_element_indices.shape[0],
+            boundary_elements=i64(m.boundary_element_indices))
+        td = _native.TablesDesc(
+            order=basis.order, n_basis=basis.dof, n_cell_gp=gauss_points.cell_gp_number,
+            n_edge_gp=gauss_points.edge_gp_number, n_deriv_keys=basis.nkeys, _pad=0,
+            cell_weights=f64(gauss_points.cell_weights), edge_weights=f64(gauss_points.edge_weights),
+            phi_cell=f64(basis.phis_cell_gps), phi_edge=f64(basis.phis_edge_gps),
+            dphi_cell_ref=f64(basis.dphis_cell_gps), mass_diag=f64(basis.mass_mat_diag))
+        pr = _native.Params(hcr=flow_param.hcr, cfl=solver_param.cfl, final_time=solver_param.final_time,
+                            final_step=solver_param.final_step, limiter=1 if limiter else 0, device=device)
+        status = ctypes.c_int32(0)
+        ctx = L.dgm_create(ctypes.byref(md), ctypes.byref(td), ctypes.byref(pr), ctypes.byref(status))
+        if not ctx:
+            raise DgmError(status.value, what="dgm_create")
+        self._ctx = ctypes.c_void_p(ctx)
+        self._lib = L
+        self.ne = m.n_elements
+        self.nb = basis.dof
+
+    # ---- plumbing ----
+    def _check(self, st: int, what: str) -> None:
+        if st != 0:
+            raise DgmError(st, int(self._lib.dgm_error_location(self._ctx)), what)
+
+    @property
+    def ctx(self):
+        return self._ctx
+
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            self._lib.dgm_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def new_state(self) -> np.ndarray:
+        return np.zeros((self.ne, 4, self.nb))
+
+    # ---- reference API ----
+    def compute_residuals(self, residuals: np.ndarray, solutions: np.ndarray) -> None:
+        """residuals = (residuals + volume + edge + boundary terms) / mass (spatial_disc.rs:27-39)."""
+        _check_state(residuals, self.ne, self.nb, "residuals")
+        _check_state(solutions, self.ne, self.nb, "solutions")
+        self._check(self._lib.dgm_compute_residuals(self._ctx, _native.dptr(residuals), _native.dptr(solutions)),
+                    "compute_residuals")
+
+    def apply_limiter(self, solutions: np.ndarray) -> int:
+        """KXRCF + WENO in place, reference element order (limiter.rs:7, weno.rs:86-269).
+        Returns the number of limited cells."""
+        _check_state(solutions, self.ne, self.nb, "solutions")
+        n = ctypes.c_int64(0)
+        self._check(self._lib.dgm_apply_limiter(self._ctx, _native.dptr(solutions), ctypes.byref(n)), "apply_limiter")
+        return int(n.value)
+
+    def limiter_stats(self) -> tuple[int, int]:
+        t, w = ctypes.c_int64(0), ctypes.c_int32(0)
+        self._lib.dgm_limiter_stats(self._ctx, ctypes.byref(t), ctypes.byref(w))
+        return int(t.value), int(w.value)
+
+
+class TemperalDisc:
+    """TemperalDisc (src/temporal_disc.rs:8-93): SSP-RK3 and the time-march loop on the GPU."""
+
+    def __init__(self, spatial_disc: SpatialDisc):
+        self._sd = spatial_disc
+        self.solver_param = spatial_disc.solver_param
+
+    @property
+    def current_time(self) -> float:
+        t, s = ctypes.c_double(0.0), ctypes.c_int64(0)
+        self._sd._lib.dgm_get_clock(self._sd._ctx, ctypes.byref(t), ctypes.byref(s))
+        return float(t.value)
+
+    @property
+    def current_step(self) -> int:
+        t, s = ctypes.c_double(0.0), ctypes.c_int64(0)
+        self._sd._lib.dgm_get_clock(self._sd._ctx, ctypes.byref(t), ctypes.byref(s))
+        return int(s.value)
+
+    def set_clock(self, current_time: float, current_step: int) -> None:
+        self._sd._check(self._sd._lib.dgm_set_clock(self._sd._ctx, float(current_time), int(current_step)),
+                        "set_clock")
+
+    def compute_time_step(self, solutions: np.ndarray) -> float:
+        _check_state(solutions, self._sd.ne, self._sd.nb, "solutions")
+        dt = ctypes.c_double(0.0)
+        self._sd._check(self._sd._lib.dgm_compute_time_step(self._sd._ctx, _native.dptr(solutions), ctypes.byref(dt)),
+                        "compute_time_step")
+        return float(dt.value)
+
+    def rk3(self, spatial_disc: SpatialDisc, residuals: np.ndarray, solutions: np.ndarray, time_step: float) -> None:
+        sd = spatial_disc
+        _check_state(residuals, sd.ne, sd.nb, "residuals")
+        _check_state(solutions, sd.ne, sd.nb, "solutions")
+        sd._check(sd._lib.dgm_rk3(sd._ctx, _native.dptr(residuals), _native.dptr(solutions), float(time_step)), "rk3")
+
+    def time_march(self, spatial_disc: SpatialDisc, residuals: np.ndarray, solutions: np.ndarray) -> None:
+        sd = spatial_disc
+        _check_state(residuals, sd.ne, sd.nb, "residuals")
+        _check_state(solutions, sd.ne, sd.nb, "solutions")
+        sd._check(sd._lib.dgm_time_march(sd._ctx, _native.dptr(residuals), _native.dptr(solutions)), "time_march")
+
+    # ---- device-resident path ----
+    def upload(self, solutions: np.ndarray) -> None:
+        self._sd._check(self._sd._lib.dgm_upload_solutions(self._sd._ctx, _native.dptr(solutions)), "upload")
+
+    def download(self, solutions: np.ndarray) -> None:
+        self._sd._check(self._sd._lib.dgm_download_solutions(self._sd._ctx, _native.dptr(solutions)), "download")
+
+    def advance(self, n_steps: int) -> None:
+        self._sd._check(self._sd._lib.dgm_advance(self._sd._ctx, int(n_steps)), "advance")
+
+    def synchronize(self) -> None:
+        self._sd._check(self._sd._lib.dgm_synchronize(self._sd._ctx), "synchronize")
+
+
+class Solver:
+    """Solver (src/solver.rs:32-82): owns residuals/solutions and drives the time march."""
+
+    def __init__(self, mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints, flow_param: FlowParameters,
+                 solver_param: SolverParameters, limiter: bool = True, device: int = 0):
+        self.mesh = mesh
+        self.basis = basis
+        self.gauss_points = gauss_points
+        self.flow_param = flow_param
+        self.solver_param = solver_param
+        self.mesh_param = MeshParameters.of(mesh)
+        self.spatial_disc = SpatialDisc(mesh, basis, gauss_points, flow_param, self.mesh_param, solver_param,
+                                        limiter=limiter, device=device)
+        self.temporal_disc = TemperalDisc(self.spatial_disc)
+        self.residuals = self.spatial_disc.new_state()
+        self.solutions = self.spatial_disc.new_state()
+
+    def set_initial_solution(self, initial: InitialSolution) -> None:
+        self.solutions[...] = initial_state(self.mesh, self.basis, self.gauss_points, self.flow_param.hcr, initial)
+
+    def solve(self) -> None:
+        self.temporal_disc.time_march(self.spatial_disc, self.residuals, self.solutions)
+
+    def close(self) -> None:
+        self.spatial_disc.close()
+
+
+def build_solver(mesh: Mesh, order: int, hcr: float, cfl: float, final_time: float, final_step: int,
+                 limiter: bool = True, device: int = 0) -> Solver:
+    """Convenience: tables for ``order`` with the default rules, then a Solver."""
+    nq, ng = default_rules(order)
+    g = GaussPoints(nq, ng)
+    b = DubinerBasis(order, g)
+    sp = SolverParameters(cfl=cfl, final_time=final_time, final_step=final_step, order_of_polynomials=order,
+                          number_of_cell_gp=nq, number_of_edge_gp=ng)
+    return Solver(mesh, b, g, FlowParameters(hcr=hcr), sp, limiter=limiter, device=device)

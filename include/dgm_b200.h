@@ -1,0 +1,177 @@
+/*
+ * dgm_b200.h -- C ABI of the B200 (sm_100a) DG residual + SSP-RK3 library.
+ *
+ * Drop-in boundary for DGM_in_rust's hot path.  A host (the Rust FFI crate, Python ctypes,
+ * C++) passes the already-processed mesh, basis/quadrature tables and parameters once, then
+ * calls the entry points below in place of the reference's methods.  Arrays crossing the
+ * boundary use the reference's own layout: states and residuals are Array<f64, Ix3>
+ * [element][variable][basis] in C order (initialization.rs:70-71).  No torch types, no
+ * ownership transfer: the caller keeps every pointer it passes.
+ *
+ * Error convention: every entry point returns a DGM_* status.  The reference panics in these
+ * cases (flux.rs:56-61 via spatial_disc.rs:195-200; weno.rs:107); the FFI crate maps a non-OK
+ * status to panic!(dgm_status_string(status)).  dgm_error_location() gives the edge or element
+ * the device flagged first.
+ *
+ * Threading: a context is not thread-safe; it owns one CUDA stream and device-resident
+ * buffers.  One context per mesh instance.  There is no CPU fallback: without a usable
+ * CUDA device dgm_create fails with DGM_NO_DEVICE.
+ */
+#ifndef DGM_B200_H
+#define DGM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define DGM_OK 0
+#define DGM_NEG_DENSITY 1             /* "Negative density found in HLLC!"  flux.rs:56-57   */
+#define DGM_NEG_PRESSURE 2            /* "Negative pressure found in HLLC!" flux.rs:59-60   */
+#define DGM_NONFINITE 3               /* non-finite time step                                */
+#define DGM_TOO_MANY_BOUNDARY_EDGES 4 /* "Invalid number of boundary neighbours!" weno.rs:107 */
+#define DGM_OOM 5                     /* device allocation failed                           */
+#define DGM_TIMEOUT 6                 /* a bounded device wait gave up                      */
+#define DGM_BAD_ARG 7                 /* unsupported order/rule, bad sizes or pointers       */
+#define DGM_CUDA_ERROR 9              /* a CUDA runtime call failed                         */
+#define DGM_NO_DEVICE 10              /* no usable CUDA device                              */
+
+/* ---- boundary types (mesh.rs:174-178) ---------------------------------------------------- */
+#define DGM_WALL 0
+#define DGM_FARFIELD 1
+
+/* Processed mesh, i.e. the fields of Mesh/Element/Edge/Patch (mesh.rs:5-189) as they stand
+ * after process_mesh and the Mesh::compute_* calls (initialization.rs:40-66).  All arrays are
+ * dense, 0-based, C order. */
+typedef struct dgm_mesh_desc {
+  int64_t n_vertices;
+  int64_t n_elements;
+  int64_t n_edges;
+  int64_t n_patches;
+  const double* vertex_xy;          /* [n_vertices][2]            Vertex {x, y}             */
+  const int64_t* elem_vertices;     /* [n_elements][3]            Element::ivertices        */
+  const int64_t* elem_edges;        /* [n_elements][3]            Element::iedges           */
+  const int64_t* elem_neighbours;   /* [n_elements][3], -1 = none Element::ineighbours      */
+  const double* elem_jacob_det;     /* [n_elements]               Element::jacob_det        */
+  const double* elem_circumradius;  /* [n_elements]               Element::circumradius     */
+  const double* elem_minimum_height;/* [n_elements]               Element::minimum_height   */
+  const int64_t* edge_elements;     /* [n_edges][2], [1] = -1 on the boundary  Edge::ielements */
+  const int64_t* edge_vertices;     /* [n_edges][2]               Edge::ivertices           */
+  const int64_t* edge_in_cell;      /* [n_edges][2]               Edge::in_cell_indices     */
+  const double* edge_jacob_det;     /* [n_edges]                  Edge::jacob_det (length)  */
+  const double* edge_normal;        /* [n_edges][2]               Edge::normal              */
+  const int64_t* edge_patch;        /* [n_edges], -1 = internal   Edge::ipatch              */
+  const int32_t* patch_type;        /* [n_patches] DGM_WALL / DGM_FARFIELD  Patch::boundary_type */
+  const double* patch_quantity;     /* [n_patches][4] rho,u,v,p (far field)  BoundaryQuantity */
+  int64_t n_internal_edges;
+  const int64_t* internal_edges;    /* Mesh::internal_edge_indices                          */
+  int64_t n_boundary_elements;
+  const int64_t* boundary_elements; /* Mesh::boundary_element_indices                       */
+} dgm_mesh_desc;
+
+/* Basis and quadrature tables: DubinerBasis (basis_function.rs:6-13) and GaussPoints
+ * (gauss_point.rs:4-11).  Supported (order, cell rule, edge rule): (1,3,2), (2,6,3), (3,12,4). */
+typedef struct dgm_tables_desc {
+  int32_t order;                    /* SolverParameters::order_of_polynomials               */
+  int32_t n_basis;                  /* number_of_basis_functions                            */
+  int32_t n_cell_gp;                /* number_of_cell_gp                                    */
+  int32_t n_edge_gp;                /* number_of_edge_gp                                    */
+  int32_t n_deriv_keys;             /* keys in dphi_cell_ref: (order+1)(order+2)/2 - 1, >= 2 */
+  int32_t _pad;
+  const double* cell_weights;       /* [n_cell_gp]                                          */
+  const double* edge_weights;       /* [n_edge_gp]                                          */
+  const double* phi_cell;           /* [n_cell_gp][n_basis]       phis_cell_gps             */
+  const double* phi_edge;           /* [3][n_edge_gp][n_basis]    phis_edge_gps             */
+  /* Reference-space derivatives d^a/dxi^a d^b/deta^b of each mode at the cell points,
+   * [n_cell_gp][n_basis][n_deriv_keys], keys ordered (1,0),(0,1),(2,0),(1,1),(0,2),(3,0),...
+   * (the HashMap keys of dphis_cell_gps, basis_function.rs:114-151). */
+  const double* dphi_cell_ref;
+  const double* mass_diag;          /* [n_basis]                  mass_mat_diag             */
+} dgm_tables_desc;
+
+typedef struct dgm_params {
+  double hcr;                       /* FlowParameters::hcr (ratio of specific heats)        */
+  double cfl;                       /* SolverParameters::cfl                                */
+  double final_time;                /* SolverParameters::final_time                         */
+  int64_t final_step;               /* SolverParameters::final_step                         */
+  int32_t limiter;                  /* 1 = WENO/KXRCF limiter after each stage (reference), 0 = off */
+  int32_t device;                   /* CUDA device ordinal                                  */
+} dgm_params;
+
+typedef struct dgm_ctx dgm_ctx;
+
+/* Build a device-resident solver context (the GPU side of Solver/SpatialDisc/TemperalDisc,
+ * solver.rs:32-43, spatial_disc.rs:17-25, temporal_disc.rs:8-19).  Copies everything it needs;
+ * the descriptors may be freed after the call.  *status receives DGM_OK or an error. */
+dgm_ctx* dgm_create(const dgm_mesh_desc* mesh, const dgm_tables_desc* tables,
+                    const dgm_params* params, int32_t* status);
+void dgm_destroy(dgm_ctx* ctx);
+
+/* SpatialDisc::compute_residuals(&self, residuals: &mut Array3, solutions: &Array3)
+ * (src/spatial_disc.rs:27).  Same semantics: residuals = (residuals + volume + edge +
+ * boundary terms) / mass, host buffers of n_elements*4*n_basis doubles. */
+int32_t dgm_compute_residuals(dgm_ctx* ctx, double* residuals, const double* solutions);
+
+/* SpatialDisc::apply_limiter(&self, solutions: &mut Array3) (src/spatial_disc/limiter.rs:7):
+ * modified-KXRCF detection + characteristic WENO, in place, with the reference's in-order
+ * semantics (weno.rs:90,263).  *troubled (may be NULL) receives the number of limited cells. */
+int32_t dgm_apply_limiter(dgm_ctx* ctx, double* solutions, int64_t* troubled);
+
+/* TemperalDisc::compute_time_step(&self, solutions) -> f64 (src/temporal_disc.rs:58). */
+int32_t dgm_compute_time_step(dgm_ctx* ctx, const double* solutions, double* time_step);
+
+/* TemperalDisc::rk3(&mut self, spatial_disc, residuals, solutions, time_step)
+ * (src/temporal_disc/rk3.rs:7).  One SSP-RK3 step of size time_step with the limiter after
+ * each stage; on return solutions holds U^{n+1} and residuals the third stage's residual. */
+int32_t dgm_rk3(dgm_ctx* ctx, double* residuals, double* solutions, double time_step);
+
+/* TemperalDisc::time_march(&mut self, spatial_disc, residuals, solutions)
+ * (src/temporal_disc.rs:21): while current_step < final_step && current_time < final_time
+ * { dt = compute_time_step; clamp to final_time; rk3; advance }.  The loop runs on the device
+ * (CUDA graphs, no host round trip per step); the context keeps current_time/current_step
+ * across calls like TemperalDisc does. */
+int32_t dgm_time_march(dgm_ctx* ctx, double* residuals, double* solutions);
+
+/* TemperalDisc::current_time / current_step (temporal_disc.rs:10-11). */
+int32_t dgm_get_clock(dgm_ctx* ctx, double* current_time, int64_t* current_step);
+int32_t dgm_set_clock(dgm_ctx* ctx, double current_time, int64_t current_step);
+
+/* ---- device-resident fast path (no host copies of the state per step) ------------------- */
+
+/* Copy a host state ([element][variable][basis]) into the context's resident state, or back. */
+int32_t dgm_upload_solutions(dgm_ctx* ctx, const double* solutions);
+int32_t dgm_download_solutions(dgm_ctx* ctx, double* solutions);
+
+/* Run up to n_steps steps of time_march on the resident state (stops early at final_step /
+ * final_time, as the reference loop does).  Asynchronous: returns after enqueueing; the
+ * status of the steps is reported by dgm_synchronize. */
+int32_t dgm_advance(dgm_ctx* ctx, int64_t n_steps);
+
+/* Wait for the context's stream; returns the first device-side status raised since the last
+ * synchronize (DGM_OK if none). */
+int32_t dgm_synchronize(dgm_ctx* ctx);
+
+/* The context's CUDA stream (cudaStream_t as void*), for callers that order their own work
+ * (copies, events) against the solver. */
+void* dgm_stream(dgm_ctx* ctx);
+
+/* Edge (HLLC failures) or element (limiter failures) index flagged by the last error. */
+int64_t dgm_error_location(dgm_ctx* ctx);
+
+/* Limited cells and limiter waves of the most recent limiter pass (diagnostics). */
+int32_t dgm_limiter_stats(dgm_ctx* ctx, int64_t* troubled, int32_t* waves);
+
+/* Bytes of device memory held by the context. */
+int64_t dgm_device_bytes(dgm_ctx* ctx);
+
+const char* dgm_status_string(int32_t status);
+
+/* Library version string. */
+const char* dgm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGM_B200_H */

@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""DOF-stage updates/s of the DG residual + SSP-RK3 time step on B200.
+
+Workload: synthetic NACA 0012 O-grid, 256 x 128 quads -> 65,536 triangles, p = 2 Dubiner basis
+(6 modes, 6-point triangle / 3-point edge rules), Euler gamma = 1.4, M = 0.8, AoA = 1.25 deg,
+uniform free-stream start, HLLC + slip wall + characteristic far field, KXRCF/WENO limiter after
+every stage, SSP-RK3 with CFL 0.1 -- the transonic limiter configuration, computed in FP64.
+
+One step = one iteration of the reference's time_march loop (CFL time step + three RK stages,
+each residual + stage update + limiter).  DOF = elements * 4 variables * 6 modes; a step
+updates 3 * DOF DOF-stages.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank advances its own replica of the workload (the path does not
+shard: replicas only); the timed region is bracketed by barriers and the slowest rank's time
+is reported.  ``--impl reference`` times the reference's CPU algorithm (the C++ restatement in
+oracle/, since the Rust reference cannot be built here) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NI, NJ, ORDER = 256, 128, 2
+MACH, AOA, CFL, HCR = 0.8, 1.25, 0.1, 1.4
+RHO_INF, P_INF = 1.0, 1.0 / 1.4
+WORKLOAD = ("naca0012_ogrid_256x128_p2: 65,536 triangles, 6 modes, M=0.8, AoA=1.25deg, "
+            "HLLC, WENO/KXRCF limiter on, SSP-RK3 CFL=0.1, FP64")
+METRIC = "DOF-stage updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_mesh():
+    from dgm_in_rust_b200 import freestream_quantity, naca0012_ogrid, process_mesh
+    raw = naca0012_ogrid(NI, NJ)
+    mesh = process_mesh(raw, freestream_quantity(MACH, AOA, RHO_INF, P_INF, HCR), HCR)
+    return raw, mesh
+
+
+def dofs_per_step(ne, nb):
+    return ne * 4 * nb * 3
+
+
+# ------------------------------------------------------------------------------------------
+# CPU (reference algorithm) timing
+# ------------------------------------------------------------------------------------------
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def time_cpu(raw, steps, warmup, threads, budget_s=None):
+    """Time the oracle's time_march on the full workload; returns (DOF-stage/s, steps timed)."""
+    from oracle.oracle import Oracle
+    o = Oracle(raw=raw, order=ORDER, ncell_gp=6, nedge_gp=3, hcr=HCR, cfl=CFL, final_time=1.0e30,
+               final_step=10 ** 9, limiter=True, threads=threads, freestream=(AOA, MACH, RHO_INF, P_INF))
+    U = o.initial_solution()
+    R = o.new_state()
+    for _ in range(warmup):
+        o.rk3(R, U, o.compute_time_step(U))
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        o.rk3(R, U, o.compute_time_step(U))
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return dofs_per_step(o.ne, o.nb) * done / el, done, el
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    raw, _ = make_mesh()
+    threads = cpu_threads()
+    # each step is a full RK3 step of the workload; cap the count so the run stays within minutes
+    steps = min(args.steps, 200)
+    warm = min(args.warmup, 3)
+    value, done, el = time_cpu(raw, steps, warm, threads, budget_s=150.0)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": args.gpus,
+        "steps": done, "warmup": warm, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": NI * NJ * 2, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "DOF-stage/s", "cores": threads, "kind": "port",
+                         "sample": f"{done} full RK3 steps of the workload after {warm} warm-up steps; C++ "
+                                   "restatement of the reference CPU algorithm (Rust reference not buildable "
+                                   "here), OpenMP over volume/edge/boundary passes, serial limiter and dt"},
+        "e2e": {"value": value, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while the timed region runs."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown", 0x1: "gpu_idle",
+               0x2: "applications_clocks_setting"}
+
+    def __init__(self, device_index):
+        self.samples, self.reasons_seen, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            import torch
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            try:
+                self._h = pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+            except Exception:
+                self._h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._h = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if r & bit and name != "gpu_idle":
+                        self.reasons_seen.add(name)
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self._h is not None:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons_seen), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons_seen), "samples": len(self.samples)}
+
+
+PHASES = {0: "k_time_step", 1: "k_edge_flux", 2: "k_element", 3: "k_limiter"}
+
+
+def phase_bytes(phase, mesh, nb, n_int, n_bnd):
+    """Algorithmic DRAM bytes of one launch of each kernel (FP64): state arrays counted once,
+    geometry/connectivity at their stored width, edge-flux intermediates once."""
+    ne = mesh.n_elements
+    s = 8
+    state = ne * 4 * nb * s
+    ng = 3
+    flux = (n_int + n_bnd) * ng * 4 * s
+    if phase == 0:
+        return state + ne * 8
+    if phase == 1:
+        return state + n_int * (8 + 4 + 32) + n_bnd * (4 + 4 + 32) + flux
+    if phase == 2:
+        return 3 * state + ne * (8 + 32 + 12) + flux
+    # limiter: KXRCF reads the state once (neighbour traces come from the same array), face and
+    # neighbour ids, h^1.5, per-edge normal/length; writes flags and status words
+    return state + ne * (12 + 12 + 8 + 1 + 4) + n_int * 32
+
+
+def load_traffic():
+    """Per-element DRAM traffic of each kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic_c2.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            parts = line.split()
+            if len(parts) == 3 and parts[0].startswith("k_"):
+                try:
+                    out[parts[0]] = (float(parts[1]), float(parts[2]))  # bytes per launch, elements
+                except ValueError:
+                    pass
+    return out
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from dgm_in_rust_b200 import InitialSolution, build_solver, initial_state
+    from dgm_in_rust_b200.build import build
+    build()
+    raw, mesh = make_mesh()
+    solver = build_solver(mesh, ORDER, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, device=local)
+    sd, td = solver.spatial_disc, solver.temporal_disc
+    L = sd._lib
+    ctx = sd.ctx
+    U0 = initial_state(mesh, solver.basis, solver.gauss_points, HCR, InitialSolution(RHO_INF, AOA, MACH, P_INF))
+    td.upload(U0)
+    stream = torch.cuda.ExternalStream(L.dgm_stream(ctx))
+    ne, nb = mesh.n_elements, solver.basis.dof
+    dps = dofs_per_step(ne, nb)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (also instantiates the step graphs)
+    td.advance(args.warmup)
+    td.synchronize()
+    # timed region: K steps, L2 flushed before each step, each step bracketed by events
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    sampler = ClockSampler(local)
+    with sampler:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+                evs[i][0].record(stream)
+            td.advance(1)
+            with torch.cuda.stream(stream):
+                evs[i][1].record(stream)
+        td.synchronize()
+    barrier()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    troubled, waves = sd.limiter_stats()
+    # L2-resident throughput: the same steps back to back in CUDA graphs (no flush)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+    td.advance(args.steps)
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    td.synchronize()
+    ms_resident = e0.elapsed_time(e1)
+    # per-kernel timing (L2 flushed before each launch) for the roofline
+    n_int = int(mesh.internal_edge_indices.shape[0])
+    n_bnd = int((mesh.edge_elements[:, 1] == -1).sum())
+    reps = 20
+    kernel_us = {}
+    for ph in range(4):
+        tot = 0.0
+        for r in range(reps + 2):
+            if ph == 3:  # the limiter acts on the stage buffer written by phase 2
+                L.dgm_launch_phase(ctx, 1)
+                L.dgm_launch_phase(ctx, 2)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                flush.fill_(float(r))
+                a.record(stream)
+            st = L.dgm_launch_phase(ctx, ph)
+            if st != 0:
+                raise SystemExit(f"dgm_launch_phase({ph}) failed: {st}")
+            with torch.cuda.stream(stream):
+                b.record(stream)
+            td.synchronize()
+            if r >= 2:
+                tot += a.elapsed_time(b)
+        kernel_us[PHASES[ph]] = 1e3 * tot / reps
+    share = {k: kernel_us[k] * L.dgm_phase_launches_per_step(ctx, ph) for ph, k in PHASES.items()}
+    dom_phase = max(PHASES, key=lambda ph: share[PHASES[ph]])
+    dom = PHASES[dom_phase]
+    alg = phase_bytes(dom_phase, mesh, nb, n_int, n_bnd)
+    peaks = {}
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peaks = json.load(f)
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    achieved = alg / (kernel_us[dom] * 1e-6) / 1e9
+    traffic = load_traffic().get(dom)
+    traffic_per_launch = traffic[0] * ne / traffic[1] if traffic else None
+
+    # e2e: the reference-facing call per step -- time_march over one iteration with host
+    # (pinned) buffers: upload of the state, the step, download of state and residual
+    Uh = torch.from_numpy(U0.copy()).pin_memory()
+    Rh = torch.zeros_like(Uh).pin_memory()
+    Un, Rn = Uh.numpy(), Rh.numpy()
+    td.set_clock(0.0, 0)
+    for i in range(3):
+        td.set_limits(1.0e30, i + 1)
+        td.time_march(sd, Rn, Un)
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        td.set_limits(1.0e30, 3 + i + 1)
+        td.time_march(sd, Rn, Un)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    barrier()
+    state_bytes = ne * 4 * nb * 8
+
+    # max over ranks
+    vals = torch.tensor([ms, ms_resident, e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    ms, ms_resident, e2e_s = [float(v) for v in vals.tolist()]
+    value = world * dps * args.steps / (ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": ne, "order": ORDER, "dof_stage_per_step": dps,
+                   "l2": "flushed (256 MiB write) before every timed step; per-step CUDA events",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "value_l2_resident": world * dps * args.steps / (ms_resident * 1e-3),
+        "e2e": {"value": world * dps * args.steps / e2e_s, "unit": "DOF-stage/s",
+                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": 2 * state_bytes,
+                "call": "dgm_time_march over one iteration (dgm_set_limits + dgm_time_march), pinned host arrays"},
+        "gpu_launches": L.dgm_launches_per_step(ctx) * args.steps,
+        "kernel_us": {k: round(v, 3) for k, v in kernel_us.items()},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": alg,
+                     "traffic": traffic_per_launch},
+        "limiter": {"troubled_cells_last_step": troubled, "waves_last_pass": waves},
+        "clocks": sampler.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = cpu_threads()
+        v, done, el = time_cpu(raw, 1000, 1, threads, budget_s=12.0)
+        line["cpu_baseline"] = {"value": v, "unit": "DOF-stage/s", "cores": threads, "kind": "port",
+                                "sample": f"{done} full RK3 steps ({el:.1f} s) of the workload after 1 warm-up "
+                                          "step; C++ restatement of the reference CPU algorithm"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

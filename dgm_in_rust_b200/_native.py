@@ -133,6 +133,10 @@ def lib() -> ctypes.CDLL:
     L.dgm_time_march.argtypes = [vp, P_D, P_D]
     L.dgm_get_clock.argtypes = [vp, P_D, P_I64]
     L.dgm_set_clock.argtypes = [vp, ctypes.c_double, ctypes.c_int64]
+    L.dgm_set_limits.argtypes = [vp, ctypes.c_double, ctypes.c_int64]
+    L.dgm_launch_phase.argtypes = [vp, ctypes.c_int32]
+    L.dgm_phase_launches_per_step.argtypes = [vp, ctypes.c_int32]
+    L.dgm_launches_per_step.argtypes = [vp]
     L.dgm_upload_solutions.argtypes = [vp, P_D]
     L.dgm_download_solutions.argtypes = [vp, P_D]
     L.dgm_advance.argtypes = [vp, ctypes.c_int64]
@@ -150,7 +154,8 @@ def lib() -> ctypes.CDLL:
     L.dgm_version.restype = ctypes.c_char_p
     for name in ("dgm_compute_residuals", "dgm_apply_limiter", "dgm_compute_time_step", "dgm_rk3",
                  "dgm_time_march", "dgm_get_clock", "dgm_set_clock", "dgm_upload_solutions",
-                 "dgm_download_solutions", "dgm_advance", "dgm_synchronize", "dgm_limiter_stats"):
+                 "dgm_download_solutions", "dgm_advance", "dgm_synchronize", "dgm_limiter_stats",
+                 "dgm_set_limits", "dgm_launch_phase", "dgm_phase_launches_per_step", "dgm_launches_per_step"):
         getattr(L, name).restype = ctypes.c_int32
     _lib = L
     return L

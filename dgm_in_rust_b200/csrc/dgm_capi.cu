@@ -36,15 +36,17 @@ struct dgm_ctx {
   double *U = nullptr, *U1 = nullptr, *U2 = nullptr, *R = nullptr, *F = nullptr, *stage = nullptr;
   unsigned char* t0 = nullptr;
   unsigned int* status = nullptr;
+  int* work = nullptr;
   Control* ctl = nullptr;
   std::vector<void*> allocs;
   int64_t bytes = 0;
   int coop_blocks = 1;
   bool coop_ok = true;
-  // graphs: [0] = steps without residual output, [1] = with residual output
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // graphs[with_residual][g]: g = 0 captures graph_steps steps, g = 1 a single step
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int graph_steps = 8;
   bool graphs_broken = false;
+  bool limits_dirty = false;
   int64_t err_where = -1;
   int64_t last_troubled = 0;
   int last_waves = 0;
@@ -110,8 +112,8 @@ struct Ops {
   template <int MODE>
   static int element(dgm_ctx* c, const double* Uin, const double* Ubase, double* Uout, const double* Rin,
                      double* Rout) {
-    const int threads = 128;
-    const int blocks = (int)std::max<int64_t>(1, (c->ne + threads - 1) / threads);
+    const int threads = 256;  // 8 warps x 8 elements, 4 threads (variables) per element
+    const int blocks = (int)std::max<int64_t>(1, (c->ne + 63) / 64);
     dgm::k_element<P, MODE><<<blocks, threads, 0, c->stream>>>(kp_of<P>(c), Uin, Ubase, c->F, Uout, Rin, Rout);
     CK(cudaGetLastError());
     return DGM_OK;
@@ -119,13 +121,9 @@ struct Ops {
 
   static int limiter(dgm_ctx* c, double* U) {
     if (!c->limiter) return DGM_OK;
-    const int threads = 256;
-    int blocks = (int)std::max<int64_t>(1, (c->ne + threads - 1) / threads);
-    dgm::k_detect<P><<<blocks, threads, 0, c->stream>>>(kp_of<P>(c), U, c->t0, c->status);
-    CK(cudaGetLastError());
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c->coop_blocks);
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(dgm::kLimiterWarps * 32);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = c->stream;
     cudaLaunchAttribute attr[1];
@@ -133,8 +131,7 @@ struct Ops {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter_waves<P>, kp_of<P>(c), U,
-                          (const unsigned char*)c->t0, c->status));
+    CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter<P>, kp_of<P>(c), U, c->t0, c->status, c->work));
     return DGM_OK;
   }
 
@@ -191,9 +188,9 @@ struct Ops {
 
   static int occupancy(dgm_ctx* c) {
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dgm::k_limiter_waves<P>, 256, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dgm::k_limiter<P>, dgm::kLimiterWarps * 32, 0));
     per_sm = std::max(1, per_sm);
-    const int64_t want = std::max<int64_t>(1, (c->ne + 7) / 8);  // 8 warps per block
+    const int64_t want = std::max<int64_t>(1, (c->ne + 32 * dgm::kLimiterWarps - 1) / (32 * dgm::kLimiterWarps));
     c->coop_blocks = (int)std::min<int64_t>((int64_t)per_sm * c->num_sms, want);
     return DGM_OK;
   }
@@ -298,11 +295,12 @@ int write_clock(dgm_ctx* c) {
   h.cfl = c->cfl;
   CK(cudaMemcpyAsync(c->ctl, &h, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  c->limits_dirty = false;
   return DGM_OK;
 }
 
-int build_graph(dgm_ctx* c, int with_residual) {
-  if (c->graph[with_residual] || c->graphs_broken) return DGM_OK;
+int build_graph(dgm_ctx* c, int with_residual, int single) {
+  if (c->graph[with_residual][single] || c->graphs_broken) return DGM_OK;
   cudaGraph_t g = nullptr;
   if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
@@ -310,7 +308,8 @@ int build_graph(dgm_ctx* c, int with_residual) {
     return DGM_OK;
   }
   int st = DGM_OK;
-  for (int i = 0; i < c->graph_steps && st == DGM_OK; ++i)
+  const int n = single ? 1 : c->graph_steps;
+  for (int i = 0; i < n && st == DGM_OK; ++i)
     st = dispatch(c, [&](auto ops) { return decltype(ops)::step(c, with_residual ? c->R : nullptr); });
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (st != DGM_OK || e != cudaSuccess || g == nullptr) {
@@ -327,18 +326,19 @@ int build_graph(dgm_ctx* c, int with_residual) {
     c->graphs_broken = true;
     return DGM_OK;
   }
-  c->graph[with_residual] = exec;
+  c->graph[with_residual][single] = exec;
   return DGM_OK;
 }
 
 // Enqueue n time-march iterations on the resident state.
 int enqueue_steps(dgm_ctx* c, int64_t n, int with_residual) {
-  int st = build_graph(c, with_residual);
-  if (st) return st;
+  int st;
   while (n > 0) {
-    if (!c->graphs_broken && n >= c->graph_steps) {
-      CK(cudaGraphLaunch(c->graph[with_residual], c->stream));
-      n -= c->graph_steps;
+    const int single = n >= c->graph_steps ? 0 : 1;
+    if ((st = build_graph(c, with_residual, single))) return st;
+    if (!c->graphs_broken) {
+      CK(cudaGraphLaunch(c->graph[with_residual][single], c->stream));
+      n -= single ? 1 : c->graph_steps;
     } else {
       st = dispatch(c, [&](auto ops) { return decltype(ops)::step(c, with_residual ? c->R : nullptr); });
       if (st) return st;
@@ -511,8 +511,9 @@ void dgm_destroy(dgm_ctx* c) {
   if (!c) return;
   if (c->device >= 0) cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (auto& g : c->graph)
-    if (g) cudaGraphExecDestroy(g);
+  for (auto& row : c->graph)
+    for (auto& g : row)
+      if (g) cudaGraphExecDestroy(g);
   for (void* p : c->allocs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -572,7 +573,8 @@ dgm_ctx* dgm_create(const dgm_mesh_desc* mesh, const dgm_tables_desc* tables, co
   if ((st = dev_alloc(c, &c->U, n_state)) || (st = dev_alloc(c, &c->U1, n_state)) ||
       (st = dev_alloc(c, &c->U2, n_state)) || (st = dev_alloc(c, &c->R, n_state)) ||
       (st = dev_alloc(c, &c->F, n_flux)) || (st = dev_alloc(c, &c->stage, (size_t)c->ne * NEQ * c->nb)) ||
-      (st = dev_alloc(c, &c->t0, (size_t)c->ne)) || (st = dev_alloc(c, &c->status, (size_t)c->ne)))
+      (st = dev_alloc(c, &c->t0, (size_t)c->ne)) || (st = dev_alloc(c, &c->status, (size_t)c->ne)) ||
+      (st = dev_alloc(c, &c->work, (size_t)c->ne)))
     return fail(st);
   for (double* p : {c->U, c->U1, c->U2, c->R})
     if (cudaMemset(p, 0, n_state * sizeof(double)) != cudaSuccess) return fail(DGM_CUDA_ERROR);
@@ -673,6 +675,14 @@ int32_t dgm_set_clock(dgm_ctx* c, double t, int64_t step) {
   return write_clock(c);
 }
 
+int32_t dgm_set_limits(dgm_ctx* c, double final_time, int64_t final_step) {
+  if (!c) return DGM_BAD_ARG;
+  c->final_time = final_time;
+  c->final_step = final_step;
+  c->limits_dirty = true;
+  return DGM_OK;
+}
+
 int32_t dgm_upload_solutions(dgm_ctx* c, const double* solutions) {
   if (!c || !solutions) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
@@ -694,6 +704,10 @@ int32_t dgm_download_solutions(dgm_ctx* c, double* solutions) {
 int32_t dgm_advance(dgm_ctx* c, int64_t n_steps) {
   if (!c || n_steps < 0) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  if (c->limits_dirty) {
+    int st = write_clock(c);
+    if (st) return st;
+  }
   return enqueue_steps(c, n_steps, 0);
 }
 
@@ -705,6 +719,35 @@ int32_t dgm_synchronize(dgm_ctx* c) {
 }
 
 void* dgm_stream(dgm_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int32_t dgm_launch_phase(dgm_ctx* c, int32_t phase) {
+  if (!c || phase < 0 || phase > 3) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  int st = set_active(c, 0.0, false);
+  if (st) return st;
+  return dispatch(c, [&](auto ops) {
+    using O = decltype(ops);
+    switch (phase) {
+      case 0: return O::time_step(c, c->U);
+      case 1: return O::edge_flux(c, c->U);
+      case 2: return O::template element<2>(c, c->U, c->U, c->U2, nullptr, nullptr);
+      default: return O::limiter(c, c->U2);
+    }
+  });
+}
+
+int32_t dgm_phase_launches_per_step(dgm_ctx* c, int32_t phase) {
+  if (!c) return 0;
+  static const int per_step[4] = {1, 3, 3, 3};
+  if (phase < 0 || phase > 3) return 0;
+  if (!c->limiter && phase == 3) return 0;
+  return per_step[phase];
+}
+
+int32_t dgm_launches_per_step(dgm_ctx* c) {
+  if (!c) return 0;
+  return 3 /* step control */ + 1 /* time step */ + 3 * (2 + (c->limiter ? 1 : 0));
+}
 
 int64_t dgm_error_location(dgm_ctx* c) { return c ? c->err_where : -1; }
 

@@ -82,6 +82,7 @@ struct Control {
   int troubled;                // cells limited by the last limiter pass
   int waves;                   // limiter waves of the last pass
   int unknown[2];              // per-wave count of unsettled cells (double-buffered)
+  int wl_count[2];             // per-wave worklist length (double-buffered)
   unsigned int bar_count, bar_gen;  // grid barrier of the limiter kernel
 };
 
@@ -126,9 +127,11 @@ __device__ __forceinline__ int hllc(const double lv[4], const double rv[4], doub
   const double cr = sqrt(hcr * pr / qr0);
   const double fl0 = ql1, fl1 = ql1 * ul + pl, fl2 = ql2 * ul, fl3 = ul * (ql3 + pl);
   const double fr0 = qr1, fr1 = qr1 * ur + pr, fr2 = qr2 * ur, fr3 = ur * (qr3 + pr);
+  // PVRS-type p* of flux.rs:75-78, x^y evaluated as exp(y log x) (the libm pow of the
+  // reference rounds differently in the last bits; the difference stays at round-off level)
   const double zeta = (hcr - 1.0) / (2.0 * hcr);
-  const double p_star = pow((cl + cr - (zeta - 1.0) / 2.0 * (ur - ul)) / (cl / pow(pl, zeta) + cr / pow(pr, zeta)),
-                            1.0 / zeta);
+  const double p_star = exp((1.0 / zeta) * log((cl + cr - (zeta - 1.0) / 2.0 * (ur - ul)) /
+                                              (cl / exp(zeta * log(pl)) + cr / exp(zeta * log(pr)))));
   const double ql_lower = (p_star <= pl) ? 1.0 : sqrt(1.0 + (hcr + 1.0) / (2.0 * hcr) * (p_star / pl - 1.0));
   const double sl = ul - cl * ql_lower;
   const double qr_lower = (p_star <= pr) ? 1.0 : sqrt(1.0 + (hcr + 1.0) / (2.0 * hcr) * (p_star / pr - 1.0));
@@ -249,7 +252,7 @@ __device__ __forceinline__ double ld_state(const double* p) { return __ldcg(p); 
 // boundary_condition.rs:19-97).  Writes F[slot][g][v] * half length.
 // ------------------------------------------------------------------------------------------
 template <int P>
-__global__ void __launch_bounds__(256) k_edge_flux(const __grid_constant__ KParams<P> kp,
+__global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KParams<P> kp,
                                                    const double* __restrict__ U, double* __restrict__ F) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
@@ -358,18 +361,21 @@ __global__ void __launch_bounds__(256) k_edge_flux(const __grid_constant__ KPara
 }
 
 // ------------------------------------------------------------------------------------------
-// Element pass: one thread per element.  Volume integral (integrate_over_cell_euler,
-// spatial_disc.rs:40-69, and boundary_condition.rs:98-117 for boundary elements), gather of
-// the three faces' edge fluxes with the left/right sign and Gauss-point reversal of
-// spatial_disc.rs:202-206, inverse mass (spatial_disc.rs:349-357), then the SSP-RK3 stage
-// combination of rk3.rs:10,16,22.
+// Element pass: volume integral (integrate_over_cell_euler, spatial_disc.rs:40-69, and
+// boundary_condition.rs:98-117 for boundary elements), gather of the three faces' edge fluxes
+// with the left/right sign and Gauss-point reversal of spatial_disc.rs:202-206, inverse mass
+// (spatial_disc.rs:349-357), then the SSP-RK3 stage combination of rk3.rs:10,16,22.
 //   MODE 0: out = (Rin + terms) / mass            (compute_residuals semantics)
 //   MODE 1: out = Uin + dt R
 //   MODE 2: out = 0.75 Ubase + 0.25 (Uin + dt R)
 //   MODE 3: out = 1/3 Ubase + 2/3 (Uin + dt R)
+// Four threads per element, one per conserved variable: lane = v * 8 + i within a warp that
+// covers 8 elements.  The quadrature-point states are exchanged with shuffles, so a thread
+// holds only its variable's NB modes and residuals (few registers, full occupancy), and each
+// (v, b) load of the 8 elements is one contiguous 64-byte run.
 // ------------------------------------------------------------------------------------------
 template <int P, int MODE>
-__global__ void __launch_bounds__(128) k_element(const __grid_constant__ KParams<P> kp,
+__global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KParams<P> kp,
                                                  const double* __restrict__ Uin,
                                                  const double* Ubase,
                                                  const double* __restrict__ F,
@@ -379,87 +385,79 @@ __global__ void __launch_bounds__(128) k_element(const __grid_constant__ KParams
   using V = Variant<P>;
   constexpr int NB = V::NB, NQ = V::NQ, NG = V::NG;
   Control* ctl = kp.ctl;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {  // counters of the limiter pass that follows
     ctl->t0_count = 0;
-    ctl->unknown[0] = 0;
-    ctl->unknown[1] = 0;
+    ctl->unknown[0] = ctl->unknown[1] = 0;
+    ctl->wl_count[0] = ctl->wl_count[1] = 0;
   }
   if (!ctl->active) return;
   const MeshDev& m = kp.m;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= m.ne) return;
+  const int lane = threadIdx.x & 31;
+  const int var = lane >> 3, i = lane & 7;
+  const int e_raw = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 8 + i;
+  if ((e_raw & ~7) >= m.ne) return;  // whole warp past the end
+  const bool valid = e_raw < m.ne;
+  const int e = valid ? e_raw : m.ne - 1;
   const size_t ld = m.ld;
-  double u[NEQ][NB], r[NEQ][NB];
+  double u[NB], r[NB];
 #pragma unroll
-  for (int v = 0; v < NEQ; ++v)
-#pragma unroll
-    for (int b = 0; b < NB; ++b) {
-      u[v][b] = ld_state(&Uin[(v * NB + b) * ld + e]);
-      r[v][b] = 0.0;
-    }
+  for (int b = 0; b < NB; ++b) {
+    u[b] = ld_state(&Uin[(var * NB + b) * ld + e]);
+    r[b] = 0.0;
+  }
   const double J = m.jac[e];
   const double xx = m.dinv[0 * ld + e], xy = m.dinv[1 * ld + e], ex = m.dinv[2 * ld + e], ey = m.dinv[3 * ld + e];
   const double hcr = kp.hcr;
-  // volume term
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
+    double mine = 0.0;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) mine += u[b] * kp.tab.phi_cell[q][b];
     double uq[NEQ];
 #pragma unroll
-    for (int v = 0; v < NEQ; ++v) {
-      double a = 0.0;
-#pragma unroll
-      for (int b = 0; b < NB; ++b) a += u[v][b] * kp.tab.phi_cell[q][b];
-      uq[v] = a;
-    }
+    for (int w = 0; w < NEQ; ++w) uq[w] = __shfl_sync(0xffffffffu, mine, w * 8 + i);
     double f[NEQ], g[NEQ];
     euler_flux(uq, hcr, f, g);
+    const double fv = var == 0 ? f[0] : var == 1 ? f[1] : var == 2 ? f[2] : f[3];
+    const double gv = var == 0 ? g[0] : var == 1 ? g[1] : var == 2 ? g[2] : g[3];
     const double sc = kp.tab.cell_w[q] * 0.5 * J;
+    const double fx = sc * (fv * xx + gv * xy);
+    const double fe = sc * (fv * ex + gv * ey);
 #pragma unroll
-    for (int v = 0; v < NEQ; ++v) {
-      const double fx = sc * (f[v] * xx + g[v] * xy);
-      const double fe = sc * (f[v] * ex + g[v] * ey);
-#pragma unroll
-      for (int b = 0; b < NB; ++b) r[v][b] += fx * kp.tab.dxi[q][b] + fe * kp.tab.deta[q][b];
-    }
+    for (int b = 0; b < NB; ++b) r[b] += fx * kp.tab.dxi[q][b] + fe * kp.tab.deta[q][b];
   }
-  // face terms
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const int fw = m.face[k * ld + e];
     const int slot = fw >> 1;
     const bool right = fw & 1;
-    const double* Fs = &F[(size_t)slot * NG * 4];
+    const double* Fs = &F[(size_t)slot * NG * 4 + var];
 #pragma unroll
     for (int gp = 0; gp < NG; ++gp) {
       const int src = right ? (NG - 1 - gp) : gp;
-      const double2 a = __ldcg(reinterpret_cast<const double2*>(&Fs[src * 4]));
-      const double2 c = __ldcg(reinterpret_cast<const double2*>(&Fs[src * 4 + 2]));
       const double coef = right ? kp.tab.edge_w[gp] : -kp.tab.edge_w[gp];
-      const double fv[4] = {coef * a.x, coef * a.y, coef * c.x, coef * c.y};
+      const double fv = coef * __ldcg(&Fs[src * 4]);
 #pragma unroll
-      for (int v = 0; v < NEQ; ++v)
-#pragma unroll
-        for (int b = 0; b < NB; ++b) r[v][b] += fv[v] * kp.tab.phi_edge[k][gp][b];
+      for (int b = 0; b < NB; ++b) r[b] += fv * kp.tab.phi_edge[k][gp][b];
     }
   }
+  if (!valid) return;
   const double dt = ctl->dt;
 #pragma unroll
-  for (int v = 0; v < NEQ; ++v)
-#pragma unroll
-    for (int b = 0; b < NB; ++b) {
-      const size_t idx = (v * NB + b) * ld + e;
-      double rr = r[v][b];
-      if constexpr (MODE == 0) rr = Rin[idx] + rr;
-      rr = rr / (kp.tab.mass[b] * 0.5 * J);
-      if (Rout) Rout[idx] = rr;
-      if constexpr (MODE == 1) {
-        Uout[idx] = u[v][b] + dt * rr;
-      } else if constexpr (MODE == 2) {
-        Uout[idx] = 0.75 * Ubase[idx] + 0.25 * (u[v][b] + dt * rr);
-      } else if constexpr (MODE == 3) {
-        Uout[idx] = (1.0 / 3.0) * Ubase[idx] + (2.0 / 3.0) * (u[v][b] + dt * rr);
-      }
+  for (int b = 0; b < NB; ++b) {
+    const size_t idx = (var * NB + b) * ld + e;
+    double rr = r[b];
+    if constexpr (MODE == 0) rr = Rin[idx] + rr;
+    rr = rr / (kp.tab.mass[b] * 0.5 * J);
+    if (Rout) Rout[idx] = rr;
+    if constexpr (MODE == 1) {
+      Uout[idx] = u[b] + dt * rr;
+    } else if constexpr (MODE == 2) {
+      Uout[idx] = 0.75 * Ubase[idx] + 0.25 * (u[b] + dt * rr);
+    } else if constexpr (MODE == 3) {
+      Uout[idx] = (1.0 / 3.0) * Ubase[idx] + (2.0 / 3.0) * (u[b] + dt * rr);
     }
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -530,45 +528,34 @@ __device__ __forceinline__ bool kxrcf(const KParams<P>& kp, const double* __rest
   return (ind_d >= 1.0) || (ind_e >= 1.0);
 }
 
-// Parallel KXRCF pass on the unlimited stage state: flags t0[e], resets the limiter status.
-template <int P>
-__global__ void __launch_bounds__(256) k_detect(const __grid_constant__ KParams<P> kp,
-                                                const double* __restrict__ U,
-                                                unsigned char* __restrict__ t0,
-                                                unsigned int* __restrict__ status) {
-  Control* ctl = kp.ctl;
-  if (!ctl->active) return;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  int flag = 0;
-  if (e < kp.m.ne) {
-    flag = kxrcf<P>(kp, U, e) ? 1 : 0;
-    t0[e] = (unsigned char)flag;
-    status[e] = 0u;
-  }
-  const unsigned int ballot = __ballot_sync(0xffffffffu, flag);
-  if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(&ctl->t0_count, __popc(ballot));
-}
-
 // ------------------------------------------------------------------------------------------
-// weno, weno.rs:86-269: characteristic WENO reconstruction of element e, one warp per element.
-// Lanes split the projections (lane -> (r, b)), the smoothness indicators (lane -> (j, v)) and
-// the recombination (lane -> (r, b)); sums run in the reference's order within each lane.
+// weno, weno.rs:86-269: characteristic WENO reconstruction of element e by one warp.
+//
+// The smoothness indicator of a projected polynomial P (weno.rs:125-143, 156-174),
+//   beta = sum_{l=1..p} sum_{l1+l2=l} J^(l-1) int_e (sum_b P_b d^{l1,l2} phi_b)^2,
+// is the quadratic form P^T Q P with the element's Gram matrix
+//   Q[b][b'] = sum_keys J^(l-1) sum_q 0.5 J w_q D_{q,b,key} D_{q,b',key},
+// built once per element and shared by the 3 faces x 4 polynomials x 4 variables (the
+// reference re-evaluates the derivative sums for each of those 48 indicators).  The three
+// faces are processed concurrently (lane -> (face, poly, variable, mode)); projections,
+// normalisation, recombination and the area average keep the reference's summation order.
 // ------------------------------------------------------------------------------------------
 template <int P>
 struct WenoScratch {
   using V = Variant<P>;
-  double tgt[NEQ][V::NB];
-  double nbp[3][NEQ][V::NB];
-  double proj[4][NEQ][V::NB];
-  double pol_new[NEQ][V::NB];
-  double recon[NEQ][V::NB];
-  double L[4][4], R[4][4];
-  double nlw[4][NEQ];
+  static constexpr int ND = (P <= 2) ? V::NQ * V::NB * V::NK : 1;
+  double D[ND];                        // physical derivatives at the cell points (P <= 2)
+  double Q[V::NB][V::NB];
+  double pol[4][NEQ][V::NB];           // pol[0] = target, pol[j+1] = neighbour j, mode 0 <- target's
+  double L[3][4][4], R[3][4][4];
+  double proj[3][4][NEQ][V::NB];
+  double nlw[3][4][NEQ];
+  double pol_new[3][NEQ][V::NB];
 };
 
 template <int P>
 __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __restrict__ U, int e, int lane,
-                                WenoScratch<P>& S) {
+                                                WenoScratch<P>& S, const double* __restrict__ s_dref) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NQ = V::NQ, NK = V::NK;
   const MeshDev& m = kp.m;
@@ -592,96 +579,129 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
   if (nbd == 0) lw[0] = 0.997;
   else if (nbd == 1) lw[1] = 0.998;
   else lw[2] = 0.999;
-  for (int i = lane; i < NEQ * NB; i += 32) {
-    const int v = i / NB, b = i - v * NB;
-    S.tgt[v][b] = ld_state(&U[(v * NB + b) * ld + e]);
-    S.recon[v][b] = 0.0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) S.nbp[k][v][b] = interior[k] ? ld_state(&U[(v * NB + b) * ld + nbrs[k]]) : 0.0;
-  }
-  __syncwarp();
   const double J = m.jac[e];
   const double xx = m.dinv[0 * ld + e], xy = m.dinv[1 * ld + e], ex = m.dinv[2 * ld + e], ey = m.dinv[3 * ld + e];
-  double neighbour_area = 0.0;
-  for (int i = 0; i < 3; ++i) {
-    if (!interior[i]) continue;
-    const double Jnb = m.jac[nbrs[i]];
-    neighbour_area += Jnb * 0.5;
-    const double4 geo = m.ie_geo[faces[i] >> 1];
-    if (lane == 0) {
-      double mean[4];
+  for (int i = lane; i < NEQ * NB; i += 32) {
+    const int v = i / NB, b = i - v * NB;
+    S.pol[0][v][b] = ld_state(&U[(v * NB + b) * ld + e]);
 #pragma unroll
-      for (int v = 0; v < NEQ; ++v) mean[v] = S.tgt[v][0];
-      eigenmatrix(mean, geo.x, geo.y, kp.hcr, S.L, S.R);
+    for (int k = 0; k < 3; ++k)
+      S.pol[k + 1][v][b] = (interior[k] && b > 0) ? ld_state(&U[(v * NB + b) * ld + nbrs[k]]) : 0.0;
+  }
+  if constexpr (P <= 2) {
+    for (int i = lane; i < NQ * NB; i += 32) {
+      const double(&r)[NK] = *reinterpret_cast<const double(*)[NK]>(&s_dref[i * NK]);
+#pragma unroll
+      for (int kk = 0; kk < NK; ++kk) S.D[i * NK + kk] = phys_deriv<NK>(r, xx, xy, ex, ey, kk);
     }
-    __syncwarp();
-    // projections: proj[0] = L tgt, proj[j+1] = L (nb_j with mode 0 <- tgt mode 0)
-    for (int idx = lane; idx < 4 * NEQ * NB; idx += 32) {
-      const int j = idx / (NEQ * NB), rem = idx - j * NEQ * NB, r = rem / NB, b = rem - r * NB;
-      double sum = 0.0;
-      if (j == 0) {
+  }
+  __syncwarp();
+  if (lane < NEQ) {
 #pragma unroll
-        for (int k = 0; k < NEQ; ++k) sum += S.L[r][k] * S.tgt[k][b];
-      } else if (interior[j - 1]) {
+    for (int k = 0; k < 3; ++k)
+      if (interior[k]) S.pol[k + 1][lane][0] = S.pol[0][lane][0];
+  }
+  if (lane < 3 && interior[lane]) {
+    const double4 geo = m.ie_geo[faces[lane] >> 1];  // unoriented normal (weno.rs:121-122)
+    double mean[4];
 #pragma unroll
-        for (int k = 0; k < NEQ; ++k) sum += S.L[r][k] * (b == 0 ? S.tgt[k][0] : S.nbp[j - 1][k][b]);
-      }
-      S.proj[j][r][b] = sum;
-    }
-    __syncwarp();
-    // smoothness indicators (weno.rs:125-143, 156-174)
-    if (lane < 4 * NEQ) {
-      const int j = lane >> 2, v = lane & 3;
-      double w = 0.0;
-      if (j == 0 || interior[j - 1]) {
-        double beta = 0.0;
+    for (int v = 0; v < NEQ; ++v) mean[v] = S.pol[0][v][0];
+    eigenmatrix(mean, geo.x, geo.y, kp.hcr, S.L[lane], S.R[lane]);
+  }
+  // Gram matrix of the smoothness indicator
+  for (int pr = lane; pr < NB * NB; pr += 32) {
+    const int b = pr / NB, c = pr - b * NB;
+    if (c < b) continue;
+    double acc = 0.0;
 #pragma unroll
-        for (int l = 1; l <= P; ++l) {
+    for (int l = 1; l <= P; ++l) {
+      const double jp = (l == 1) ? 1.0 : (l == 2 ? J : J * J);
 #pragma unroll
-          for (int l1 = 0; l1 <= l; ++l1) {
-            const int l2 = l - l1;
-            const int kk = l * (l + 1) / 2 - 1 + l2;  // key (l1, l2)
-            double integral = 0.0;
+      for (int l1 = 0; l1 <= l; ++l1) {
+        const int kk = l * (l + 1) / 2 - 1 + (l - l1);
+        double integral = 0.0;
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-              double value = 0.0;
-#pragma unroll
-              for (int b = 0; b < NB; ++b)
-                value += S.proj[j][v][b] * phys_deriv<NK>(kp.tab.dref[q][b], xx, xy, ex, ey, kk);
-              integral += 0.5 * J * kp.tab.cell_w[q] * (value * value);
-            }
-            const double jp = (l == 1) ? 1.0 : (l == 2 ? J : J * J);
-            beta += jp * integral;
+        for (int q = 0; q < NQ; ++q) {
+          double db, dc;
+          if constexpr (P <= 2) {
+            db = S.D[(q * NB + b) * NK + kk];
+            dc = S.D[(q * NB + c) * NK + kk];
+          } else {
+            const double(&rb)[NK] = *reinterpret_cast<const double(*)[NK]>(&s_dref[(q * NB + b) * NK]);
+            const double(&rc)[NK] = *reinterpret_cast<const double(*)[NK]>(&s_dref[(q * NB + c) * NK]);
+            db = phys_deriv<NK>(rb, xx, xy, ex, ey, kk);
+            dc = phys_deriv<NK>(rc, xx, xy, ex, ey, kk);
           }
+          integral += 0.5 * J * kp.tab.cell_w[q] * (db * dc);
         }
-        w = lw[j] / ((beta + F64_EPS) * (beta + F64_EPS));
+        acc += jp * integral;
       }
-      S.nlw[j][v] = w;
     }
-    __syncwarp();
-    // normalise and combine (weno.rs:180-194)
-    for (int idx = lane; idx < NEQ * NB; idx += 32) {
-      const int v = idx / NB, b = idx - v * NB;
-      const double den = ((S.nlw[0][v] + S.nlw[1][v]) + S.nlw[2][v]) + S.nlw[3][v];
-      double acc = 0.0;
+    S.Q[b][c] = acc;
+    S.Q[c][b] = acc;
+  }
+  __syncwarp();
+  // projections onto the characteristic fields of each face (weno.rs:123-124, 155)
+  for (int idx = lane; idx < 3 * 4 * NEQ * NB; idx += 32) {
+    const int f = idx / (4 * NEQ * NB), r1 = idx - f * 4 * NEQ * NB;
+    const int j = r1 / (NEQ * NB), r2 = r1 - j * NEQ * NB, r = r2 / NB, b = r2 - r * NB;
+    double sum = 0.0;
+    if (interior[f] && (j == 0 || interior[j - 1])) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc += (S.nlw[j][v] / den) * S.proj[j][v][b];
-      S.pol_new[v][b] = acc;
+      for (int k = 0; k < NEQ; ++k) sum += S.L[f][r][k] * S.pol[j][k][b];
     }
-    __syncwarp();
-    // back to conserved variables and area weighting (weno.rs:195-196)
-    for (int idx = lane; idx < NEQ * NB; idx += 32) {
-      const int r = idx / NB, b = idx - r * NB;
-      double sum = 0.0;
+    S.proj[f][j][r][b] = sum;
+  }
+  __syncwarp();
+  // nonlinear weights (weno.rs:142, 173)
+  for (int idx = lane; idx < 3 * 4 * NEQ; idx += 32) {
+    const int f = idx >> 4, j = (idx >> 2) & 3, v = idx & 3;
+    double w = 0.0;
+    if (interior[f] && (j == 0 || interior[j - 1])) {
+      double beta = 0.0;
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) sum += S.R[r][k] * S.pol_new[k][b];
-      S.recon[r][b] = S.recon[r][b] + sum * Jnb * 0.5;
+      for (int b = 0; b < NB; ++b) {
+        double t = 0.0;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) t += S.Q[b][c] * S.proj[f][j][v][c];
+        beta += S.proj[f][j][v][b] * t;
+      }
+      w = lw[j] / ((beta + F64_EPS) * (beta + F64_EPS));
     }
-    __syncwarp();
+    S.nlw[f][j][v] = w;
+  }
+  __syncwarp();
+  // normalise and combine (weno.rs:180-194)
+  for (int idx = lane; idx < 3 * NEQ * NB; idx += 32) {
+    const int f = idx / (NEQ * NB), r1 = idx - f * NEQ * NB, v = r1 / NB, b = r1 - v * NB;
+    double acc = 0.0;
+    if (interior[f]) {
+      const double den = ((S.nlw[f][0][v] + S.nlw[f][1][v]) + S.nlw[f][2][v]) + S.nlw[f][3][v];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc += (S.nlw[f][j][v] / den) * S.proj[f][j][v][b];
+    }
+    S.pol_new[f][v][b] = acc;
+  }
+  __syncwarp();
+  // back to conserved variables, area-weighted average over the faces in order (weno.rs:195-263)
+  double neighbour_area = 0.0, Jn[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    Jn[k] = interior[k] ? m.jac[nbrs[k]] : 0.0;
+    if (interior[k]) neighbour_area += Jn[k] * 0.5;
   }
   for (int idx = lane; idx < NEQ * NB; idx += 32) {
-    const int v = idx / NB, b = idx - v * NB;
-    U[(v * NB + b) * ld + e] = S.recon[v][b] / neighbour_area;
+    const int r = idx / NB, b = idx - r * NB;
+    double recon = 0.0;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      if (!interior[f]) continue;
+      double sum = 0.0;
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) sum += S.R[f][r][k] * S.pol_new[f][k][b];
+      recon = recon + sum * Jn[f] * 0.5;
+    }
+    U[(r * NB + b) * ld + e] = recon / neighbour_area;
   }
   __syncwarp();
   return ST_OK;
@@ -709,7 +729,7 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int nblocks)
           s_fail = 1;
           break;
         }
-        __nanosleep(40);
+        __nanosleep(20);
       }
     }
     __threadfence();
@@ -718,69 +738,117 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int nblocks)
   return s_fail == 0;
 }
 
-// Limiter waves.  Reproduces the reference's sequential, in-place limiter (weno.rs:90-263,
-// element order) exactly, in parallel: an element settles in wave w once every lower-index
-// neighbour settled in an earlier wave.  Its KXRCF flag is recomputed when such a neighbour
-// was rewritten (else the parallel flag t0 stands); a troubled element is reconstructed from
-// final lower neighbours and untouched higher neighbours, exactly the values the sequential
-// loop sees.  Elements settled in one wave are never neighbours with one reading the other,
-// so in-place writes are race free.  Status word: (wave << 2) | kind, kind 1 clean, 2 limited.
+constexpr int kLimiterWarps = 4;
+
+// The limiter (apply_limiter -> weno, limiter.rs:7, weno.rs:86-269), exact in the reference's
+// sequential, in-place element order, run in parallel waves:
+//   * an element settles in wave w once every lower-index neighbour settled in an earlier
+//     wave; it is limited iff modified_kxrcf flags it on the values the sequential loop would
+//     see at that point: the parallel flag of wave 1 when no lower neighbour was rewritten,
+//     else recomputed;
+//   * a limited element is reconstructed from final lower neighbours and untouched higher
+//     neighbours -- again what the sequential loop reads;
+//   * elements that settle in the same wave never read one another, so in-place writes are
+//     race free.
+// Wave 1 also evaluates modified_kxrcf on every element (the parallel flags t0).  Each wave:
+// (A) every warp scans 32 elements at a time, settles the clean ready ones and appends the
+// troubled ready ones to a worklist; grid barrier; (B) one warp per worklist element
+// reconstructs; grid barrier.  Status word: (wave << 2) | kind, kind 1 clean, 2 limited.
+// Wave count = longest chain of increasing-index neighbours through unsettled elements: 2 on
+// the O-grid's 2-colour numbering.
 template <int P>
-__global__ void __launch_bounds__(256) k_limiter_waves(const __grid_constant__ KParams<P> kp,
-                                                       double* __restrict__ U,
-                                                       const unsigned char* __restrict__ t0,
-                                                       unsigned int* __restrict__ status) {
+__global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_constant__ KParams<P> kp,
+                                                                double* __restrict__ U,
+                                                                unsigned char* __restrict__ t0,
+                                                                unsigned int* __restrict__ status,
+                                                                int* __restrict__ work) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NQ = V::NQ, NK = V::NK;
   Control* ctl = kp.ctl;
   if (!ctl->active) return;
-  if (ctl->t0_count == 0) {  // nothing flagged: the sequential loop changes nothing
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      ctl->troubled = 0;
-      ctl->waves = 0;
-    }
-    return;
-  }
   const MeshDev& m = kp.m;
-  __shared__ WenoScratch<P> scratch[8];
+  __shared__ WenoScratch<P> scratch[kLimiterWarps];
+  __shared__ double s_dref[NQ * NB * NK];
+  for (int i = threadIdx.x; i < NQ * NB * NK; i += blockDim.x) s_dref[i] = (&kp.tab.dref[0][0][0])[i];
+  __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int gwarp = blockIdx.x * (blockDim.x >> 5) + wib;
-  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  const int gwarp = blockIdx.x * kLimiterWarps + wib;
+  const int nwarps = gridDim.x * kLimiterWarps;
   int troubled_local = 0;
   int wave = 1;
   for (;; ++wave) {
-    int unknown_local = 0;
-    for (int e = gwarp; e < m.ne; e += nwarps) {
-      const unsigned int st = __ldcg(&status[e]);
-      if (st & 3u) continue;
-      bool ready = true, any_mod = false;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const int nb = m.nbr[k * m.ld + e];
-        if (nb >= 0 && nb < e) {
-          const unsigned int sn = __ldcg(&status[nb]);
-          if ((sn & 3u) == 0u || (int)(sn >> 2) >= wave) ready = false;
-          else if ((sn & 3u) == 2u) any_mod = true;
+    // ---- phase A: readiness scan, settle clean elements, enlist troubled ones ----
+    int unknown_local = 0, flagged_local = 0;
+    for (int base = gwarp * 32; base < m.ne; base += nwarps * 32) {
+      const int e = base + lane;
+      bool pending = false, ready = false, trouble = false;
+      if (e < m.ne) {
+        bool flag0 = false;
+        if (wave == 1) {
+          flag0 = kxrcf<P>(kp, U, e);
+          t0[e] = flag0 ? 1 : 0;
+          flagged_local += flag0 ? 1 : 0;
+          pending = true;
+        } else {
+          pending = (__ldcg(&status[e]) & 3u) == 0u;
         }
+        if (pending) {
+          ready = true;
+          bool any_mod = false;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const int nb = m.nbr[k * m.ld + e];
+            if (nb >= 0 && nb < e) {
+              if (wave == 1) {
+                ready = false;
+              } else {
+                const unsigned int sn = __ldcg(&status[nb]);
+                if ((sn & 3u) == 0u || (int)(sn >> 2) >= wave) ready = false;
+                else if ((sn & 3u) == 2u) any_mod = true;
+              }
+            }
+          }
+          if (ready) trouble = (wave == 1) ? flag0 : (any_mod ? kxrcf<P>(kp, U, e) : (t0[e] != 0));
+        }
+        if (wave == 1 && !ready) status[e] = 0u;
+        if (ready && !trouble) status[e] = ((unsigned int)wave << 2) | 1u;
       }
-      if (!ready) {
-        ++unknown_local;
-        continue;
+      const unsigned int tb = __ballot_sync(0xffffffffu, ready && trouble);
+      if (tb) {
+        int slot0 = 0;
+        if (lane == 0) slot0 = atomicAdd(&ctl->wl_count[wave & 1], __popc(tb));
+        slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+        if (ready && trouble) work[slot0 + __popc(tb & ((1u << lane) - 1u))] = e;
       }
-      bool trouble = t0[e] != 0;
-      if (any_mod) trouble = kxrcf<P>(kp, U, e);
-      if (trouble) {
-        const int rs = weno_reconstruct<P>(kp, U, e, lane, scratch[wib]);
-        if (rs != ST_OK && lane == 0) raise_status(ctl, rs, e);
-        ++troubled_local;
-      }
-      __threadfence();
-      if (lane == 0) status[e] = ((unsigned int)wave << 2) | (trouble ? 2u : 1u);
+      unknown_local += (pending && !ready) ? 1 : 0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unknown_local += __shfl_xor_sync(0xffffffffu, unknown_local, o);
+      flagged_local += __shfl_xor_sync(0xffffffffu, flagged_local, o);
     }
     if (lane == 0 && unknown_local) atomicAdd(&ctl->unknown[wave & 1], unknown_local);
+    if (lane == 0 && flagged_local) atomicAdd(&ctl->t0_count, flagged_local);
     if (!grid_barrier(ctl, gridDim.x)) break;
+    if (wave == 1 && *((volatile int*)&ctl->t0_count) == 0) break;  // nothing to limit
+    const int n_work = *((volatile int*)&ctl->wl_count[wave & 1]);
     const int remaining = *((volatile int*)&ctl->unknown[wave & 1]);
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->unknown[(wave + 1) & 1] = 0;
-    if (remaining == 0 || wave > m.ne + 2) break;
+    // the other parity's counters were last read before the previous wave's second barrier
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctl->wl_count[(wave + 1) & 1] = 0;
+      ctl->unknown[(wave + 1) & 1] = 0;
+    }
+    // ---- phase B: reconstruct the enlisted elements, one warp each ----
+    for (int i = gwarp; i < n_work; i += nwarps) {
+      const int et = __ldcg(&work[i]);
+      const int rs = weno_reconstruct<P>(kp, U, et, lane, scratch[wib], s_dref);
+      if (rs != ST_OK && lane == 0) raise_status(ctl, rs, et);
+      __threadfence();
+      if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
+      ++troubled_local;
+    }
     if (!grid_barrier(ctl, gridDim.x)) break;
+    if (remaining == 0 || wave > m.ne + 2) break;
   }
   if (lane == 0 && troubled_local) atomicAdd(&ctl->troubled, troubled_local);
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->waves = wave;
@@ -860,6 +928,8 @@ __global__ void k_set_active(Control* ctl, double dt, int reset_dt) {
   ctl->dt_bits = (unsigned long long)__double_as_longlong(1.0e10);
   ctl->troubled = 0;
   ctl->t0_count = 0;
+  ctl->unknown[0] = ctl->unknown[1] = 0;
+  ctl->wl_count[0] = ctl->wl_count[1] = 0;
 }
 
 // Layout transposes between the reference's [element][variable][basis] and the SoA state.

@@ -256,6 +256,12 @@ class TemperalDisc:
         self._sd._lib.dgm_get_clock(self._sd._ctx, ctypes.byref(t), ctypes.byref(s))
         return int(s.value)
 
+    def set_limits(self, final_time: float, final_step: int) -> None:
+        """SolverParameters::final_time / final_step for the next time_march / advance."""
+        self.solver_param.final_time = float(final_time)
+        self.solver_param.final_step = int(final_step)
+        self._sd._check(self._sd._lib.dgm_set_limits(self._sd._ctx, float(final_time), int(final_step)), "set_limits")
+
     def set_clock(self, current_time: float, current_step: int) -> None:
         self._sd._check(self._sd._lib.dgm_set_clock(self._sd._ctx, float(current_time), int(current_step)),
                         "set_clock")

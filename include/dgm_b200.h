@@ -138,6 +138,10 @@ int32_t dgm_time_march(dgm_ctx* ctx, double* residuals, double* solutions);
 int32_t dgm_get_clock(dgm_ctx* ctx, double* current_time, int64_t* current_step);
 int32_t dgm_set_clock(dgm_ctx* ctx, double current_time, int64_t current_step);
 
+/* SolverParameters::final_time / final_step (solver.rs:12-13): the loop bounds used by
+ * dgm_time_march and dgm_advance from the next call on. */
+int32_t dgm_set_limits(dgm_ctx* ctx, double final_time, int64_t final_step);
+
 /* ---- device-resident fast path (no host copies of the state per step) ------------------- */
 
 /* Copy a host state ([element][variable][basis]) into the context's resident state, or back. */
@@ -156,6 +160,15 @@ int32_t dgm_synchronize(dgm_ctx* ctx);
 /* The context's CUDA stream (cudaStream_t as void*), for callers that order their own work
  * (copies, events) against the solver. */
 void* dgm_stream(dgm_ctx* ctx);
+
+/* Diagnostics for per-kernel timing: enqueue one launch of a single kernel of the step on the
+ * resident state (phase 0 time step, 1 edge flux, 2 element update (stage-2 form, writes the
+ * second stage buffer), 3 limiter (KXRCF + WENO waves) on that buffer).  Callers time it with
+ * events on dgm_stream().  No counterpart in the reference (it has no kernels). */
+int32_t dgm_launch_phase(dgm_ctx* ctx, int32_t phase);
+/* Launches of that kernel, and of all kernels, per time-march step. */
+int32_t dgm_phase_launches_per_step(dgm_ctx* ctx, int32_t phase);
+int32_t dgm_launches_per_step(dgm_ctx* ctx);
 
 /* Edge (HLLC failures) or element (limiter failures) index flagged by the last error. */
 int64_t dgm_error_location(dgm_ctx* ctx);

@@ -1557,4 +1557,16 @@ void orc_reset_clock(void* h) {
 
 void orc_set_threads(void* h, int32_t threads) { static_cast<Solver*>(h)->threads = threads; }
 
+// Single-state kernels of the flux module, for known-answer tests.
+int32_t orc_hllc(const double* lv, const double* rv, double nx, double ny, double hcr, double* flux) {
+  return hllc(lv, rv, nx, ny, hcr, flux);
+}
+void orc_flux(const double* q, double hcr, double* f, double* g) { euler_flux(q, hcr, f, g); }
+void orc_eigenmatrix(const double* q, double nx, double ny, double hcr, double* L, double* R) {
+  double Lm[4][4], Rm[4][4];
+  eigenmatrix(q, nx, ny, hcr, Lm, Rm);
+  std::memcpy(L, Lm, sizeof(Lm));
+  std::memcpy(R, Rm, sizeof(Rm));
+}
+
 }  // extern "C"

@@ -67,8 +67,7 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
-            build()
+        build()
         L = ctypes.CDLL(LIB)
         vp = ctypes.c_void_p
         L.orc_create_from_msh.argtypes = [ctypes.c_char_p, ctypes.POINTER(OrcConfig), P_I32]
@@ -98,12 +97,35 @@ def lib():
         L.orc_time_march.restype = ctypes.c_int32
         L.orc_reset_clock.argtypes = [vp]
         L.orc_set_threads.argtypes = [vp, ctypes.c_int32]
+        L.orc_hllc.argtypes = [P_D, P_D, ctypes.c_double, ctypes.c_double, ctypes.c_double, P_D]
+        L.orc_hllc.restype = ctypes.c_int32
+        L.orc_flux.argtypes = [P_D, ctypes.c_double, P_D, P_D]
+        L.orc_eigenmatrix.argtypes = [P_D, ctypes.c_double, ctypes.c_double, ctypes.c_double, P_D, P_D]
         _lib = L
     return _lib
 
 
 def _d(a):
     return a.ctypes.data_as(P_D)
+
+
+def hllc(lv, rv, nx, ny, hcr=1.4):
+    """flux::hllc of one interface state pair; returns (status, flux[4])."""
+    lv, rv, out = np.ascontiguousarray(lv, np.float64), np.ascontiguousarray(rv, np.float64), np.zeros(4)
+    st = lib().orc_hllc(_d(lv), _d(rv), float(nx), float(ny), float(hcr), _d(out))
+    return int(st), out
+
+
+def euler_flux(q, hcr=1.4):
+    q, f, g = np.ascontiguousarray(q, np.float64), np.zeros(4), np.zeros(4)
+    lib().orc_flux(_d(q), float(hcr), _d(f), _d(g))
+    return f, g
+
+
+def eigenmatrix(q, nx, ny, hcr=1.4):
+    q, L, R = np.ascontiguousarray(q, np.float64), np.zeros((4, 4)), np.zeros((4, 4))
+    lib().orc_eigenmatrix(_d(q), float(nx), float(ny), float(hcr), _d(L), _d(R))
+    return L, R
 
 
 class Oracle:

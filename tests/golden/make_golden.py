@@ -1,0 +1,84 @@
+"""Regenerate the golden fixtures in this folder.
+
+  python tests/golden/make_golden.py
+
+* airfoil_mesh.npz -- the reference's own mesh fixture (inputfiles/airfoil.msh of
+  DGM_in_rust: 1961 nodes, 3738 triangles, Wall/Farfield lines), parsed with the package's
+  GmshParser and checked against the oracle's parser; stored as arrays so the tests do not need
+  the reference tree.
+* airfoil_run.npz -- the reference's configured run on that mesh (its parameters.json /
+  freestream.json / initial_solution.json: p = 2, 6/3-point rules, gamma 1.4, M 0.8,
+  AoA 1.5 deg, rho 1, p 1e5, CFL from the formula of initialization.rs:29-33, 20 steps),
+  computed by the oracle.
+* ogrid16x8.npz -- a 16 x 8 O-grid (p = 2): initial state, its residual, a seeded perturbed
+  state with its residual and limited state, and 3 time-march steps.
+
+The oracle is the C++ restatement under oracle/ (parity with the Rust reference unpinned).
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from dgm_in_rust_b200 import GmshParser, naca0012_ogrid  # noqa: E402
+from oracle.oracle import Oracle  # noqa: E402
+
+AIRFOIL = "/root/reference/inputfiles/airfoil.msh"
+REF_FS = (1.5, 0.8, 1.0, 100000.0)  # aoa, mach, rho, p of freestream.json / initial_solution.json
+
+
+def airfoil():
+    raw = GmshParser.parse(AIRFOIL)
+    o = Oracle(msh_path=AIRFOIL, order=2, ncell_gp=6, nedge_gp=3, freestream=REF_FS)
+    assert np.array_equal(o.get("xy"), raw.vertices.reshape(-1, 2))
+    arrays = {"vertices": raw.vertices}
+    for k, b in enumerate(raw.edge_blocks):
+        arrays[f"edge_block_{k}"] = b.node_pairs
+    for k, t in enumerate(raw.element_blocks):
+        arrays[f"tri_block_{k}"] = t
+    arrays["edge_block_names"] = np.array([b.physical_name for b in raw.edge_blocks])
+    np.savez_compressed(os.path.join(HERE, "airfoil_mesh.npz"), **arrays)
+    # the reference's configured run: cfl <= 0 selects the formula
+    o = Oracle(raw=raw, order=2, ncell_gp=6, nedge_gp=3, hcr=1.4, cfl=-1.0, final_time=5.0, final_step=20,
+               freestream=REF_FS)
+    U = o.initial_solution()
+    R = o.new_state()
+    t, s = o.time_march(R, U)
+    np.savez_compressed(os.path.join(HERE, "airfoil_run.npz"), U20=U, t20=np.array(t), steps=np.array(s),
+                        cfl=np.array(o.cfl))
+    print("airfoil:", o.ne, "elements, t after 20 steps", t)
+
+
+def ogrid():
+    raw = naca0012_ogrid(16, 8)
+    fs = (1.25, 0.8, 1.0, 1.0 / 1.4)
+    o = Oracle(raw=raw, order=2, ncell_gp=6, nedge_gp=3, cfl=0.1, final_time=1.0e30, final_step=3, freestream=fs)
+    U0 = o.initial_solution()
+    R0 = o.new_state()
+    o.compute_residuals(R0, U0)
+    rng = np.random.default_rng(2024)
+    noise = rng.standard_normal(U0[:, :, 1:].shape) * np.abs(U0[:, :, :1])
+    Up = U0.copy()
+    Up[:, :, 1:] += 0.03 * noise  # mild: residual well defined
+    Rp = o.new_state()
+    o.compute_residuals(Rp, Up)
+    Ut = U0.copy()
+    Ut[:, :, 1:] += 0.1 * noise  # strong: limiter active
+    Ul = Ut.copy()
+    n = o.apply_limiter(Ul)
+    assert np.isfinite(Ul).all() and n > 0
+    U3 = U0.copy()
+    R3 = o.new_state()
+    t, s = o.time_march(R3, U3)
+    np.savez_compressed(os.path.join(HERE, "ogrid16x8.npz"), U0=U0, R0=R0, Up=Up, Rp=Rp, Ut=Ut, Ul=Ul,
+                        troubled=np.array(n), U3=U3, R3=R3, t3=np.array(t), dt0=np.array(o.compute_time_step(U0)))
+    print("ogrid16x8: troubled", n, "t3", t)
+
+
+if __name__ == "__main__":
+    airfoil()
+    ogrid()

@@ -1,0 +1,251 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and the golden fixtures.
+
+Tolerances (FP64): residuals 1e-12 relative L2; limited states and states after N RK3 steps
+1e-10 relative L2; time steps 1e-14 relative.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, airfoil_raw, rel_l2
+from dgm_in_rust_b200 import (DgmError, InitialSolution, build_solver, default_rules, freestream_quantity,
+                              initial_state, naca0012_ogrid, process_mesh)
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+FS = (1.25, 0.8, 1.0, 1.0 / 1.4)  # aoa, mach, rho, p
+REF_FS = (1.5, 0.8, 1.0, 100000.0)
+TOL_RES, TOL_STATE, TOL_DT = 1e-12, 1e-10, 1e-14
+
+
+def pair(raw, order=2, fs=FS, cfl=0.1, final_time=1.0e30, final_step=10, limiter=True, threads=4):
+    nq, ng = default_rules(order)
+    mesh = process_mesh(raw, freestream_quantity(fs[1], fs[0], fs[2], fs[3], 1.4), 1.4)
+    s = build_solver(mesh, order, 1.4, cfl, final_time, final_step, limiter=limiter)
+    o = Oracle(raw=raw, order=order, ncell_gp=nq, nedge_gp=ng, cfl=cfl, final_time=final_time,
+               final_step=final_step, limiter=limiter, threads=threads, freestream=fs)
+    U0 = initial_state(mesh, s.basis, s.gauss_points, 1.4, InitialSolution(fs[2], fs[0], fs[1], fs[3]))
+    return s, o, U0
+
+
+def perturbed(U0, amp, seed):
+    rng = np.random.default_rng(seed)
+    U = U0.copy()
+    U[:, :, 1:] += amp * rng.standard_normal(U[:, :, 1:].shape) * np.abs(U[:, :, :1])
+    return U
+
+
+MESHES = {
+    "ogrid64x32": lambda: naca0012_ogrid(64, 32),
+    "ogrid32x16quad": lambda: naca0012_ogrid(32, 16, order="quad"),
+    "airfoil": airfoil_raw,
+}
+
+
+@pytest.fixture(autouse=True)
+def _lib(built):
+    return built
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("mesh", sorted(MESHES))
+def test_residual_parity(order, mesh):
+    s, o, U0 = pair(MESHES[mesh](), order=order)
+    for U in (U0, perturbed(U0, 0.02, 1)):
+        Ro, Rg = o.new_state(), s.spatial_disc.new_state()
+        o.compute_residuals(Ro, U)
+        s.spatial_disc.compute_residuals(Rg, U.copy())
+        assert rel_l2(Rg, Ro) < TOL_RES
+    s.close()
+
+
+def test_residual_accumulates_into_input():
+    """compute_residuals adds to the residual array it is given (spatial_disc.rs:46,167 + :353)."""
+    s, o, U0 = pair(naca0012_ogrid(32, 16))
+    U = perturbed(U0, 0.02, 2)
+    Rin = np.random.default_rng(3).standard_normal(U.shape)
+    Ro, Rg = Rin.copy(), Rin.copy()
+    o.compute_residuals(Ro, U)
+    s.spatial_disc.compute_residuals(Rg, U.copy())
+    assert rel_l2(Rg, Ro) < TOL_RES
+    s.close()
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("mesh", sorted(MESHES))
+def test_limiter_parity(order, mesh):
+    s, o, U0 = pair(MESHES[mesh](), order=order)
+    U = perturbed(U0, 0.1, 4)
+    Uo, Ug = U.copy(), U.copy()
+    no = o.apply_limiter(Uo)
+    ng = s.spatial_disc.apply_limiter(Ug)
+    assert ng == no
+    assert rel_l2(Ug, Uo) < TOL_STATE
+    assert np.abs(Ug - Uo).max() <= 1e-10 * np.abs(Uo).max()
+    troubled, waves = s.spatial_disc.limiter_stats()
+    if mesh == "ogrid64x32" and no > 0:
+        assert waves <= 2  # 2-colour numbering: chains of increasing-index neighbours are short
+    s.close()
+
+
+def test_limiter_heavy_sequential_dependencies():
+    """Many touching troubled cells in quad numbering: exercises long wave chains."""
+    s, o, U0 = pair(naca0012_ogrid(48, 24, order="quad"))
+    U = perturbed(U0, 0.25, 5)
+    Uo, Ug = U.copy(), U.copy()
+    assert s.spatial_disc.apply_limiter(Ug) == o.apply_limiter(Uo)
+    assert rel_l2(Ug, Uo) < TOL_STATE
+    s.close()
+
+
+@pytest.mark.parametrize("mesh", sorted(MESHES))
+def test_time_step_parity(mesh):
+    fs = REF_FS if mesh == "airfoil" else FS
+    s, o, U0 = pair(MESHES[mesh](), fs=fs)
+    for U in (U0, perturbed(U0, 0.02, 6)):
+        dg = s.temporal_disc.compute_time_step(U)
+        do = o.compute_time_step(U)
+        assert abs(dg - do) <= TOL_DT * abs(do)
+    s.close()
+
+
+def test_rk3_parity():
+    s, o, U0 = pair(naca0012_ogrid(64, 32))
+    U = perturbed(U0, 0.02, 7)
+    dt = o.compute_time_step(U)
+    Ro, Uo = o.new_state(), U.copy()
+    o.rk3(Ro, Uo, dt)
+    Rg, Ug = s.spatial_disc.new_state(), U.copy()
+    s.temporal_disc.rk3(s.spatial_disc, Rg, Ug, dt)
+    assert rel_l2(Ug, Uo) < TOL_RES
+    assert rel_l2(Rg, Ro) < 1e-11
+    s.close()
+
+
+def test_time_march_c1_p1():
+    """64 x 32 O-grid, p = 1, M 0.5, AoA 2 deg, CFL 0.1, 100 steps (p = 1 is an extension)."""
+    fs = (2.0, 0.5, 1.0, 1.0 / 1.4)
+    s, o, U0 = pair(naca0012_ogrid(64, 32), order=1, fs=fs, final_step=100)
+    Uo, Ro = U0.copy(), o.new_state()
+    to, so = o.time_march(Ro, Uo)
+    Ug, Rg = U0.copy(), s.spatial_disc.new_state()
+    s.temporal_disc.time_march(s.spatial_disc, Rg, Ug)
+    assert so == s.temporal_disc.current_step == 100
+    assert abs(s.temporal_disc.current_time - to) <= 1e-13 * to
+    assert rel_l2(Ug, Uo) < TOL_STATE
+    s.close()
+
+
+def test_time_march_c2_full_mesh():
+    """The transonic limiter configuration at full size (256 x 128, 65,536 triangles, p = 2,
+    M 0.8, AoA 1.25 deg) for 24 steps against the oracle."""
+    s, o, U0 = pair(naca0012_ogrid(256, 128), final_step=24, threads=8)
+    Uo, Ro = U0.copy(), o.new_state()
+    o.time_march(Ro, Uo)
+    Ug, Rg = U0.copy(), s.spatial_disc.new_state()
+    s.temporal_disc.time_march(s.spatial_disc, Rg, Ug)
+    assert rel_l2(Ug, Uo) < TOL_STATE
+    # the last stage's residual of a nearly uniform state on 5e-8-thick wall cells is flux
+    # differences over tiny areas: ill-conditioned, so it only agrees to ~1e-8 relative
+    assert rel_l2(Rg, Ro) < 1e-7
+    # limiter active in this run
+    flags = o.troubled_flags(Uo)
+    assert flags.sum() > 0
+    s.close()
+
+
+def test_airfoil_reference_run_golden():
+    """The reference's configured run (its JSON inputs) on its airfoil.msh, 20 steps."""
+    z = np.load(os.path.join(GOLDEN, "airfoil_run.npz"))
+    raw = airfoil_raw()
+    mesh = process_mesh(raw, freestream_quantity(0.8, 1.5, 1.0, 100000.0, 1.4), 1.4)
+    from dgm_in_rust_b200 import reference_cfl
+    s = build_solver(mesh, 2, 1.4, reference_cfl(2), 5.0, 20)
+    U = initial_state(mesh, s.basis, s.gauss_points, 1.4, InitialSolution(1.0, 1.5, 0.8, 100000.0))
+    R = np.zeros_like(U)
+    s.temporal_disc.time_march(s.spatial_disc, R, U)
+    assert s.temporal_disc.current_step == 20
+    assert abs(s.temporal_disc.current_time - float(z["t20"])) <= 1e-13 * float(z["t20"])
+    assert rel_l2(U, z["U20"]) < TOL_STATE
+    s.close()
+
+
+def test_ogrid_golden_on_gpu():
+    z = np.load(os.path.join(GOLDEN, "ogrid16x8.npz"))
+    s, _, U0 = pair(naca0012_ogrid(16, 8), final_step=3)
+    sd, td = s.spatial_disc, s.temporal_disc
+    R = sd.new_state()
+    sd.compute_residuals(R, z["U0"].copy())
+    assert rel_l2(R, z["R0"]) < TOL_RES
+    R = sd.new_state()
+    sd.compute_residuals(R, z["Up"].copy())
+    assert rel_l2(R, z["Rp"]) < TOL_RES
+    Ul = z["Ut"].copy()
+    assert sd.apply_limiter(Ul) == int(z["troubled"])
+    assert rel_l2(Ul, z["Ul"]) < TOL_STATE
+    U = z["U0"].copy()
+    R = sd.new_state()
+    td.time_march(sd, R, U)
+    assert rel_l2(U, z["U3"]) < TOL_STATE and abs(td.current_time - float(z["t3"])) < 1e-17
+    s.close()
+
+
+def test_negative_pressure_raises():
+    s, o, U0 = pair(naca0012_ogrid(16, 8))
+    U = U0.copy()
+    U[5, 3, :] *= -1.0
+    with pytest.raises(Exception) as eo:
+        o.compute_residuals(o.new_state(), U)
+    with pytest.raises(DgmError) as eg:
+        s.spatial_disc.compute_residuals(s.spatial_disc.new_state(), U.copy())
+    assert eg.value.status == eo.value.status
+    assert 0 <= eg.value.where < s.mesh.n_edges
+    # the context stays usable after the error
+    R = s.spatial_disc.new_state()
+    s.spatial_disc.compute_residuals(R, U0.copy())
+    Ro = o.new_state()
+    o.compute_residuals(Ro, U0)
+    assert rel_l2(R, Ro) < TOL_RES
+    s.close()
+
+
+def test_determinism():
+    s, _, U0 = pair(naca0012_ogrid(64, 32), final_step=6)
+    outs = []
+    for _ in range(2):
+        U, R = U0.copy(), s.spatial_disc.new_state()
+        s.temporal_disc.set_clock(0.0, 0)
+        s.temporal_disc.time_march(s.spatial_disc, R, U)
+        outs.append(U)
+    assert np.array_equal(outs[0], outs[1])
+    s.close()
+
+
+def test_advance_matches_time_march():
+    s, _, U0 = pair(naca0012_ogrid(64, 32), final_step=11)
+    td = s.temporal_disc
+    U, R = U0.copy(), s.spatial_disc.new_state()
+    td.time_march(s.spatial_disc, R, U)
+    td.set_clock(0.0, 0)
+    td.upload(U0)
+    td.advance(11)
+    td.synchronize()
+    V = np.zeros_like(U0)
+    td.download(V)
+    assert np.array_equal(U, V)
+    assert td.current_step == 11
+    s.close()
+
+
+def test_final_time_clamp():
+    s, o, U0 = pair(naca0012_ogrid(32, 16), final_time=2.5e-4, final_step=1000)
+    U, R = U0.copy(), s.spatial_disc.new_state()
+    s.temporal_disc.time_march(s.spatial_disc, R, U)
+    Uo, Ro = U0.copy(), o.new_state()
+    to, so = o.time_march(Ro, Uo)
+    assert s.temporal_disc.current_time == 2.5e-4 == to
+    assert s.temporal_disc.current_step == so
+    assert rel_l2(U, Uo) < TOL_STATE
+    s.close()

@@ -214,8 +214,20 @@ struct Ops {
         for (int b = 0; b < NB; ++b) tb.phi_edge[k][g][b] = t->phi_edge[(k * NG + g) * NB + b];
     for (int q = 0; q < NQ; ++q) tb.cell_w[q] = t->cell_weights[q];
     for (int g = 0; g < NG; ++g) tb.edge_w[g] = t->edge_weights[g];
-    for (int b = 0; b < NB; ++b) tb.mass[b] = t->mass_diag[b];
-    kp.hcr = c->hcr;
+    for (int b = 0; b < NB; ++b) {
+      tb.mass[b] = t->mass_diag[b];
+      kp.inv_mass[b] = 1.0 / t->mass_diag[b];
+    }
+    // gas constants with the reference's expressions (flux.rs:76-77, 85, 96)
+    dgm::Gas& gas = kp.gas;
+    gas.hcr = c->hcr;
+    gas.gm1 = c->hcr - 1.0;
+    gas.zeta = (c->hcr - 1.0) / (2.0 * c->hcr);
+    gas.inv_zeta = 1.0 / gas.zeta;
+    gas.zm1h = (gas.zeta - 1.0) / 2.0;
+    gas.gp1h = (c->hcr + 1.0) / (2.0 * c->hcr);
+    const double n = std::nearbyint(gas.inv_zeta);
+    gas.inv_zeta_int = (n >= 1.0 && n <= 16.0 && std::fabs(gas.inv_zeta - n) <= 1e-12 * n) ? (int)n : 0;
     kp.ctl = c->ctl;
     return DGM_OK;
   }

@@ -86,11 +86,24 @@ struct Control {
   unsigned int bar_count, bar_gen;  // grid barrier of the limiter kernel
 };
 
+// Gas constants, computed once on the host from hcr with the reference's expressions.
+struct Gas {
+  double hcr;        // ratio of specific heats
+  double gm1;        // hcr - 1
+  double zeta;       // (hcr - 1) / (2 hcr)                      flux.rs:76
+  double inv_zeta;   // 1 / zeta
+  double zm1h;       // (zeta - 1) / 2                            flux.rs:77
+  double gp1h;       // (hcr + 1) / (2 hcr)                       flux.rs:85,96
+  int inv_zeta_int;  // 1/zeta when it is an integer to round-off (7 for hcr = 1.4), else 0
+  int _pad;
+};
+
 template <int P>
 struct KParams {
   Tables<P> tab;
   MeshDev m;
-  double hcr;
+  Gas gas;
+  double inv_mass[Variant<P>::NB];  // 1 / mass_mat_diag
   Control* ctl;
 };
 
@@ -98,11 +111,12 @@ __device__ __forceinline__ void raise_status(Control* ctl, int code, long long w
   if (atomicCAS(&ctl->status, 0, code) == 0) ctl->err_where = where;
 }
 
-// flux::flux, flux.rs:154-169
-__device__ __forceinline__ void euler_flux(const double q[4], double hcr, double f[4], double g[4]) {
-  const double u = q[1] / q[0];
-  const double v = q[2] / q[0];
-  const double p = (hcr - 1.0) * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+// flux::flux, flux.rs:154-169 (one reciprocal of the density instead of three divisions)
+__device__ __forceinline__ void euler_flux(const double q[4], const Gas& gas, double f[4], double g[4]) {
+  const double rq = 1.0 / q[0];
+  const double u = q[1] * rq;
+  const double v = q[2] * rq;
+  const double p = gas.gm1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) * rq);
   f[0] = q[1];
   f[1] = q[1] * u + p;
   f[2] = q[2] * u;
@@ -114,27 +128,40 @@ __device__ __forceinline__ void euler_flux(const double q[4], double hcr, double
 }
 
 // flux::hllc, flux.rs:28-153.  Returns ST_NEG_DENSITY / ST_NEG_PRESSURE like the reference's Err.
+// Same formulas; densities enter through their reciprocals, x^zeta as exp(zeta log x), and
+// (.)^(1/zeta) as an integer power when 1/zeta is an integer to round-off (hcr = 1.4: 7);
+// both differ from the reference's libm pow only in the last bits.
+__device__ __forceinline__ double ipow(double x, int n) {
+  double r = 1.0;
+  while (n) {
+    if (n & 1) r *= x;
+    x *= x;
+    n >>= 1;
+  }
+  return r;
+}
+
 __device__ __forceinline__ int hllc(const double lv[4], const double rv[4], double nx, double ny,
-                                    double hcr, double flux[4]) {
+                                    const Gas& gas, double flux[4]) {
   const double ql0 = lv[0], ql1 = lv[1] * nx + lv[2] * ny, ql2 = -lv[1] * ny + lv[2] * nx, ql3 = lv[3];
   const double qr0 = rv[0], qr1 = rv[1] * nx + rv[2] * ny, qr2 = -rv[1] * ny + rv[2] * nx, qr3 = rv[3];
-  const double ul = ql1 / ql0, ur = qr1 / qr0, vl = ql2 / ql0, vr = qr2 / qr0;
-  const double pl = (hcr - 1.0) * (ql3 - 0.5 * (ql1 * ql1 + ql2 * ql2) / ql0);
-  const double pr = (hcr - 1.0) * (qr3 - 0.5 * (qr1 * qr1 + qr2 * qr2) / qr0);
+  const double rl = 1.0 / ql0, rr = 1.0 / qr0;
+  const double ul = ql1 * rl, ur = qr1 * rr, vl = ql2 * rl, vr = qr2 * rr;
+  const double pl = gas.gm1 * (ql3 - 0.5 * (ql1 * ql1 + ql2 * ql2) * rl);
+  const double pr = gas.gm1 * (qr3 - 0.5 * (qr1 * qr1 + qr2 * qr2) * rr);
   if (ql0 < 0.0 || qr0 < 0.0) return ST_NEG_DENSITY;
   if (pl < 0.0 || pr < 0.0) return ST_NEG_PRESSURE;
-  const double cl = sqrt(hcr * pl / ql0);
-  const double cr = sqrt(hcr * pr / qr0);
+  const double cl = sqrt(gas.hcr * pl * rl);
+  const double cr = sqrt(gas.hcr * pr * rr);
   const double fl0 = ql1, fl1 = ql1 * ul + pl, fl2 = ql2 * ul, fl3 = ul * (ql3 + pl);
   const double fr0 = qr1, fr1 = qr1 * ur + pr, fr2 = qr2 * ur, fr3 = ur * (qr3 + pr);
-  // PVRS-type p* of flux.rs:75-78, x^y evaluated as exp(y log x) (the libm pow of the
-  // reference rounds differently in the last bits; the difference stays at round-off level)
-  const double zeta = (hcr - 1.0) / (2.0 * hcr);
-  const double p_star = exp((1.0 / zeta) * log((cl + cr - (zeta - 1.0) / 2.0 * (ur - ul)) /
-                                              (cl / exp(zeta * log(pl)) + cr / exp(zeta * log(pr)))));
-  const double ql_lower = (p_star <= pl) ? 1.0 : sqrt(1.0 + (hcr + 1.0) / (2.0 * hcr) * (p_star / pl - 1.0));
+  // PVRS-type p*, flux.rs:75-78
+  const double base = (cl + cr - gas.zm1h * (ur - ul)) /
+                      (cl * exp(-gas.zeta * log(pl)) + cr * exp(-gas.zeta * log(pr)));
+  const double p_star = gas.inv_zeta_int ? ipow(base, gas.inv_zeta_int) : exp(gas.inv_zeta * log(base));
+  const double ql_lower = (p_star <= pl) ? 1.0 : sqrt(1.0 + gas.gp1h * (p_star / pl - 1.0));
   const double sl = ul - cl * ql_lower;
-  const double qr_lower = (p_star <= pr) ? 1.0 : sqrt(1.0 + (hcr + 1.0) / (2.0 * hcr) * (p_star / pr - 1.0));
+  const double qr_lower = (p_star <= pr) ? 1.0 : sqrt(1.0 + gas.gp1h * (p_star / pr - 1.0));
   const double sr = ur + cr * qr_lower;
   double f0, fn, ft, f3;
   if (sl >= 0.0) {
@@ -144,17 +171,19 @@ __device__ __forceinline__ int hllc(const double lv[4], const double rv[4], doub
   } else {
     const double s_star = (pr - pl + ql0 * ul * (sl - ul) - qr0 * ur * (sr - ur)) / (ql0 * (sl - ul) - qr0 * (sr - ur));
     if (s_star >= 0.0) {
-      const double m = ql0 * (sl - ul) / (sl - s_star);
+      const double dl = ql0 * (sl - ul);
+      const double m = dl / (sl - s_star);
       const double qs0 = m, qs1 = m * s_star, qs2 = m * vl;
-      const double qs3 = m * (ql3 / ql0 + (s_star - ul) * (s_star + pl / (ql0 * (sl - ul))));
+      const double qs3 = m * (ql3 * rl + (s_star - ul) * (s_star + pl / dl));
       f0 = fl0 + sl * (qs0 - ql0);
       fn = fl1 + sl * (qs1 - ql1);
       ft = fl2 + sl * (qs2 - ql2);
       f3 = fl3 + sl * (qs3 - ql3);
     } else {
-      const double m = qr0 * (sr - ur) / (sr - s_star);
+      const double dr = qr0 * (sr - ur);
+      const double m = dr / (sr - s_star);
       const double qs0 = m, qs1 = m * s_star, qs2 = m * vr;
-      const double qs3 = m * (qr3 / qr0 + (s_star - ur) * (s_star + pr / (qr0 * (sr - ur))));
+      const double qs3 = m * (qr3 * rr + (s_star - ur) * (s_star + pr / dr));
       f0 = fr0 + sr * (qs0 - qr0);
       fn = fr1 + sr * (qs1 - qr1);
       ft = fr2 + sr * (qs2 - qr2);
@@ -168,21 +197,23 @@ __device__ __forceinline__ int hllc(const double lv[4], const double rv[4], doub
   return ST_OK;
 }
 
-// compute_eigenmatrix, local_characteristics.rs:4-50
-__device__ __forceinline__ void eigenmatrix(const double q[4], double nx, double ny, double hcr,
+// compute_eigenmatrix, local_characteristics.rs:4-50 (reciprocals of rho and c)
+__device__ __forceinline__ void eigenmatrix(const double q[4], double nx, double ny, const Gas& gas,
                                             double L[4][4], double R[4][4]) {
-  const double u = q[1] / q[0];
-  const double v = q[2] / q[0];
-  const double p = (hcr - 1.0) * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
-  const double c = sqrt(hcr * p / q[0]);
-  const double h = (q[3] + p) / q[0];
-  const double b1 = (hcr - 1.0) / (c * c);
-  const double b2 = b1 * (u * u + v * v) / 2.0;
+  const double rq = 1.0 / q[0];
+  const double u = q[1] * rq;
+  const double v = q[2] * rq;
+  const double p = gas.gm1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) * rq);
+  const double c = sqrt(gas.hcr * p * rq);
+  const double ic = 1.0 / c;
+  const double h = (q[3] + p) * rq;
+  const double b1 = gas.gm1 * (ic * ic);
+  const double b2 = b1 * (u * u + v * v) * 0.5;
   const double vn = u * nx + v * ny;
-  L[0][0] = (b2 + vn / c) / 2.0;
-  L[0][1] = -(b1 * u + nx / c) / 2.0;
-  L[0][2] = -(b1 * v + ny / c) / 2.0;
-  L[0][3] = b1 / 2.0;
+  L[0][0] = (b2 + vn * ic) * 0.5;
+  L[0][1] = -(b1 * u + nx * ic) * 0.5;
+  L[0][2] = -(b1 * v + ny * ic) * 0.5;
+  L[0][3] = b1 * 0.5;
   L[1][0] = ny * u - nx * v;
   L[1][1] = -ny;
   L[1][2] = nx;
@@ -191,10 +222,10 @@ __device__ __forceinline__ void eigenmatrix(const double q[4], double nx, double
   L[2][1] = b1 * u;
   L[2][2] = b1 * v;
   L[2][3] = -b1;
-  L[3][0] = (b2 - vn / c) / 2.0;
-  L[3][1] = -(b1 * u - nx / c) / 2.0;
-  L[3][2] = -(b1 * v - ny / c) / 2.0;
-  L[3][3] = b1 / 2.0;
+  L[3][0] = (b2 - vn * ic) * 0.5;
+  L[3][1] = -(b1 * u - nx * ic) * 0.5;
+  L[3][2] = -(b1 * v - ny * ic) * 0.5;
+  L[3][3] = b1 * 0.5;
   R[0][0] = 1.0;
   R[0][1] = 0.0;
   R[0][2] = 1.0;
@@ -209,7 +240,7 @@ __device__ __forceinline__ void eigenmatrix(const double q[4], double nx, double
   R[2][3] = v + c * ny;
   R[3][0] = h - c * vn;
   R[3][1] = -u * ny + v * nx;
-  R[3][2] = (u * u + v * v) / 2.0;
+  R[3][2] = (u * u + v * v) * 0.5;
   R[3][3] = h + c * vn;
 }
 
@@ -261,7 +292,7 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
   __syncthreads();
   if (!kp.ctl->active) return;
   const MeshDev& m = kp.m;
-  const double hcr = kp.hcr;
+  const Gas& gas = kp.gas;
   const int total = (m.n_int + m.n_bnd) * NG;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     const int s = t / NG, g = t - s * NG;
@@ -284,7 +315,7 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
         rv[v] = c;
       }
       const double4 geo = m.ie_geo[s];
-      const int st = hllc(lv, rv, geo.x, geo.y, hcr, out);
+      const int st = hllc(lv, rv, geo.x, geo.y, gas, out);
       if (st != ST_OK) raise_status(kp.ctl, st, m.slot_ref[s]);
 #pragma unroll
       for (int v = 0; v < NEQ; ++v) out[v] *= geo.z;
@@ -305,7 +336,7 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
       const double nx = geo.x, ny = geo.y;
       if (((info >> 2) & 1) == 0) {
         // slip wall, boundary_condition.rs:31-47
-        const double pressure = (hcr - 1.0) * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+        const double pressure = gas.gm1 * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
         out[0] = 0.0;
         out[1] = pressure * nx;
         out[2] = pressure * ny;
@@ -316,11 +347,11 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
         const double bc[4] = {bq.x, bq.y, bq.z, bq.w};
         const double u = lv[1] / lv[0];
         const double v = lv[2] / lv[0];
-        const double p = (hcr - 1.0) * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
-        const double c = sqrt(hcr * p / lv[0]);
+        const double p = gas.gm1 * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+        const double c = sqrt(gas.hcr * p / lv[0]);
         const double vn = u * nx + v * ny;
         double Lm[4][4], Rm[4][4];
-        eigenmatrix(lv, nx, ny, hcr, Lm, Rm);
+        eigenmatrix(lv, nx, ny, gas, Lm, Rm);
         const double lam[4] = {vn - c, vn, vn, vn + c};
         double mix[4];
 #pragma unroll
@@ -344,7 +375,7 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
         const double un = q[1] / q[0];
         const double vv = q[2] / q[0];
         const double vn_new = un * nx + vv * ny;
-        const double p_new = (hcr - 1.0) * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+        const double p_new = gas.gm1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
         const double h_new = q[3] + p_new;
         out[0] = q[0] * vn_new;
         out[1] = q[1] * vn_new + p_new * nx;
@@ -407,7 +438,6 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
   }
   const double J = m.jac[e];
   const double xx = m.dinv[0 * ld + e], xy = m.dinv[1 * ld + e], ex = m.dinv[2 * ld + e], ey = m.dinv[3 * ld + e];
-  const double hcr = kp.hcr;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
     double mine = 0.0;
@@ -417,7 +447,7 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
 #pragma unroll
     for (int w = 0; w < NEQ; ++w) uq[w] = __shfl_sync(0xffffffffu, mine, w * 8 + i);
     double f[NEQ], g[NEQ];
-    euler_flux(uq, hcr, f, g);
+    euler_flux(uq, kp.gas, f, g);
     const double fv = var == 0 ? f[0] : var == 1 ? f[1] : var == 2 ? f[2] : f[3];
     const double gv = var == 0 ? g[0] : var == 1 ? g[1] : var == 2 ? g[2] : g[3];
     const double sc = kp.tab.cell_w[q] * 0.5 * J;
@@ -443,12 +473,13 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
   }
   if (!valid) return;
   const double dt = ctl->dt;
+  const double inv_half_j = 1.0 / (0.5 * J);
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const size_t idx = (var * NB + b) * ld + e;
     double rr = r[b];
     if constexpr (MODE == 0) rr = Rin[idx] + rr;
-    rr = rr / (kp.tab.mass[b] * 0.5 * J);
+    rr = rr * kp.inv_mass[b] * inv_half_j;  // divide_residual_by_mass_mat_diag
     if (Rout) Rout[idx] = rr;
     if constexpr (MODE == 1) {
       Uout[idx] = u[b] + dt * rr;
@@ -581,7 +612,10 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
   else lw[2] = 0.999;
   const double J = m.jac[e];
   const double xx = m.dinv[0 * ld + e], xy = m.dinv[1 * ld + e], ex = m.dinv[2 * ld + e], ey = m.dinv[3 * ld + e];
-  for (int i = lane; i < NEQ * NB; i += 32) {
+#pragma unroll
+  for (int it = 0; it < (NEQ * NB + 31) / 32; ++it) {
+    const int i = lane + 32 * it;
+    if (i >= NEQ * NB) break;
     const int v = i / NB, b = i - v * NB;
     S.pol[0][v][b] = ld_state(&U[(v * NB + b) * ld + e]);
 #pragma unroll
@@ -589,7 +623,10 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
       S.pol[k + 1][v][b] = (interior[k] && b > 0) ? ld_state(&U[(v * NB + b) * ld + nbrs[k]]) : 0.0;
   }
   if constexpr (P <= 2) {
-    for (int i = lane; i < NQ * NB; i += 32) {
+#pragma unroll
+    for (int it = 0; it < (NQ * NB + 31) / 32; ++it) {
+      const int i = lane + 32 * it;
+      if (i >= NQ * NB) break;
       const double(&r)[NK] = *reinterpret_cast<const double(*)[NK]>(&s_dref[i * NK]);
 #pragma unroll
       for (int kk = 0; kk < NK; ++kk) S.D[i * NK + kk] = phys_deriv<NK>(r, xx, xy, ex, ey, kk);
@@ -606,10 +643,13 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
     double mean[4];
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) mean[v] = S.pol[0][v][0];
-    eigenmatrix(mean, geo.x, geo.y, kp.hcr, S.L[lane], S.R[lane]);
+    eigenmatrix(mean, geo.x, geo.y, kp.gas, S.L[lane], S.R[lane]);
   }
   // Gram matrix of the smoothness indicator
-  for (int pr = lane; pr < NB * NB; pr += 32) {
+#pragma unroll
+  for (int it = 0; it < (NB * NB + 31) / 32; ++it) {
+    const int pr = lane + 32 * it;
+    if (pr >= NB * NB) break;
     const int b = pr / NB, c = pr - b * NB;
     if (c < b) continue;
     double acc = 0.0;
@@ -642,7 +682,10 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
   }
   __syncwarp();
   // projections onto the characteristic fields of each face (weno.rs:123-124, 155)
-  for (int idx = lane; idx < 3 * 4 * NEQ * NB; idx += 32) {
+#pragma unroll
+  for (int it = 0; it < (3 * 4 * NEQ * NB + 31) / 32; ++it) {
+    const int idx = lane + 32 * it;
+    if (idx >= 3 * 4 * NEQ * NB) break;
     const int f = idx / (4 * NEQ * NB), r1 = idx - f * 4 * NEQ * NB;
     const int j = r1 / (NEQ * NB), r2 = r1 - j * NEQ * NB, r = r2 / NB, b = r2 - r * NB;
     double sum = 0.0;
@@ -654,17 +697,23 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
   }
   __syncwarp();
   // nonlinear weights (weno.rs:142, 173)
-  for (int idx = lane; idx < 3 * 4 * NEQ; idx += 32) {
+#pragma unroll
+  for (int it = 0; it < (3 * 4 * NEQ + 31) / 32; ++it) {
+    const int idx = lane + 32 * it;
+    if (idx >= 3 * 4 * NEQ) break;
     const int f = idx >> 4, j = (idx >> 2) & 3, v = idx & 3;
     double w = 0.0;
     if (interior[f] && (j == 0 || interior[j - 1])) {
+      double pv[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) pv[b] = S.proj[f][j][v][b];
       double beta = 0.0;
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
         double t = 0.0;
 #pragma unroll
-        for (int c = 0; c < NB; ++c) t += S.Q[b][c] * S.proj[f][j][v][c];
-        beta += S.proj[f][j][v][b] * t;
+        for (int c = 0; c < NB; ++c) t += S.Q[b][c] * pv[c];
+        beta += pv[b] * t;
       }
       w = lw[j] / ((beta + F64_EPS) * (beta + F64_EPS));
     }
@@ -672,13 +721,16 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
   }
   __syncwarp();
   // normalise and combine (weno.rs:180-194)
-  for (int idx = lane; idx < 3 * NEQ * NB; idx += 32) {
+#pragma unroll
+  for (int it = 0; it < (3 * NEQ * NB + 31) / 32; ++it) {
+    const int idx = lane + 32 * it;
+    if (idx >= 3 * NEQ * NB) break;
     const int f = idx / (NEQ * NB), r1 = idx - f * NEQ * NB, v = r1 / NB, b = r1 - v * NB;
     double acc = 0.0;
     if (interior[f]) {
-      const double den = ((S.nlw[f][0][v] + S.nlw[f][1][v]) + S.nlw[f][2][v]) + S.nlw[f][3][v];
+      const double inv_den = 1.0 / (((S.nlw[f][0][v] + S.nlw[f][1][v]) + S.nlw[f][2][v]) + S.nlw[f][3][v]);
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc += (S.nlw[f][j][v] / den) * S.proj[f][j][v][b];
+      for (int j = 0; j < 4; ++j) acc += (S.nlw[f][j][v] * inv_den) * S.proj[f][j][v][b];
     }
     S.pol_new[f][v][b] = acc;
   }
@@ -690,6 +742,7 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
     Jn[k] = interior[k] ? m.jac[nbrs[k]] : 0.0;
     if (interior[k]) neighbour_area += Jn[k] * 0.5;
   }
+  const double inv_area = 1.0 / neighbour_area;
   for (int idx = lane; idx < NEQ * NB; idx += 32) {
     const int r = idx / NB, b = idx - r * NB;
     double recon = 0.0;
@@ -701,7 +754,7 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
       for (int k = 0; k < NEQ; ++k) sum += S.R[f][r][k] * S.pol_new[f][k][b];
       recon = recon + sum * Jn[f] * 0.5;
     }
-    U[(r * NB + b) * ld + e] = recon / neighbour_area;
+    U[(r * NB + b) * ld + e] = recon * inv_area;
   }
   __syncwarp();
   return ST_OK;
@@ -874,7 +927,7 @@ __global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KPara
       for (int b = 0; b < NB; ++b) a += ld_state(&U[(size_t)(v * NB + b) * m.ld + e]);
       s[v] = a;
     }
-    const double hcr = kp.hcr;
+    const double hcr = kp.gas.hcr;
     const double rho = s[0];
     const double u = s[1] / rho;
     const double v = s[2] / rho;

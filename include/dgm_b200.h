@@ -181,6 +181,25 @@ int64_t dgm_device_bytes(dgm_ctx* ctx);
 
 const char* dgm_status_string(int32_t status);
 
+/* ---- allocation-free variant ------------------------------------------------------------ */
+
+/* The CFL time step (the minimum of TemperalDisc::compute_time_step) for callers that cannot
+ * allocate device memory: hosts whose device memory belongs to another allocator, code running
+ * while a stream is captured into a CUDA graph, real-time loops.  It needs no dgm_ctx and calls
+ * no cudaMalloc/cudaFree: the caller passes device pointers to the state in the reference layout
+ * [n_elements][4][n_basis] and to the element minimum heights [n_elements], and a device double
+ * that receives the time step; the work is enqueued on `stream` (cudaStream_t, NULL = default).
+ * Scratch is a fixed 32 KiB array in the library image (every GPU that loads the library holds
+ * it until exit) of 4096 per-block minima, which caps n_elements at 8,388,608: larger sizes
+ * return DGM_BAD_ARG without launching anything.  Every used scratch slot is rewritten by every
+ * call; calls that overlap on the GPU (other streams, other host threads) share the array and
+ * race.  The first call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * with that device current; make that first call before any stream capture.  This entry point
+ * has no counterpart in the reference, which allocates freely. */
+int32_t dgm_compute_time_step_noalloc(const double* solutions, const double* minimum_height,
+                                      int64_t n_elements, int32_t n_basis, double cfl, double hcr,
+                                      double* time_step, void* stream);
+
 /* Library version string. */
 const char* dgm_version(void);
 

@@ -106,6 +106,8 @@ class Params(ctypes.Structure):
         ("final_step", ctypes.c_int64),
         ("limiter", ctypes.c_int32),
         ("device", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("_reserved", ctypes.c_int32),
     ]
 
 
@@ -137,6 +139,19 @@ def lib() -> ctypes.CDLL:
     L.dgm_launch_phase.argtypes = [vp, ctypes.c_int32]
     L.dgm_phase_launches_per_step.argtypes = [vp, ctypes.c_int32]
     L.dgm_launches_per_step.argtypes = [vp]
+    L.dgm_create_batch.argtypes = [ctypes.c_int32, ctypes.POINTER(MeshDesc), ctypes.POINTER(TablesDesc),
+                                   ctypes.POINTER(Params), P_I32]
+    L.dgm_create_batch.restype = vp
+    L.dgm_instance_count.argtypes = [vp]
+    L.dgm_instance_upload.argtypes = [vp, ctypes.c_int32, P_D]
+    L.dgm_instance_download.argtypes = [vp, ctypes.c_int32, P_D]
+    L.dgm_instance_download_residual.argtypes = [vp, ctypes.c_int32, P_D]
+    L.dgm_instance_state.argtypes = [vp, ctypes.c_int32, P_D, P_I64, P_I32, P_I64]
+    L.dgm_instance_set.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
+                                   ctypes.c_int64]
+    L.dgm_advance_with_residual.argtypes = [vp, ctypes.c_int64]
+    L.dgm_diagnostics.argtypes = [vp, ctypes.c_int32, P_D]
+    L.dgm_precision.argtypes = [vp]
     L.dgm_upload_solutions.argtypes = [vp, P_D]
     L.dgm_download_solutions.argtypes = [vp, P_D]
     L.dgm_advance.argtypes = [vp, ctypes.c_int64]
@@ -155,7 +170,10 @@ def lib() -> ctypes.CDLL:
     for name in ("dgm_compute_residuals", "dgm_apply_limiter", "dgm_compute_time_step", "dgm_rk3",
                  "dgm_time_march", "dgm_get_clock", "dgm_set_clock", "dgm_upload_solutions",
                  "dgm_download_solutions", "dgm_advance", "dgm_synchronize", "dgm_limiter_stats",
-                 "dgm_set_limits", "dgm_launch_phase", "dgm_phase_launches_per_step", "dgm_launches_per_step"):
+                 "dgm_set_limits", "dgm_launch_phase", "dgm_phase_launches_per_step", "dgm_launches_per_step",
+                 "dgm_instance_count", "dgm_instance_upload", "dgm_instance_download",
+                 "dgm_instance_download_residual", "dgm_instance_state", "dgm_instance_set",
+                 "dgm_advance_with_residual", "dgm_diagnostics", "dgm_precision"):
         getattr(L, name).restype = ctypes.c_int32
     _lib = L
     return L

@@ -1,9 +1,10 @@
 // dgm_capi.cu -- host side of the C ABI declared in include/dgm_b200.h.
 //
 // A dgm_ctx owns one CUDA stream, the device-resident state (U and the two RK stage buffers
-// of TemperalDisc::temporary_solutions, temporal_disc.rs:9), the SoA mesh/geometry arrays and
-// the control block through which the time-march loop runs on the device.  Whole time steps
-// are captured into CUDA graphs (one launch per group of steps).
+// of TemperalDisc::temporary_solutions, temporal_disc.rs:9), the SoA mesh/geometry arrays of
+// one or more mesh instances (a disconnected union mesh), a control block per instance and the
+// context-wide control block through which the time-march loop runs on the device.  Whole time
+// steps are captured into CUDA graphs (one launch per group of steps).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -16,32 +17,47 @@
 #include "dgm_device.cuh"
 
 using dgm::Control;
+using dgm::InstCtl;
 using dgm::KParams;
 using dgm::MeshDev;
 using dgm::NEQ;
+
+struct HostInst {
+  int64_t elem_off = 0, ne = 0;         // element range in the union mesh
+  int64_t bslot_off = 0, nb_slots = 0;  // boundary-slot range (relative to n_int)
+  double cfl = 0.0, final_time = 0.0;
+  int64_t final_step = 0;
+  double t = 0.0;
+  int64_t step = 0;
+  int32_t status = 0;
+  int64_t err_where = -1;
+};
 
 struct dgm_ctx {
   int device = 0;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
   int P = 0, nb = 0, nq = 0, ng = 0;
-  int64_t ne = 0, ld = 0, n_int = 0, n_bnd = 0, np = 0;
+  int prec = 0;  // 0: FP64 state, 1: FP32 state and bulk arithmetic
+  int64_t ne = 0, ld = 0, n_int = 0, n_bnd = 0, np = 0, max_inst_ne = 0;
   int limiter = 1;
-  double hcr = 1.4, cfl = 0.0, final_time = 0.0;
-  int64_t final_step = 0;
-  double current_time = 0.0;
-  int64_t current_step = 0;
-  std::vector<unsigned char> kparams;  // host image of KParams<P>
-  // device buffers
-  double *U = nullptr, *U1 = nullptr, *U2 = nullptr, *R = nullptr, *F = nullptr, *stage = nullptr;
+  double hcr = 1.4;
+  std::vector<HostInst> inst;
+  std::vector<unsigned char> kparams;  // host image of KParams<P, T>
+  // device buffers (state arrays are of the storage type)
+  void *U = nullptr, *U1 = nullptr, *U2 = nullptr, *R = nullptr, *F = nullptr;
+  double* stage = nullptr;  // FP64 staging in the reference layout (largest instance)
   unsigned char* t0 = nullptr;
   unsigned int* status = nullptr;
   int* work = nullptr;
+  int* d_elem_off = nullptr;
+  int* d_bslot_off = nullptr;
+  double* d_diag = nullptr;
   Control* ctl = nullptr;
+  InstCtl* ic = nullptr;
   std::vector<void*> allocs;
   int64_t bytes = 0;
   int coop_blocks = 1;
-  bool coop_ok = true;
   // graphs[with_residual][g]: g = 0 captures graph_steps steps, g = 1 a single step
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int graph_steps = 8;
@@ -80,6 +96,18 @@ int dev_alloc(dgm_ctx* c, T** p, size_t count) {
   return DGM_OK;
 }
 
+int dev_alloc_bytes(dgm_ctx* c, void** p, size_t nbytes) {
+  void* ptr = nullptr;
+  if (cudaMalloc(&ptr, std::max<size_t>(nbytes, 16)) != cudaSuccess) {
+    cudaGetLastError();
+    return DGM_OOM;
+  }
+  c->allocs.push_back(ptr);
+  c->bytes += (int64_t)nbytes;
+  *p = ptr;
+  return DGM_OK;
+}
+
 template <class T>
 int upload(dgm_ctx* c, T** p, const std::vector<T>& h) {
   int st = dev_alloc(c, p, h.size());
@@ -88,38 +116,39 @@ int upload(dgm_ctx* c, T** p, const std::vector<T>& h) {
   return DGM_OK;
 }
 
-template <int P>
-KParams<P>& kp_of(dgm_ctx* c) {
-  return *reinterpret_cast<KParams<P>*>(c->kparams.data());
+template <int P, typename T>
+KParams<P, T>& kp_of(dgm_ctx* c) {
+  return *reinterpret_cast<KParams<P, T>*>(c->kparams.data());
 }
 
 // ---------------------------------------------------------------------------------------------
-// Kernel launch helpers, one instantiation per supported order.
+// Kernel launch helpers, one instantiation per (order, storage type).
 // ---------------------------------------------------------------------------------------------
-template <int P>
+template <int P, typename T>
 struct Ops {
   using V = dgm::Variant<P>;
+  static T* S(void* p) { return static_cast<T*>(p); }
 
-  static int edge_flux(dgm_ctx* c, const double* U) {
+  static int edge_flux(dgm_ctx* c, const T* U) {
     const int64_t total = (c->n_int + c->n_bnd) * V::NG;
     const int threads = 256;
     const int blocks = (int)std::max<int64_t>(1, (total + threads - 1) / threads);
-    dgm::k_edge_flux<P><<<blocks, threads, 0, c->stream>>>(kp_of<P>(c), U, c->F);
+    dgm::k_edge_flux<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, S(c->F));
     CK(cudaGetLastError());
     return DGM_OK;
   }
 
   template <int MODE>
-  static int element(dgm_ctx* c, const double* Uin, const double* Ubase, double* Uout, const double* Rin,
-                     double* Rout) {
+  static int element(dgm_ctx* c, const T* Uin, const T* Ubase, T* Uout, const T* Rin, T* Rout) {
     const int threads = 256;  // 8 warps x 8 elements, 4 threads (variables) per element
     const int blocks = (int)std::max<int64_t>(1, (c->ne + 63) / 64);
-    dgm::k_element<P, MODE><<<blocks, threads, 0, c->stream>>>(kp_of<P>(c), Uin, Ubase, c->F, Uout, Rin, Rout);
+    dgm::k_element<P, T, MODE><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), Uin, Ubase, S(c->F), Uout, Rin,
+                                                                   Rout);
     CK(cudaGetLastError());
     return DGM_OK;
   }
 
-  static int limiter(dgm_ctx* c, double* U) {
+  static int limiter(dgm_ctx* c, T* U) {
     if (!c->limiter) return DGM_OK;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c->coop_blocks);
@@ -131,64 +160,76 @@ struct Ops {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter<P>, kp_of<P>(c), U, c->t0, c->status, c->work));
+    CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter<P, T>, kp_of<P, T>(c), U, c->t0, c->status, c->work));
     return DGM_OK;
   }
 
-  static int time_step(dgm_ctx* c, const double* U) {
+  static int time_step(dgm_ctx* c, const T* U) {
     const int threads = 256;
     const int blocks = (int)std::max<int64_t>(1, (c->ne + threads - 1) / threads);
-    dgm::k_time_step<P><<<blocks, threads, 0, c->stream>>>(kp_of<P>(c), U);
+    dgm::k_time_step<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U);
     CK(cudaGetLastError());
     return DGM_OK;
   }
 
-  // One SSP-RK3 step on the resident state (rk3.rs:7-26); dt is read from the control block.
-  static int rk3(dgm_ctx* c, double* Rout) {
-    int st;
-    if ((st = edge_flux(c, c->U))) return st;
-    if ((st = element<1>(c, c->U, nullptr, c->U1, nullptr, nullptr))) return st;
-    if ((st = limiter(c, c->U1))) return st;
-    if ((st = edge_flux(c, c->U1))) return st;
-    if ((st = element<2>(c, c->U1, c->U, c->U2, nullptr, nullptr))) return st;
-    if ((st = limiter(c, c->U2))) return st;
-    if ((st = edge_flux(c, c->U2))) return st;
-    if ((st = element<3>(c, c->U2, c->U, c->U, nullptr, Rout))) return st;
-    return limiter(c, c->U);
+  static int diagnostics(dgm_ctx* c, const T* R) {
+    dgm::k_diagnostics<P, T><<<(int)c->inst.size(), 256, 0, c->stream>>>(kp_of<P, T>(c), S(c->U), R, c->d_elem_off,
+                                                                          c->d_bslot_off, c->d_diag);
+    CK(cudaGetLastError());
+    return DGM_OK;
   }
 
-  // One iteration of time_march (temporal_disc.rs:22-33), fully on the device.
-  static int step(dgm_ctx* c, double* Rout) {
-    dgm::k_step_begin<<<1, 1, 0, c->stream>>>(c->ctl);
+  // One SSP-RK3 step on the resident state (rk3.rs:7-26); dt is read from the control blocks.
+  static int rk3(dgm_ctx* c, T* Rout) {
+    T *U = S(c->U), *U1 = S(c->U1), *U2 = S(c->U2);
+    int st;
+    if ((st = edge_flux(c, U))) return st;
+    if ((st = element<1>(c, U, nullptr, U1, nullptr, nullptr))) return st;
+    if ((st = limiter(c, U1))) return st;
+    if ((st = edge_flux(c, U1))) return st;
+    if ((st = element<2>(c, U1, U, U2, nullptr, nullptr))) return st;
+    if ((st = limiter(c, U2))) return st;
+    if ((st = edge_flux(c, U2))) return st;
+    if ((st = element<3>(c, U2, U, U, nullptr, Rout))) return st;
+    return limiter(c, U);
+  }
+
+  // One iteration of time_march (temporal_disc.rs:22-33) for every instance, on the device.
+  static int step(dgm_ctx* c, T* Rout) {
+    const int n = (int)c->inst.size();
+    const int tb = 128, nblk = (n + tb - 1) / tb;
+    dgm::k_step_begin<<<nblk, tb, 0, c->stream>>>(c->ctl, c->ic, n);
     CK(cudaGetLastError());
     int st;
-    if ((st = time_step(c, c->U))) return st;
-    dgm::k_step_dt<<<1, 1, 0, c->stream>>>(c->ctl);
+    if ((st = time_step(c, S(c->U)))) return st;
+    dgm::k_step_dt<<<nblk, tb, 0, c->stream>>>(c->ic, n);
     CK(cudaGetLastError());
     if ((st = rk3(c, Rout))) return st;
-    dgm::k_step_end<<<1, 1, 0, c->stream>>>(c->ctl);
+    dgm::k_step_end<<<nblk, tb, 0, c->stream>>>(c->ic, n);
     CK(cudaGetLastError());
     return DGM_OK;
   }
 
-  static int to_soa(dgm_ctx* c, const double* src_aos, double* dst) {
-    const int64_t n = c->ne * NEQ * V::NB;
+  static int to_soa(dgm_ctx* c, const double* src_aos, void* dst, int64_t elem_off, int64_t ne) {
+    const int64_t n = ne * NEQ * V::NB;
     const int threads = 256;
-    dgm::k_aos_to_soa<V::NB><<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(src_aos, dst, (int)c->ne, (int)c->ld);
+    dgm::k_aos_to_soa<V::NB, T><<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(
+        src_aos, S(dst) + elem_off, (int)ne, (int)c->ld);
     CK(cudaGetLastError());
     return DGM_OK;
   }
-  static int to_aos(dgm_ctx* c, const double* src, double* dst_aos) {
-    const int64_t n = c->ne * NEQ * V::NB;
+  static int to_aos(dgm_ctx* c, const void* src, double* dst_aos, int64_t elem_off, int64_t ne) {
+    const int64_t n = ne * NEQ * V::NB;
     const int threads = 256;
-    dgm::k_soa_to_aos<V::NB><<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(src, dst_aos, (int)c->ne, (int)c->ld);
+    dgm::k_soa_to_aos<V::NB, T><<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(
+        static_cast<const T*>(src) + elem_off, dst_aos, (int)ne, (int)c->ld);
     CK(cudaGetLastError());
     return DGM_OK;
   }
 
   static int occupancy(dgm_ctx* c) {
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dgm::k_limiter<P>, dgm::kLimiterWarps * 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dgm::k_limiter<P, T>, dgm::kLimiterWarps * 32, 0));
     per_sm = std::max(1, per_sm);
     const int64_t want = std::max<int64_t>(1, (c->ne + 32 * dgm::kLimiterWarps - 1) / (32 * dgm::kLimiterWarps));
     c->coop_blocks = (int)std::min<int64_t>((int64_t)per_sm * c->num_sms, want);
@@ -196,28 +237,35 @@ struct Ops {
   }
 
   static int fill_tables(dgm_ctx* c, const dgm_tables_desc* t) {
-    c->kparams.assign(sizeof(KParams<P>), 0);
-    auto& kp = kp_of<P>(c);
-    auto& tb = kp.tab;
+    c->kparams.assign(sizeof(KParams<P, T>), 0);
+    auto& kp = kp_of<P, T>(c);
+    auto& tb = kp.t;
+    auto& td = kp.d;
     const int NB = V::NB, NQ = V::NQ, NG = V::NG, NK = V::NK;
     const int nk_in = t->n_deriv_keys;
     if (nk_in < NK) return DGM_BAD_ARG;
     for (int q = 0; q < NQ; ++q)
       for (int b = 0; b < NB; ++b) {
-        tb.phi_cell[q][b] = t->phi_cell[q * NB + b];
-        tb.dxi[q][b] = t->dphi_cell_ref[((size_t)q * NB + b) * nk_in + 0];
-        tb.deta[q][b] = t->dphi_cell_ref[((size_t)q * NB + b) * nk_in + 1];
-        for (int k = 0; k < NK; ++k) tb.dref[q][b][k] = t->dphi_cell_ref[((size_t)q * NB + b) * nk_in + k];
+        tb.phi_cell[q][b] = T(t->phi_cell[q * NB + b]);
+        tb.dxi[q][b] = T(t->dphi_cell_ref[((size_t)q * NB + b) * nk_in + 0]);
+        tb.deta[q][b] = T(t->dphi_cell_ref[((size_t)q * NB + b) * nk_in + 1]);
+        for (int k = 0; k < NK; ++k) td.dref[q][b][k] = t->dphi_cell_ref[((size_t)q * NB + b) * nk_in + k];
       }
     for (int k = 0; k < 3; ++k)
       for (int g = 0; g < NG; ++g)
-        for (int b = 0; b < NB; ++b) tb.phi_edge[k][g][b] = t->phi_edge[(k * NG + g) * NB + b];
-    for (int q = 0; q < NQ; ++q) tb.cell_w[q] = t->cell_weights[q];
-    for (int g = 0; g < NG; ++g) tb.edge_w[g] = t->edge_weights[g];
-    for (int b = 0; b < NB; ++b) {
-      tb.mass[b] = t->mass_diag[b];
-      kp.inv_mass[b] = 1.0 / t->mass_diag[b];
+        for (int b = 0; b < NB; ++b) {
+          tb.phi_edge[k][g][b] = T(t->phi_edge[(k * NG + g) * NB + b]);
+          td.phi_edge[k][g][b] = t->phi_edge[(k * NG + g) * NB + b];
+        }
+    for (int q = 0; q < NQ; ++q) {
+      tb.cell_w[q] = T(t->cell_weights[q]);
+      td.cell_w[q] = t->cell_weights[q];
     }
+    for (int g = 0; g < NG; ++g) {
+      tb.edge_w[g] = T(t->edge_weights[g]);
+      td.edge_w[g] = t->edge_weights[g];
+    }
+    for (int b = 0; b < NB; ++b) tb.inv_mass[b] = T(1.0 / t->mass_diag[b]);
     // gas constants with the reference's expressions (flux.rs:76-77, 85, 96)
     dgm::Gas& gas = kp.gas;
     gas.hcr = c->hcr;
@@ -229,47 +277,69 @@ struct Ops {
     const double n = std::nearbyint(gas.inv_zeta);
     gas.inv_zeta_int = (n >= 1.0 && n <= 16.0 && std::fabs(gas.inv_zeta - n) <= 1e-12 * n) ? (int)n : 0;
     kp.ctl = c->ctl;
+    kp.ic = c->ic;
+    return DGM_OK;
+  }
+
+  static int set_mesh(dgm_ctx* c, const MeshDev& md) {
+    kp_of<P, T>(c).m = md;
     return DGM_OK;
   }
 };
 
 template <class F>
 int dispatch(dgm_ctx* c, F&& f) {
-  switch (c->P) {
-    case 1: return f(Ops<1>{});
-    case 2: return f(Ops<2>{});
-    case 3: return f(Ops<3>{});
+  if (c->prec == 0) {
+    switch (c->P) {
+      case 1: return f(Ops<1, double>{});
+      case 2: return f(Ops<2, double>{});
+      case 3: return f(Ops<3, double>{});
+    }
+  } else {
+    switch (c->P) {
+      case 1: return f(Ops<1, float>{});
+      case 2: return f(Ops<2, float>{});
+      case 3: return f(Ops<3, float>{});
+    }
   }
   return DGM_BAD_ARG;
 }
 
-MeshDev& mesh_of(dgm_ctx* c) {
-  switch (c->P) {
-    case 1: return kp_of<1>(c).m;
-    case 2: return kp_of<2>(c).m;
-    default: return kp_of<3>(c).m;
-  }
-}
+size_t elem_bytes(const dgm_ctx* c) { return c->prec == 0 ? sizeof(double) : sizeof(float); }
 
-int read_control(dgm_ctx* c, Control* h) {
+int read_control(dgm_ctx* c, Control* h, std::vector<InstCtl>* hi) {
   CK(cudaMemcpyAsync(h, c->ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+  if (hi) {
+    hi->resize(c->inst.size());
+    CK(cudaMemcpyAsync(hi->data(), c->ic, sizeof(InstCtl) * c->inst.size(), cudaMemcpyDeviceToHost, c->stream));
+  }
   CK(cudaStreamSynchronize(c->stream));
   return DGM_OK;
 }
 
-// Resets the device status word and returns the status raised since the last call.
+// Pulls the device clocks/statuses into the host mirrors; resets the device status words and
+// returns the first status raised since the last call (DGM_OK if none).
 int collect_status(dgm_ctx* c) {
   Control h;
-  int st = read_control(c, &h);
+  std::vector<InstCtl> hi;
+  int st = read_control(c, &h, &hi);
   if (st) return st;
-  c->current_time = h.t;
-  c->current_step = h.step;
+  for (size_t i = 0; i < c->inst.size(); ++i) {
+    c->inst[i].t = hi[i].t;
+    c->inst[i].step = hi[i].step;
+    if (hi[i].status) {
+      c->inst[i].status = hi[i].status;
+      c->inst[i].err_where = hi[i].err_where;
+    }
+  }
   c->last_troubled = h.troubled;
   c->last_waves = h.waves;
   if (h.status != 0) {
     c->err_where = h.err_where;
     const int zero = 0;
     CK(cudaMemcpyAsync(&c->ctl->status, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    for (size_t i = 0; i < c->inst.size(); ++i)
+      if (hi[i].status) CK(cudaMemcpyAsync(&c->ic[i].status, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return h.status;
   }
@@ -277,35 +347,46 @@ int collect_status(dgm_ctx* c) {
 }
 
 int set_active(dgm_ctx* c, double dt, bool set_dt) {
-  dgm::k_set_active<<<1, 1, 0, c->stream>>>(c->ctl, dt, set_dt ? 1 : 0);
+  const int n = (int)c->inst.size();
+  dgm::k_set_active<<<(n + 127) / 128, 128, 0, c->stream>>>(c->ctl, c->ic, n, dt, set_dt ? 1 : 0);
   CK(cudaGetLastError());
   return DGM_OK;
 }
 
-int upload_state(dgm_ctx* c, const double* host, double* dst) {
-  const size_t n = (size_t)c->ne * NEQ * c->nb;
+// Host state ([element][variable][basis], FP64) of instance i -> device SoA array dst.
+int upload_state(dgm_ctx* c, int64_t i, const double* host, void* dst) {
+  const HostInst& h = c->inst[i];
+  const size_t n = (size_t)h.ne * NEQ * c->nb;
   CK(cudaMemcpyAsync(c->stage, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  return dispatch(c, [&](auto ops) { return decltype(ops)::to_soa(c, c->stage, dst); });
+  return dispatch(c, [&](auto ops) { return decltype(ops)::to_soa(c, c->stage, dst, h.elem_off, h.ne); });
 }
 
-int download_state(dgm_ctx* c, const double* src, double* host) {
-  const size_t n = (size_t)c->ne * NEQ * c->nb;
-  int st = dispatch(c, [&](auto ops) { return decltype(ops)::to_aos(c, src, c->stage); });
+int download_state(dgm_ctx* c, int64_t i, const void* src, double* host) {
+  const HostInst& h = c->inst[i];
+  const size_t n = (size_t)h.ne * NEQ * c->nb;
+  int st = dispatch(c, [&](auto ops) { return decltype(ops)::to_aos(c, src, c->stage, h.elem_off, h.ne); });
   if (st) return st;
   CK(cudaMemcpyAsync(host, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));  // the staging buffer is reused by the next copy
   return DGM_OK;
 }
 
+// Host clocks and loop bounds -> device control blocks (statuses and dt are kept).
 int write_clock(dgm_ctx* c) {
   Control h;
-  int st = read_control(c, &h);
+  std::vector<InstCtl> hi;
+  int st = read_control(c, &h, &hi);
   if (st) return st;
-  h.t = c->current_time;
-  h.step = c->current_step;
-  h.final_time = c->final_time;
-  h.final_step = c->final_step;
-  h.cfl = c->cfl;
-  CK(cudaMemcpyAsync(c->ctl, &h, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
+  for (size_t i = 0; i < c->inst.size(); ++i) {
+    hi[i].t = c->inst[i].t;
+    hi[i].step = c->inst[i].step;
+    hi[i].final_time = c->inst[i].final_time;
+    hi[i].final_step = c->inst[i].final_step;
+    hi[i].cfl = c->inst[i].cfl;
+    hi[i].status = c->inst[i].status;
+    hi[i].err_where = c->inst[i].err_where;
+  }
+  CK(cudaMemcpyAsync(c->ic, hi.data(), sizeof(InstCtl) * hi.size(), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->limits_dirty = false;
   return DGM_OK;
@@ -322,7 +403,10 @@ int build_graph(dgm_ctx* c, int with_residual, int single) {
   int st = DGM_OK;
   const int n = single ? 1 : c->graph_steps;
   for (int i = 0; i < n && st == DGM_OK; ++i)
-    st = dispatch(c, [&](auto ops) { return decltype(ops)::step(c, with_residual ? c->R : nullptr); });
+    st = dispatch(c, [&](auto ops) {
+      using O = decltype(ops);
+      return O::step(c, with_residual ? O::S(c->R) : nullptr);
+    });
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (st != DGM_OK || e != cudaSuccess || g == nullptr) {
     cudaGetLastError();
@@ -352,7 +436,10 @@ int enqueue_steps(dgm_ctx* c, int64_t n, int with_residual) {
       CK(cudaGraphLaunch(c->graph[with_residual][single], c->stream));
       n -= single ? 1 : c->graph_steps;
     } else {
-      st = dispatch(c, [&](auto ops) { return decltype(ops)::step(c, with_residual ? c->R : nullptr); });
+      st = dispatch(c, [&](auto ops) {
+        using O = decltype(ops);
+        return O::step(c, with_residual ? O::S(c->R) : nullptr);
+      });
       if (st) return st;
       n -= 1;
     }
@@ -360,124 +447,161 @@ int enqueue_steps(dgm_ctx* c, int64_t n, int with_residual) {
   return DGM_OK;
 }
 
-int build_mesh(dgm_ctx* c, const dgm_mesh_desc* m) {
-  const int64_t ne = m->n_elements, ned = m->n_edges;
-  if (ne <= 0 || ned <= 0 || ne > (1ll << 30) || ned > (1ll << 29)) return DGM_BAD_ARG;
+// Union mesh of all instances: element, slot and patch indices offset per instance; internal
+// edges of every instance first (each in Mesh::internal_edge_indices order), then boundary
+// edges (each instance in edge-id order).  Validates every index against process_mesh's
+// conventions before anything reaches the device.
+int build_mesh(dgm_ctx* c, const dgm_mesh_desc* meshes, int n_inst, MeshDev& md) {
+  int64_t ne = 0, np = 0;
+  for (int i = 0; i < n_inst; ++i) {
+    const dgm_mesh_desc* m = &meshes[i];
+    if (m->n_elements <= 0 || m->n_edges <= 0 || m->n_vertices <= 0 || m->n_patches < 0) return DGM_BAD_ARG;
+    ne += m->n_elements;
+    np += m->n_patches;
+  }
+  if (ne > (1ll << 30)) return DGM_BAD_ARG;
   const int64_t ld = (ne + 31) / 32 * 32;
   c->ne = ne;
   c->ld = ld;
-  c->np = m->n_patches;
-  auto X = [&](int64_t v) { return m->vertex_xy[2 * v]; };
-  auto Y = [&](int64_t v) { return m->vertex_xy[2 * v + 1]; };
+  c->np = np;
   auto in_range = [](int64_t i, int64_t n) { return i >= 0 && i < n; };
-  // edge slots: internal edges in Mesh::internal_edge_indices order, then boundary edges
-  std::vector<int64_t> slot_of(ned, -1), slot_ref;
+  std::vector<int64_t> slot_ref;
   std::vector<int2> ie_lr;
   std::vector<int> ie_ic;
   std::vector<double4> ie_geo;
-  for (int64_t i = 0; i < m->n_internal_edges; ++i) {
-    const int64_t d = m->internal_edges[i];
-    if (!in_range(d, ned) || slot_of[d] >= 0) return DGM_BAD_ARG;
-    const int64_t L = m->edge_elements[2 * d], R = m->edge_elements[2 * d + 1];
-    const int64_t il = m->edge_in_cell[2 * d], ir = m->edge_in_cell[2 * d + 1];
-    if (!in_range(L, ne) || !in_range(R, ne) || L == R || !in_range(il, 3) || !in_range(ir, 3)) return DGM_BAD_ARG;
-    slot_of[d] = (int64_t)slot_ref.size();
-    slot_ref.push_back(d);
-    ie_lr.push_back(make_int2((int)L, (int)R));
-    ie_ic.push_back((int)(il | (ir << 2)));
-    const double jd = m->edge_jacob_det[d];
-    ie_geo.push_back(make_double4(m->edge_normal[2 * d], m->edge_normal[2 * d + 1], 0.5 * jd, jd));
-  }
-  c->n_int = (int64_t)slot_ref.size();
   std::vector<int> be_elem, be_info;
   std::vector<double4> be_geo;
-  for (int64_t d = 0; d < ned; ++d) {
-    if (m->edge_elements[2 * d + 1] != -1) continue;
-    const int64_t e = m->edge_elements[2 * d], k = m->edge_in_cell[2 * d], patch = m->edge_patch[d];
-    if (!in_range(e, ne) || !in_range(k, 3) || !in_range(patch, m->n_patches)) return DGM_BAD_ARG;
-    slot_of[d] = (int64_t)slot_ref.size();
-    slot_ref.push_back(d);
-    const int type = m->patch_type[patch];
-    if (type != DGM_WALL && type != DGM_FARFIELD) return DGM_BAD_ARG;
-    be_elem.push_back((int)e);
-    be_info.push_back((int)(k | (type << 2) | (patch << 3)));
-    // outward orientation, boundary_condition.rs:22-28
-    const bool same = m->elem_vertices[3 * e + k] == m->edge_vertices[2 * d];
-    const double nx = same ? m->edge_normal[2 * d] : -m->edge_normal[2 * d];
-    const double ny = same ? m->edge_normal[2 * d + 1] : -m->edge_normal[2 * d + 1];
-    const double jd = m->edge_jacob_det[d];
-    be_geo.push_back(make_double4(nx, ny, 0.5 * jd, jd));
+  std::vector<double4> patch_q(std::max<int64_t>(1, np));
+  std::vector<int> face(3 * ld, 0), nbr(3 * ld, -1), inst_of(ne, 0);
+  std::vector<double> jac(ne), hmin(ne), h15(ne), dinv(4 * ld, 0.0);
+  std::vector<std::vector<int64_t>> slot_of(n_inst);
+  // pass 1: internal edges of every instance
+  int64_t eo = 0;
+  for (int i = 0; i < n_inst; ++i) {
+    const dgm_mesh_desc* m = &meshes[i];
+    const int64_t ned = m->n_edges, nei = m->n_elements;
+    slot_of[i].assign(ned, -1);
+    for (int64_t k = 0; k < m->n_internal_edges; ++k) {
+      const int64_t d = m->internal_edges[k];
+      if (!in_range(d, ned) || slot_of[i][d] >= 0) return DGM_BAD_ARG;
+      const int64_t L = m->edge_elements[2 * d], R = m->edge_elements[2 * d + 1];
+      const int64_t il = m->edge_in_cell[2 * d], ir = m->edge_in_cell[2 * d + 1];
+      if (!in_range(L, nei) || !in_range(R, nei) || L == R || !in_range(il, 3) || !in_range(ir, 3)) return DGM_BAD_ARG;
+      slot_of[i][d] = (int64_t)slot_ref.size();
+      slot_ref.push_back(d);
+      ie_lr.push_back(make_int2((int)(eo + L), (int)(eo + R)));
+      ie_ic.push_back((int)(il | (ir << 2)));
+      const double jd = m->edge_jacob_det[d];
+      ie_geo.push_back(make_double4(m->edge_normal[2 * d], m->edge_normal[2 * d + 1], 0.5 * jd, jd));
+    }
+    eo += nei;
+  }
+  c->n_int = (int64_t)slot_ref.size();
+  // pass 2: boundary edges, patches, elements
+  eo = 0;
+  int64_t po = 0;
+  for (int i = 0; i < n_inst; ++i) {
+    const dgm_mesh_desc* m = &meshes[i];
+    const int64_t ned = m->n_edges, nei = m->n_elements;
+    HostInst& hi = c->inst[i];
+    hi.elem_off = eo;
+    hi.ne = nei;
+    hi.bslot_off = (int64_t)be_elem.size();
+    for (int64_t d = 0; d < ned; ++d) {
+      if (m->edge_elements[2 * d + 1] != -1) continue;
+      const int64_t e = m->edge_elements[2 * d], k = m->edge_in_cell[2 * d], patch = m->edge_patch[d];
+      if (!in_range(e, nei) || !in_range(k, 3) || !in_range(patch, m->n_patches)) return DGM_BAD_ARG;
+      if (slot_of[i][d] >= 0) return DGM_BAD_ARG;
+      slot_of[i][d] = c->n_int + (int64_t)be_elem.size();
+      slot_ref.push_back(d);
+      const int type = m->patch_type[patch];
+      if (type != DGM_WALL && type != DGM_FARFIELD) return DGM_BAD_ARG;
+      be_elem.push_back((int)(eo + e));
+      be_info.push_back((int)(k | (type << 2) | ((po + patch) << 3)));
+      // outward orientation, boundary_condition.rs:22-28
+      const bool same = m->elem_vertices[3 * e + k] == m->edge_vertices[2 * d];
+      const double nx = same ? m->edge_normal[2 * d] : -m->edge_normal[2 * d];
+      const double ny = same ? m->edge_normal[2 * d + 1] : -m->edge_normal[2 * d + 1];
+      const double jd = m->edge_jacob_det[d];
+      be_geo.push_back(make_double4(nx, ny, 0.5 * jd, jd));
+    }
+    hi.nb_slots = (int64_t)be_elem.size() - hi.bslot_off;
+    // far-field conserved state, boundary_condition.rs:50-55
+    for (int64_t p = 0; p < m->n_patches; ++p) {
+      const double* bq = &m->patch_quantity[4 * p];
+      patch_q[po + p] = make_double4(bq[0], bq[0] * bq[1], bq[0] * bq[2],
+                                     bq[3] / (c->hcr - 1.0) + 0.5 * bq[0] * (bq[1] * bq[1] + bq[2] * bq[2]));
+    }
+    std::vector<unsigned char> in_list(nei, 0);
+    for (int64_t k = 0; k < m->n_boundary_elements; ++k) {
+      const int64_t e = m->boundary_elements[k];
+      if (!in_range(e, nei)) return DGM_BAD_ARG;
+      in_list[e] = 1;
+    }
+    auto X = [&](int64_t v) { return m->vertex_xy[2 * v]; };
+    auto Y = [&](int64_t v) { return m->vertex_xy[2 * v + 1]; };
+    for (int64_t e = 0; e < nei; ++e) {
+      const int64_t ge = eo + e;
+      bool has_boundary = false;
+      for (int k = 0; k < 3; ++k) {
+        const int64_t d = m->elem_edges[3 * e + k];
+        if (!in_range(d, ned) || slot_of[i][d] < 0) return DGM_BAD_ARG;
+        int side;
+        if (m->edge_elements[2 * d + 1] == -1) {
+          if (m->edge_elements[2 * d] != e || m->edge_in_cell[2 * d] != k) return DGM_BAD_ARG;
+          side = 0;
+          has_boundary = true;
+          if (m->elem_neighbours[3 * e + k] != -1) return DGM_BAD_ARG;
+        } else {
+          const bool same = m->elem_vertices[3 * e + k] == m->edge_vertices[2 * d];
+          if (m->edge_elements[2 * d] == e && same && m->edge_in_cell[2 * d] == k) side = 0;
+          else if (m->edge_elements[2 * d + 1] == e && !same && m->edge_in_cell[2 * d + 1] == k) side = 1;
+          else return DGM_BAD_ARG;  // orientation inconsistent with process_mesh's left/right rule
+          const int64_t other = m->edge_elements[2 * d + (side ? 0 : 1)];
+          if (m->elem_neighbours[3 * e + k] != other) return DGM_BAD_ARG;
+          nbr[k * ld + ge] = (int)(eo + other);
+        }
+        face[k * ld + ge] = (int)((slot_of[i][d] << 1) | side);
+      }
+      // every element is in exactly one of the internal / boundary element lists
+      if (has_boundary != (in_list[e] != 0)) return DGM_BAD_ARG;
+      const double J = m->elem_jacob_det[e];
+      const int64_t v1 = m->elem_vertices[3 * e], v2 = m->elem_vertices[3 * e + 1], v3 = m->elem_vertices[3 * e + 2];
+      if (!in_range(v1, m->n_vertices) || !in_range(v2, m->n_vertices) || !in_range(v3, m->n_vertices))
+        return DGM_BAD_ARG;
+      jac[ge] = J;
+      inst_of[ge] = i;
+      // compute_dphi inverse Jacobian, mesh.rs:93-100
+      dinv[0 * ld + ge] = (Y(v3) - Y(v1)) / J;
+      dinv[1 * ld + ge] = -(X(v3) - X(v1)) / J;
+      dinv[2 * ld + ge] = -(Y(v2) - Y(v1)) / J;
+      dinv[3 * ld + ge] = (X(v2) - X(v1)) / J;
+      hmin[ge] = m->elem_minimum_height[e];
+      h15[ge] = std::pow(m->elem_circumradius[e], 1.5);  // weno.rs:81 h.powf(1.5)
+    }
+    eo += nei;
+    po += m->n_patches;
   }
   c->n_bnd = (int64_t)be_elem.size();
-  // far-field conserved state, boundary_condition.rs:50-55
-  std::vector<double4> patch_q(std::max<int64_t>(1, m->n_patches));
-  for (int64_t p = 0; p < m->n_patches; ++p) {
-    const double* bq = &m->patch_quantity[4 * p];
-    patch_q[p] = make_double4(bq[0], bq[0] * bq[1], bq[0] * bq[2],
-                              bq[3] / (c->hcr - 1.0) + 0.5 * bq[0] * (bq[1] * bq[1] + bq[2] * bq[2]));
-  }
-  // element faces, neighbours, geometry (SoA)
-  std::vector<int> face(3 * ld, 0), nbr(3 * ld, -1);
-  std::vector<double> jac(ne), hmin(ne), h15(ne), dinv(4 * ld, 0.0);
-  std::vector<unsigned char> in_list(ne, 0);
-  for (int64_t i = 0; i < m->n_boundary_elements; ++i) {
-    const int64_t e = m->boundary_elements[i];
-    if (!in_range(e, ne)) return DGM_BAD_ARG;
-    in_list[e] = 1;
-  }
-  for (int64_t e = 0; e < ne; ++e) {
-    bool has_boundary = false;
-    for (int k = 0; k < 3; ++k) {
-      const int64_t d = m->elem_edges[3 * e + k];
-      if (!in_range(d, ned) || slot_of[d] < 0) return DGM_BAD_ARG;
-      int side;
-      if (m->edge_elements[2 * d + 1] == -1) {
-        if (m->edge_elements[2 * d] != e || m->edge_in_cell[2 * d] != k) return DGM_BAD_ARG;
-        side = 0;
-        has_boundary = true;
-        if (m->elem_neighbours[3 * e + k] != -1) return DGM_BAD_ARG;
-      } else {
-        const bool same = m->elem_vertices[3 * e + k] == m->edge_vertices[2 * d];
-        if (m->edge_elements[2 * d] == e && same && m->edge_in_cell[2 * d] == k) side = 0;
-        else if (m->edge_elements[2 * d + 1] == e && !same && m->edge_in_cell[2 * d + 1] == k) side = 1;
-        else return DGM_BAD_ARG;  // orientation inconsistent with process_mesh's left/right rule
-        const int64_t other = m->edge_elements[2 * d + (side ? 0 : 1)];
-        if (m->elem_neighbours[3 * e + k] != other) return DGM_BAD_ARG;
-        nbr[k * ld + e] = (int)other;
-      }
-      face[k * ld + e] = (int)((slot_of[d] << 1) | side);
-    }
-    // every element is in exactly one of the internal / boundary element lists
-    if (has_boundary != (in_list[e] != 0)) return DGM_BAD_ARG;
-    const double J = m->elem_jacob_det[e];
-    const int64_t v1 = m->elem_vertices[3 * e], v2 = m->elem_vertices[3 * e + 1], v3 = m->elem_vertices[3 * e + 2];
-    if (!in_range(v1, m->n_vertices) || !in_range(v2, m->n_vertices) || !in_range(v3, m->n_vertices)) return DGM_BAD_ARG;
-    jac[e] = J;
-    // compute_dphi inverse Jacobian, mesh.rs:93-100
-    dinv[0 * ld + e] = (Y(v3) - Y(v1)) / J;
-    dinv[1 * ld + e] = -(X(v3) - X(v1)) / J;
-    dinv[2 * ld + e] = -(Y(v2) - Y(v1)) / J;
-    dinv[3 * ld + e] = (X(v2) - X(v1)) / J;
-    hmin[e] = m->elem_minimum_height[e];
-    h15[e] = std::pow(m->elem_circumradius[e], 1.5);  // weno.rs:81 h.powf(1.5)
-  }
-  MeshDev md{};
+  if (c->n_int + c->n_bnd > (1ll << 29)) return DGM_BAD_ARG;
+  md = MeshDev{};
   md.ne = (int)ne;
   md.ld = (int)ld;
   md.n_int = (int)c->n_int;
   md.n_bnd = (int)c->n_bnd;
+  md.n_inst = n_inst;
   int st;
   double *d_jac, *d_dinv, *d_hmin, *d_h15;
-  int *d_face, *d_nbr, *d_ie_ic, *d_be_elem, *d_be_info;
+  int *d_face, *d_nbr, *d_inst, *d_ie_ic, *d_be_elem, *d_be_info;
   int2* d_ie_lr;
   double4 *d_ie_geo, *d_be_geo, *d_patch;
   int64_t* d_slot_ref;
   if ((st = upload(c, &d_jac, jac)) || (st = upload(c, &d_dinv, dinv)) || (st = upload(c, &d_hmin, hmin)) ||
       (st = upload(c, &d_h15, h15)) || (st = upload(c, &d_face, face)) || (st = upload(c, &d_nbr, nbr)) ||
-      (st = upload(c, &d_ie_lr, ie_lr)) || (st = upload(c, &d_ie_ic, ie_ic)) || (st = upload(c, &d_ie_geo, ie_geo)) ||
-      (st = upload(c, &d_be_elem, be_elem)) || (st = upload(c, &d_be_info, be_info)) ||
-      (st = upload(c, &d_be_geo, be_geo)) || (st = upload(c, &d_patch, patch_q)) ||
-      (st = upload(c, &d_slot_ref, slot_ref)))
+      (st = upload(c, &d_inst, inst_of)) || (st = upload(c, &d_ie_lr, ie_lr)) || (st = upload(c, &d_ie_ic, ie_ic)) ||
+      (st = upload(c, &d_ie_geo, ie_geo)) || (st = upload(c, &d_be_elem, be_elem)) ||
+      (st = upload(c, &d_be_info, be_info)) || (st = upload(c, &d_be_geo, be_geo)) ||
+      (st = upload(c, &d_patch, patch_q)) || (st = upload(c, &d_slot_ref, slot_ref)))
     return st;
   md.jac = d_jac;
   md.dinv = d_dinv;
@@ -485,6 +609,7 @@ int build_mesh(dgm_ctx* c, const dgm_mesh_desc* m) {
   md.h15 = d_h15;
   md.face = d_face;
   md.nbr = d_nbr;
+  md.inst = d_inst;
   md.ie_lr = d_ie_lr;
   md.ie_ic = d_ie_ic;
   md.ie_geo = d_ie_geo;
@@ -493,15 +618,115 @@ int build_mesh(dgm_ctx* c, const dgm_mesh_desc* m) {
   md.be_geo = d_be_geo;
   md.patch_q = d_patch;
   md.slot_ref = d_slot_ref;
-  mesh_of(c) = md;
+  // instance ranges for the diagnostics
+  std::vector<int> elem_off(n_inst + 1), bslot_off(n_inst + 1);
+  for (int i = 0; i < n_inst; ++i) {
+    elem_off[i] = (int)c->inst[i].elem_off;
+    bslot_off[i] = (int)c->inst[i].bslot_off;
+  }
+  elem_off[n_inst] = (int)ne;
+  bslot_off[n_inst] = (int)c->n_bnd;
+  if ((st = upload(c, &c->d_elem_off, elem_off)) || (st = upload(c, &c->d_bslot_off, bslot_off))) return st;
+  int64_t mx = 0;
+  for (auto& h : c->inst) mx = std::max(mx, h.ne);
+  c->max_inst_ne = mx;
   return DGM_OK;
 }
+
+bool variant_ok(const dgm_tables_desc* t) {
+  const int P = t->order;
+  return (P == 1 && t->n_basis == 3 && t->n_cell_gp == 3 && t->n_edge_gp == 2) ||
+         (P == 2 && t->n_basis == 6 && t->n_cell_gp == 6 && t->n_edge_gp == 3) ||
+         (P == 3 && t->n_basis == 10 && t->n_cell_gp == 12 && t->n_edge_gp == 4);
+}
+
+dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* tables, const dgm_params* params,
+                int32_t* status) {
+  int32_t dummy;
+  if (!status) status = &dummy;
+  if (n_inst < 1 || !meshes || !tables || !params) {
+    *status = DGM_BAD_ARG;
+    return nullptr;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || params->device < 0 || params->device >= ndev) {
+    cudaGetLastError();
+    *status = DGM_NO_DEVICE;
+    return nullptr;
+  }
+  if (!variant_ok(tables) || (params->precision != 0 && params->precision != 1)) {
+    *status = DGM_BAD_ARG;
+    return nullptr;
+  }
+  for (int i = 1; i < n_inst; ++i)
+    if (params[i].hcr != params[0].hcr) {  // the gas constants are shared by the whole context
+      *status = DGM_BAD_ARG;
+      return nullptr;
+    }
+  auto* c = new dgm_ctx();
+  c->device = params->device;
+  c->P = tables->order;
+  c->nb = tables->n_basis;
+  c->nq = tables->n_cell_gp;
+  c->ng = tables->n_edge_gp;
+  c->prec = params->precision;
+  c->hcr = params->hcr;
+  c->limiter = params->limiter ? 1 : 0;
+  c->inst.resize(n_inst);
+  for (int i = 0; i < n_inst; ++i) {
+    c->inst[i].cfl = params[i].cfl;
+    c->inst[i].final_time = params[i].final_time;
+    c->inst[i].final_step = params[i].final_step;
+  }
+  auto fail = [&](int st) {
+    *status = st;
+    dgm_destroy(c);
+    return (dgm_ctx*)nullptr;
+  };
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(DGM_NO_DEVICE);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return fail(DGM_NO_DEVICE);
+  c->num_sms = prop.multiProcessorCount;
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+  if (!coop) return fail(DGM_NO_DEVICE);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  int st;
+  if ((st = dev_alloc(c, &c->ctl, 1)) || (st = dev_alloc(c, &c->ic, (size_t)n_inst))) return fail(st);
+  if (cudaMemset(c->ctl, 0, sizeof(Control)) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  if (cudaMemset(c->ic, 0, sizeof(InstCtl) * n_inst) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  st = dispatch(c, [&](auto ops) { return decltype(ops)::fill_tables(c, tables); });
+  if (st) return fail(st);
+  MeshDev md;
+  if ((st = build_mesh(c, meshes, n_inst, md))) return fail(st);
+  dispatch(c, [&](auto ops) { return decltype(ops)::set_mesh(c, md); });
+  const size_t n_state = (size_t)NEQ * c->nb * c->ld;
+  const size_t n_flux = (size_t)(c->n_int + c->n_bnd) * c->ng * 4;
+  const size_t eb = elem_bytes(c);
+  if ((st = dev_alloc_bytes(c, &c->U, n_state * eb)) || (st = dev_alloc_bytes(c, &c->U1, n_state * eb)) ||
+      (st = dev_alloc_bytes(c, &c->U2, n_state * eb)) || (st = dev_alloc_bytes(c, &c->R, n_state * eb)) ||
+      (st = dev_alloc_bytes(c, &c->F, n_flux * eb)) ||
+      (st = dev_alloc(c, &c->stage, (size_t)c->max_inst_ne * NEQ * c->nb)) ||
+      (st = dev_alloc(c, &c->t0, (size_t)c->ne)) || (st = dev_alloc(c, &c->status, (size_t)c->ne)) ||
+      (st = dev_alloc(c, &c->work, (size_t)c->ne)) || (st = dev_alloc(c, &c->d_diag, (size_t)n_inst * 8)))
+    return fail(st);
+  for (void* p : {c->U, c->U1, c->U2, c->R})
+    if (cudaMemset(p, 0, n_state * eb) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  if (cudaMemset(c->status, 0, (size_t)c->ne * sizeof(unsigned int)) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::occupancy(c); }))) return fail(st);
+  c->graph_steps = (int)kGraphSteps;
+  if ((st = write_clock(c))) return fail(st);
+  *status = DGM_OK;
+  return c;
+}
+
+bool inst_ok(dgm_ctx* c, int64_t i) { return c && i >= 0 && i < (int64_t)c->inst.size(); }
 
 }  // namespace
 
 extern "C" {
 
-const char* dgm_version(void) { return "dgm_b200 0.1 (sm_100a, FP64 DG residual + SSP-RK3)"; }
+const char* dgm_version(void) { return "dgm_b200 0.2 (sm_100a; FP64 and FP32 DG residual + SSP-RK3, batched)"; }
 
 const char* dgm_status_string(int32_t s) {
   switch (s) {
@@ -533,184 +758,179 @@ void dgm_destroy(dgm_ctx* c) {
 
 dgm_ctx* dgm_create(const dgm_mesh_desc* mesh, const dgm_tables_desc* tables, const dgm_params* params,
                     int32_t* status) {
-  int32_t dummy;
-  if (!status) status = &dummy;
-  if (!mesh || !tables || !params) {
-    *status = DGM_BAD_ARG;
-    return nullptr;
-  }
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || params->device < 0 || params->device >= ndev) {
-    cudaGetLastError();
-    *status = DGM_NO_DEVICE;
-    return nullptr;
-  }
-  const int P = tables->order;
-  const bool ok_variant = (P == 1 && tables->n_basis == 3 && tables->n_cell_gp == 3 && tables->n_edge_gp == 2) ||
-                          (P == 2 && tables->n_basis == 6 && tables->n_cell_gp == 6 && tables->n_edge_gp == 3) ||
-                          (P == 3 && tables->n_basis == 10 && tables->n_cell_gp == 12 && tables->n_edge_gp == 4);
-  if (!ok_variant) {
-    *status = DGM_BAD_ARG;
-    return nullptr;
-  }
-  auto* c = new dgm_ctx();
-  c->device = params->device;
-  c->P = P;
-  c->nb = tables->n_basis;
-  c->nq = tables->n_cell_gp;
-  c->ng = tables->n_edge_gp;
-  c->hcr = params->hcr;
-  c->cfl = params->cfl;
-  c->final_time = params->final_time;
-  c->final_step = params->final_step;
-  c->limiter = params->limiter ? 1 : 0;
-  auto fail = [&](int st) {
-    *status = st;
-    dgm_destroy(c);
-    return (dgm_ctx*)nullptr;
-  };
-  if (cudaSetDevice(c->device) != cudaSuccess) return fail(DGM_NO_DEVICE);
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return fail(DGM_NO_DEVICE);
-  c->num_sms = prop.multiProcessorCount;
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(DGM_CUDA_ERROR);
-  int st;
-  if ((st = dev_alloc(c, &c->ctl, 1))) return fail(st);
-  if (cudaMemset(c->ctl, 0, sizeof(Control)) != cudaSuccess) return fail(DGM_CUDA_ERROR);
-  st = dispatch(c, [&](auto ops) { return decltype(ops)::fill_tables(c, tables); });
-  if (st) return fail(st);
-  if ((st = build_mesh(c, mesh))) return fail(st);
-  const size_t n_state = (size_t)NEQ * c->nb * c->ld;
-  const size_t n_flux = (size_t)(c->n_int + c->n_bnd) * c->ng * 4;
-  if ((st = dev_alloc(c, &c->U, n_state)) || (st = dev_alloc(c, &c->U1, n_state)) ||
-      (st = dev_alloc(c, &c->U2, n_state)) || (st = dev_alloc(c, &c->R, n_state)) ||
-      (st = dev_alloc(c, &c->F, n_flux)) || (st = dev_alloc(c, &c->stage, (size_t)c->ne * NEQ * c->nb)) ||
-      (st = dev_alloc(c, &c->t0, (size_t)c->ne)) || (st = dev_alloc(c, &c->status, (size_t)c->ne)) ||
-      (st = dev_alloc(c, &c->work, (size_t)c->ne)))
-    return fail(st);
-  for (double* p : {c->U, c->U1, c->U2, c->R})
-    if (cudaMemset(p, 0, n_state * sizeof(double)) != cudaSuccess) return fail(DGM_CUDA_ERROR);
-  if (cudaMemset(c->status, 0, (size_t)c->ne * sizeof(unsigned int)) != cudaSuccess) return fail(DGM_CUDA_ERROR);
-  if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::occupancy(c); }))) return fail(st);
-  int coop = 0;
-  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
-  if (!coop) return fail(DGM_NO_DEVICE);
-  c->graph_steps = (int)kGraphSteps;
-  if ((st = write_clock(c))) return fail(st);
-  *status = DGM_OK;
-  return c;
+  return create(1, mesh, tables, params, status);
 }
 
+dgm_ctx* dgm_create_batch(int32_t n_instances, const dgm_mesh_desc* meshes, const dgm_tables_desc* tables,
+                          const dgm_params* params, int32_t* status) {
+  return create(n_instances, meshes, tables, params, status);
+}
+
+int32_t dgm_instance_upload(dgm_ctx* c, int32_t i, const double* solutions) {
+  if (!inst_ok(c, i) || !solutions) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  int st = upload_state(c, i, solutions, c->U);
+  if (st) return st;
+  CK(cudaStreamSynchronize(c->stream));
+  return DGM_OK;
+}
+
+int32_t dgm_instance_download(dgm_ctx* c, int32_t i, double* solutions) {
+  if (!inst_ok(c, i) || !solutions) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  return download_state(c, i, c->U, solutions);
+}
+
+int32_t dgm_instance_download_residual(dgm_ctx* c, int32_t i, double* residuals) {
+  if (!inst_ok(c, i) || !residuals) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  return download_state(c, i, c->R, residuals);
+}
+
+int32_t dgm_instance_state(dgm_ctx* c, int32_t i, double* t, int64_t* step, int32_t* status, int64_t* where) {
+  if (!inst_ok(c, i)) return DGM_BAD_ARG;
+  const HostInst& h = c->inst[i];
+  if (t) *t = h.t;
+  if (step) *step = h.step;
+  if (status) *status = h.status;
+  if (where) *where = h.err_where;
+  return DGM_OK;
+}
+
+int32_t dgm_instance_set(dgm_ctx* c, int32_t i, double t, int64_t step, double final_time, int64_t final_step) {
+  if (!inst_ok(c, i)) return DGM_BAD_ARG;
+  HostInst& h = c->inst[i];
+  h.t = t;
+  h.step = step;
+  h.final_time = final_time;
+  h.final_step = final_step;
+  h.status = 0;
+  h.err_where = -1;
+  c->limits_dirty = true;
+  return DGM_OK;
+}
+
+int32_t dgm_instance_count(dgm_ctx* c) { return c ? (int32_t)c->inst.size() : 0; }
+
 int32_t dgm_compute_residuals(dgm_ctx* c, double* residuals, const double* solutions) {
-  if (!c || !residuals || !solutions) return DGM_BAD_ARG;
+  if (!c || !residuals || !solutions || c->inst.size() != 1) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st;
-  if ((st = upload_state(c, solutions, c->U1))) return st;
-  if ((st = upload_state(c, residuals, c->U2))) return st;
+  if ((st = upload_state(c, 0, solutions, c->U1))) return st;
+  if ((st = upload_state(c, 0, residuals, c->U2))) return st;
   if ((st = set_active(c, 0.0, false))) return st;
   st = dispatch(c, [&](auto ops) {
     using O = decltype(ops);
-    int s2 = O::edge_flux(c, c->U1);
+    int s2 = O::edge_flux(c, O::S(c->U1));
     if (s2) return s2;
-    return O::template element<0>(c, c->U1, nullptr, nullptr, c->U2, c->R);
+    return O::template element<0>(c, O::S(c->U1), nullptr, nullptr, O::S(c->U2), O::S(c->R));
   });
   if (st) return st;
-  if ((st = download_state(c, c->R, residuals))) return st;
+  if ((st = download_state(c, 0, c->R, residuals))) return st;
   return collect_status(c);
 }
 
 int32_t dgm_apply_limiter(dgm_ctx* c, double* solutions, int64_t* troubled) {
-  if (!c || !solutions) return DGM_BAD_ARG;
+  if (!c || !solutions || c->inst.size() != 1) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st;
-  if ((st = upload_state(c, solutions, c->U1))) return st;
+  if ((st = upload_state(c, 0, solutions, c->U1))) return st;
   if ((st = set_active(c, 0.0, false))) return st;
-  if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::limiter(c, c->U1); }))) return st;
-  if ((st = download_state(c, c->U1, solutions))) return st;
+  if ((st = dispatch(c, [&](auto ops) {
+         using O = decltype(ops);
+         return O::limiter(c, O::S(c->U1));
+       })))
+    return st;
+  if ((st = download_state(c, 0, c->U1, solutions))) return st;
   st = collect_status(c);
   if (troubled) *troubled = c->last_troubled;
   return st;
 }
 
 int32_t dgm_compute_time_step(dgm_ctx* c, const double* solutions, double* time_step) {
-  if (!c || !solutions || !time_step) return DGM_BAD_ARG;
+  if (!c || !solutions || !time_step || c->inst.size() != 1) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st;
-  if ((st = upload_state(c, solutions, c->U1))) return st;
+  if ((st = upload_state(c, 0, solutions, c->U1))) return st;
   if ((st = set_active(c, 0.0, false))) return st;
-  if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::time_step(c, c->U1); }))) return st;
+  if ((st = dispatch(c, [&](auto ops) {
+         using O = decltype(ops);
+         return O::time_step(c, O::S(c->U1));
+       })))
+    return st;
   Control h;
-  if ((st = read_control(c, &h))) return st;
-  unsigned long long bits = h.dt_bits;
+  std::vector<InstCtl> hi;
+  if ((st = read_control(c, &h, &hi))) return st;
+  unsigned long long bits = hi[0].dt_bits;
   std::memcpy(time_step, &bits, sizeof(double));
   return collect_status(c);
 }
 
 int32_t dgm_rk3(dgm_ctx* c, double* residuals, double* solutions, double time_step) {
-  if (!c || !residuals || !solutions) return DGM_BAD_ARG;
+  if (!c || !residuals || !solutions || c->inst.size() != 1) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st;
-  if ((st = upload_state(c, solutions, c->U))) return st;
+  if ((st = upload_state(c, 0, solutions, c->U))) return st;
   if ((st = set_active(c, time_step, true))) return st;
-  if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::rk3(c, c->R); }))) return st;
-  if ((st = download_state(c, c->U, solutions))) return st;
-  if ((st = download_state(c, c->R, residuals))) return st;
+  if ((st = dispatch(c, [&](auto ops) {
+         using O = decltype(ops);
+         return O::rk3(c, O::S(c->R));
+       })))
+    return st;
+  if ((st = download_state(c, 0, c->U, solutions))) return st;
+  if ((st = download_state(c, 0, c->R, residuals))) return st;
   return collect_status(c);
 }
 
 int32_t dgm_time_march(dgm_ctx* c, double* residuals, double* solutions) {
-  if (!c || !residuals || !solutions) return DGM_BAD_ARG;
+  if (!c || !residuals || !solutions || c->inst.size() != 1) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st;
   if ((st = write_clock(c))) return st;
-  if ((st = upload_state(c, solutions, c->U))) return st;
-  const int64_t remaining = std::max<int64_t>(0, c->final_step - c->current_step);
+  if ((st = upload_state(c, 0, solutions, c->U))) return st;
+  const int64_t remaining = std::max<int64_t>(0, c->inst[0].final_step - c->inst[0].step);
   if ((st = enqueue_steps(c, remaining, 1))) return st;
-  if ((st = download_state(c, c->U, solutions))) return st;
+  if ((st = download_state(c, 0, c->U, solutions))) return st;
   if (remaining > 0)
-    if ((st = download_state(c, c->R, residuals))) return st;
+    if ((st = download_state(c, 0, c->R, residuals))) return st;
   return collect_status(c);
 }
 
 int32_t dgm_get_clock(dgm_ctx* c, double* t, int64_t* step) {
   if (!c) return DGM_BAD_ARG;
-  if (t) *t = c->current_time;
-  if (step) *step = c->current_step;
+  if (t) *t = c->inst[0].t;
+  if (step) *step = c->inst[0].step;
   return DGM_OK;
 }
 
 int32_t dgm_set_clock(dgm_ctx* c, double t, int64_t step) {
   if (!c) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
-  c->current_time = t;
-  c->current_step = step;
+  for (auto& h : c->inst) {
+    h.t = t;
+    h.step = step;
+  }
   return write_clock(c);
 }
 
 int32_t dgm_set_limits(dgm_ctx* c, double final_time, int64_t final_step) {
   if (!c) return DGM_BAD_ARG;
-  c->final_time = final_time;
-  c->final_step = final_step;
+  for (auto& h : c->inst) {
+    h.final_time = final_time;
+    h.final_step = final_step;
+  }
   c->limits_dirty = true;
   return DGM_OK;
 }
 
 int32_t dgm_upload_solutions(dgm_ctx* c, const double* solutions) {
-  if (!c || !solutions) return DGM_BAD_ARG;
-  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
-  int st = upload_state(c, solutions, c->U);
-  if (st) return st;
-  CK(cudaStreamSynchronize(c->stream));
-  return DGM_OK;
+  if (!c || !solutions || c->inst.size() != 1) return DGM_BAD_ARG;
+  return dgm_instance_upload(c, 0, solutions);
 }
 
 int32_t dgm_download_solutions(dgm_ctx* c, double* solutions) {
-  if (!c || !solutions) return DGM_BAD_ARG;
-  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
-  int st = download_state(c, c->U, solutions);
-  if (st) return st;
-  CK(cudaStreamSynchronize(c->stream));
-  return DGM_OK;
+  if (!c || !solutions || c->inst.size() != 1) return DGM_BAD_ARG;
+  return dgm_instance_download(c, 0, solutions);
 }
 
 int32_t dgm_advance(dgm_ctx* c, int64_t n_steps) {
@@ -721,6 +941,16 @@ int32_t dgm_advance(dgm_ctx* c, int64_t n_steps) {
     if (st) return st;
   }
   return enqueue_steps(c, n_steps, 0);
+}
+
+int32_t dgm_advance_with_residual(dgm_ctx* c, int64_t n_steps) {
+  if (!c || n_steps < 0) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  if (c->limits_dirty) {
+    int st = write_clock(c);
+    if (st) return st;
+  }
+  return enqueue_steps(c, n_steps, 1);
 }
 
 int32_t dgm_synchronize(dgm_ctx* c) {
@@ -740,10 +970,10 @@ int32_t dgm_launch_phase(dgm_ctx* c, int32_t phase) {
   return dispatch(c, [&](auto ops) {
     using O = decltype(ops);
     switch (phase) {
-      case 0: return O::time_step(c, c->U);
-      case 1: return O::edge_flux(c, c->U);
-      case 2: return O::template element<2>(c, c->U, c->U, c->U2, nullptr, nullptr);
-      default: return O::limiter(c, c->U2);
+      case 0: return O::time_step(c, O::S(c->U));
+      case 1: return O::edge_flux(c, O::S(c->U));
+      case 2: return O::template element<2>(c, O::S(c->U), O::S(c->U), O::S(c->U2), nullptr, nullptr);
+      default: return O::limiter(c, O::S(c->U2));
     }
   });
 }
@@ -771,5 +1001,20 @@ int32_t dgm_limiter_stats(dgm_ctx* c, int64_t* troubled, int32_t* waves) {
 }
 
 int64_t dgm_device_bytes(dgm_ctx* c) { return c ? c->bytes : 0; }
+
+int32_t dgm_diagnostics(dgm_ctx* c, int32_t use_residual, double* out) {
+  if (!c || !out) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  int st = dispatch(c, [&](auto ops) {
+    using O = decltype(ops);
+    return O::diagnostics(c, use_residual ? O::S(c->R) : nullptr);
+  });
+  if (st) return st;
+  CK(cudaMemcpyAsync(out, c->d_diag, sizeof(double) * 8 * c->inst.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DGM_OK;
+}
+
+int32_t dgm_precision(dgm_ctx* c) { return c ? c->prec : -1; }
 
 }  // extern "C"

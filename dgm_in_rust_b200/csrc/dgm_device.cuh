@@ -1,21 +1,28 @@
-// dgm_device.cuh -- device code of the B200 DG residual + SSP-RK3 path (FP64).
+// dgm_device.cuh -- device code of the B200 DG residual + SSP-RK3 path.
 //
-// Data layout in HBM (one solver instance):
-//   state      U[v*NB + b][ld]        SoA, v = conserved variable, b = Dubiner mode, ld = padded
-//                                      element count; a warp's 32 consecutive elements read one
-//                                      256-byte segment per (v, b).
+// One context holds one or more independent mesh instances as a single disconnected union
+// mesh (element, edge and patch indices offset per instance), so every launch covers all
+// instances; each instance has its own time-march control (time, dt, step, loop bounds, status).
+//
+// Data layout in HBM:
+//   state      U[v*NB + b][ld]        SoA in the storage type T (double or float), v = conserved
+//                                      variable, b = Dubiner mode, ld = element count padded to 32
 //   geometry   jac[ne], dinv[4][ld]   (dxi/dx, dxi/dy, deta/dx, deta/dy), hmin[ne], h15[ne]
 //   faces      face[3][ld]            (edge slot << 1) | side, side 1 = element is the edge's
 //                                      right element; slots [0, n_int) are internal edges,
 //                                      [n_int, n_int + n_bnd) boundary edges
-//   edge flux  F[slot][NG][4]          HLLC / boundary flux at the edge Gauss points, already
-//                                      multiplied by half the edge length; written by the edge
-//                                      pass, gathered by the element pass (no atomics).
-// Tables (basis, quadrature) travel in the kernel parameter block (constant bank), so every
-// compile-time-indexed table read is a broadcast operand.
+//   instance   inst[ne]               instance of each element
+//   edge flux  F[slot][NG][4]          HLLC / boundary flux at the edge Gauss points times half
+//                                      the edge length (type T); written by the edge pass,
+//                                      gathered by the element pass (no atomics)
+// Tables travel in the kernel parameter block (constant bank): every compile-time-indexed table
+// read is a broadcast operand.  With T = float the volume/edge contractions, fluxes and stage
+// updates run in FP32; the limiter (KXRCF detection, WENO indicators and weights), the
+// positivity checks of HLLC and the time step stay in FP64.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <type_traits>
 
 namespace dgm {
 
@@ -38,27 +45,38 @@ template <> struct Variant<1> { static constexpr int NB = 3, NQ = 3, NG = 2, NK 
 template <> struct Variant<2> { static constexpr int NB = 6, NQ = 6, NG = 3, NK = 5; };
 template <> struct Variant<3> { static constexpr int NB = 10, NQ = 12, NG = 4, NK = 9; };
 
-template <int P>
-struct Tables {
+// Tables of the bulk kernels, in the storage type.
+template <int P, typename T>
+struct TablesT {
   using V = Variant<P>;
-  double phi_cell[V::NQ][V::NB];          // phis_cell_gps
-  double dxi[V::NQ][V::NB];               // d/dxi  at cell points
-  double deta[V::NQ][V::NB];              // d/deta at cell points
-  double dref[V::NQ][V::NB][V::NK];       // all reference derivatives up to order P
-  double phi_edge[3][V::NG][V::NB];       // phis_edge_gps
+  T phi_cell[V::NQ][V::NB];          // phis_cell_gps
+  T dxi[V::NQ][V::NB];               // d/dxi  at cell points
+  T deta[V::NQ][V::NB];              // d/deta at cell points
+  T phi_edge[3][V::NG][V::NB];       // phis_edge_gps
+  T cell_w[V::NQ];
+  T edge_w[V::NG];
+  T inv_mass[V::NB];                 // 1 / mass_mat_diag
+};
+
+// FP64 tables of the limiter and the diagnostics.
+template <int P>
+struct TablesD {
+  using V = Variant<P>;
+  double phi_edge[3][V::NG][V::NB];
   double cell_w[V::NQ];
   double edge_w[V::NG];
-  double mass[V::NB];
+  double dref[V::NQ][V::NB][V::NK];  // reference derivatives up to order P
 };
 
 struct MeshDev {
-  int ne, ld, n_int, n_bnd;
+  int ne, ld, n_int, n_bnd, n_inst, _pad;
   const double* __restrict__ jac;     // [ne]
   const double* __restrict__ dinv;    // [4][ld]
   const double* __restrict__ hmin;    // [ne]
   const double* __restrict__ h15;     // [ne] circumradius^1.5
   const int* __restrict__ face;       // [3][ld]
   const int* __restrict__ nbr;        // [3][ld]  -1 on the boundary
+  const int* __restrict__ inst;       // [ne] instance of each element
   const int2* __restrict__ ie_lr;     // [n_int] left, right element
   const int* __restrict__ ie_ic;      // [n_int] ilic | iric << 2
   const double4* __restrict__ ie_geo; // [n_int] nx, ny, half length, length
@@ -69,17 +87,24 @@ struct MeshDev {
   const int64_t* __restrict__ slot_ref;  // [n_int + n_bnd] reference edge id of each slot
 };
 
-// Per-context control block in device memory: the time-march loop state lives here so the
-// whole loop can run from CUDA graphs without host round trips.
-struct Control {
+// Time-march state of one instance (TemperalDisc's current_time / current_step and the loop
+// bounds of SolverParameters), advanced on the device.
+struct InstCtl {
   double t, dt, final_time, cfl;
   long long step, final_step;
-  unsigned long long dt_bits;  // atomicMin target for the global time step
+  unsigned long long dt_bits;  // atomicMin target of the instance's time step
   int active;                  // this step runs (loop condition of temporal_disc.rs:22)
-  int status;                  // first error raised on the device
+  int status;                  // first error raised in this instance
   long long err_where;         // edge / element of that error
+};
+
+// Context-wide control block: first error, limiter counters, grid barrier.
+struct Control {
+  int status;                  // first error raised on the device (any instance)
+  int _pad0;
+  long long err_where;
   int t0_count;                // cells flagged by the parallel KXRCF pass
-  int troubled;                // cells limited by the last limiter pass
+  int troubled;                // cells limited since the last step start
   int waves;                   // limiter waves of the last pass
   int unknown[2];              // per-wave count of unsettled cells (double-buffered)
   int wl_count[2];             // per-wave worklist length (double-buffered)
@@ -98,25 +123,31 @@ struct Gas {
   int _pad;
 };
 
-template <int P>
+template <int P, typename T>
 struct KParams {
-  Tables<P> tab;
+  TablesT<P, T> t;
+  TablesD<P> d;
   MeshDev m;
   Gas gas;
-  double inv_mass[Variant<P>::NB];  // 1 / mass_mat_diag
   Control* ctl;
+  InstCtl* ic;
 };
 
-__device__ __forceinline__ void raise_status(Control* ctl, int code, long long where) {
+__device__ __forceinline__ void raise_status(Control* ctl, InstCtl* ic, int code, long long where) {
+  if (atomicCAS(&ic->status, 0, code) == 0) ic->err_where = where;
   if (atomicCAS(&ctl->status, 0, code) == 0) ctl->err_where = where;
 }
 
+template <typename T>
+__device__ __forceinline__ T ld_state(const T* p) { return __ldcg(p); }
+
 // flux::flux, flux.rs:154-169 (one reciprocal of the density instead of three divisions)
-__device__ __forceinline__ void euler_flux(const double q[4], const Gas& gas, double f[4], double g[4]) {
-  const double rq = 1.0 / q[0];
-  const double u = q[1] * rq;
-  const double v = q[2] * rq;
-  const double p = gas.gm1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) * rq);
+template <typename T>
+__device__ __forceinline__ void euler_flux(const T q[4], T gm1, T f[4], T g[4]) {
+  const T rq = T(1) / q[0];
+  const T u = q[1] * rq;
+  const T v = q[2] * rq;
+  const T p = gm1 * (q[3] - T(0.5) * (q[1] * q[1] + q[2] * q[2]) * rq);
   f[0] = q[1];
   f[1] = q[1] * u + p;
   f[2] = q[2] * u;
@@ -127,12 +158,9 @@ __device__ __forceinline__ void euler_flux(const double q[4], const Gas& gas, do
   g[3] = v * (q[3] + p);
 }
 
-// flux::hllc, flux.rs:28-153.  Returns ST_NEG_DENSITY / ST_NEG_PRESSURE like the reference's Err.
-// Same formulas; densities enter through their reciprocals, x^zeta as exp(zeta log x), and
-// (.)^(1/zeta) as an integer power when 1/zeta is an integer to round-off (hcr = 1.4: 7);
-// both differ from the reference's libm pow only in the last bits.
-__device__ __forceinline__ double ipow(double x, int n) {
-  double r = 1.0;
+template <typename T>
+__device__ __forceinline__ T ipow(T x, int n) {
+  T r = T(1);
   while (n) {
     if (n & 1) r *= x;
     x *= x;
@@ -141,49 +169,63 @@ __device__ __forceinline__ double ipow(double x, int n) {
   return r;
 }
 
-__device__ __forceinline__ int hllc(const double lv[4], const double rv[4], double nx, double ny,
-                                    const Gas& gas, double flux[4]) {
-  const double ql0 = lv[0], ql1 = lv[1] * nx + lv[2] * ny, ql2 = -lv[1] * ny + lv[2] * nx, ql3 = lv[3];
-  const double qr0 = rv[0], qr1 = rv[1] * nx + rv[2] * ny, qr2 = -rv[1] * ny + rv[2] * nx, qr3 = rv[3];
-  const double rl = 1.0 / ql0, rr = 1.0 / qr0;
-  const double ul = ql1 * rl, ur = qr1 * rr, vl = ql2 * rl, vr = qr2 * rr;
-  const double pl = gas.gm1 * (ql3 - 0.5 * (ql1 * ql1 + ql2 * ql2) * rl);
-  const double pr = gas.gm1 * (qr3 - 0.5 * (qr1 * qr1 + qr2 * qr2) * rr);
-  if (ql0 < 0.0 || qr0 < 0.0) return ST_NEG_DENSITY;
-  if (pl < 0.0 || pr < 0.0) return ST_NEG_PRESSURE;
-  const double cl = sqrt(gas.hcr * pl * rl);
-  const double cr = sqrt(gas.hcr * pr * rr);
-  const double fl0 = ql1, fl1 = ql1 * ul + pl, fl2 = ql2 * ul, fl3 = ul * (ql3 + pl);
-  const double fr0 = qr1, fr1 = qr1 * ur + pr, fr2 = qr2 * ur, fr3 = ur * (qr3 + pr);
+// flux::hllc, flux.rs:28-153.  Returns ST_NEG_DENSITY / ST_NEG_PRESSURE like the reference's Err.
+// Same formulas; densities enter through their reciprocals, x^zeta as exp(zeta log x), and
+// (.)^(1/zeta) as an integer power when 1/zeta is an integer to round-off (hcr = 1.4: 7);
+// both differ from the reference's libm pow only in the last bits.  In FP32 the density and
+// pressure checks are evaluated in FP64.
+template <typename T>
+__device__ __forceinline__ int hllc(const T lv[4], const T rv[4], T nx, T ny, const Gas& gas, T flux[4]) {
+  const T gm1 = T(gas.gm1), hcr = T(gas.hcr);
+  const T ql0 = lv[0], ql1 = lv[1] * nx + lv[2] * ny, ql2 = -lv[1] * ny + lv[2] * nx, ql3 = lv[3];
+  const T qr0 = rv[0], qr1 = rv[1] * nx + rv[2] * ny, qr2 = -rv[1] * ny + rv[2] * nx, qr3 = rv[3];
+  const T rl = T(1) / ql0, rr = T(1) / qr0;
+  const T ul = ql1 * rl, ur = qr1 * rr, vl = ql2 * rl, vr = qr2 * rr;
+  const T pl = gm1 * (ql3 - T(0.5) * (ql1 * ql1 + ql2 * ql2) * rl);
+  const T pr = gm1 * (qr3 - T(0.5) * (qr1 * qr1 + qr2 * qr2) * rr);
+  if constexpr (std::is_same<T, double>::value) {
+    if (ql0 < 0.0 || qr0 < 0.0) return ST_NEG_DENSITY;
+    if (pl < 0.0 || pr < 0.0) return ST_NEG_PRESSURE;
+  } else {
+    const double dl0 = lv[0], dr0 = rv[0];
+    if (dl0 < 0.0 || dr0 < 0.0) return ST_NEG_DENSITY;
+    const double dpl = gas.gm1 * ((double)lv[3] - 0.5 * ((double)lv[1] * lv[1] + (double)lv[2] * lv[2]) / dl0);
+    const double dpr = gas.gm1 * ((double)rv[3] - 0.5 * ((double)rv[1] * rv[1] + (double)rv[2] * rv[2]) / dr0);
+    if (dpl < 0.0 || dpr < 0.0) return ST_NEG_PRESSURE;
+  }
+  const T cl = sqrt(hcr * pl * rl);
+  const T cr = sqrt(hcr * pr * rr);
+  const T fl0 = ql1, fl1 = ql1 * ul + pl, fl2 = ql2 * ul, fl3 = ul * (ql3 + pl);
+  const T fr0 = qr1, fr1 = qr1 * ur + pr, fr2 = qr2 * ur, fr3 = ur * (qr3 + pr);
   // PVRS-type p*, flux.rs:75-78
-  const double base = (cl + cr - gas.zm1h * (ur - ul)) /
-                      (cl * exp(-gas.zeta * log(pl)) + cr * exp(-gas.zeta * log(pr)));
-  const double p_star = gas.inv_zeta_int ? ipow(base, gas.inv_zeta_int) : exp(gas.inv_zeta * log(base));
-  const double ql_lower = (p_star <= pl) ? 1.0 : sqrt(1.0 + gas.gp1h * (p_star / pl - 1.0));
-  const double sl = ul - cl * ql_lower;
-  const double qr_lower = (p_star <= pr) ? 1.0 : sqrt(1.0 + gas.gp1h * (p_star / pr - 1.0));
-  const double sr = ur + cr * qr_lower;
-  double f0, fn, ft, f3;
-  if (sl >= 0.0) {
+  const T zeta = T(gas.zeta);
+  const T base = (cl + cr - T(gas.zm1h) * (ur - ul)) / (cl * exp(-zeta * log(pl)) + cr * exp(-zeta * log(pr)));
+  const T p_star = gas.inv_zeta_int ? ipow(base, gas.inv_zeta_int) : exp(T(gas.inv_zeta) * log(base));
+  const T ql_lower = (p_star <= pl) ? T(1) : sqrt(T(1) + T(gas.gp1h) * (p_star / pl - T(1)));
+  const T sl = ul - cl * ql_lower;
+  const T qr_lower = (p_star <= pr) ? T(1) : sqrt(T(1) + T(gas.gp1h) * (p_star / pr - T(1)));
+  const T sr = ur + cr * qr_lower;
+  T f0, fn, ft, f3;
+  if (sl >= T(0)) {
     f0 = fl0; fn = fl1; ft = fl2; f3 = fl3;
-  } else if (sr <= 0.0) {
+  } else if (sr <= T(0)) {
     f0 = fr0; fn = fr1; ft = fr2; f3 = fr3;
   } else {
-    const double s_star = (pr - pl + ql0 * ul * (sl - ul) - qr0 * ur * (sr - ur)) / (ql0 * (sl - ul) - qr0 * (sr - ur));
-    if (s_star >= 0.0) {
-      const double dl = ql0 * (sl - ul);
-      const double m = dl / (sl - s_star);
-      const double qs0 = m, qs1 = m * s_star, qs2 = m * vl;
-      const double qs3 = m * (ql3 * rl + (s_star - ul) * (s_star + pl / dl));
+    const T s_star = (pr - pl + ql0 * ul * (sl - ul) - qr0 * ur * (sr - ur)) / (ql0 * (sl - ul) - qr0 * (sr - ur));
+    if (s_star >= T(0)) {
+      const T dl = ql0 * (sl - ul);
+      const T m = dl / (sl - s_star);
+      const T qs0 = m, qs1 = m * s_star, qs2 = m * vl;
+      const T qs3 = m * (ql3 * rl + (s_star - ul) * (s_star + pl / dl));
       f0 = fl0 + sl * (qs0 - ql0);
       fn = fl1 + sl * (qs1 - ql1);
       ft = fl2 + sl * (qs2 - ql2);
       f3 = fl3 + sl * (qs3 - ql3);
     } else {
-      const double dr = qr0 * (sr - ur);
-      const double m = dr / (sr - s_star);
-      const double qs0 = m, qs1 = m * s_star, qs2 = m * vr;
-      const double qs3 = m * (qr3 * rr + (s_star - ur) * (s_star + pr / dr));
+      const T dr = qr0 * (sr - ur);
+      const T m = dr / (sr - s_star);
+      const T qs0 = m, qs1 = m * s_star, qs2 = m * vr;
+      const T qs3 = m * (qr3 * rr + (s_star - ur) * (s_star + pr / dr));
       f0 = fr0 + sr * (qs0 - qr0);
       fn = fr1 + sr * (qs1 - qr1);
       ft = fr2 + sr * (qs2 - qr2);
@@ -198,38 +240,39 @@ __device__ __forceinline__ int hllc(const double lv[4], const double rv[4], doub
 }
 
 // compute_eigenmatrix, local_characteristics.rs:4-50 (reciprocals of rho and c)
-__device__ __forceinline__ void eigenmatrix(const double q[4], double nx, double ny, const Gas& gas,
-                                            double L[4][4], double R[4][4]) {
-  const double rq = 1.0 / q[0];
-  const double u = q[1] * rq;
-  const double v = q[2] * rq;
-  const double p = gas.gm1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) * rq);
-  const double c = sqrt(gas.hcr * p * rq);
-  const double ic = 1.0 / c;
-  const double h = (q[3] + p) * rq;
-  const double b1 = gas.gm1 * (ic * ic);
-  const double b2 = b1 * (u * u + v * v) * 0.5;
-  const double vn = u * nx + v * ny;
-  L[0][0] = (b2 + vn * ic) * 0.5;
-  L[0][1] = -(b1 * u + nx * ic) * 0.5;
-  L[0][2] = -(b1 * v + ny * ic) * 0.5;
-  L[0][3] = b1 * 0.5;
+template <typename T>
+__device__ __forceinline__ void eigenmatrix(const T q[4], T nx, T ny, const Gas& gas, T L[4][4], T R[4][4]) {
+  const T gm1 = T(gas.gm1), hcr = T(gas.hcr);
+  const T rq = T(1) / q[0];
+  const T u = q[1] * rq;
+  const T v = q[2] * rq;
+  const T p = gm1 * (q[3] - T(0.5) * (q[1] * q[1] + q[2] * q[2]) * rq);
+  const T c = sqrt(hcr * p * rq);
+  const T ic = T(1) / c;
+  const T h = (q[3] + p) * rq;
+  const T b1 = gm1 * (ic * ic);
+  const T b2 = b1 * (u * u + v * v) * T(0.5);
+  const T vn = u * nx + v * ny;
+  L[0][0] = (b2 + vn * ic) * T(0.5);
+  L[0][1] = -(b1 * u + nx * ic) * T(0.5);
+  L[0][2] = -(b1 * v + ny * ic) * T(0.5);
+  L[0][3] = b1 * T(0.5);
   L[1][0] = ny * u - nx * v;
   L[1][1] = -ny;
   L[1][2] = nx;
-  L[1][3] = 0.0;
-  L[2][0] = 1.0 - b2;
+  L[1][3] = T(0);
+  L[2][0] = T(1) - b2;
   L[2][1] = b1 * u;
   L[2][2] = b1 * v;
   L[2][3] = -b1;
-  L[3][0] = (b2 - vn * ic) * 0.5;
-  L[3][1] = -(b1 * u - nx * ic) * 0.5;
-  L[3][2] = -(b1 * v - ny * ic) * 0.5;
-  L[3][3] = b1 * 0.5;
-  R[0][0] = 1.0;
-  R[0][1] = 0.0;
-  R[0][2] = 1.0;
-  R[0][3] = 1.0;
+  L[3][0] = (b2 - vn * ic) * T(0.5);
+  L[3][1] = -(b1 * u - nx * ic) * T(0.5);
+  L[3][2] = -(b1 * v - ny * ic) * T(0.5);
+  L[3][3] = b1 * T(0.5);
+  R[0][0] = T(1);
+  R[0][1] = T(0);
+  R[0][2] = T(1);
+  R[0][3] = T(1);
   R[1][0] = u - c * nx;
   R[1][1] = -ny;
   R[1][2] = u;
@@ -240,7 +283,7 @@ __device__ __forceinline__ void eigenmatrix(const double q[4], double nx, double
   R[2][3] = v + c * ny;
   R[3][0] = h - c * vn;
   R[3][1] = -u * ny + v * nx;
-  R[3][2] = (u * u + v * v) * 0.5;
+  R[3][2] = (u * u + v * v) * T(0.5);
   R[3][3] = h + c * vn;
 }
 
@@ -274,38 +317,38 @@ __device__ __forceinline__ double phys_deriv(const double (&r)[NK], double xx, d
   return 0.0;
 }
 
-__device__ __forceinline__ double ld_state(const double* p) { return __ldcg(p); }
-
 // ------------------------------------------------------------------------------------------
 // Edge pass: one thread per (edge slot, Gauss point).  Internal slots: traces of both
 // elements + HLLC (integrate_over_edges_euler, spatial_disc.rs:161-211).  Boundary slots:
 // slip-wall pressure flux or characteristic far-field flux (apply_bc_euler,
-// boundary_condition.rs:19-97).  Writes F[slot][g][v] * half length.
+// boundary_condition.rs:19-97).  Writes F[slot][g][v] * half length.  Slots of instances that
+// are not stepping are skipped.
 // ------------------------------------------------------------------------------------------
-template <int P>
-__global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KParams<P> kp,
-                                                   const double* __restrict__ U, double* __restrict__ F) {
+template <int P, typename T>
+__global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KParams<P, T> kp,
+                                                      const T* __restrict__ U, T* __restrict__ F) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
-  __shared__ double s_pe[3 * NG * NB];
-  for (int i = threadIdx.x; i < 3 * NG * NB; i += blockDim.x) s_pe[i] = (&kp.tab.phi_edge[0][0][0])[i];
+  __shared__ T s_pe[3 * NG * NB];
+  for (int i = threadIdx.x; i < 3 * NG * NB; i += blockDim.x) s_pe[i] = (&kp.t.phi_edge[0][0][0])[i];
   __syncthreads();
-  if (!kp.ctl->active) return;
   const MeshDev& m = kp.m;
   const Gas& gas = kp.gas;
   const int total = (m.n_int + m.n_bnd) * NG;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     const int s = t / NG, g = t - s * NG;
-    double out[4];
+    T out[4];
     if (s < m.n_int) {
       const int2 lr = m.ie_lr[s];
+      const int inst = m.n_inst > 1 ? m.inst[lr.x] : 0;
+      if (!kp.ic[inst].active) continue;
       const int ic = m.ie_ic[s];
-      const double* pl = &s_pe[((ic & 3) * NG + g) * NB];
-      const double* pr = &s_pe[((ic >> 2) * NG + (NG - 1 - g)) * NB];
-      double lv[4], rv[4];
+      const T* pl = &s_pe[((ic & 3) * NG + g) * NB];
+      const T* pr = &s_pe[((ic >> 2) * NG + (NG - 1 - g)) * NB];
+      T lv[4], rv[4];
 #pragma unroll
       for (int v = 0; v < NEQ; ++v) {
-        double a = 0.0, c = 0.0;
+        T a = T(0), c = T(0);
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
           a += ld_state(&U[(size_t)(v * NB + b) * m.ld + lr.x]) * pl[b];
@@ -315,79 +358,86 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
         rv[v] = c;
       }
       const double4 geo = m.ie_geo[s];
-      const int st = hllc(lv, rv, geo.x, geo.y, gas, out);
-      if (st != ST_OK) raise_status(kp.ctl, st, m.slot_ref[s]);
+      const int st = hllc<T>(lv, rv, T(geo.x), T(geo.y), gas, out);
+      if (st != ST_OK) raise_status(kp.ctl, &kp.ic[inst], st, m.slot_ref[s]);
 #pragma unroll
-      for (int v = 0; v < NEQ; ++v) out[v] *= geo.z;
+      for (int v = 0; v < NEQ; ++v) out[v] *= T(geo.z);
     } else {
       const int sb = s - m.n_int;
       const int e = m.be_elem[sb];
+      const int inst = m.n_inst > 1 ? m.inst[e] : 0;
+      if (!kp.ic[inst].active) continue;
       const int info = m.be_info[sb];
-      const double* pe = &s_pe[((info & 3) * NG + g) * NB];
-      double lv[4];
+      const T* pe = &s_pe[((info & 3) * NG + g) * NB];
+      T lv[4];
 #pragma unroll
       for (int v = 0; v < NEQ; ++v) {
-        double a = 0.0;
+        T a = T(0);
 #pragma unroll
         for (int b = 0; b < NB; ++b) a += ld_state(&U[(size_t)(v * NB + b) * m.ld + e]) * pe[b];
         lv[v] = a;
       }
       const double4 geo = m.be_geo[sb];
-      const double nx = geo.x, ny = geo.y;
+      const T nx = T(geo.x), ny = T(geo.y);
+      const T gm1 = T(gas.gm1);
       if (((info >> 2) & 1) == 0) {
         // slip wall, boundary_condition.rs:31-47
-        const double pressure = gas.gm1 * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
-        out[0] = 0.0;
+        const T pressure = gm1 * (lv[3] - T(0.5) * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+        out[0] = T(0);
         out[1] = pressure * nx;
         out[2] = pressure * ny;
-        out[3] = 0.0;
+        out[3] = T(0);
       } else {
         // characteristic far field, boundary_condition.rs:48-94
         const double4 bq = m.patch_q[info >> 3];
-        const double bc[4] = {bq.x, bq.y, bq.z, bq.w};
-        const double u = lv[1] / lv[0];
-        const double v = lv[2] / lv[0];
-        const double p = gas.gm1 * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
-        const double c = sqrt(gas.hcr * p / lv[0]);
-        const double vn = u * nx + v * ny;
-        double Lm[4][4], Rm[4][4];
-        eigenmatrix(lv, nx, ny, gas, Lm, Rm);
-        const double lam[4] = {vn - c, vn, vn, vn + c};
-        double mix[4];
+        const T bc[4] = {T(bq.x), T(bq.y), T(bq.z), T(bq.w)};
+        const T u = lv[1] / lv[0];
+        const T v = lv[2] / lv[0];
+        const T p = gm1 * (lv[3] - T(0.5) * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+        const T c = sqrt(T(gas.hcr) * p / lv[0]);
+        const T vn = u * nx + v * ny;
+        T Lm[4][4], Rm[4][4];
+        eigenmatrix<T>(lv, nx, ny, gas, Lm, Rm);
+        const T lam[4] = {vn - c, vn, vn, vn + c};
+        T mix[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          double alpha = 0.0, beta = 0.0;
+          T alpha = T(0), beta = T(0);
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             alpha += Lm[i][j] * lv[j];
             beta += Lm[i][j] * bc[j];
           }
-          mix[i] = lam[i] >= 0.0 ? alpha : beta;
+          mix[i] = lam[i] >= T(0) ? alpha : beta;
         }
-        double q[4];
+        T q[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          double sum = 0.0;
+          T sum = T(0);
 #pragma unroll
           for (int j = 0; j < 4; ++j) sum += Rm[i][j] * mix[j];
           q[i] = sum;
         }
-        const double un = q[1] / q[0];
-        const double vv = q[2] / q[0];
-        const double vn_new = un * nx + vv * ny;
-        const double p_new = gas.gm1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
-        const double h_new = q[3] + p_new;
+        const T un = q[1] / q[0];
+        const T vv = q[2] / q[0];
+        const T vn_new = un * nx + vv * ny;
+        const T p_new = gm1 * (q[3] - T(0.5) * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+        const T h_new = q[3] + p_new;
         out[0] = q[0] * vn_new;
         out[1] = q[1] * vn_new + p_new * nx;
         out[2] = q[2] * vn_new + p_new * ny;
         out[3] = h_new * vn_new;
       }
 #pragma unroll
-      for (int v = 0; v < NEQ; ++v) out[v] *= geo.z;
+      for (int v = 0; v < NEQ; ++v) out[v] *= T(geo.z);
     }
-    double2* dst = reinterpret_cast<double2*>(&F[((size_t)s * NG + g) * 4]);
-    dst[0] = make_double2(out[0], out[1]);
-    dst[1] = make_double2(out[2], out[3]);
+    T* dst = &F[((size_t)s * NG + g) * 4];
+    if constexpr (std::is_same<T, double>::value) {
+      reinterpret_cast<double2*>(dst)[0] = make_double2(out[0], out[1]);
+      reinterpret_cast<double2*>(dst)[1] = make_double2(out[2], out[3]);
+    } else {
+      reinterpret_cast<float4*>(dst)[0] = make_float4(out[0], out[1], out[2], out[3]);
+    }
   }
 }
 
@@ -402,17 +452,13 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
 //   MODE 3: out = 1/3 Ubase + 2/3 (Uin + dt R)
 // Four threads per element, one per conserved variable: lane = v * 8 + i within a warp that
 // covers 8 elements.  The quadrature-point states are exchanged with shuffles, so a thread
-// holds only its variable's NB modes and residuals (few registers, full occupancy), and each
-// (v, b) load of the 8 elements is one contiguous 64-byte run.
+// holds only its variable's NB modes and residuals, and each (v, b) load of the 8 elements is
+// one contiguous run.  Elements of instances that are not stepping are left untouched.
 // ------------------------------------------------------------------------------------------
-template <int P, int MODE>
-__global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KParams<P> kp,
-                                                 const double* __restrict__ Uin,
-                                                 const double* Ubase,
-                                                 const double* __restrict__ F,
-                                                 double* Uout,
-                                                 const double* Rin,
-                                                 double* Rout) {
+template <int P, typename T, int MODE>
+__global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KParams<P, T> kp,
+                                                    const T* __restrict__ Uin, const T* Ubase,
+                                                    const T* __restrict__ F, T* Uout, const T* Rin, T* Rout) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NQ = V::NQ, NG = V::NG;
   Control* ctl = kp.ctl;
@@ -421,83 +467,85 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
     ctl->unknown[0] = ctl->unknown[1] = 0;
     ctl->wl_count[0] = ctl->wl_count[1] = 0;
   }
-  if (!ctl->active) return;
   const MeshDev& m = kp.m;
   const int lane = threadIdx.x & 31;
   const int var = lane >> 3, i = lane & 7;
   const int e_raw = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 8 + i;
   if ((e_raw & ~7) >= m.ne) return;  // whole warp past the end
-  const bool valid = e_raw < m.ne;
-  const int e = valid ? e_raw : m.ne - 1;
+  const int e = e_raw < m.ne ? e_raw : m.ne - 1;
+  const int inst = m.n_inst > 1 ? m.inst[e] : 0;
+  const bool valid = e_raw < m.ne && kp.ic[inst].active;
   const size_t ld = m.ld;
-  double u[NB], r[NB];
+  T u[NB], r[NB];
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     u[b] = ld_state(&Uin[(var * NB + b) * ld + e]);
-    r[b] = 0.0;
+    r[b] = T(0);
   }
-  const double J = m.jac[e];
-  const double xx = m.dinv[0 * ld + e], xy = m.dinv[1 * ld + e], ex = m.dinv[2 * ld + e], ey = m.dinv[3 * ld + e];
+  const T J = T(m.jac[e]);
+  const T xx = T(m.dinv[0 * ld + e]), xy = T(m.dinv[1 * ld + e]), ex = T(m.dinv[2 * ld + e]),
+          ey = T(m.dinv[3 * ld + e]);
+  const T gm1 = T(kp.gas.gm1);
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
-    double mine = 0.0;
+    T mine = T(0);
 #pragma unroll
-    for (int b = 0; b < NB; ++b) mine += u[b] * kp.tab.phi_cell[q][b];
-    double uq[NEQ];
+    for (int b = 0; b < NB; ++b) mine += u[b] * kp.t.phi_cell[q][b];
+    T uq[NEQ];
 #pragma unroll
     for (int w = 0; w < NEQ; ++w) uq[w] = __shfl_sync(0xffffffffu, mine, w * 8 + i);
-    double f[NEQ], g[NEQ];
-    euler_flux(uq, kp.gas, f, g);
-    const double fv = var == 0 ? f[0] : var == 1 ? f[1] : var == 2 ? f[2] : f[3];
-    const double gv = var == 0 ? g[0] : var == 1 ? g[1] : var == 2 ? g[2] : g[3];
-    const double sc = kp.tab.cell_w[q] * 0.5 * J;
-    const double fx = sc * (fv * xx + gv * xy);
-    const double fe = sc * (fv * ex + gv * ey);
+    T f[NEQ], g[NEQ];
+    euler_flux<T>(uq, gm1, f, g);
+    const T fv = var == 0 ? f[0] : var == 1 ? f[1] : var == 2 ? f[2] : f[3];
+    const T gv = var == 0 ? g[0] : var == 1 ? g[1] : var == 2 ? g[2] : g[3];
+    const T sc = kp.t.cell_w[q] * T(0.5) * J;
+    const T fx = sc * (fv * xx + gv * xy);
+    const T fe = sc * (fv * ex + gv * ey);
 #pragma unroll
-    for (int b = 0; b < NB; ++b) r[b] += fx * kp.tab.dxi[q][b] + fe * kp.tab.deta[q][b];
+    for (int b = 0; b < NB; ++b) r[b] += fx * kp.t.dxi[q][b] + fe * kp.t.deta[q][b];
   }
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const int fw = m.face[k * ld + e];
     const int slot = fw >> 1;
     const bool right = fw & 1;
-    const double* Fs = &F[(size_t)slot * NG * 4 + var];
+    const T* Fs = &F[(size_t)slot * NG * 4 + var];
 #pragma unroll
     for (int gp = 0; gp < NG; ++gp) {
       const int src = right ? (NG - 1 - gp) : gp;
-      const double coef = right ? kp.tab.edge_w[gp] : -kp.tab.edge_w[gp];
-      const double fv = coef * __ldcg(&Fs[src * 4]);
+      const T coef = right ? kp.t.edge_w[gp] : -kp.t.edge_w[gp];
+      const T fv = coef * __ldcg(&Fs[src * 4]);
 #pragma unroll
-      for (int b = 0; b < NB; ++b) r[b] += fv * kp.tab.phi_edge[k][gp][b];
+      for (int b = 0; b < NB; ++b) r[b] += fv * kp.t.phi_edge[k][gp][b];
     }
   }
   if (!valid) return;
-  const double dt = ctl->dt;
-  const double inv_half_j = 1.0 / (0.5 * J);
+  const T dt = T(kp.ic[inst].dt);
+  const T inv_half_j = T(1) / (T(0.5) * J);
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const size_t idx = (var * NB + b) * ld + e;
-    double rr = r[b];
+    T rr = r[b];
     if constexpr (MODE == 0) rr = Rin[idx] + rr;
-    rr = rr * kp.inv_mass[b] * inv_half_j;  // divide_residual_by_mass_mat_diag
+    rr = rr * kp.t.inv_mass[b] * inv_half_j;  // divide_residual_by_mass_mat_diag
     if (Rout) Rout[idx] = rr;
     if constexpr (MODE == 1) {
       Uout[idx] = u[b] + dt * rr;
     } else if constexpr (MODE == 2) {
-      Uout[idx] = 0.75 * Ubase[idx] + 0.25 * (u[b] + dt * rr);
+      Uout[idx] = T(0.75) * Ubase[idx] + T(0.25) * (u[b] + dt * rr);
     } else if constexpr (MODE == 3) {
-      Uout[idx] = (1.0 / 3.0) * Ubase[idx] + (2.0 / 3.0) * (u[b] + dt * rr);
+      Uout[idx] = T(1.0 / 3.0) * Ubase[idx] + T(2.0 / 3.0) * (u[b] + dt * rr);
     }
   }
 }
 
 // ------------------------------------------------------------------------------------------
-// modified_kxrcf, weno.rs:7-85, for element e on state U.  Keeps the reference's exterior-trace
-// indexing: the neighbour's modes are evaluated with this element's own local edge index k
-// (weno.rs:21-27 pick in_cell_indices[side], which is always this element's index).
+// modified_kxrcf, weno.rs:7-85, for element e on state U (FP64 arithmetic).  Keeps the
+// reference's exterior-trace indexing: the neighbour's modes are evaluated with this element's
+// own local edge index k (weno.rs:21-27 pick in_cell_indices[side], always this element's).
 // ------------------------------------------------------------------------------------------
-template <int P>
-__device__ __forceinline__ bool kxrcf(const KParams<P>& kp, const double* __restrict__ U, int e) {
+template <int P, typename T>
+__device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restrict__ U, int e) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
   const MeshDev& m = kp.m;
@@ -519,8 +567,8 @@ __device__ __forceinline__ bool kxrcf(const KParams<P>& kp, const double* __rest
       double rho = 0.0, rho_e = 0.0;
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        rho += ld_state(&U[(0 * NB + b) * ld + e]) * kp.tab.phi_edge[k][g][b];
-        rho_e += ld_state(&U[(3 * NB + b) * ld + e]) * kp.tab.phi_edge[k][g][b];
+        rho += (double)ld_state(&U[(0 * NB + b) * ld + e]) * kp.d.phi_edge[k][g][b];
+        rho_e += (double)ld_state(&U[(3 * NB + b) * ld + e]) * kp.d.phi_edge[k][g][b];
       }
       own_rho[g] = rho;
       own_rhoe[g] = rho_e;
@@ -531,8 +579,8 @@ __device__ __forceinline__ bool kxrcf(const KParams<P>& kp, const double* __rest
     double rho_u = 0.0, rho_v = 0.0;
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      rho_u += ld_state(&U[(1 * NB + b) * ld + e]) * kp.tab.phi_edge[k][cg][b];
-      rho_v += ld_state(&U[(2 * NB + b) * ld + e]) * kp.tab.phi_edge[k][cg][b];
+      rho_u += (double)ld_state(&U[(1 * NB + b) * ld + e]) * kp.d.phi_edge[k][cg][b];
+      rho_v += (double)ld_state(&U[(2 * NB + b) * ld + e]) * kp.d.phi_edge[k][cg][b];
     }
     if (rho_u * nx + rho_v * ny < 0.0) {
       double rho_jump = 0.0, rho_e_jump = 0.0;
@@ -542,11 +590,11 @@ __device__ __forceinline__ bool kxrcf(const KParams<P>& kp, const double* __rest
         double er = 0.0, ere = 0.0;
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-          er += ld_state(&U[(0 * NB + b) * ld + nb]) * kp.tab.phi_edge[k][NG - 1 - g][b];
-          ere += ld_state(&U[(3 * NB + b) * ld + nb]) * kp.tab.phi_edge[k][NG - 1 - g][b];
+          er += (double)ld_state(&U[(0 * NB + b) * ld + nb]) * kp.d.phi_edge[k][NG - 1 - g][b];
+          ere += (double)ld_state(&U[(3 * NB + b) * ld + nb]) * kp.d.phi_edge[k][NG - 1 - g][b];
         }
-        rho_jump += 0.5 * jd * kp.tab.edge_w[g] * (own_rho[g] - er);
-        rho_e_jump += 0.5 * jd * kp.tab.edge_w[g] * (own_rhoe[g] - ere);
+        rho_jump += 0.5 * jd * kp.d.edge_w[g] * (own_rho[g] - er);
+        rho_e_jump += 0.5 * jd * kp.d.edge_w[g] * (own_rhoe[g] - ere);
       }
       density_jump += rho_jump;
       total_energy_jump += rho_e_jump;
@@ -560,7 +608,7 @@ __device__ __forceinline__ bool kxrcf(const KParams<P>& kp, const double* __rest
 }
 
 // ------------------------------------------------------------------------------------------
-// weno, weno.rs:86-269: characteristic WENO reconstruction of element e by one warp.
+// weno, weno.rs:86-269: characteristic WENO reconstruction of element e by one warp (FP64).
 //
 // The smoothness indicator of a projected polynomial P (weno.rs:125-143, 156-174),
 //   beta = sum_{l=1..p} sum_{l1+l2=l} J^(l-1) int_e (sum_b P_b d^{l1,l2} phi_b)^2,
@@ -584,8 +632,8 @@ struct WenoScratch {
   double pol_new[3][NEQ][V::NB];
 };
 
-template <int P>
-__device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __restrict__ U, int e, int lane,
+template <int P, typename T>
+__device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __restrict__ U, int e, int lane,
                                                 WenoScratch<P>& S, const double* __restrict__ s_dref) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NQ = V::NQ, NK = V::NK;
@@ -617,10 +665,10 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
     const int i = lane + 32 * it;
     if (i >= NEQ * NB) break;
     const int v = i / NB, b = i - v * NB;
-    S.pol[0][v][b] = ld_state(&U[(v * NB + b) * ld + e]);
+    S.pol[0][v][b] = (double)ld_state(&U[(v * NB + b) * ld + e]);
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-      S.pol[k + 1][v][b] = (interior[k] && b > 0) ? ld_state(&U[(v * NB + b) * ld + nbrs[k]]) : 0.0;
+      S.pol[k + 1][v][b] = (interior[k] && b > 0) ? (double)ld_state(&U[(v * NB + b) * ld + nbrs[k]]) : 0.0;
   }
   if constexpr (P <= 2) {
 #pragma unroll
@@ -643,7 +691,7 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
     double mean[4];
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) mean[v] = S.pol[0][v][0];
-    eigenmatrix(mean, geo.x, geo.y, kp.gas, S.L[lane], S.R[lane]);
+    eigenmatrix<double>(mean, geo.x, geo.y, kp.gas, S.L[lane], S.R[lane]);
   }
   // Gram matrix of the smoothness indicator
 #pragma unroll
@@ -672,7 +720,7 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
             db = phys_deriv<NK>(rb, xx, xy, ex, ey, kk);
             dc = phys_deriv<NK>(rc, xx, xy, ex, ey, kk);
           }
-          integral += 0.5 * J * kp.tab.cell_w[q] * (db * dc);
+          integral += 0.5 * J * kp.d.cell_w[q] * (db * dc);
         }
         acc += jp * integral;
       }
@@ -754,7 +802,7 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P>& kp, double* __
       for (int k = 0; k < NEQ; ++k) sum += S.R[f][r][k] * S.pol_new[f][k][b];
       recon = recon + sum * Jn[f] * 0.5;
     }
-    U[(r * NB + b) * ld + e] = recon * inv_area;
+    U[(r * NB + b) * ld + e] = T(recon * inv_area);
   }
   __syncwarp();
   return ST_OK;
@@ -778,7 +826,7 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int nblocks)
       long long it = 0;
       while (*gen == g) {
         if (++it > (1ll << 25)) {  // ~ seconds: co-residency is guaranteed, so this is a fault
-          raise_status(ctl, ST_TIMEOUT, -1);
+          if (atomicCAS(&ctl->status, 0, ST_TIMEOUT) == 0) ctl->err_where = -1;
           s_fail = 1;
           break;
         }
@@ -808,21 +856,20 @@ constexpr int kLimiterWarps = 4;
 // troubled ready ones to a worklist; grid barrier; (B) one warp per worklist element
 // reconstructs; grid barrier.  Status word: (wave << 2) | kind, kind 1 clean, 2 limited.
 // Wave count = longest chain of increasing-index neighbours through unsettled elements: 2 on
-// the O-grid's 2-colour numbering.
-template <int P>
-__global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_constant__ KParams<P> kp,
-                                                                double* __restrict__ U,
-                                                                unsigned char* __restrict__ t0,
+// the O-grid's 2-colour numbering.  Instances never share neighbours, so one pass limits all of
+// them; elements of instances that are not stepping settle clean without evaluation.
+template <int P, typename T>
+__global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_constant__ KParams<P, T> kp,
+                                                                T* __restrict__ U, unsigned char* __restrict__ t0,
                                                                 unsigned int* __restrict__ status,
                                                                 int* __restrict__ work) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NQ = V::NQ, NK = V::NK;
   Control* ctl = kp.ctl;
-  if (!ctl->active) return;
   const MeshDev& m = kp.m;
   __shared__ WenoScratch<P> scratch[kLimiterWarps];
   __shared__ double s_dref[NQ * NB * NK];
-  for (int i = threadIdx.x; i < NQ * NB * NK; i += blockDim.x) s_dref[i] = (&kp.tab.dref[0][0][0])[i];
+  for (int i = threadIdx.x; i < NQ * NB * NK; i += blockDim.x) s_dref[i] = (&kp.d.dref[0][0][0])[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * kLimiterWarps + wib;
@@ -838,10 +885,15 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
       if (e < m.ne) {
         bool flag0 = false;
         if (wave == 1) {
-          flag0 = kxrcf<P>(kp, U, e);
+          const int inst = m.n_inst > 1 ? m.inst[e] : 0;
+          if (kp.ic[inst].active) {
+            flag0 = kxrcf<P, T>(kp, U, e);
+            pending = true;
+          } else {
+            ready = true;  // not stepping: settles clean, never read as rewritten
+          }
           t0[e] = flag0 ? 1 : 0;
           flagged_local += flag0 ? 1 : 0;
-          pending = true;
         } else {
           pending = (__ldcg(&status[e]) & 3u) == 0u;
         }
@@ -861,7 +913,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
               }
             }
           }
-          if (ready) trouble = (wave == 1) ? flag0 : (any_mod ? kxrcf<P>(kp, U, e) : (t0[e] != 0));
+          if (ready) trouble = (wave == 1) ? flag0 : (any_mod ? kxrcf<P, T>(kp, U, e) : (t0[e] != 0));
         }
         if (wave == 1 && !ready) status[e] = 0u;
         if (ready && !trouble) status[e] = ((unsigned int)wave << 2) | 1u;
@@ -894,8 +946,11 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
     // ---- phase B: reconstruct the enlisted elements, one warp each ----
     for (int i = gwarp; i < n_work; i += nwarps) {
       const int et = __ldcg(&work[i]);
-      const int rs = weno_reconstruct<P>(kp, U, et, lane, scratch[wib], s_dref);
-      if (rs != ST_OK && lane == 0) raise_status(ctl, rs, et);
+      const int rs = weno_reconstruct<P, T>(kp, U, et, lane, scratch[wib], s_dref);
+      if (rs != ST_OK && lane == 0) {
+        const int inst = m.n_inst > 1 ? m.inst[et] : 0;
+        raise_status(ctl, &kp.ic[inst], rs, et);
+      }
       __threadfence();
       if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
       ++troubled_local;
@@ -907,24 +962,24 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->waves = wave;
 }
 
-// compute_time_step, temporal_disc.rs:58-88: global minimum over elements (deterministic).
-template <int P>
-__global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KParams<P> kp,
-                                                   const double* __restrict__ U) {
+// compute_time_step, temporal_disc.rs:58-88: each instance's minimum over its elements
+// (FP64 arithmetic, deterministic: min of IEEE bit patterns of non-negative doubles).
+template <int P, typename T>
+__global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U) {
   using V = Variant<P>;
   constexpr int NB = V::NB;
-  Control* ctl = kp.ctl;
-  if (!ctl->active) return;
   const MeshDev& m = kp.m;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ec = e < m.ne ? e : m.ne - 1;
+  const int inst = m.n_inst > 1 ? m.inst[ec] : 0;
   unsigned long long bits = 0x7ff0000000000000ull;  // +inf never wins against 1e10
-  if (e < m.ne) {
+  if (e < m.ne && kp.ic[inst].active) {
     double s[NEQ];
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
       double a = 0.0;
 #pragma unroll
-      for (int b = 0; b < NB; ++b) a += ld_state(&U[(size_t)(v * NB + b) * m.ld + e]);
+      for (int b = 0; b < NB; ++b) a += (double)ld_state(&U[(size_t)(v * NB + b) * m.ld + e]);
       s[v] = a;
     }
     const double hcr = kp.gas.hcr;
@@ -934,73 +989,150 @@ __global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KPara
     const double p = (hcr - 1.0) * (s[3] - 0.5 * rho * (u * u + v * v));
     const double c = sqrt(hcr * p / rho);
     const double speed = sqrt(u * u + v * v) + c;
-    const double dt = ctl->cfl * m.hmin[e] / speed;
+    const double dt = kp.ic[inst].cfl * m.hmin[e] / speed;
     if (dt < 1.0e10) bits = (unsigned long long)__double_as_longlong(dt);  // NaN never passes
   }
+  const int inst0 = __shfl_sync(0xffffffffu, inst, 0);
+  if (__all_sync(0xffffffffu, inst == inst0)) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
-    bits = other < bits ? other : bits;
-  }
-  __shared__ unsigned long long s_min[8];
-  if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = bits;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long b = s_min[0];
-    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) b = s_min[i] < b ? s_min[i] : b;
-    atomicMin(&ctl->dt_bits, b);
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+      bits = other < bits ? other : bits;
+    }
+    if ((threadIdx.x & 31) == 0 && bits != 0x7ff0000000000000ull) atomicMin(&kp.ic[inst0].dt_bits, bits);
+  } else if (bits != 0x7ff0000000000000ull) {
+    atomicMin(&kp.ic[inst].dt_bits, bits);  // warp straddles two instances
   }
 }
 
-// Loop head of time_march (temporal_disc.rs:22): decide whether this step runs.
-__global__ void k_step_begin(Control* ctl) {
-  const bool run = ctl->status == 0 && ctl->step < ctl->final_step && ctl->t < ctl->final_time;
-  ctl->active = run ? 1 : 0;
-  ctl->dt_bits = (unsigned long long)__double_as_longlong(1.0e10);
-  ctl->troubled = 0;
+// Loop head of time_march (temporal_disc.rs:22), per instance: decide whether this step runs.
+__global__ void k_step_begin(Control* ctl, InstCtl* ic, int n_inst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) ctl->troubled = 0;
+  if (i >= n_inst) return;
+  InstCtl& c = ic[i];
+  c.active = (c.status == 0 && c.step < c.final_step && c.t < c.final_time) ? 1 : 0;
+  c.dt_bits = (unsigned long long)__double_as_longlong(1.0e10);
 }
 // temporal_disc.rs:23-26: the step's dt, clamped to reach final_time exactly.
-__global__ void k_step_dt(Control* ctl) {
-  if (!ctl->active) return;
-  double dt = __longlong_as_double((long long)ctl->dt_bits);
-  if (ctl->t + dt > ctl->final_time) dt = ctl->final_time - ctl->t;
-  ctl->dt = dt;
+__global__ void k_step_dt(InstCtl* ic, int n_inst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_inst || !ic[i].active) return;
+  double dt = __longlong_as_double((long long)ic[i].dt_bits);
+  if (ic[i].t + dt > ic[i].final_time) dt = ic[i].final_time - ic[i].t;
+  ic[i].dt = dt;
 }
 // temporal_disc.rs:32-33
-__global__ void k_step_end(Control* ctl) {
-  if (!ctl->active) return;
-  ctl->t += ctl->dt;
-  ctl->step += 1;
+__global__ void k_step_end(InstCtl* ic, int n_inst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_inst || !ic[i].active) return;
+  ic[i].t += ic[i].dt;
+  ic[i].step += 1;
 }
-// Host-driven calls (compute_residuals / apply_limiter / rk3 with a given dt).
-__global__ void k_set_active(Control* ctl, double dt, int reset_dt) {
-  ctl->active = 1;
-  if (reset_dt) {
-    ctl->dt = dt;
+// Host-driven calls (compute_residuals / apply_limiter / rk3 with a given dt): every instance
+// steps; set_dt writes the given dt into every instance.
+__global__ void k_set_active(Control* ctl, InstCtl* ic, int n_inst, double dt, int set_dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    ctl->troubled = 0;
+    ctl->t0_count = 0;
+    ctl->unknown[0] = ctl->unknown[1] = 0;
+    ctl->wl_count[0] = ctl->wl_count[1] = 0;
   }
-  ctl->dt_bits = (unsigned long long)__double_as_longlong(1.0e10);
-  ctl->troubled = 0;
-  ctl->t0_count = 0;
-  ctl->unknown[0] = ctl->unknown[1] = 0;
-  ctl->wl_count[0] = ctl->wl_count[1] = 0;
+  if (i >= n_inst) return;
+  ic[i].active = 1;
+  if (set_dt) ic[i].dt = dt;
+  ic[i].dt_bits = (unsigned long long)__double_as_longlong(1.0e10);
 }
 
-// Layout transposes between the reference's [element][variable][basis] and the SoA state.
-template <int NB>
-__global__ void k_aos_to_soa(const double* __restrict__ src, double* __restrict__ dst, int ne, int ld) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)ne * NEQ * NB) return;
-  const int e = (int)(i / (NEQ * NB));
-  const int c = (int)(i - (long long)e * NEQ * NB);
-  dst[(size_t)c * ld + e] = src[i];
+
+// FP64 diagnostics of each instance, one block per instance (deterministic: fixed per-thread
+// order, fixed tree): out[i] = { integral of rho, rho u, rho v, rho E over the mesh (mode-0
+// coefficient times the element area), pressure force (Fx, Fy) exerted on the wall patches
+// (sum over wall edges and Gauss points of w p n |e|/2 with the element's outward normal,
+// i.e. the force on the body), sum of squares of the density residual's modal coefficients
+// (from R, when given), number of elements }.  Not part of the reference, which computes no
+// forces or norms.
+template <int P, typename T>
+__global__ void __launch_bounds__(256) k_diagnostics(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U,
+                                                     const T* __restrict__ R, const int* __restrict__ elem_off,
+                                                     const int* __restrict__ bslot_off, double* __restrict__ out) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NG = V::NG, NQ = V::NQ;
+  const MeshDev& m = kp.m;
+  const int inst = blockIdx.x;
+  const int e0 = elem_off[inst], e1 = elem_off[inst + 1];
+  const int b0 = bslot_off[inst], b1 = bslot_off[inst + 1];
+  double wsum = 0.0;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) wsum += kp.d.cell_w[q];
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const double area = 0.5 * m.jac[e] * wsum;
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) acc[v] += area * (double)U[(size_t)(v * NB) * m.ld + e];
+    if (R) {
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const double r = (double)R[(size_t)b * m.ld + e];
+        acc[6] += r * r;
+      }
+    }
+  }
+  for (int sb = b0 + threadIdx.x; sb < b1; sb += blockDim.x) {
+    const int info = m.be_info[sb];
+    if (((info >> 2) & 1) != 0) continue;  // far field
+    const int e = m.be_elem[sb], k = info & 3;
+    const double4 geo = m.be_geo[sb];
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+      double q[4];
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) {
+        double a = 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) a += (double)U[(size_t)(v * NB + b) * m.ld + e] * kp.d.phi_edge[k][g][b];
+        q[v] = a;
+      }
+      const double p = kp.gas.gm1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+      acc[4] += kp.d.edge_w[g] * p * geo.x * geo.z;
+      acc[5] += kp.d.edge_w[g] * p * geo.y * geo.z;
+    }
+  }
+  __shared__ double red[7][256];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) red[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int k = 0; k < 7; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k) out[inst * 8 + k] = red[k][0];
+    out[inst * 8 + 7] = (double)(e1 - e0);
+  }
 }
-template <int NB>
-__global__ void k_soa_to_aos(const double* __restrict__ src, double* __restrict__ dst, int ne, int ld) {
+
+// Layout transposes between the reference's [element][variable][basis] (FP64) and the SoA
+// state in the storage type.
+template <int NB, typename T>
+__global__ void k_aos_to_soa(const double* __restrict__ src, T* __restrict__ dst, int ne, int ld) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= (long long)ne * NEQ * NB) return;
   const int e = (int)(i / (NEQ * NB));
   const int c = (int)(i - (long long)e * NEQ * NB);
-  dst[i] = src[(size_t)c * ld + e];
+  dst[(size_t)c * ld + e] = T(src[i]);
+}
+template <int NB, typename T>
+__global__ void k_soa_to_aos(const T* __restrict__ src, double* __restrict__ dst, int ne, int ld) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)ne * NEQ * NB) return;
+  const int e = (int)(i / (NEQ * NB));
+  const int c = (int)(i - (long long)e * NEQ * NB);
+  dst[i] = (double)src[(size_t)c * ld + e];
 }
 
 }  // namespace dgm

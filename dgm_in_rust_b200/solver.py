@@ -37,6 +37,8 @@ __all__ = [
     "Solver",
     "reference_cfl",
     "initial_state",
+    "Batch",
+    "forces_to_coefficients",
 ]
 
 
@@ -131,12 +133,62 @@ def _check_state(a: np.ndarray, ne: int, nb: int, name: str) -> None:
         raise ValueError(f"{name} must be a C-contiguous float64 array of shape ({ne}, 4, {nb})")
 
 
+def _mesh_desc(m: Mesh, keep: list) -> "_native.MeshDesc":
+    def f64(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return _native.dptr(a)
+
+    def i64(a):
+        a = np.ascontiguousarray(a, dtype=np.int64)
+        keep.append(a)
+        return _native.iptr(a)
+
+    def i32(a):
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        keep.append(a)
+        return _native.i32ptr(a)
+
+    return _native.MeshDesc(
+        n_vertices=m.vertices.shape[0], n_elements=m.n_elements, n_edges=m.n_edges,
+        n_patches=m.patch_type.shape[0], vertex_xy=f64(m.vertices), elem_vertices=i64(m.elem_vertices),
+        elem_edges=i64(m.elem_edges), elem_neighbours=i64(m.elem_neighbours),
+        elem_jacob_det=f64(m.elem_jacob_det), elem_circumradius=f64(m.elem_circumradius),
+        elem_minimum_height=f64(m.elem_minimum_height), edge_elements=i64(m.edge_elements),
+        edge_vertices=i64(m.edge_vertices), edge_in_cell=i64(m.edge_in_cell),
+        edge_jacob_det=f64(m.edge_jacob_det), edge_normal=f64(m.edge_normal), edge_patch=i64(m.edge_patch),
+        patch_type=i32(m.patch_type), patch_quantity=f64(m.patch_quantity),
+        n_internal_edges=m.internal_edge_indices.shape[0], internal_edges=i64(m.internal_edge_indices),
+        n_boundary_elements=m.boundary_element_indices.shape[0],
+        boundary_elements=i64(m.boundary_element_indices))
+
+
+def _tables_desc(basis: DubinerBasis, g: GaussPoints, keep: list) -> "_native.TablesDesc":
+    def f64(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return _native.dptr(a)
+
+    return _native.TablesDesc(
+        order=basis.order, n_basis=basis.dof, n_cell_gp=g.cell_gp_number, n_edge_gp=g.edge_gp_number,
+        n_deriv_keys=basis.nkeys, _pad=0, cell_weights=f64(g.cell_weights), edge_weights=f64(g.edge_weights),
+        phi_cell=f64(basis.phis_cell_gps), phi_edge=f64(basis.phis_edge_gps),
+        dphi_cell_ref=f64(basis.dphis_cell_gps), mass_diag=f64(basis.mass_mat_diag))
+
+
+PRECISIONS = {"fp64": 0, "fp32": 1}
+
+
 class SpatialDisc:
-    """GPU-resident SpatialDisc (src/spatial_disc.rs:17-25).  Owns the device context."""
+    """GPU-resident SpatialDisc (src/spatial_disc.rs:17-25).  Owns the device context.
+
+    ``precision="fp64"`` reproduces the reference's arithmetic; ``"fp32"`` keeps the state and
+    the bulk arithmetic in FP32 with the limiter, positivity checks and time step in FP64.
+    """
 
     def __init__(self, mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints,
                  flow_param: FlowParameters, mesh_param: MeshParameters, solver_param: SolverParameters,
-                 limiter: bool = True, device: int = 0):
+                 limiter: bool = True, device: int = 0, precision: str = "fp64"):
         self.mesh = mesh
         self.basis = basis
         self.gauss_points = gauss_points
@@ -144,52 +196,21 @@ class SpatialDisc:
         self.mesh_param = mesh_param
         self.solver_param = solver_param
         self.limiter = bool(limiter)
+        self.precision = precision
         L = _native.lib()
-        keep = []
-
-        def f64(a):
-            a = np.ascontiguousarray(a, dtype=np.float64)
-            keep.append(a)
-            return _native.dptr(a)
-
-        def i64(a):
-            a = np.ascontiguousarray(a, dtype=np.int64)
-            keep.append(a)
-            return _native.iptr(a)
-
-        def i32(a):
-            a = np.ascontiguousarray(a, dtype=np.int32)
-            keep.append(a)
-            return _native.i32ptr(a)
-
-        m = mesh
-        md = _native.MeshDesc(
-            n_vertices=m.vertices.shape[0], n_elements=m.n_elements, n_edges=m.n_edges,
-            n_patches=m.patch_type.shape[0], vertex_xy=f64(m.vertices), elem_vertices=i64(m.elem_vertices),
-            elem_edges=i64(m.elem_edges), elem_neighbours=i64(m.elem_neighbours),
-            elem_jacob_det=f64(m.elem_jacob_det), elem_circumradius=f64(m.elem_circumradius),
-            elem_minimum_height=f64(m.elem_minimum_height), edge_elements=i64(m.edge_elements),
-            edge_vertices=i64(m.edge_vertices), edge_in_cell=i64(m.edge_in_cell),
-            edge_jacob_det=f64(m.edge_jacob_det), edge_normal=f64(m.edge_normal), edge_patch=i64(m.edge_patch),
-            patch_type=i32(m.patch_type), patch_quantity=f64(m.patch_quantity),
-            n_internal_edges=m.internal_edge_indices.shape[0], internal_edges=i64(m.internal_edge_indices),
-            n_boundary_elements=m.boundary_element_indices.shape[0],
-            boundary_elements=i64(m.boundary_element_indices))
-        td = _native.TablesDesc(
-            order=basis.order, n_basis=basis.dof, n_cell_gp=gauss_points.cell_gp_number,
-            n_edge_gp=gauss_points.edge_gp_number, n_deriv_keys=basis.nkeys, _pad=0,
-            cell_weights=f64(gauss_points.cell_weights), edge_weights=f64(gauss_points.edge_weights),
-            phi_cell=f64(basis.phis_cell_gps), phi_edge=f64(basis.phis_edge_gps),
-            dphi_cell_ref=f64(basis.dphis_cell_gps), mass_diag=f64(basis.mass_mat_diag))
+        keep: list = []
+        md = _mesh_desc(mesh, keep)
+        td = _tables_desc(basis, gauss_points, keep)
         pr = _native.Params(hcr=flow_param.hcr, cfl=solver_param.cfl, final_time=solver_param.final_time,
-                            final_step=solver_param.final_step, limiter=1 if limiter else 0, device=device)
+                            final_step=solver_param.final_step, limiter=1 if limiter else 0, device=device,
+                            precision=PRECISIONS[precision], _reserved=0)
         status = ctypes.c_int32(0)
         ctx = L.dgm_create(ctypes.byref(md), ctypes.byref(td), ctypes.byref(pr), ctypes.byref(status))
         if not ctx:
             raise DgmError(status.value, what="dgm_create")
         self._ctx = ctypes.c_void_p(ctx)
         self._lib = L
-        self.ne = m.n_elements
+        self.ne = mesh.n_elements
         self.nb = basis.dof
 
     # ---- plumbing ----
@@ -230,6 +251,14 @@ class SpatialDisc:
         n = ctypes.c_int64(0)
         self._check(self._lib.dgm_apply_limiter(self._ctx, _native.dptr(solutions), ctypes.byref(n)), "apply_limiter")
         return int(n.value)
+
+    def diagnostics(self, use_residual: bool = False) -> np.ndarray:
+        """[8]: integrals of rho, rho u, rho v, rho E; wall force Fx, Fy; sum of squared density
+        residual coefficients (last residual written); element count.  FP64, deterministic."""
+        out = np.zeros((1, 8))
+        self._check(self._lib.dgm_diagnostics(self._ctx, 1 if use_residual else 0, _native.dptr(out)),
+                    "diagnostics")
+        return out[0]
 
     def limiter_stats(self) -> tuple[int, int]:
         t, w = ctypes.c_int64(0), ctypes.c_int32(0)
@@ -292,8 +321,9 @@ class TemperalDisc:
     def download(self, solutions: np.ndarray) -> None:
         self._sd._check(self._sd._lib.dgm_download_solutions(self._sd._ctx, _native.dptr(solutions)), "download")
 
-    def advance(self, n_steps: int) -> None:
-        self._sd._check(self._sd._lib.dgm_advance(self._sd._ctx, int(n_steps)), "advance")
+    def advance(self, n_steps: int, with_residual: bool = False) -> None:
+        f = self._sd._lib.dgm_advance_with_residual if with_residual else self._sd._lib.dgm_advance
+        self._sd._check(f(self._sd._ctx, int(n_steps)), "advance")
 
     def synchronize(self) -> None:
         self._sd._check(self._sd._lib.dgm_synchronize(self._sd._ctx), "synchronize")
@@ -303,7 +333,7 @@ class Solver:
     """Solver (src/solver.rs:32-82): owns residuals/solutions and drives the time march."""
 
     def __init__(self, mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints, flow_param: FlowParameters,
-                 solver_param: SolverParameters, limiter: bool = True, device: int = 0):
+                 solver_param: SolverParameters, limiter: bool = True, device: int = 0, precision: str = "fp64"):
         self.mesh = mesh
         self.basis = basis
         self.gauss_points = gauss_points
@@ -311,7 +341,7 @@ class Solver:
         self.solver_param = solver_param
         self.mesh_param = MeshParameters.of(mesh)
         self.spatial_disc = SpatialDisc(mesh, basis, gauss_points, flow_param, self.mesh_param, solver_param,
-                                        limiter=limiter, device=device)
+                                        limiter=limiter, device=device, precision=precision)
         self.temporal_disc = TemperalDisc(self.spatial_disc)
         self.residuals = self.spatial_disc.new_state()
         self.solutions = self.spatial_disc.new_state()
@@ -327,11 +357,109 @@ class Solver:
 
 
 def build_solver(mesh: Mesh, order: int, hcr: float, cfl: float, final_time: float, final_step: int,
-                 limiter: bool = True, device: int = 0) -> Solver:
+                 limiter: bool = True, device: int = 0, precision: str = "fp64") -> Solver:
     """Convenience: tables for ``order`` with the default rules, then a Solver."""
     nq, ng = default_rules(order)
     g = GaussPoints(nq, ng)
     b = DubinerBasis(order, g)
     sp = SolverParameters(cfl=cfl, final_time=final_time, final_step=final_step, order_of_polynomials=order,
                           number_of_cell_gp=nq, number_of_edge_gp=ng)
-    return Solver(mesh, b, g, FlowParameters(hcr=hcr), sp, limiter=limiter, device=device)
+    return Solver(mesh, b, g, FlowParameters(hcr=hcr), sp, limiter=limiter, device=device, precision=precision)
+
+
+def forces_to_coefficients(fx: float, fy: float, aoa_deg: float, rho: float, speed: float, chord: float = 1.0):
+    """Lift and drag coefficients from the pressure force on the body (wind axes at ``aoa_deg``)."""
+    a = aoa_deg * (math.pi / 180.0)
+    q = 0.5 * rho * speed * speed * chord
+    lift = -fx * math.sin(a) + fy * math.cos(a)
+    drag = fx * math.cos(a) + fy * math.sin(a)
+    return lift / q, drag / q
+
+
+class Batch:
+    """Many independent meshes advanced together: one launch per kernel of a step covers all of
+    them (a disconnected union mesh on the device), each with its own time step, clock, loop
+    bounds and status.  All share one polynomial order, hcr, precision and limiter setting.
+    No counterpart in the reference (one mesh per run)."""
+
+    def __init__(self, meshes: list, order: int, hcr: float, cfls, final_times, final_steps,
+                 limiter: bool = True, device: int = 0, precision: str = "fp64"):
+        nq, ng = default_rules(order)
+        self.gauss_points = GaussPoints(nq, ng)
+        self.basis = DubinerBasis(order, self.gauss_points)
+        self.meshes = list(meshes)
+        n = len(self.meshes)
+        keep: list = []
+        mds = (_native.MeshDesc * n)(*[_mesh_desc(m, keep) for m in self.meshes])
+        td = _tables_desc(self.basis, self.gauss_points, keep)
+        prs = (_native.Params * n)(*[
+            _native.Params(hcr=hcr, cfl=float(cfls[i]), final_time=float(final_times[i]),
+                           final_step=int(final_steps[i]), limiter=1 if limiter else 0, device=device,
+                           precision=PRECISIONS[precision], _reserved=0) for i in range(n)])
+        L = _native.lib()
+        status = ctypes.c_int32(0)
+        ctx = L.dgm_create_batch(n, mds, ctypes.byref(td), prs, ctypes.byref(status))
+        if not ctx:
+            raise DgmError(status.value, what="dgm_create_batch")
+        self._ctx = ctypes.c_void_p(ctx)
+        self._lib = L
+        self.n = n
+        self.nb = self.basis.dof
+        self.precision = precision
+
+    def _check(self, st: int, what: str) -> None:
+        if st != 0:
+            raise DgmError(st, int(self._lib.dgm_error_location(self._ctx)), what)
+
+    @property
+    def ctx(self):
+        return self._ctx
+
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            self._lib.dgm_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, i: int, solutions: np.ndarray) -> None:
+        _check_state(solutions, self.meshes[i].n_elements, self.nb, "solutions")
+        self._check(self._lib.dgm_instance_upload(self._ctx, i, _native.dptr(solutions)), "upload")
+
+    def download(self, i: int) -> np.ndarray:
+        out = np.zeros((self.meshes[i].n_elements, 4, self.nb))
+        self._check(self._lib.dgm_instance_download(self._ctx, i, _native.dptr(out)), "download")
+        return out
+
+    def advance(self, n_steps: int, with_residual: bool = False) -> None:
+        f = self._lib.dgm_advance_with_residual if with_residual else self._lib.dgm_advance
+        self._check(f(self._ctx, int(n_steps)), "advance")
+
+    def synchronize(self) -> int:
+        """Wait for the device; returns the first device status (0 = ok) without raising, since
+        a failing instance stops alone (see state())."""
+        return int(self._lib.dgm_synchronize(self._ctx))
+
+    def state(self, i: int):
+        """(current_time, current_step, status, error_location) of instance i."""
+        t, s, st, w = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int64()
+        self._lib.dgm_instance_state(self._ctx, i, ctypes.byref(t), ctypes.byref(s), ctypes.byref(st),
+                                     ctypes.byref(w))
+        return float(t.value), int(s.value), int(st.value), int(w.value)
+
+    def set_instance(self, i: int, current_time: float, current_step: int, final_time: float,
+                     final_step: int) -> None:
+        self._check(self._lib.dgm_instance_set(self._ctx, i, float(current_time), int(current_step),
+                                               float(final_time), int(final_step)), "set_instance")
+
+    def diagnostics(self, use_residual: bool = False) -> np.ndarray:
+        """[n, 8]: integrals of rho, rho u, rho v, rho E; wall force Fx, Fy; sum of squared density
+        residual coefficients; element count (FP64 on the device)."""
+        out = np.zeros((self.n, 8))
+        self._check(self._lib.dgm_diagnostics(self._ctx, 1 if use_residual else 0, _native.dptr(out)),
+                    "diagnostics")
+        return out

@@ -98,6 +98,11 @@ typedef struct dgm_params {
   int64_t final_step;               /* SolverParameters::final_step                         */
   int32_t limiter;                  /* 1 = WENO/KXRCF limiter after each stage (reference), 0 = off */
   int32_t device;                   /* CUDA device ordinal                                  */
+  /* 0 = FP64 throughout (the reference's arithmetic); 1 = FP32 state, contractions, fluxes and
+   * stage updates, with the limiter, the HLLC positivity checks, the time step and the
+   * diagnostics kept in FP64.  No counterpart in the reference (FP64 only). */
+  int32_t precision;
+  int32_t _reserved;
 } dgm_params;
 
 typedef struct dgm_ctx dgm_ctx;
@@ -169,6 +174,41 @@ int32_t dgm_launch_phase(dgm_ctx* ctx, int32_t phase);
 /* Launches of that kernel, and of all kernels, per time-march step. */
 int32_t dgm_phase_launches_per_step(dgm_ctx* ctx, int32_t phase);
 int32_t dgm_launches_per_step(dgm_ctx* ctx);
+
+/* ---- batches: many independent meshes advanced by the same launches ------------------------
+ * No counterpart in the reference, which solves one mesh per run.  A batch context holds the
+ * n meshes as one disconnected union mesh; every launch of the step covers all of them, and
+ * each instance keeps its own time step, clock, loop bounds and error status (an instance
+ * that stops -- final step/time reached or an error raised -- is left untouched by later
+ * steps while the others continue).  All instances share the tables (one polynomial order)
+ * and hcr; params[i] supplies instance i's cfl / final_time / final_step, and limiter, device
+ * and precision are taken from params[0]. */
+dgm_ctx* dgm_create_batch(int32_t n_instances, const dgm_mesh_desc* meshes, const dgm_tables_desc* tables,
+                          const dgm_params* params, int32_t* status);
+int32_t dgm_instance_count(dgm_ctx* ctx);
+/* State of instance i in the reference layout, host <-> device-resident state. */
+int32_t dgm_instance_upload(dgm_ctx* ctx, int32_t i, const double* solutions);
+int32_t dgm_instance_download(dgm_ctx* ctx, int32_t i, double* solutions);
+/* The last residual written by dgm_advance_with_residual / dgm_time_march for instance i. */
+int32_t dgm_instance_download_residual(dgm_ctx* ctx, int32_t i, double* residuals);
+/* Clock and status of instance i as of the last dgm_synchronize. */
+int32_t dgm_instance_state(dgm_ctx* ctx, int32_t i, double* current_time, int64_t* current_step,
+                           int32_t* status, int64_t* error_location);
+/* Reset instance i's clock, loop bounds and status (applied at the next advance). */
+int32_t dgm_instance_set(dgm_ctx* ctx, int32_t i, double current_time, int64_t current_step,
+                         double final_time, int64_t final_step);
+/* As dgm_advance, additionally writing each step's third-stage residual (for residual norms). */
+int32_t dgm_advance_with_residual(dgm_ctx* ctx, int64_t n_steps);
+
+/* FP64 diagnostics of every instance (deterministic reductions), out[8 * i + k]:
+ * k = 0..3 integrals of rho, rho u, rho v, rho E over the mesh; 4, 5 pressure force (Fx, Fy)
+ * on the wall patches (the force on the body); 6 sum of squares of the density residual's
+ * modal coefficients of the last residual written (0 unless use_residual); 7 element count.
+ * No counterpart in the reference (it computes no forces or norms). */
+int32_t dgm_diagnostics(dgm_ctx* ctx, int32_t use_residual, double* out);
+
+/* The context's precision mode (dgm_params::precision). */
+int32_t dgm_precision(dgm_ctx* ctx);
 
 /* Edge (HLLC failures) or element (limiter failures) index flagged by the last error. */
 int64_t dgm_error_location(dgm_ctx* ctx);

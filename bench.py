@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the many-instance measurement")
+    ap.add_argument("--batched-instances", type=int, default=256)
+    ap.add_argument("--batched-steps", type=int, default=20)
     return ap.parse_args()
 
 
@@ -218,6 +221,98 @@ def load_traffic():
     return out
 
 
+# ------------------------------------------------------------------------------------------
+# Batched workload: many uneven instances per launch, FP32 vs FP64, vs one at a time
+# ------------------------------------------------------------------------------------------
+def run_batched(args, local):
+    """256 seeded instances (Ni uniform on {32..256}, Nj = Ni/2, Mach U[0.3,0.85], AoA U[-4,6] deg,
+    p in {1,2}): DOF-stage updates/s of (a) FP32 batches, (b) FP64 batches -- one batch context
+    per order, both groups on their own streams -- and (c) FP64 one instance at a time on a
+    DOF-weighted sample of 32 instances.  Inputs exceed the L2 (no flush needed); device time by
+    CUDA events."""
+    import torch
+    from dgm_in_rust_b200 import Batch, build_solver, initial_state
+    from dgm_in_rust_b200.workloads import batch_instances, instance_mesh
+    seed = 2024
+    insts = batch_instances(args.batched_instances, seed=seed)
+    t_setup = time.perf_counter()
+    built = [(inst, *instance_mesh(inst)) for inst in insts]
+    groups = {p: [b for b in built if b[0].order == p] for p in (1, 2)}
+    K, W = args.batched_steps, 3
+    res = {"workload": f"{len(insts)} NACA 0012 O-grids, Ni uniform on {{32,...,256}}, Nj = Ni/2, "
+                       f"Mach U[0.3,0.85], AoA U[-4,6] deg, p in {{1,2}} (numpy default_rng({seed})), "
+                       f"limiter on, CFL 0.1",
+           "instances": len(insts), "elements": int(sum(i.elements for i in insts)),
+           "dof": int(sum(i.dofs for i in insts)), "steps": K, "warmup": W}
+
+    def batched(precision):
+        batches = []
+        for p, items in groups.items():
+            if not items:
+                continue
+            b = Batch([m for _, m, _ in items], p, HCR, [CFL] * len(items), [1.0e30] * len(items),
+                      [10 ** 12] * len(items), limiter=True, device=local, precision=precision)
+            for i, (_, m, init) in enumerate(items):
+                b.upload(i, initial_state(m, b.basis, b.gauss_points, HCR, init))
+            batches.append(b)
+        for b in batches:
+            b.advance(W)
+        for b in batches:
+            b.synchronize()
+        streams = [torch.cuda.ExternalStream(b._lib.dgm_stream(b.ctx)) for b in batches]
+        start = torch.cuda.Event(enable_timing=True)
+        ends = [torch.cuda.Event(enable_timing=True) for _ in batches]
+        start.record(streams[0])
+        for st in streams[1:]:
+            st.wait_event(start)
+        for b in batches:
+            b.advance(K)
+        for st, ev in zip(streams, ends):
+            ev.record(st)
+        for b in batches:
+            st_code = b.synchronize()
+            if st_code != 0:
+                raise SystemExit(f"batched run failed with status {st_code}")
+        ms = max(start.elapsed_time(ev) for ev in ends)
+        dev_bytes = sum(int(b._lib.dgm_device_bytes(b.ctx)) for b in batches)
+        for b in batches:
+            b.close()
+        return res["dof"] * 3 * K / (ms * 1e-3), ms / K, dev_bytes
+
+    v32, ms32, bytes32 = batched("fp32")
+    v64, ms64, bytes64 = batched("fp64")
+    # one at a time, FP64: a DOF-weighted sample (every 8th instance in DOF order)
+    order = sorted(range(len(built)), key=lambda k: built[k][0].dofs)
+    sample = [built[k] for k in order[::max(1, len(built) // 32)]]
+    tot_ms, tot_dof = 0.0, 0
+    for inst, m, init in sample:
+        s = build_solver(m, inst.order, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, device=local)
+        td = s.temporal_disc
+        td.upload(initial_state(m, s.basis, s.gauss_points, HCR, init))
+        td.advance(W)
+        td.synchronize()
+        st = torch.cuda.ExternalStream(s.spatial_disc._lib.dgm_stream(s.spatial_disc.ctx))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        td.advance(K)
+        b.record(st)
+        td.synchronize()
+        tot_ms += a.elapsed_time(b)
+        tot_dof += inst.dofs
+        s.close()
+    v_single = tot_dof * 3 * K / (tot_ms * 1e-3)
+    res.update({
+        "fp32_batched": v32, "fp64_batched": v64, "fp64_one_at_a_time": v_single,
+        "ms_per_step_fp32_batched": ms32, "ms_per_step_fp64_batched": ms64,
+        "device_bytes_fp32": bytes32, "device_bytes_fp64": bytes64,
+        "speedup_fp32_batched_vs_fp64_one_at_a_time": v32 / v_single,
+        "speedup_fp32_batched_vs_fp64_batched": v32 / v64,
+        "one_at_a_time_sample": f"{len(sample)} instances, every {max(1, len(built) // 32)}th by DOF count",
+        "setup_s": time.perf_counter() - t_setup,
+    })
+    return res
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_env()
@@ -364,6 +459,8 @@ def run_ours(args):
         "limiter": {"troubled_cells_last_step": troubled, "waves_last_pass": waves},
         "clocks": sampler.summary(),
     }
+    if world == 1 and not args.no_batched:
+        line["batched"] = run_batched(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         v, done, el = time_cpu(raw, 1000, 1, threads, budget_s=12.0)

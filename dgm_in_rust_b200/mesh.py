@@ -34,6 +34,7 @@ __all__ = [
     "GmshParser",
     "process_mesh",
     "naca0012_ogrid",
+    "radial_distribution",
     "write_gmsh",
     "freestream_quantity",
 ]
@@ -368,8 +369,33 @@ def _naca0012_half_thickness(x: np.ndarray) -> np.ndarray:
     return 0.6 * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
 
 
+def radial_distribution(nj: int, stretch: float = 1.15, radius: float = 20.0,
+                        min_spacing: float = 1.0e-8) -> np.ndarray:
+    """Normalised radial stations s_0 = 0 < ... < s_nj = 1, geometric with ratio ``stretch``.
+
+    When that ratio would make the first spacing (s_1 * radius) smaller than ``min_spacing``
+    chords -- from nj of about 130 up at ratio 1.15, e.g. 1e-31 chords at nj = 512, below the
+    FP64 resolution of the vertex coordinates -- the ratio is lowered (bisection) until the first
+    spacing equals ``min_spacing``."""
+    def first(r):
+        return (r - 1.0) / (r ** nj - 1.0) if r != 1.0 else 1.0 / nj
+    r = stretch
+    if stretch > 1.0 and first(stretch) * radius < min_spacing:
+        lo, hi = 1.0 + 1e-12, stretch
+        for _ in range(200):
+            mid = 0.5 * (lo + hi)
+            if first(mid) * radius < min_spacing:
+                hi = mid
+            else:
+                lo = mid
+        r = lo
+    if r == 1.0:
+        return np.arange(nj + 1) / nj
+    return (r ** np.arange(nj + 1) - 1.0) / (r ** nj - 1.0)
+
+
 def naca0012_ogrid(ni: int, nj: int, radius: float = 20.0, stretch: float = 1.15,
-                   order: str = "colored") -> RawMesh:
+                   order: str = "colored", min_spacing: float = 1.0e-8) -> RawMesh:
     """NACA 0012 O-grid: ``ni`` quads around the airfoil, ``nj`` quads outward.
 
     Surface points use cosine clustering (x = (1 + cos th)/2, th = 2 pi i/ni, upper surface
@@ -394,10 +420,7 @@ def naca0012_ogrid(ni: int, nj: int, radius: float = 20.0, stretch: float = 1.15
     xs[0], ys[0] = 1.0, 0.0
     ox = 0.5 + radius * np.cos(th)
     oy = radius * np.sin(th)
-    if stretch == 1.0:
-        sj = np.arange(nj + 1) / nj
-    else:
-        sj = (stretch ** np.arange(nj + 1) - 1.0) / (stretch ** nj - 1.0)
+    sj = radial_distribution(nj, stretch, radius, min_spacing)
     X = (1.0 - sj)[:, None] * xs[None, :] + sj[:, None] * ox[None, :]
     Y = (1.0 - sj)[:, None] * ys[None, :] + sj[:, None] * oy[None, :]
     vertices = np.stack([X.reshape(-1), Y.reshape(-1)], axis=1)  # node (i, j) = j * ni + i

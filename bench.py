@@ -50,6 +50,13 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the many-instance measurement")
     ap.add_argument("--batched-instances", type=int, default=256)
     ap.add_argument("--batched-steps", type=int, default=20)
+    ap.add_argument("--no-serving", action="store_true", help="skip the request-stream measurement")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 p=3 measurement")
+    ap.add_argument("--precision-steps", type=int, default=500)
+    ap.add_argument("--serving-requests", type=int, default=48)
+    ap.add_argument("--serving-rate", type=float, default=20.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serving-max-steps", type=int, default=400)
+    ap.add_argument("--serving-budget-gib", type=float, default=16.0)
     return ap.parse_args()
 
 
@@ -231,7 +238,7 @@ def run_batched(args, local):
     DOF-weighted sample of 32 instances.  Inputs exceed the L2 (no flush needed); device time by
     CUDA events."""
     import torch
-    from dgm_in_rust_b200 import Batch, build_solver, initial_state
+    from dgm_in_rust_b200 import Batch, build_solver, forces_to_coefficients
     from dgm_in_rust_b200.workloads import batch_instances, instance_mesh
     seed = 2024
     insts = batch_instances(args.batched_instances, seed=seed)
@@ -253,7 +260,7 @@ def run_batched(args, local):
             b = Batch([m for _, m, _ in items], p, HCR, [CFL] * len(items), [1.0e30] * len(items),
                       [10 ** 12] * len(items), limiter=True, device=local, precision=precision)
             for i, (_, m, init) in enumerate(items):
-                b.upload(i, initial_state(m, b.basis, b.gauss_points, HCR, init))
+                b.set_initial(i, init)
             batches.append(b)
         for b in batches:
             b.advance(W)
@@ -275,12 +282,29 @@ def run_batched(args, local):
                 raise SystemExit(f"batched run failed with status {st_code}")
         ms = max(start.elapsed_time(ev) for ev in ends)
         dev_bytes = sum(int(b._lib.dgm_device_bytes(b.ctx)) for b in batches)
+        # end states for the accuracy comparison: C_L / C_D of every instance, the density field
+        # of every 8th instance of each group
+        acc = {}
+        for (p, items), b in zip([(p, it) for p, it in groups.items() if it], batches):
+            d = b.diagnostics()
+            for i, (inst, m, _) in enumerate(items):
+                cl, cd = forces_to_coefficients(d[i, 4], d[i, 5], inst.aoa, 1.0, inst.mach)
+                rho = b.download(i)[:, 0].copy() if i % 8 == 0 else None
+                w = (b.basis.mass_mat_diag[None, :] * (0.5 * m.elem_jacob_det)[:, None]) if rho is not None else None
+                acc[(p, i)] = (cl, cd, rho, w)
         for b in batches:
             b.close()
-        return res["dof"] * 3 * K / (ms * 1e-3), ms / K, dev_bytes
+        return res["dof"] * 3 * K / (ms * 1e-3), ms / K, dev_bytes, acc
 
-    v32, ms32, bytes32 = batched("fp32")
-    v64, ms64, bytes64 = batched("fp64")
+    v32, ms32, bytes32, acc32 = batched("fp32")
+    v64, ms64, bytes64, acc64 = batched("fp64")
+    dcl = [abs(acc32[k][0] - acc64[k][0]) for k in acc64]
+    dcd = [abs(acc32[k][1] - acc64[k][1]) for k in acc64]
+    errs = [field_rel_l2(acc32[k][2], acc64[k][2], acc64[k][3]) for k in acc64 if acc64[k][2] is not None]
+    res["fp32_vs_fp64_after_steps"] = {
+        "steps": W + K, "max_abs_delta_cl": max(dcl), "max_abs_delta_cd": max(dcd),
+        "density_rel_l2_max": max(errs), "density_rel_l2_median": float(np.median(errs)),
+        "density_sample": f"{len(errs)} instances (every 8th of each order group)"}
     # one at a time, FP64: a DOF-weighted sample (every 8th instance in DOF order)
     order = sorted(range(len(built)), key=lambda k: built[k][0].dofs)
     sample = [built[k] for k in order[::max(1, len(built) // 32)]]
@@ -288,7 +312,7 @@ def run_batched(args, local):
     for inst, m, init in sample:
         s = build_solver(m, inst.order, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, device=local)
         td = s.temporal_disc
-        td.upload(initial_state(m, s.basis, s.gauss_points, HCR, init))
+        td.set_initial_on_device(init)
         td.advance(W)
         td.synchronize()
         st = torch.cuda.ExternalStream(s.spatial_disc._lib.dgm_stream(s.spatial_disc.ctx))
@@ -311,6 +335,105 @@ def run_batched(args, local):
         "setup_s": time.perf_counter() - t_setup,
     })
     return res
+
+
+# ------------------------------------------------------------------------------------------
+# Precision: FP32 vs FP64 on the large p = 3 workload
+# ------------------------------------------------------------------------------------------
+def field_rel_l2(a, b, w):
+    """Relative L2 error of the fields whose modal coefficients are a, b ([element][mode]); w =
+    mass_b * J_e / 2, so sum(w * c^2) is the integral of the square (orthogonal basis)."""
+    return float(np.sqrt(np.sum(w * (a - b) ** 2) / np.sum(w * b * b)))
+
+
+def run_precision(args, local):
+    """NACA 0012 O-grid 1024 x 512 (1,048,576 triangles), p = 3 (10 modes, 12-point triangle /
+    4-point edge rules), M = 0.7, AoA = 2 deg, free-stream start, limiter on, CFL 0.1: the same
+    steps in FP64 and in FP32 (limiter, positivity checks, time step and reductions in FP64).
+    Reports relative L2 errors of the FP32 fields against FP64, C_L / C_D of both, and each
+    mode's DOF-stage updates/s (CUDA events on the library stream; the state exceeds L2)."""
+    import torch
+    from dgm_in_rust_b200 import build_solver, forces_to_coefficients
+    from dgm_in_rust_b200.workloads import Instance, instance_mesh
+    inst = Instance(1024, 512, 0.7, 2.0, 3)
+    K = args.precision_steps
+    mesh, init = instance_mesh(inst)
+    res = {"workload": "naca0012_ogrid_1024x512_p3: 1,048,576 triangles, 10 modes, M=0.7, AoA=2deg, limiter on, "
+                       f"CFL 0.1, free-stream start, {K} steps", "steps": K}
+    out = {}
+    for prec in ("fp64", "fp32"):
+        s = build_solver(mesh, 3, HCR, CFL, 1.0e30, K, limiter=True, device=local, precision=prec)
+        td, sd = s.temporal_disc, s.spatial_disc
+        td.set_initial_on_device(init)
+        st = torch.cuda.ExternalStream(sd._lib.dgm_stream(sd.ctx))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        td.advance(K)
+        b.record(st)
+        td.synchronize()
+        ms = a.elapsed_time(b)
+        U = sd.new_state()
+        td.download(U)
+        d = sd.diagnostics()
+        cl, cd = forces_to_coefficients(d[4], d[5], inst.aoa, 1.0, inst.mach)
+        troubled, waves = sd.limiter_stats()
+        out[prec] = (U, cl, cd, d)
+        res[prec] = {"dof_stage_updates_per_s": inst.dofs * 3 * td.current_step / (ms * 1e-3),
+                     "ms_per_step": ms / max(td.current_step, 1), "steps_done": td.current_step,
+                     "time": td.current_time, "cl": cl, "cd": cd, "troubled_cells_last_stage": troubled}
+        w_basis = s.basis.mass_mat_diag
+        s.close()
+    (U32, cl32, cd32, _), (U64, cl64, cd64, _) = out["fp32"], out["fp64"]
+    w = w_basis[None, :] * (0.5 * mesh.elem_jacob_det)[:, None]
+    names = ("rho", "rho_u", "rho_v", "rho_E")
+    res["rel_l2_fp32_vs_fp64"] = {n: field_rel_l2(U32[:, v], U64[:, v], w) for v, n in enumerate(names)}
+    res["rel_l2_coefficients_fp32_vs_fp64"] = {
+        n: float(np.linalg.norm(U32[:, v] - U64[:, v]) / np.linalg.norm(U64[:, v])) for v, n in enumerate(names)}
+    res["abs_delta_cl"] = abs(cl32 - cl64)
+    res["abs_delta_cd"] = abs(cd32 - cd64)
+    res["speedup_fp32_vs_fp64"] = (res["fp32"]["dof_stage_updates_per_s"] / res["fp64"]["dof_stage_updates_per_s"])
+    return res
+
+
+# ------------------------------------------------------------------------------------------
+# Serving: Poisson request stream, continuous batching, vs FP64 one at a time
+# ------------------------------------------------------------------------------------------
+def run_serving(args, local):
+    """A seeded Poisson stream of solve requests (triangles log-uniform in [2e3, 5e5], O-grid
+    aspect 2:1, Mach U[0.3,0.85], AoA U[-4,6] deg, p in {1,2,3}), each run to a density-residual
+    drop of 1e-6 or the step cap, served (a) by the continuous-batching loop in FP32 with real
+    arrival times and an HBM budget, and (b) one request at a time on the plain FP64 context,
+    first come first served (service times measured back to back, latencies from the FIFO queue
+    under the same arrival times).  Latency = arrival to retirement; throughput = DOF-stage
+    updates / wall time (a) or / total service time (b), host mesh preparation included in both."""
+    from dgm_in_rust_b200.serving import ServingLoop, latency_summary, one_at_a_time, requests_from_stream
+    from dgm_in_rust_b200.workloads import request_stream
+    seed = 7
+    reqs = requests_from_stream(request_stream(args.serving_requests, args.serving_rate, seed=seed))
+    kw = dict(chunk_steps=32, tol=1e-6, max_steps=args.serving_max_steps)
+    budget = int(args.serving_budget_gib * (1 << 30))
+    loop = ServingLoop(hbm_budget_bytes=budget, device=local, precision="fp32", **kw)
+    t = time.perf_counter()
+    served = loop.run(reqs, realtime=True)
+    wall = time.perf_counter() - t
+    s32 = latency_summary(served, wall)
+    alone, busy, prep = one_at_a_time(reqs, precision="fp64", device=local, **kw)
+    s64 = latency_summary(alone, busy)
+    gpu_only = sum(r.dofs * 3 * r.steps for r in alone) / max(busy - prep, 1e-9)
+    return {
+        "workload": f"{len(reqs)} requests, Poisson arrivals at {args.serving_rate:g}/s "
+                    f"(request_stream seed {seed}), triangles log-uniform [2e3, 5e5], p in {{1,2,3}}, "
+                    f"Mach U[0.3,0.85], AoA U[-4,6] deg; stop at density-residual drop 1e-6 or "
+                    f"{args.serving_max_steps} steps (the configuration's cap is 5000; bounded here so the "
+                    f"default run stays within minutes); convergence checked at step 1 then every 32",
+        "elements_total": int(sum(r.instance.elements for r in reqs)),
+        "hbm_budget_bytes": budget, "peak_resident_bytes": loop.peak_bytes, "cohorts": loop.cohorts_formed,
+        "max_concurrent_requests": loop.max_concurrent,
+        "fp32_serving": s32, "fp64_one_at_a_time": s64,
+        "fp64_one_at_a_time_excluding_host_prep_dof_stage_per_s": gpu_only,
+        "throughput_speedup": s32["dof_stage_updates_per_s"] / s64["dof_stage_updates_per_s"],
+        "p99_speedup": s64["p99_s"] / s32["p99_s"],
+    }
 
 
 def run_ours(args):
@@ -461,6 +584,10 @@ def run_ours(args):
     }
     if world == 1 and not args.no_batched:
         line["batched"] = run_batched(args, local)
+    if world == 1 and not args.no_precision:
+        line["precision"] = run_precision(args, local)
+    if world == 1 and not args.no_serving:
+        line["serving"] = run_serving(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         v, done, el = time_cpu(raw, 1000, 1, threads, budget_s=12.0)

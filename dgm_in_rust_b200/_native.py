@@ -26,7 +26,9 @@ STATUS = {
     7: "Invalid argument",
     9: "CUDA runtime error",
     10: "No usable CUDA device",
+    11: "Work still in flight",
 }
+DGM_NOT_READY = 11
 
 
 class DgmError(RuntimeError):
@@ -150,12 +152,15 @@ def lib() -> ctypes.CDLL:
     L.dgm_instance_set.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
                                    ctypes.c_int64]
     L.dgm_advance_with_residual.argtypes = [vp, ctypes.c_int64]
+    L.dgm_set_initial_solution.argtypes = [vp] + [ctypes.c_double] * 4
+    L.dgm_instance_set_initial.argtypes = [vp, ctypes.c_int32] + [ctypes.c_double] * 4
     L.dgm_diagnostics.argtypes = [vp, ctypes.c_int32, P_D]
     L.dgm_precision.argtypes = [vp]
     L.dgm_upload_solutions.argtypes = [vp, P_D]
     L.dgm_download_solutions.argtypes = [vp, P_D]
     L.dgm_advance.argtypes = [vp, ctypes.c_int64]
     L.dgm_synchronize.argtypes = [vp]
+    L.dgm_query.argtypes = [vp]
     L.dgm_stream.argtypes = [vp]
     L.dgm_stream.restype = vp
     L.dgm_error_location.argtypes = [vp]
@@ -169,11 +174,12 @@ def lib() -> ctypes.CDLL:
     L.dgm_version.restype = ctypes.c_char_p
     for name in ("dgm_compute_residuals", "dgm_apply_limiter", "dgm_compute_time_step", "dgm_rk3",
                  "dgm_time_march", "dgm_get_clock", "dgm_set_clock", "dgm_upload_solutions",
-                 "dgm_download_solutions", "dgm_advance", "dgm_synchronize", "dgm_limiter_stats",
+                 "dgm_download_solutions", "dgm_advance", "dgm_synchronize", "dgm_query", "dgm_limiter_stats",
                  "dgm_set_limits", "dgm_launch_phase", "dgm_phase_launches_per_step", "dgm_launches_per_step",
                  "dgm_instance_count", "dgm_instance_upload", "dgm_instance_download",
                  "dgm_instance_download_residual", "dgm_instance_state", "dgm_instance_set",
-                 "dgm_advance_with_residual", "dgm_diagnostics", "dgm_precision"):
+                 "dgm_advance_with_residual", "dgm_diagnostics", "dgm_precision", "dgm_set_initial_solution",
+                 "dgm_instance_set_initial"):
         getattr(L, name).restype = ctypes.c_int32
     _lib = L
     return L

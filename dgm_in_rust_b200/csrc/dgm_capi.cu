@@ -44,6 +44,7 @@ struct dgm_ctx {
   double hcr = 1.4;
   std::vector<HostInst> inst;
   std::vector<unsigned char> kparams;  // host image of KParams<P, T>
+  std::vector<double> proj_phi, proj_w, proj_mass;  // FP64 tables of the initial projection
   // device buffers (state arrays are of the storage type)
   void *U = nullptr, *U1 = nullptr, *U2 = nullptr, *R = nullptr, *F = nullptr;
   double* stage = nullptr;  // FP64 staging in the reference layout (largest instance)
@@ -218,6 +219,21 @@ struct Ops {
     CK(cudaGetLastError());
     return DGM_OK;
   }
+  static int project(dgm_ctx* c, int64_t i, const double q[NEQ]) {
+    dgm::Projection<P> pr;
+    for (int g = 0; g < V::NQ; ++g) {
+      for (int b = 0; b < V::NB; ++b) pr.phi[g][b] = c->proj_phi[g * V::NB + b];
+      pr.w[g] = c->proj_w[g];
+    }
+    for (int b = 0; b < V::NB; ++b) pr.mass[b] = c->proj_mass[b];
+    for (int v = 0; v < NEQ; ++v) pr.q[v] = q[v];
+    const HostInst& h = c->inst[i];
+    const int threads = 256;
+    dgm::k_project_uniform<P, T><<<(int)((h.ne + threads - 1) / threads), threads, 0, c->stream>>>(
+        pr, kp_of<P, T>(c).m.jac, S(c->U), (int)h.elem_off, (int)h.ne, (int)c->ld);
+    CK(cudaGetLastError());
+    return DGM_OK;
+  }
   static int to_aos(dgm_ctx* c, const void* src, double* dst_aos, int64_t elem_off, int64_t ne) {
     const int64_t n = ne * NEQ * V::NB;
     const int threads = 256;
@@ -266,6 +282,9 @@ struct Ops {
       td.edge_w[g] = t->edge_weights[g];
     }
     for (int b = 0; b < NB; ++b) tb.inv_mass[b] = T(1.0 / t->mass_diag[b]);
+    c->proj_phi.assign(t->phi_cell, t->phi_cell + NQ * NB);
+    c->proj_w.assign(t->cell_weights, t->cell_weights + NQ);
+    c->proj_mass.assign(t->mass_diag, t->mass_diag + NB);
     // gas constants with the reference's expressions (flux.rs:76-77, 85, 96)
     dgm::Gas& gas = kp.gas;
     gas.hcr = c->hcr;
@@ -740,6 +759,7 @@ const char* dgm_status_string(int32_t s) {
     case DGM_BAD_ARG: return "Invalid argument";
     case DGM_CUDA_ERROR: return "CUDA runtime error";
     case DGM_NO_DEVICE: return "No usable CUDA device";
+    case DGM_NOT_READY: return "Work still in flight";
   }
   return "unknown status";
 }
@@ -807,6 +827,46 @@ int32_t dgm_instance_set(dgm_ctx* c, int32_t i, double t, int64_t step, double f
   h.status = 0;
   h.err_where = -1;
   c->limits_dirty = true;
+  return DGM_OK;
+}
+
+// Solver::set_initial_solution (solver.rs:45-79) on the device: the free-stream state of
+// InitialSolution, with the reference's expressions, projected onto the basis of every element
+// of instance i (all instances for dgm_set_initial_solution) in the resident state.
+static int set_initial(dgm_ctx* c, int64_t i, double density, double angle_of_attack, double mach_number,
+                       double pressure) {
+  if (!(density > 0.0) || !(pressure > 0.0) || !std::isfinite(angle_of_attack) || !std::isfinite(mach_number))
+    return DGM_BAD_ARG;
+  const double sound_speed = std::sqrt(c->hcr * pressure / density);
+  const double pi = 3.14159265358979323846;           // f64::consts::PI
+  const double a = angle_of_attack * (pi / 180.0);   // f64::to_radians
+  const double x_velocity = mach_number * std::cos(a) * sound_speed;
+  const double y_velocity = mach_number * std::sin(a) * sound_speed;
+  const double total_energy =
+      pressure / (c->hcr - 1.0) + 0.5 * density * (x_velocity * x_velocity + y_velocity * y_velocity);
+  const double q[NEQ] = {density, density * x_velocity, density * y_velocity, total_energy};
+  return dispatch(c, [&](auto ops) { return decltype(ops)::project(c, i, q); });
+}
+
+int32_t dgm_instance_set_initial(dgm_ctx* c, int32_t i, double density, double angle_of_attack,
+                                 double mach_number, double pressure) {
+  if (!inst_ok(c, i)) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  int st = set_initial(c, i, density, angle_of_attack, mach_number, pressure);
+  if (st) return st;
+  CK(cudaStreamSynchronize(c->stream));
+  return DGM_OK;
+}
+
+int32_t dgm_set_initial_solution(dgm_ctx* c, double density, double angle_of_attack, double mach_number,
+                                 double pressure) {
+  if (!c) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  for (size_t i = 0; i < c->inst.size(); ++i) {
+    int st = set_initial(c, (int64_t)i, density, angle_of_attack, mach_number, pressure);
+    if (st) return st;
+  }
+  CK(cudaStreamSynchronize(c->stream));
   return DGM_OK;
 }
 
@@ -957,6 +1017,15 @@ int32_t dgm_synchronize(dgm_ctx* c) {
   if (!c) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   CK(cudaStreamSynchronize(c->stream));
+  return collect_status(c);
+}
+
+int32_t dgm_query(dgm_ctx* c) {
+  if (!c) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  const cudaError_t e = cudaStreamQuery(c->stream);
+  if (e == cudaErrorNotReady) return DGM_NOT_READY;
+  CK(e);
   return collect_status(c);
 }
 

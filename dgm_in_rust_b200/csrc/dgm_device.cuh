@@ -1135,4 +1135,39 @@ __global__ void k_soa_to_aos(const T* __restrict__ src, double* __restrict__ dst
   dst[i] = (double)src[(size_t)c * ld + e];
 }
 
+// Initial L2 projection of a uniform state onto the basis (Solver::set_initial_solution,
+// solver.rs:45-79): U[e][v][b] = (sum_g 0.5 J_e w_g q_v phi_gb) / (m_b 0.5 J_e), with the
+// reference's operation order and no contraction into FMAs, so the result is bit-identical to
+// the reference loop.  One thread per element of one instance.
+template <int P>
+struct Projection {
+  using V = Variant<P>;
+  double phi[V::NQ][V::NB];
+  double w[V::NQ];
+  double mass[V::NB];
+  double q[NEQ];
+};
+
+template <int P, typename T>
+__global__ void k_project_uniform(const __grid_constant__ Projection<P> pr, const double* __restrict__ jac,
+                                  T* __restrict__ U, int e0, int ne, int ld) {
+  using V = Variant<P>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  const int e = e0 + i;
+  const double J = jac[e];
+  const double hj = __dmul_rn(0.5, J);
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v) {
+#pragma unroll
+    for (int b = 0; b < V::NB; ++b) {
+      double acc = 0.0;
+#pragma unroll
+      for (int g = 0; g < V::NQ; ++g)
+        acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(__dmul_rn(hj, pr.w[g]), pr.q[v]), pr.phi[g][b]));
+      U[(size_t)(v * V::NB + b) * ld + e] = T(acc / __dmul_rn(__dmul_rn(pr.mass[b], 0.5), J));
+    }
+  }
+}
+
 }  // namespace dgm

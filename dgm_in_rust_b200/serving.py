@@ -1,0 +1,394 @@
+"""Continuous-batching solve server: a host scheduler over device-resident batched solves.
+
+No counterpart in the reference, which runs one configured solve per process.  Requests (an
+O-grid size, flow condition and polynomial order) arrive over time.  The loop
+
+* prepares each request's mesh in a pool of worker processes (or threads) as soon as it arrives;
+  the initial state is projected on the device at admission;
+* admits prepared requests in arrival order while the device footprint of the active solves
+  plus theirs fits the HBM budget (a request that does not fit waits, and so does every prepared
+  request behind it, until running solves retire and free their memory; a request still being
+  prepared does not hold back those behind it);
+* packs the requests it admits together into cohorts -- one :class:`Batch` context per
+  polynomial order, so that every launch of a step covers all of a cohort's meshes -- and runs
+  each cohort on its own CUDA stream, so cohorts admitted at different times overlap on the
+  GPU;
+* polls every cohort without blocking; when a cohort's chunk of steps is done it reads each
+  member's density-residual norm, retires the members that have converged (residual dropped by
+  ``tol`` relative to the first step's) or reached ``max_steps``, and enqueues the next chunk
+  for the rest.  A retired member is switched off inside its cohort (later launches skip its
+  elements); the cohort's memory returns to the budget when its last member retires.
+
+Each member of a cohort is computed exactly as it would be alone (instances of a batch are
+disconnected meshes with their own time step and clock, and every reduction is per instance
+and deterministic), and convergence is tested at the same step counts (step 1, then every
+``chunk_steps``), so a request's result does not depend on what else was running; the tests
+check this bitwise.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import multiprocessing
+import queue
+import threading
+import time
+from concurrent.futures import ProcessPoolExecutor, ThreadPoolExecutor
+
+import numpy as np
+
+from .basis_function import default_rules
+from ._native import DgmError
+from .solver import Batch, build_solver
+from .workloads import HCR, Instance, instance_mesh
+
+__all__ = ["Request", "Result", "ServingLoop", "footprint_bytes", "latency_summary", "requests_from_stream",
+           "solve_alone", "one_at_a_time"]
+
+CFL = 0.1
+NEQ = 4
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    arrival_s: float
+    instance: Instance
+
+
+@dataclasses.dataclass
+class Result:
+    rid: int
+    arrival_s: float
+    admitted_s: float
+    finished_s: float
+    steps: int
+    time: float
+    residual_drop: float
+    converged: bool
+    status: int
+    dofs: int
+    state: np.ndarray | None = None
+
+    @property
+    def latency_s(self) -> float:
+        return self.finished_s - self.arrival_s
+
+
+def requests_from_stream(stream: list) -> list:
+    """[(arrival_s, Instance)] as produced by workloads.request_stream -> [Request]."""
+    return [Request(i, float(t), inst) for i, (t, inst) in enumerate(stream)]
+
+
+def footprint_bytes(meshes: list, order: int, precision: str) -> int:
+    """Device bytes a batch context of ``meshes`` allocates: the sum of the requested sizes of
+    its allocations (what dgm_device_bytes reports), following dgm_create's allocation list."""
+    nb = (order + 1) * (order + 2) // 2
+    ng = default_rules(order)[1]
+    eb = 4 if precision == "fp32" else 8
+    n = len(meshes)
+    ne = sum(m.n_elements for m in meshes)
+    ld = (ne + 31) // 32 * 32
+    n_int = sum(len(m.internal_edge_indices) for m in meshes)
+    n_bnd = sum(int(np.count_nonzero(m.edge_elements[:, 1] == -1)) for m in meshes)
+    n_patch = sum(len(m.patch_type) for m in meshes)
+    max_ne = max(m.n_elements for m in meshes)
+
+    def arr(count, size):             # dev_alloc: at least one element
+        return max(count, 1) * size
+
+    control = 56 + n * 72                                            # Control, InstCtl[n]
+    geometry = 3 * ne * 8 + 4 * ld * 8 + 2 * 3 * ld * 4 + ne * 4     # jac, hmin, h15, dinv, face, nbr, inst
+    edges = (arr(n_int, 8) + arr(n_int, 4) + arr(n_int, 32) + arr(n_bnd, 4) + arr(n_bnd, 4) + arr(n_bnd, 32)
+             + max(n_patch, 1) * 32 + (n_int + n_bnd) * 8)          # internal, boundary, patches, slot_ref
+    offsets = 2 * (n + 1) * 4
+    state = 4 * NEQ * nb * ld * eb                                   # U, U1, U2, R
+    flux = (n_int + n_bnd) * ng * 4 * eb                             # F
+    stage = max_ne * NEQ * nb * 8                                    # FP64 staging
+    limiter = ne * (1 + 4 + 4)                                       # t0, status, work
+    diag = n * 8 * 8
+    return int(control + geometry + edges + offsets + state + flux + stage + limiter + diag)
+
+
+def _prepare_request(req: Request):
+    """Host preparation of one request (runs in a worker): the processed O-grid and its
+    free-stream initial condition."""
+    if req.instance.order not in (1, 2, 3):
+        raise ValueError(f"unsupported polynomial order {req.instance.order}")
+    mesh, init = instance_mesh(req.instance)
+    return req, mesh, init
+
+
+def _warm():
+    return 0
+
+
+class _Member:
+    def __init__(self, req: Request, index: int):
+        self.req = req
+        self.index = index
+        self.r0 = None
+        self.drop = 1.0
+        self.done = False
+
+
+class _Cohort:
+    def __init__(self, items: list, order: int, precision: str, device: int, max_steps: int, now: float):
+        meshes = [it[1] for it in items]
+        n = len(items)
+        self.batch = Batch(meshes, order, HCR, [CFL] * n, [1.0e30] * n, [max_steps] * n, limiter=True,
+                           device=device, precision=precision)
+        for i, it in enumerate(items):
+            self.batch.set_initial(i, it[2])
+        self.members = [_Member(it[0], i) for i, it in enumerate(items)]
+        self.admitted = now
+        self.bytes = self.batch.device_bytes()
+        self.checks = 0
+        # the first chunk is one step: its residual is the reference for the convergence test
+        self.batch.advance(1, with_residual=True)
+
+    def close(self):
+        self.batch.close()
+
+
+class ServingLoop:
+    """Serve solve requests with continuous batching under an HBM budget.
+
+    ``precision`` is the batched contexts' precision ("fp32": FP32 bulk arithmetic with the
+    limiter, positivity checks, time step and diagnostics in FP64; "fp64": the reference's
+    arithmetic).  ``window_s`` is how long a new arrival may wait for others to share its
+    cohort while the GPU is busy (an idle GPU admits at once).  ``prep`` selects worker
+    processes ("process", started with spawn before the clock starts, like a server's standing
+    pool) or threads ("thread") for mesh preparation."""
+
+    def __init__(self, hbm_budget_bytes: int = 40 << 30, device: int = 0, precision: str = "fp32",
+                 chunk_steps: int = 32, tol: float = 1e-6, max_steps: int = 5000, window_s: float = 0.002,
+                 max_cohort_elements: int = 4 << 20, prep_workers: int = 4, prep: str = "process",
+                 keep_states: bool = False):
+        if chunk_steps < 1 or max_steps < 1:
+            raise ValueError("chunk_steps and max_steps must be positive")
+        self.budget = int(hbm_budget_bytes)
+        self.device = int(device)
+        self.precision = precision
+        self.chunk = int(chunk_steps)
+        self.tol = float(tol)
+        self.max_steps = int(max_steps)
+        self.window = float(window_s)
+        self.max_cohort_elements = int(max_cohort_elements)
+        if prep not in ("process", "thread"):
+            raise ValueError("prep must be 'process' or 'thread'")
+        self.prep_workers = max(1, int(prep_workers))
+        self.prep = prep
+        self.keep_states = keep_states
+        self.peak_bytes = 0
+        self.cohorts_formed = 0
+        self.max_concurrent = 0
+        self._realtime = True
+
+    def run(self, requests: list, realtime: bool = True) -> list:
+        """Serve ``requests`` (list of Request).  With ``realtime`` each request becomes visible
+        at its arrival time on the wall clock (latency is measured from it); otherwise all are
+        visible at once (latency from the start of the run).  Returns the Results ordered by
+        request id."""
+        reqs = sorted(requests, key=lambda r: (r.arrival_s, r.rid))
+        if not reqs:
+            return []
+        ready: "queue.Queue" = queue.Queue()
+        self._realtime = bool(realtime)
+        if self.prep == "process":
+            pool = ProcessPoolExecutor(max_workers=self.prep_workers, mp_context=multiprocessing.get_context("spawn"))
+            for f in [pool.submit(_warm) for _ in range(self.prep_workers)]:
+                f.result()
+        else:
+            pool = ThreadPoolExecutor(max_workers=self.prep_workers)
+        t0 = time.perf_counter()
+
+        def now():
+            return time.perf_counter() - t0
+
+        def done(fut, r):
+            exc = fut.exception()
+            ready.put((r, None, exc) if exc is not None else fut.result())
+
+        def feeder():
+            for r in reqs:
+                if realtime:
+                    wait = r.arrival_s - now()
+                    if wait > 0:
+                        time.sleep(wait)
+                pool.submit(_prepare_request, r).add_done_callback(lambda f, r=r: done(f, r))
+
+        feed = threading.Thread(target=feeder, daemon=True)
+        feed.start()
+        waiting: list = []       # prepared, not admitted: (req, mesh, initial, ready_s), in arrival order
+        active: list = []        # cohorts
+        results: list = []
+        used = 0
+        try:
+            while len(results) < len(reqs):
+                got = False
+                while True:
+                    try:
+                        item = ready.get_nowait()
+                    except queue.Empty:
+                        break
+                    if item[1] is None:
+                        raise RuntimeError(f"preparing request {item[0].rid} failed") from item[2]
+                    waiting.append(item + (now(),))
+                    got = True
+                if got:
+                    waiting.sort(key=lambda it: (it[0].arrival_s, it[0].rid))
+                used = self._admit(waiting, active, used, now)
+                progressed = False
+                for co in list(active):
+                    st = co.batch.query()
+                    if st is None:
+                        continue
+                    progressed = True
+                    finished = self._check(co, results, now)
+                    if finished:
+                        active.remove(co)
+                        used -= co.bytes
+                        co.close()
+                if not progressed and not got:
+                    time.sleep(0.0002)
+        finally:
+            feed.join()
+            pool.shutdown(wait=True)
+            for co in active:
+                co.close()
+        return sorted(results, key=lambda r: r.rid)
+
+    def _admit(self, waiting: list, active: list, used: int, now) -> int:
+        if not waiting:
+            return used
+        if active and (now() - min(it[3] for it in waiting)) < self.window:
+            return used
+        take: list = []
+        need_total = 0
+        for item in waiting:
+            need = footprint_bytes([item[1]], item[0].instance.order, self.precision)
+            if (active or take) and used + need_total + need > self.budget:
+                break           # first-come first-served: nothing overtakes a request that waits for memory
+            take.append(item)
+            need_total += need
+        if not take:
+            return used
+        del waiting[:len(take)]
+        groups: dict = {}
+        for item in take:
+            groups.setdefault(item[0].instance.order, []).append(item)
+        for order, items in sorted(groups.items()):
+            chunk: list = []
+            ne = 0
+            for item in items + [None]:
+                if item is None or (chunk and ne + item[1].n_elements > self.max_cohort_elements):
+                    co = _Cohort(chunk, order, self.precision, self.device, self.max_steps, now())
+                    active.append(co)
+                    used += co.bytes
+                    self.cohorts_formed += 1
+                    chunk, ne = [], 0
+                if item is not None:
+                    chunk.append(item)
+                    ne += item[1].n_elements
+        self.peak_bytes = max(self.peak_bytes, used)
+        self.max_concurrent = max(self.max_concurrent, sum(sum(not m.done for m in c.members) for c in active))
+        return used
+
+    def _check(self, co: _Cohort, results: list, now) -> bool:
+        """Convergence test after a chunk; retires members, enqueues the next chunk.  Returns True
+        when every member has retired."""
+        b = co.batch
+        diag = b.diagnostics(use_residual=True)
+        co.checks += 1
+        for m in co.members:
+            if m.done:
+                continue
+            t, step, status, _ = b.state(m.index)
+            r = math.sqrt(max(float(diag[m.index, 6]), 0.0))
+            if m.r0 is None:
+                m.r0 = r if r > 0.0 else 1.0
+            m.drop = r / m.r0
+            converged = step > 1 and m.drop <= self.tol
+            if status != 0 or converged or step >= self.max_steps:
+                state = b.download(m.index) if self.keep_states else None
+                arrival = m.req.arrival_s if self._realtime else 0.0
+                results.append(Result(m.req.rid, arrival, co.admitted, now(), step, t, m.drop, converged,
+                                      status, m.req.instance.dofs, state))
+                b.set_instance(m.index, t, step, 1.0e30, step)   # switched off from the next launch on
+                m.done = True
+        if all(m.done for m in co.members):
+            return True
+        b.advance(self.chunk, with_residual=True)
+        return False
+
+
+def solve_alone(req: Request, precision: str = "fp64", device: int = 0, chunk_steps: int = 32, tol: float = 1e-6,
+                max_steps: int = 5000, keep_state: bool = False) -> tuple:
+    """One request on a plain single-mesh context (the reference-shaped Solver path), with the
+    serving loop's convergence schedule (step 1, then every ``chunk_steps``).  Returns
+    (Result with finished_s = service time, service time in s, of which host preparation in s)."""
+    t0 = time.perf_counter()
+    _, mesh, init = _prepare_request(req)
+    prep = time.perf_counter() - t0
+    solver = build_solver(mesh, req.instance.order, HCR, CFL, 1.0e30, max_steps, limiter=True, device=device,
+                          precision=precision)
+    try:
+        td, sd = solver.temporal_disc, solver.spatial_disc
+        td.set_initial_on_device(init)
+        r0, drop, converged, status = None, 1.0, False, 0
+        n = 1
+        while True:
+            td.advance(n, with_residual=True)
+            try:
+                td.synchronize()
+            except DgmError as e:
+                status = e.status
+            step = td.current_step
+            r = math.sqrt(max(float(sd.diagnostics(use_residual=True)[6]), 0.0))
+            if r0 is None:
+                r0 = r if r > 0.0 else 1.0
+            drop = r / r0
+            converged = step > 1 and drop <= tol
+            if status != 0 or converged or step >= max_steps:
+                break
+            n = chunk_steps
+        state = None
+        if keep_state:
+            state = sd.new_state()
+            td.download(state)
+        service = time.perf_counter() - t0
+        return Result(req.rid, 0.0, 0.0, service, step, td.current_time, drop, converged, status, req.instance.dofs,
+                      state), service, prep
+    finally:
+        solver.close()
+
+
+def one_at_a_time(requests: list, precision: str = "fp64", device: int = 0, chunk_steps: int = 32, tol: float = 1e-6,
+                  max_steps: int = 5000) -> tuple:
+    """A first-come first-served server that runs one request at a time on the plain context.
+    Each request is solved back to back (service times measured); its latency is then that of
+    the FIFO queue under the requests' arrival times: finish_i = max(arrival_i, finish_{i-1}) +
+    service_i.  Returns (Results, total service time in s, of which host preparation in s)."""
+    out = []
+    busy = 0.0
+    prep_total = 0.0
+    finish = 0.0
+    for req in sorted(requests, key=lambda r: (r.arrival_s, r.rid)):
+        res, service, prep = solve_alone(req, precision, device, chunk_steps, tol, max_steps)
+        busy += service
+        prep_total += prep
+        start = max(req.arrival_s, finish)
+        finish = start + service
+        res.arrival_s, res.admitted_s, res.finished_s = req.arrival_s, start, finish
+        out.append(res)
+    return sorted(out, key=lambda r: r.rid), busy, prep_total
+
+
+def latency_summary(results: list, wall_s: float) -> dict:
+    """p50/p99/mean latency (arrival to retirement) and throughput in DOF-stage updates/s."""
+    lat = np.array([r.latency_s for r in results])
+    dof_stages = sum(r.dofs * 3 * r.steps for r in results)
+    return {"requests": len(results), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "wall_s": wall_s, "dof_stage_updates_per_s": dof_stages / wall_s,
+            "converged": int(sum(r.converged for r in results)), "failed": int(sum(r.status != 0 for r in results))}

@@ -321,12 +321,28 @@ class TemperalDisc:
     def download(self, solutions: np.ndarray) -> None:
         self._sd._check(self._sd._lib.dgm_download_solutions(self._sd._ctx, _native.dptr(solutions)), "download")
 
+    def set_initial_on_device(self, initial: "InitialSolution") -> None:
+        """Solver::set_initial_solution (solver.rs:45-79) computed on the device into the resident
+        state; bit-identical to :func:`initial_state` followed by :meth:`upload`."""
+        self._sd._check(self._sd._lib.dgm_set_initial_solution(
+            self._sd._ctx, float(initial.density), float(initial.angle_of_attack), float(initial.mach_number),
+            float(initial.pressure)), "set_initial_solution")
+
     def advance(self, n_steps: int, with_residual: bool = False) -> None:
         f = self._sd._lib.dgm_advance_with_residual if with_residual else self._sd._lib.dgm_advance
         self._sd._check(f(self._sd._ctx, int(n_steps)), "advance")
 
     def synchronize(self) -> None:
         self._sd._check(self._sd._lib.dgm_synchronize(self._sd._ctx), "synchronize")
+
+    def query(self) -> bool:
+        """True once the enqueued steps have finished (raising their error, if any); False while
+        they are still running.  Does not block."""
+        st = int(self._sd._lib.dgm_query(self._sd._ctx))
+        if st == _native.DGM_NOT_READY:
+            return False
+        self._sd._check(st, "query")
+        return True
 
 
 class Solver:
@@ -430,6 +446,12 @@ class Batch:
         _check_state(solutions, self.meshes[i].n_elements, self.nb, "solutions")
         self._check(self._lib.dgm_instance_upload(self._ctx, i, _native.dptr(solutions)), "upload")
 
+    def set_initial(self, i: int, initial: "InitialSolution") -> None:
+        """Solver::set_initial_solution for instance i, computed on the device."""
+        self._check(self._lib.dgm_instance_set_initial(self._ctx, i, float(initial.density),
+                                                       float(initial.angle_of_attack), float(initial.mach_number),
+                                                       float(initial.pressure)), "set_initial")
+
     def download(self, i: int) -> np.ndarray:
         out = np.zeros((self.meshes[i].n_elements, 4, self.nb))
         self._check(self._lib.dgm_instance_download(self._ctx, i, _native.dptr(out)), "download")
@@ -443,6 +465,15 @@ class Batch:
         """Wait for the device; returns the first device status (0 = ok) without raising, since
         a failing instance stops alone (see state())."""
         return int(self._lib.dgm_synchronize(self._ctx))
+
+    def query(self):
+        """Non-blocking synchronize: None while steps are in flight, else the status that
+        synchronize() would return."""
+        st = int(self._lib.dgm_query(self._ctx))
+        return None if st == _native.DGM_NOT_READY else st
+
+    def device_bytes(self) -> int:
+        return int(self._lib.dgm_device_bytes(self._ctx))
 
     def state(self, i: int):
         """(current_time, current_step, status, error_location) of instance i."""

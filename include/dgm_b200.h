@@ -37,6 +37,7 @@ extern "C" {
 #define DGM_BAD_ARG 7                 /* unsupported order/rule, bad sizes or pointers       */
 #define DGM_CUDA_ERROR 9              /* a CUDA runtime call failed                         */
 #define DGM_NO_DEVICE 10              /* no usable CUDA device                              */
+#define DGM_NOT_READY 11              /* dgm_query: work still in flight (not an error)     */
 
 /* ---- boundary types (mesh.rs:174-178) ---------------------------------------------------- */
 #define DGM_WALL 0
@@ -162,6 +163,11 @@ int32_t dgm_advance(dgm_ctx* ctx, int64_t n_steps);
  * synchronize (DGM_OK if none). */
 int32_t dgm_synchronize(dgm_ctx* ctx);
 
+/* Non-blocking dgm_synchronize: DGM_NOT_READY while work enqueued on the context's stream is
+ * still running, otherwise what dgm_synchronize returns.  No counterpart in the reference; used
+ * by schedulers that poll many contexts. */
+int32_t dgm_query(dgm_ctx* ctx);
+
 /* The context's CUDA stream (cudaStream_t as void*), for callers that order their own work
  * (copies, events) against the solver. */
 void* dgm_stream(dgm_ctx* ctx);
@@ -197,6 +203,15 @@ int32_t dgm_instance_state(dgm_ctx* ctx, int32_t i, double* current_time, int64_
 /* Reset instance i's clock, loop bounds and status (applied at the next advance). */
 int32_t dgm_instance_set(dgm_ctx* ctx, int32_t i, double current_time, int64_t current_step,
                          double final_time, int64_t final_step);
+/* Solver::set_initial_solution (solver.rs:45-79) on the device: the uniform state of
+ * InitialSolution (density, angle of attack in degrees, Mach number, pressure; the reference's
+ * expressions) projected onto the basis of every element, written to the resident state --
+ * bit-identical to the reference's loop.  dgm_set_initial_solution sets every instance,
+ * dgm_instance_set_initial instance i only.  The clock is not touched. */
+int32_t dgm_set_initial_solution(dgm_ctx* ctx, double density, double angle_of_attack, double mach_number,
+                                 double pressure);
+int32_t dgm_instance_set_initial(dgm_ctx* ctx, int32_t i, double density, double angle_of_attack,
+                                 double mach_number, double pressure);
 /* As dgm_advance, additionally writing each step's third-stage residual (for residual norms). */
 int32_t dgm_advance_with_residual(dgm_ctx* ctx, int64_t n_steps);
 

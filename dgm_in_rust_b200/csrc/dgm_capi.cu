@@ -54,11 +54,15 @@ struct dgm_ctx {
   int* d_elem_off = nullptr;
   int* d_bslot_off = nullptr;
   double* d_diag = nullptr;
+  double* gram = nullptr;   // WENO Gram matrices, [NB (NB + 1) / 2][ld] (limiter on)
   Control* ctl = nullptr;
   InstCtl* ic = nullptr;
   std::vector<void*> allocs;
   int64_t bytes = 0;
   int coop_blocks = 1;
+  // launch configuration of the edge and element passes (dgm_set_launch_config / dgm_autotune):
+  // edge_blocks = 0 launches one thread per (slot, Gauss point), else a grid-stride grid
+  int edge_threads = 256, edge_blocks = 0, elem_threads = 256;
   // graphs[with_residual][g]: g = 0 captures graph_steps steps, g = 1 a single step
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int graph_steps = 8;
@@ -132,8 +136,9 @@ struct Ops {
 
   static int edge_flux(dgm_ctx* c, const T* U) {
     const int64_t total = (c->n_int + c->n_bnd) * V::NG;
-    const int threads = 256;
-    const int blocks = (int)std::max<int64_t>(1, (total + threads - 1) / threads);
+    const int threads = c->edge_threads;
+    const int64_t full = std::max<int64_t>(1, (total + threads - 1) / threads);
+    const int blocks = (int)(c->edge_blocks > 0 ? std::min<int64_t>(c->edge_blocks, full) : full);
     dgm::k_edge_flux<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, S(c->F));
     CK(cudaGetLastError());
     return DGM_OK;
@@ -141,8 +146,9 @@ struct Ops {
 
   template <int MODE>
   static int element(dgm_ctx* c, const T* Uin, const T* Ubase, T* Uout, const T* Rin, T* Rout) {
-    const int threads = 256;  // 8 warps x 8 elements, 4 threads (variables) per element
-    const int blocks = (int)std::max<int64_t>(1, (c->ne + 63) / 64);
+    const int threads = c->elem_threads;  // warps of 8 elements, 4 threads (variables) per element
+    const int per_block = threads / 4;
+    const int blocks = (int)std::max<int64_t>(1, (c->ne + per_block - 1) / per_block);
     dgm::k_element<P, T, MODE><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), Uin, Ubase, S(c->F), Uout, Rin,
                                                                    Rout);
     CK(cudaGetLastError());
@@ -219,6 +225,16 @@ struct Ops {
     CK(cudaGetLastError());
     return DGM_OK;
   }
+  static int weno_gram(dgm_ctx* c) {
+    constexpr int NPAIR = V::NB * (V::NB + 1) / 2;
+    const int64_t n = (int64_t)NPAIR * c->ne;
+    const int threads = 256;
+    dgm::k_weno_gram<P, T><<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(kp_of<P, T>(c), c->gram);
+    CK(cudaGetLastError());
+    kp_of<P, T>(c).m.gram = c->gram;
+    return DGM_OK;
+  }
+
   static int project(dgm_ctx* c, int64_t i, const double q[NEQ]) {
     dgm::Projection<P> pr;
     for (int g = 0; g < V::NQ; ++g) {
@@ -443,6 +459,16 @@ int build_graph(dgm_ctx* c, int with_residual, int single) {
   }
   c->graph[with_residual][single] = exec;
   return DGM_OK;
+}
+
+// Drop the captured step graphs (they hold the launch configuration of their capture).
+void reset_graphs(dgm_ctx* c) {
+  for (auto& row : c->graph)
+    for (auto& g : row)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
 }
 
 // Enqueue n time-march iterations on the resident state.
@@ -731,6 +757,11 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* 
     return fail(st);
   for (void* p : {c->U, c->U1, c->U2, c->R})
     if (cudaMemset(p, 0, n_state * eb) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  if (c->limiter) {
+    if ((st = dev_alloc(c, &c->gram, (size_t)(c->nb * (c->nb + 1) / 2) * c->ld))) return fail(st);
+    if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::weno_gram(c); }))) return fail(st);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  }
   if (cudaMemset(c->status, 0, (size_t)c->ne * sizeof(unsigned int)) != cudaSuccess) return fail(DGM_CUDA_ERROR);
   if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::occupancy(c); }))) return fail(st);
   c->graph_steps = (int)kGraphSteps;
@@ -1045,6 +1076,101 @@ int32_t dgm_launch_phase(dgm_ctx* c, int32_t phase) {
       default: return O::limiter(c, O::S(c->U2));
     }
   });
+}
+
+int32_t dgm_set_launch_config(dgm_ctx* c, int32_t edge_threads, int32_t edge_blocks, int32_t element_threads) {
+  if (!c) return DGM_BAD_ARG;
+  auto threads_ok = [](int32_t t) { return t >= 32 && t <= 256 && t % 32 == 0; };
+  if (!threads_ok(edge_threads) || !threads_ok(element_threads) || edge_blocks < 0 || edge_blocks > (1 << 24))
+    return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  CK(cudaStreamSynchronize(c->stream));
+  c->edge_threads = edge_threads;
+  c->edge_blocks = edge_blocks;
+  c->elem_threads = element_threads;
+  reset_graphs(c);
+  return DGM_OK;
+}
+
+int32_t dgm_get_launch_config(dgm_ctx* c, int32_t* config) {
+  if (!c || !config) return DGM_BAD_ARG;
+  config[0] = c->edge_threads;
+  config[1] = c->edge_blocks;
+  config[2] = c->elem_threads;
+  return DGM_OK;
+}
+
+// Times every candidate configuration of the edge and element passes on the resident state
+// (CUDA events on the context's stream, after warm-up launches) and keeps the fastest.  The
+// candidates only regroup independent per-slot / per-element work, so results are unchanged.
+int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
+  if (!c || repeats < 1 || repeats > 1000) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  int st = set_active(c, 0.0, false);
+  if (st) return st;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return DGM_CUDA_ERROR;
+  }
+  const int sms = c->num_sms;
+  const int edge_cand[][2] = {{256, 0}, {128, 0}, {64, 0}, {256, 4 * sms}, {256, 8 * sms}, {128, 8 * sms},
+                              {128, 16 * sms}};
+  const int elem_cand[] = {256, 128, 64};
+  auto time_phase = [&](int phase, float* us) -> int {
+    for (int w = 0; w < 2; ++w) {
+      int s2 = dispatch(c, [&](auto ops) {
+        using O = decltype(ops);
+        return phase == 1 ? O::edge_flux(c, O::S(c->U))
+                          : O::template element<2>(c, O::S(c->U), O::S(c->U), O::S(c->U2), nullptr, nullptr);
+      });
+      if (s2) return s2;
+    }
+    CK(cudaEventRecord(e0, c->stream));
+    for (int r = 0; r < repeats; ++r) {
+      int s2 = dispatch(c, [&](auto ops) {
+        using O = decltype(ops);
+        return phase == 1 ? O::edge_flux(c, O::S(c->U))
+                          : O::template element<2>(c, O::S(c->U), O::S(c->U), O::S(c->U2), nullptr, nullptr);
+      });
+      if (s2) return s2;
+    }
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    *us = 1000.f * ms / repeats;
+    return DGM_OK;
+  };
+  float best_edge = 1e30f, best_elem = 1e30f;
+  int be_t = c->edge_threads, be_b = c->edge_blocks, bl_t = c->elem_threads;
+  for (auto& cand : edge_cand) {
+    c->edge_threads = cand[0];
+    c->edge_blocks = cand[1];
+    float us;
+    if ((st = time_phase(1, &us))) break;
+    if (us < best_edge) best_edge = us, be_t = cand[0], be_b = cand[1];
+  }
+  for (int t : elem_cand) {
+    if (st) break;
+    c->elem_threads = t;
+    float us;
+    if ((st = time_phase(2, &us))) break;
+    if (us < best_elem) best_elem = us, bl_t = t;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->edge_threads = be_t;
+  c->edge_blocks = be_b;
+  c->elem_threads = bl_t;
+  reset_graphs(c);
+  if (best_us) {
+    best_us[0] = best_edge;
+    best_us[1] = best_elem;
+  }
+  const int device_status = collect_status(c);
+  return st ? st : device_status;
 }
 
 int32_t dgm_phase_launches_per_step(dgm_ctx* c, int32_t phase) {

@@ -85,6 +85,7 @@ struct MeshDev {
   const double4* __restrict__ be_geo; // [n_bnd] outward nx, ny, half length, length
   const double4* __restrict__ patch_q;// [np] conserved far-field state
   const int64_t* __restrict__ slot_ref;  // [n_int + n_bnd] reference edge id of each slot
+  const double* __restrict__ gram;    // [NB (NB + 1) / 2][ld] WENO Gram matrices (limiter on)
 };
 
 // Time-march state of one instance (TemperalDisc's current_time / current_step and the loop
@@ -614,16 +615,67 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
 //   beta = sum_{l=1..p} sum_{l1+l2=l} J^(l-1) int_e (sum_b P_b d^{l1,l2} phi_b)^2,
 // is the quadratic form P^T Q P with the element's Gram matrix
 //   Q[b][b'] = sum_keys J^(l-1) sum_q 0.5 J w_q D_{q,b,key} D_{q,b',key},
-// built once per element and shared by the 3 faces x 4 polynomials x 4 variables (the
-// reference re-evaluates the derivative sums for each of those 48 indicators).  The three
+// which depends on the geometry only: k_weno_gram computes it once per context, and it serves
+// the 3 faces x 4 polynomials x 4 variables of every limiting pass (the reference re-evaluates
+// the derivative sums for each of those 48 indicators).  The three
 // faces are processed concurrently (lane -> (face, poly, variable, mode)); projections,
 // normalisation, recombination and the area average keep the reference's summation order.
 // ------------------------------------------------------------------------------------------
+// Entry (b, c) of an element's WENO Gram matrix,
+//   Q[b][c] = sum_{l=1..p} J^(l-1) sum_{l1+l2=l} sum_q 0.5 J w_q D_{q,b,(l1,l2)} D_{q,c,(l1,l2)},
+// with D the physical derivatives of the modes at the cell points (compute_dphi, mesh.rs:66-147):
+// P^T Q P is the smoothness indicator of weno.rs:125-143, 156-174.
+template <int P>
+__device__ __forceinline__ double gram_entry(const double* __restrict__ dref, const double* __restrict__ cell_w,
+                                             double J, double xx, double xy, double ex, double ey, int b, int c) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NQ = V::NQ, NK = V::NK;
+  double acc = 0.0;
+#pragma unroll
+  for (int l = 1; l <= P; ++l) {
+    const double jp = (l == 1) ? 1.0 : (l == 2 ? J : J * J);
+#pragma unroll
+    for (int l1 = 0; l1 <= l; ++l1) {
+      const int kk = l * (l + 1) / 2 - 1 + (l - l1);
+      double integral = 0.0;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const double(&rb)[NK] = *reinterpret_cast<const double(*)[NK]>(&dref[(q * NB + b) * NK]);
+        const double(&rc)[NK] = *reinterpret_cast<const double(*)[NK]>(&dref[(q * NB + c) * NK]);
+        const double db = phys_deriv<NK>(rb, xx, xy, ex, ey, kk);
+        const double dc = phys_deriv<NK>(rc, xx, xy, ex, ey, kk);
+        integral += 0.5 * J * cell_w[q] * (db * dc);
+      }
+      acc += jp * integral;
+    }
+  }
+  return acc;
+}
+
+// Setup kernel: every element's Gram matrix (upper triangle, pair-major), one thread per
+// (pair, element); a warp shares its pair, so the table reads are uniform.
+template <int P, typename T>
+__global__ void k_weno_gram(const __grid_constant__ KParams<P, T> kp, double* __restrict__ gram) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NPAIR = NB * (NB + 1) / 2;
+  const MeshDev& m = kp.m;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)NPAIR * m.ne) return;
+  const int pr = (int)(i / m.ne), e = (int)(i - (long long)pr * m.ne);
+  int b = 0, c = pr;
+  while (c >= NB - b) {
+    c -= NB - b;
+    ++b;
+  }
+  c += b;
+  const size_t ld = m.ld;
+  gram[(size_t)pr * ld + e] = gram_entry<P>(&kp.d.dref[0][0][0], kp.d.cell_w, m.jac[e], m.dinv[0 * ld + e],
+                                            m.dinv[1 * ld + e], m.dinv[2 * ld + e], m.dinv[3 * ld + e], b, c);
+}
+
 template <int P>
 struct WenoScratch {
   using V = Variant<P>;
-  static constexpr int ND = (P <= 2) ? V::NQ * V::NB * V::NK : 1;
-  double D[ND];                        // physical derivatives at the cell points (P <= 2)
   double Q[V::NB][V::NB];
   double pol[4][NEQ][V::NB];           // pol[0] = target, pol[j+1] = neighbour j, mode 0 <- target's
   double L[3][4][4], R[3][4][4];
@@ -634,9 +686,9 @@ struct WenoScratch {
 
 template <int P, typename T>
 __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __restrict__ U, int e, int lane,
-                                                WenoScratch<P>& S, const double* __restrict__ s_dref) {
+                                                WenoScratch<P>& S) {
   using V = Variant<P>;
-  constexpr int NB = V::NB, NQ = V::NQ, NK = V::NK;
+  constexpr int NB = V::NB;
   const MeshDev& m = kp.m;
   const size_t ld = m.ld;
   int faces[3], nbrs[3];
@@ -658,8 +710,6 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __re
   if (nbd == 0) lw[0] = 0.997;
   else if (nbd == 1) lw[1] = 0.998;
   else lw[2] = 0.999;
-  const double J = m.jac[e];
-  const double xx = m.dinv[0 * ld + e], xy = m.dinv[1 * ld + e], ex = m.dinv[2 * ld + e], ey = m.dinv[3 * ld + e];
 #pragma unroll
   for (int it = 0; it < (NEQ * NB + 31) / 32; ++it) {
     const int i = lane + 32 * it;
@@ -669,16 +719,6 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __re
 #pragma unroll
     for (int k = 0; k < 3; ++k)
       S.pol[k + 1][v][b] = (interior[k] && b > 0) ? (double)ld_state(&U[(v * NB + b) * ld + nbrs[k]]) : 0.0;
-  }
-  if constexpr (P <= 2) {
-#pragma unroll
-    for (int it = 0; it < (NQ * NB + 31) / 32; ++it) {
-      const int i = lane + 32 * it;
-      if (i >= NQ * NB) break;
-      const double(&r)[NK] = *reinterpret_cast<const double(*)[NK]>(&s_dref[i * NK]);
-#pragma unroll
-      for (int kk = 0; kk < NK; ++kk) S.D[i * NK + kk] = phys_deriv<NK>(r, xx, xy, ex, ey, kk);
-    }
   }
   __syncwarp();
   if (lane < NEQ) {
@@ -693,40 +733,17 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __re
     for (int v = 0; v < NEQ; ++v) mean[v] = S.pol[0][v][0];
     eigenmatrix<double>(mean, geo.x, geo.y, kp.gas, S.L[lane], S.R[lane]);
   }
-  // Gram matrix of the smoothness indicator
-#pragma unroll
-  for (int it = 0; it < (NB * NB + 31) / 32; ++it) {
-    const int pr = lane + 32 * it;
-    if (pr >= NB * NB) break;
-    const int b = pr / NB, c = pr - b * NB;
-    if (c < b) continue;
-    double acc = 0.0;
-#pragma unroll
-    for (int l = 1; l <= P; ++l) {
-      const double jp = (l == 1) ? 1.0 : (l == 2 ? J : J * J);
-#pragma unroll
-      for (int l1 = 0; l1 <= l; ++l1) {
-        const int kk = l * (l + 1) / 2 - 1 + (l - l1);
-        double integral = 0.0;
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-          double db, dc;
-          if constexpr (P <= 2) {
-            db = S.D[(q * NB + b) * NK + kk];
-            dc = S.D[(q * NB + c) * NK + kk];
-          } else {
-            const double(&rb)[NK] = *reinterpret_cast<const double(*)[NK]>(&s_dref[(q * NB + b) * NK]);
-            const double(&rc)[NK] = *reinterpret_cast<const double(*)[NK]>(&s_dref[(q * NB + c) * NK]);
-            db = phys_deriv<NK>(rb, xx, xy, ex, ey, kk);
-            dc = phys_deriv<NK>(rc, xx, xy, ex, ey, kk);
-          }
-          integral += 0.5 * J * kp.d.cell_w[q] * (db * dc);
-        }
-        acc += jp * integral;
-      }
+  // Gram matrix of the smoothness indicator (geometry only: precomputed by k_weno_gram)
+  for (int pr = lane; pr < NB * (NB + 1) / 2; pr += 32) {
+    int b = 0, c = pr;
+    while (c >= NB - b) {
+      c -= NB - b;
+      ++b;
     }
-    S.Q[b][c] = acc;
-    S.Q[c][b] = acc;
+    c += b;
+    const double q = m.gram[(size_t)pr * ld + e];
+    S.Q[b][c] = q;
+    S.Q[c][b] = q;
   }
   __syncwarp();
   // projections onto the characteristic fields of each face (weno.rs:123-124, 155)
@@ -863,14 +880,9 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
                                                                 T* __restrict__ U, unsigned char* __restrict__ t0,
                                                                 unsigned int* __restrict__ status,
                                                                 int* __restrict__ work) {
-  using V = Variant<P>;
-  constexpr int NB = V::NB, NQ = V::NQ, NK = V::NK;
   Control* ctl = kp.ctl;
   const MeshDev& m = kp.m;
   __shared__ WenoScratch<P> scratch[kLimiterWarps];
-  __shared__ double s_dref[NQ * NB * NK];
-  for (int i = threadIdx.x; i < NQ * NB * NK; i += blockDim.x) s_dref[i] = (&kp.d.dref[0][0][0])[i];
-  __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * kLimiterWarps + wib;
   const int nwarps = gridDim.x * kLimiterWarps;
@@ -946,7 +958,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
     // ---- phase B: reconstruct the enlisted elements, one warp each ----
     for (int i = gwarp; i < n_work; i += nwarps) {
       const int et = __ldcg(&work[i]);
-      const int rs = weno_reconstruct<P, T>(kp, U, et, lane, scratch[wib], s_dref);
+      const int rs = weno_reconstruct<P, T>(kp, U, et, lane, scratch[wib]);
       if (rs != ST_OK && lane == 0) {
         const int inst = m.n_inst > 1 ? m.inst[et] : 0;
         raise_status(ctl, &kp.ic[inst], rs, et);

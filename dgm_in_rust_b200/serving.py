@@ -69,6 +69,7 @@ class Result:
     status: int
     dofs: int
     state: np.ndarray | None = None
+    ready_s: float | None = None     # host preparation finished (serving loop only)
 
     @property
     def latency_s(self) -> float:
@@ -80,7 +81,7 @@ def requests_from_stream(stream: list) -> list:
     return [Request(i, float(t), inst) for i, (t, inst) in enumerate(stream)]
 
 
-def footprint_bytes(meshes: list, order: int, precision: str) -> int:
+def footprint_bytes(meshes: list, order: int, precision: str, limiter: bool = True) -> int:
     """Device bytes a batch context of ``meshes`` allocates: the sum of the requested sizes of
     its allocations (what dgm_device_bytes reports), following dgm_create's allocation list."""
     nb = (order + 1) * (order + 2) // 2
@@ -105,9 +106,10 @@ def footprint_bytes(meshes: list, order: int, precision: str) -> int:
     state = 4 * NEQ * nb * ld * eb                                   # U, U1, U2, R
     flux = (n_int + n_bnd) * ng * 4 * eb                             # F
     stage = max_ne * NEQ * nb * 8                                    # FP64 staging
-    limiter = ne * (1 + 4 + 4)                                       # t0, status, work
+    limiter_bytes = ne * (1 + 4 + 4)                                 # t0, status, work
     diag = n * 8 * 8
-    return int(control + geometry + edges + offsets + state + flux + stage + limiter + diag)
+    gram = nb * (nb + 1) // 2 * ld * 8 if limiter else 0              # WENO Gram matrices
+    return int(control + geometry + edges + offsets + state + flux + stage + limiter_bytes + diag + gram)
 
 
 def _prepare_request(req: Request):
@@ -124,9 +126,10 @@ def _warm():
 
 
 class _Member:
-    def __init__(self, req: Request, index: int):
+    def __init__(self, req: Request, index: int, ready_s: float):
         self.req = req
         self.index = index
+        self.ready_s = ready_s
         self.r0 = None
         self.drop = 1.0
         self.done = False
@@ -140,7 +143,7 @@ class _Cohort:
                            device=device, precision=precision)
         for i, it in enumerate(items):
             self.batch.set_initial(i, it[2])
-        self.members = [_Member(it[0], i) for i, it in enumerate(items)]
+        self.members = [_Member(it[0], i, it[3]) for i, it in enumerate(items)]
         self.admitted = now
         self.bytes = self.batch.device_bytes()
         self.checks = 0
@@ -183,6 +186,7 @@ class ServingLoop:
         self.peak_bytes = 0
         self.cohorts_formed = 0
         self.max_concurrent = 0
+        self.stats = {}
         self._realtime = True
 
     def run(self, requests: list, realtime: bool = True) -> list:
@@ -218,6 +222,7 @@ class ServingLoop:
                         time.sleep(wait)
                 pool.submit(_prepare_request, r).add_done_callback(lambda f, r=r: done(f, r))
 
+        self.stats = {"create_s": 0.0, "check_s": 0.0, "idle_s": 0.0, "chunks": 0}
         feed = threading.Thread(target=feeder, daemon=True)
         feed.start()
         waiting: list = []       # prepared, not admitted: (req, mesh, initial, ready_s), in arrival order
@@ -245,13 +250,18 @@ class ServingLoop:
                     if st is None:
                         continue
                     progressed = True
+                    tc = time.perf_counter()
                     finished = self._check(co, results, now)
+                    self.stats["check_s"] += time.perf_counter() - tc
+                    self.stats["chunks"] += 1
                     if finished:
                         active.remove(co)
                         used -= co.bytes
                         co.close()
                 if not progressed and not got:
+                    ti = time.perf_counter()
                     time.sleep(0.0002)
+                    self.stats["idle_s"] += time.perf_counter() - ti
         finally:
             feed.join()
             pool.shutdown(wait=True)
@@ -283,7 +293,9 @@ class ServingLoop:
             ne = 0
             for item in items + [None]:
                 if item is None or (chunk and ne + item[1].n_elements > self.max_cohort_elements):
+                    tc = time.perf_counter()
                     co = _Cohort(chunk, order, self.precision, self.device, self.max_steps, now())
+                    self.stats["create_s"] += time.perf_counter() - tc
                     active.append(co)
                     used += co.bytes
                     self.cohorts_formed += 1
@@ -314,7 +326,7 @@ class ServingLoop:
                 state = b.download(m.index) if self.keep_states else None
                 arrival = m.req.arrival_s if self._realtime else 0.0
                 results.append(Result(m.req.rid, arrival, co.admitted, now(), step, t, m.drop, converged,
-                                      status, m.req.instance.dofs, state))
+                                      status, m.req.instance.dofs, state, m.ready_s))
                 b.set_instance(m.index, t, step, 1.0e30, step)   # switched off from the next launch on
                 m.done = True
         if all(m.done for m in co.members):
@@ -389,6 +401,11 @@ def latency_summary(results: list, wall_s: float) -> dict:
     """p50/p99/mean latency (arrival to retirement) and throughput in DOF-stage updates/s."""
     lat = np.array([r.latency_s for r in results])
     dof_stages = sum(r.dofs * 3 * r.steps for r in results)
-    return {"requests": len(results), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "mean_s": float(lat.mean()), "wall_s": wall_s, "dof_stage_updates_per_s": dof_stages / wall_s,
-            "converged": int(sum(r.converged for r in results)), "failed": int(sum(r.status != 0 for r in results))}
+    out = {"requests": len(results), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+           "mean_s": float(lat.mean()), "wall_s": wall_s, "dof_stage_updates_per_s": dof_stages / wall_s,
+           "converged": int(sum(r.converged for r in results)), "failed": int(sum(r.status != 0 for r in results))}
+    if all(r.ready_s is not None for r in results):
+        out["mean_prep_s"] = float(np.mean([r.ready_s - r.arrival_s for r in results]))
+        out["mean_queue_s"] = float(np.mean([r.admitted_s - r.ready_s for r in results]))
+        out["mean_run_s"] = float(np.mean([r.finished_s - r.admitted_s for r in results]))
+    return out

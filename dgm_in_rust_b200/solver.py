@@ -128,6 +128,22 @@ def initial_state(mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints, hc
     return U
 
 
+def _launch_config(L, ctx) -> dict:
+    cfg = (ctypes.c_int32 * 3)()
+    L.dgm_get_launch_config(ctx, cfg)
+    return {"edge_threads": cfg[0], "edge_blocks": cfg[1], "element_threads": cfg[2]}
+
+
+def _autotune(L, ctx, repeats: int) -> dict:
+    best = (ctypes.c_double * 2)()
+    st = L.dgm_autotune(ctx, int(repeats), best)
+    if st != 0:
+        raise DgmError(st, int(L.dgm_error_location(ctx)), "autotune")
+    out = _launch_config(L, ctx)
+    out.update({"edge_us": best[0], "element_us": best[1]})
+    return out
+
+
 def _check_state(a: np.ndarray, ne: int, nb: int, name: str) -> None:
     if not isinstance(a, np.ndarray) or a.dtype != np.float64 or a.shape != (ne, 4, nb) or not a.flags.c_contiguous:
         raise ValueError(f"{name} must be a C-contiguous float64 array of shape ({ne}, 4, {nb})")
@@ -264,6 +280,20 @@ class SpatialDisc:
         t, w = ctypes.c_int64(0), ctypes.c_int32(0)
         self._lib.dgm_limiter_stats(self._ctx, ctypes.byref(t), ctypes.byref(w))
         return int(t.value), int(w.value)
+
+    # ---- launch configuration (no counterpart in the reference) ----
+    @property
+    def launch_config(self) -> dict:
+        return _launch_config(self._lib, self._ctx)
+
+    def set_launch_config(self, edge_threads: int, edge_blocks: int, element_threads: int) -> None:
+        self._check(self._lib.dgm_set_launch_config(self._ctx, int(edge_threads), int(edge_blocks),
+                                                    int(element_threads)), "set_launch_config")
+
+    def autotune(self, repeats: int = 20) -> dict:
+        """Time the candidate edge/element launch configurations on the resident state and keep
+        the fastest (a state must have been uploaded).  Returns the chosen configuration."""
+        return _autotune(self._lib, self._ctx, repeats)
 
 
 class TemperalDisc:
@@ -474,6 +504,14 @@ class Batch:
 
     def device_bytes(self) -> int:
         return int(self._lib.dgm_device_bytes(self._ctx))
+
+    @property
+    def launch_config(self) -> dict:
+        return _launch_config(self._lib, self._ctx)
+
+    def autotune(self, repeats: int = 20) -> dict:
+        """As SpatialDisc.autotune, for the whole batch (all instances' states uploaded)."""
+        return _autotune(self._lib, self._ctx, repeats)
 
     def state(self, i: int):
         """(current_time, current_step, status, error_location) of instance i."""

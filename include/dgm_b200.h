@@ -177,6 +177,16 @@ void* dgm_stream(dgm_ctx* ctx);
  * second stage buffer), 3 limiter (KXRCF + WENO waves) on that buffer).  Callers time it with
  * events on dgm_stream().  No counterpart in the reference (it has no kernels). */
 int32_t dgm_launch_phase(dgm_ctx* ctx, int32_t phase);
+/* Launch configuration of the edge pass (threads per block; blocks, 0 = one thread per
+ * (edge slot, Gauss point), else a grid-stride grid of that many blocks) and of the element pass
+ * (threads per block = 4 x elements per block).  Threads: multiples of 32 up to 256.  Results do
+ * not depend on it.  No counterpart in the reference. */
+int32_t dgm_set_launch_config(dgm_ctx* ctx, int32_t edge_threads, int32_t edge_blocks, int32_t element_threads);
+int32_t dgm_get_launch_config(dgm_ctx* ctx, int32_t* config /* [3] as above */);
+/* Autotuner: times each candidate configuration of the edge and element passes on the resident
+ * state (repeats launches each, CUDA events) and keeps the fastest; best_us (may be NULL)
+ * receives the chosen edge and element times in microseconds.  Call after a state is uploaded. */
+int32_t dgm_autotune(dgm_ctx* ctx, int32_t repeats, double* best_us /* [2] */);
 /* Launches of that kernel, and of all kernels, per time-march step. */
 int32_t dgm_phase_launches_per_step(dgm_ctx* ctx, int32_t phase);
 int32_t dgm_launches_per_step(dgm_ctx* ctx);

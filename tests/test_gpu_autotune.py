@@ -1,0 +1,78 @@
+"""Launch configuration and autotuner: the chosen grouping of edge slots and elements into blocks
+must not change any result.  Tolerance: bitwise."""
+import numpy as np
+import pytest
+
+from dgm_in_rust_b200 import Batch, DgmError, build_solver
+from dgm_in_rust_b200.workloads import Instance, instance_mesh
+
+CONFIGS = [(256, 0, 256), (64, 0, 64), (128, 7, 128), (96, 1, 32), (32, 3, 160)]
+
+
+def _advance(mesh, init, order, precision, steps, config=None, tune=False):
+    s = build_solver(mesh, order, 1.4, 0.1, 1.0e30, steps, precision=precision)
+    try:
+        sd, td = s.spatial_disc, s.temporal_disc
+        td.set_initial_on_device(init)
+        if config is not None:
+            sd.set_launch_config(*config)
+            assert tuple(sd.launch_config.values()) == config
+        if tune:
+            chosen = sd.autotune(repeats=3)
+            assert chosen["edge_us"] > 0 and chosen["element_us"] > 0
+            assert chosen["element_threads"] in (64, 128, 256)
+        td.advance(steps)
+        td.synchronize()
+        U = sd.new_state()
+        td.download(U)
+        return U, td.current_time
+    finally:
+        s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_launch_config_does_not_change_results(built, order, precision):
+    mesh, init = instance_mesh(Instance(40, 20, 0.8, 1.25, order))
+    U0, t0 = _advance(mesh, init, order, precision, 6)
+    for cfg in CONFIGS[1:]:
+        U, t = _advance(mesh, init, order, precision, 6, config=cfg)
+        assert t == t0 and np.array_equal(U, U0), cfg
+    U, t = _advance(mesh, init, order, precision, 6, tune=True)
+    assert t == t0 and np.array_equal(U, U0)
+
+
+@pytest.mark.gpu
+def test_launch_config_rejects_bad_values(built):
+    mesh, init = instance_mesh(Instance(16, 8, 0.5, 2.0, 2))
+    s = build_solver(mesh, 2, 1.4, 0.1, 1.0, 5)
+    try:
+        for bad in [(0, 0, 256), (48, 0, 256), (512, 0, 256), (256, -1, 256), (256, 0, 288)]:
+            with pytest.raises(DgmError):
+                s.spatial_disc.set_launch_config(*bad)
+        assert s.spatial_disc.launch_config == {"edge_threads": 256, "edge_blocks": 0, "element_threads": 256}
+    finally:
+        s.close()
+
+
+@pytest.mark.gpu
+def test_batch_autotune_keeps_results(built):
+    insts = [Instance(24, 12, 0.6, 1.0, 2), Instance(32, 16, 0.8, -2.0, 2)]
+    built_ = [instance_mesh(i) for i in insts]
+
+    def run(tune):
+        b = Batch([m for m, _ in built_], 2, 1.4, [0.1] * 2, [1.0e30] * 2, [5] * 2, precision="fp32")
+        try:
+            for i, (_, init) in enumerate(built_):
+                b.set_initial(i, init)
+            if tune:
+                b.autotune(repeats=3)
+            b.advance(5)
+            assert b.synchronize() == 0
+            return [b.download(i) for i in range(2)]
+        finally:
+            b.close()
+
+    for a, c in zip(run(False), run(True)):
+        assert np.array_equal(a, c)

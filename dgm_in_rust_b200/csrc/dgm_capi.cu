@@ -59,7 +59,9 @@ struct dgm_ctx {
   InstCtl* ic = nullptr;
   std::vector<void*> allocs;
   int64_t bytes = 0;
-  int coop_blocks = 1;
+  int coop_blocks[2] = {1, 1};  // co-resident limiter blocks of the compact / staged detector
+  int lim_staged = 0;            // limiter detector variant (dgm_set_limiter_variant / autotune)
+  float lim_us[2] = {0.f, 0.f};  // last autotuned limiter times, compact / staged
   // launch configuration of the edge and element passes (dgm_set_launch_config / dgm_autotune):
   // edge_blocks = 0 launches one thread per (slot, Gauss point), else a grid-stride grid
   int edge_threads = 256, edge_blocks = 0, elem_threads = 256;
@@ -158,7 +160,7 @@ struct Ops {
   static int limiter(dgm_ctx* c, T* U) {
     if (!c->limiter) return DGM_OK;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(c->coop_blocks);
+    cfg.gridDim = dim3(c->coop_blocks[c->lim_staged]);
     cfg.blockDim = dim3(dgm::kLimiterWarps * 32);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = c->stream;
@@ -167,7 +169,10 @@ struct Ops {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter<P, T>, kp_of<P, T>(c), U, c->t0, c->status, c->work));
+    if (c->lim_staged)
+      CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter<P, T, true>, kp_of<P, T>(c), U, c->t0, c->status, c->work));
+    else
+      CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter<P, T, false>, kp_of<P, T>(c), U, c->t0, c->status, c->work));
     return DGM_OK;
   }
 
@@ -260,11 +265,12 @@ struct Ops {
   }
 
   static int occupancy(dgm_ctx* c) {
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dgm::k_limiter<P, T>, dgm::kLimiterWarps * 32, 0));
-    per_sm = std::max(1, per_sm);
+    int per_sm[2] = {0, 0};
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], dgm::k_limiter<P, T, false>, dgm::kLimiterWarps * 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], dgm::k_limiter<P, T, true>, dgm::kLimiterWarps * 32, 0));
     const int64_t want = std::max<int64_t>(1, (c->ne + 32 * dgm::kLimiterWarps - 1) / (32 * dgm::kLimiterWarps));
-    c->coop_blocks = (int)std::min<int64_t>((int64_t)per_sm * c->num_sms, want);
+    for (int v = 0; v < 2; ++v)
+      c->coop_blocks[v] = (int)std::min<int64_t>((int64_t)std::max(1, per_sm[v]) * c->num_sms, want);
     return DGM_OK;
   }
 
@@ -1092,6 +1098,25 @@ int32_t dgm_set_launch_config(dgm_ctx* c, int32_t edge_threads, int32_t edge_blo
   return DGM_OK;
 }
 
+int32_t dgm_set_limiter_variant(dgm_ctx* c, int32_t staged) {
+  if (!c || (staged != 0 && staged != 1)) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  CK(cudaStreamSynchronize(c->stream));
+  c->lim_staged = staged;
+  reset_graphs(c);
+  return DGM_OK;
+}
+
+int32_t dgm_get_limiter_variant(dgm_ctx* c, int32_t* staged, double* tuned_us) {
+  if (!c) return DGM_BAD_ARG;
+  if (staged) *staged = c->lim_staged;
+  if (tuned_us) {
+    tuned_us[0] = c->lim_us[0];
+    tuned_us[1] = c->lim_us[1];
+  }
+  return DGM_OK;
+}
+
 int32_t dgm_get_launch_config(dgm_ctx* c, int32_t* config) {
   if (!c || !config) return DGM_BAD_ARG;
   config[0] = c->edge_threads;
@@ -1145,6 +1170,36 @@ int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
   };
   float best_edge = 1e30f, best_elem = 1e30f;
   int be_t = c->edge_threads, be_b = c->edge_blocks, bl_t = c->elem_threads;
+  // limiter detector variant: each timed launch limits the same stage buffer, rebuilt by an edge
+  // and an element pass before it (only the limiter sits between the events)
+  auto time_limiter = [&](float* us) -> int {
+    float tot = 0.f;
+    for (int r = 0; r < repeats + 2; ++r) {
+      int s2 = dispatch(c, [&](auto ops) {
+        using O = decltype(ops);
+        int s3 = O::edge_flux(c, O::S(c->U));
+        if (!s3) s3 = O::template element<2>(c, O::S(c->U), O::S(c->U), O::S(c->U2), nullptr, nullptr);
+        if (!s3) CK(cudaEventRecord(e0, c->stream));
+        if (!s3) s3 = O::limiter(c, O::S(c->U2));
+        if (!s3) CK(cudaEventRecord(e1, c->stream));
+        return s3;
+      });
+      if (s2) return s2;
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (r >= 2) tot += ms;
+    }
+    *us = 1000.f * tot / repeats;
+    return DGM_OK;
+  };
+  if (c->limiter) {
+    for (int v = 0; v < 2 && !st; ++v) {
+      c->lim_staged = v;
+      st = time_limiter(&c->lim_us[v]);
+    }
+    c->lim_staged = (!st && c->lim_us[1] < c->lim_us[0]) ? 1 : 0;
+  }
   for (auto& cand : edge_cand) {
     c->edge_threads = cand[0];
     c->edge_blocks = cand[1];

@@ -608,6 +608,104 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
   return (ind_d >= 1.0) || (ind_e >= 1.0);
 }
 
+// The same detector with its loads in three rounds, each issued in full before it is used: the
+// element's faces and neighbours, then its own state, the face normals and h^1.5, then the
+// neighbours' density and energy modes of the inflow faces.  Fewer dependent memory round trips
+// than kxrcf (which walks the faces one after another) at the price of registers: faster when
+// a pass is latency-bound (small meshes), slower when occupancy matters (large batches); the
+// autotuner picks one per context.  Same arithmetic in the same order, so the same flags.
+template <int P, typename T>
+__device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* __restrict__ U, int e) {
+  int fw[3], nb[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    fw[k] = kp.m.face[k * kp.m.ld + e];
+    nb[k] = kp.m.nbr[k * kp.m.ld + e];
+  }
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NG = V::NG;
+  const MeshDev& m = kp.m;
+  const size_t ld = m.ld;
+  double own[NEQ][NB];
+#pragma unroll
+  for (int v = 0; v < NEQ; ++v)
+#pragma unroll
+    for (int b = 0; b < NB; ++b) own[v][b] = (double)ld_state(&U[(v * NB + b) * ld + e]);
+  double nx[3], ny[3], jd[3];
+  bool interior[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int slot = fw[k] >> 1;
+    interior[k] = slot < m.n_int;
+    const double4 geo = interior[k] ? m.ie_geo[slot] : make_double4(0.0, 0.0, 0.0, 0.0);
+    nx[k] = (fw[k] & 1) ? -geo.x : geo.x;
+    ny[k] = (fw[k] & 1) ? -geo.y : geo.y;
+    jd[k] = geo.w;
+  }
+  const double h15 = m.h15[e];
+  // inflow test at the centre Gauss point (weno.rs:42-52)
+  constexpr int cg = NG / 2;
+  bool inflow[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double rho_u = 0.0, rho_v = 0.0;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      rho_u += own[1][b] * kp.d.phi_edge[k][cg][b];
+      rho_v += own[2][b] * kp.d.phi_edge[k][cg][b];
+    }
+    inflow[k] = interior[k] && (rho_u * nx[k] + rho_v * ny[k] < 0.0);
+  }
+  double ext_rho[3][NB], ext_rhoe[3][NB];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      ext_rho[k][b] = inflow[k] ? (double)ld_state(&U[(0 * NB + b) * ld + nb[k]]) : 0.0;
+      ext_rhoe[k][b] = inflow[k] ? (double)ld_state(&U[(3 * NB + b) * ld + nb[k]]) : 0.0;
+    }
+  double density_jump = 0.0, total_energy_jump = 0.0, surface = 0.0;
+  double min_density = 1.0e10, min_total_energy = 1.0e10;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (!interior[k]) continue;
+    double own_rho[NG], own_rhoe[NG];
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+      double rho = 0.0, rho_e = 0.0;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        rho += own[0][b] * kp.d.phi_edge[k][g][b];
+        rho_e += own[3][b] * kp.d.phi_edge[k][g][b];
+      }
+      own_rho[g] = rho;
+      own_rhoe[g] = rho_e;
+      if (rho < min_density) min_density = rho;
+      if (rho_e < min_total_energy) min_total_energy = rho_e;
+    }
+    if (inflow[k]) {
+      double rho_jump = 0.0, rho_e_jump = 0.0;
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        double er = 0.0, ere = 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          er += ext_rho[k][b] * kp.d.phi_edge[k][NG - 1 - g][b];
+          ere += ext_rhoe[k][b] * kp.d.phi_edge[k][NG - 1 - g][b];
+        }
+        rho_jump += 0.5 * jd[k] * kp.d.edge_w[g] * (own_rho[g] - er);
+        rho_e_jump += 0.5 * jd[k] * kp.d.edge_w[g] * (own_rhoe[g] - ere);
+      }
+      density_jump += rho_jump;
+      total_energy_jump += rho_e_jump;
+      surface += jd[k];
+    }
+  }
+  const double ind_d = fabs(density_jump) / (h15 * surface * min_density);
+  const double ind_e = fabs(total_energy_jump) / (h15 * surface * min_total_energy);
+  return (ind_d >= 1.0) || (ind_e >= 1.0);
+}
+
 // ------------------------------------------------------------------------------------------
 // weno, weno.rs:86-269: characteristic WENO reconstruction of element e by one warp (FP64).
 //
@@ -685,20 +783,18 @@ struct WenoScratch {
 };
 
 template <int P, typename T>
-__device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __restrict__ U, int e, int lane,
+__device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __restrict__ U, int e,
+                                                const int (&faces)[3], const int (&nbrs)[3], int lane,
                                                 WenoScratch<P>& S) {
   using V = Variant<P>;
   constexpr int NB = V::NB;
   const MeshDev& m = kp.m;
   const size_t ld = m.ld;
-  int faces[3], nbrs[3];
   bool interior[3];
   int nbd = 0;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    faces[k] = m.face[k * ld + e];
     interior[k] = (faces[k] >> 1) < m.n_int;
-    nbrs[k] = m.nbr[k * ld + e];
     if (!interior[k]) ++nbd;
   }
   if (nbd > 2) return ST_TOO_MANY_BOUNDARY_EDGES;
@@ -710,15 +806,55 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __re
   if (nbd == 0) lw[0] = 0.997;
   else if (nbd == 1) lw[1] = 0.998;
   else lw[2] = 0.999;
+  // one round of global loads: the state of e and of its interior neighbours, e's Gram matrix
+  // (geometry only: precomputed by k_weno_gram), the face normals (lanes 0-2) and the
+  // neighbours' Jacobians
+  constexpr int NLD = (NEQ * NB + 31) / 32, NPAIR = NB * (NB + 1) / 2, NQL = (NPAIR + 31) / 32;
+  double own[NLD], nbv[NLD][3], qv[NQL];
 #pragma unroll
-  for (int it = 0; it < (NEQ * NB + 31) / 32; ++it) {
+  for (int it = 0; it < NLD; ++it) {
     const int i = lane + 32 * it;
-    if (i >= NEQ * NB) break;
-    const int v = i / NB, b = i - v * NB;
-    S.pol[0][v][b] = (double)ld_state(&U[(v * NB + b) * ld + e]);
+    const bool ok = i < NEQ * NB;
+    const int b = i % NB;
+    own[it] = ok ? (double)ld_state(&U[(size_t)i * ld + e]) : 0.0;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-      S.pol[k + 1][v][b] = (interior[k] && b > 0) ? (double)ld_state(&U[(v * NB + b) * ld + nbrs[k]]) : 0.0;
+      nbv[it][k] = (ok && interior[k] && b > 0) ? (double)ld_state(&U[(size_t)i * ld + nbrs[k]]) : 0.0;
+  }
+#pragma unroll
+  for (int it = 0; it < NQL; ++it) {
+    const int pr = lane + 32 * it;
+    qv[it] = pr < NPAIR ? m.gram[(size_t)pr * ld + e] : 0.0;
+  }
+  const int my_face = lane == 0 ? faces[0] : (lane == 1 ? faces[1] : faces[2]);
+  const bool my_interior = lane < 3 && (lane == 0 ? interior[0] : (lane == 1 ? interior[1] : interior[2]));
+  const double4 geo = my_interior ? m.ie_geo[my_face >> 1] : make_double4(0.0, 0.0, 0.0, 0.0);
+  double Jn[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) Jn[k] = interior[k] ? m.jac[nbrs[k]] : 0.0;
+#pragma unroll
+  for (int it = 0; it < NLD; ++it) {
+    const int i = lane + 32 * it;
+    if (i < NEQ * NB) {
+      const int v = i / NB, b = i - v * NB;
+      S.pol[0][v][b] = own[it];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) S.pol[k + 1][v][b] = nbv[it][k];
+    }
+  }
+#pragma unroll
+  for (int it = 0; it < NQL; ++it) {
+    const int pr = lane + 32 * it;
+    if (pr < NPAIR) {
+      int b = 0, c = pr;
+      while (c >= NB - b) {
+        c -= NB - b;
+        ++b;
+      }
+      c += b;
+      S.Q[b][c] = qv[it];
+      S.Q[c][b] = qv[it];
+    }
   }
   __syncwarp();
   if (lane < NEQ) {
@@ -726,24 +862,11 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __re
     for (int k = 0; k < 3; ++k)
       if (interior[k]) S.pol[k + 1][lane][0] = S.pol[0][lane][0];
   }
-  if (lane < 3 && interior[lane]) {
-    const double4 geo = m.ie_geo[faces[lane] >> 1];  // unoriented normal (weno.rs:121-122)
+  if (my_interior) {  // unoriented normal (weno.rs:121-122)
     double mean[4];
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) mean[v] = S.pol[0][v][0];
     eigenmatrix<double>(mean, geo.x, geo.y, kp.gas, S.L[lane], S.R[lane]);
-  }
-  // Gram matrix of the smoothness indicator (geometry only: precomputed by k_weno_gram)
-  for (int pr = lane; pr < NB * (NB + 1) / 2; pr += 32) {
-    int b = 0, c = pr;
-    while (c >= NB - b) {
-      c -= NB - b;
-      ++b;
-    }
-    c += b;
-    const double q = m.gram[(size_t)pr * ld + e];
-    S.Q[b][c] = q;
-    S.Q[c][b] = q;
   }
   __syncwarp();
   // projections onto the characteristic fields of each face (weno.rs:123-124, 155)
@@ -801,12 +924,10 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __re
   }
   __syncwarp();
   // back to conserved variables, area-weighted average over the faces in order (weno.rs:195-263)
-  double neighbour_area = 0.0, Jn[3];
+  double neighbour_area = 0.0;
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    Jn[k] = interior[k] ? m.jac[nbrs[k]] : 0.0;
+  for (int k = 0; k < 3; ++k)
     if (interior[k]) neighbour_area += Jn[k] * 0.5;
-  }
   const double inv_area = 1.0 / neighbour_area;
   for (int idx = lane; idx < NEQ * NB; idx += 32) {
     const int r = idx / NB, b = idx - r * NB;
@@ -875,7 +996,7 @@ constexpr int kLimiterWarps = 4;
 // Wave count = longest chain of increasing-index neighbours through unsettled elements: 2 on
 // the O-grid's 2-colour numbering.  Instances never share neighbours, so one pass limits all of
 // them; elements of instances that are not stepping settle clean without evaluation.
-template <int P, typename T>
+template <int P, typename T, bool STAGED>
 __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_constant__ KParams<P, T> kp,
                                                                 T* __restrict__ U, unsigned char* __restrict__ t0,
                                                                 unsigned int* __restrict__ status,
@@ -899,7 +1020,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
         if (wave == 1) {
           const int inst = m.n_inst > 1 ? m.inst[e] : 0;
           if (kp.ic[inst].active) {
-            flag0 = kxrcf<P, T>(kp, U, e);
+            flag0 = STAGED ? kxrcf_staged<P, T>(kp, U, e) : kxrcf<P, T>(kp, U, e);
             pending = true;
           } else {
             ready = true;  // not stepping: settles clean, never read as rewritten
@@ -925,7 +1046,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
               }
             }
           }
-          if (ready) trouble = (wave == 1) ? flag0 : (any_mod ? kxrcf<P, T>(kp, U, e) : (t0[e] != 0));
+          if (ready) trouble = (wave == 1) ? flag0 : (any_mod ? (STAGED ? kxrcf_staged<P, T>(kp, U, e) : kxrcf<P, T>(kp, U, e)) : (t0[e] != 0));
         }
         if (wave == 1 && !ready) status[e] = 0u;
         if (ready && !trouble) status[e] = ((unsigned int)wave << 2) | 1u;
@@ -958,7 +1079,13 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
     // ---- phase B: reconstruct the enlisted elements, one warp each ----
     for (int i = gwarp; i < n_work; i += nwarps) {
       const int et = __ldcg(&work[i]);
-      const int rs = weno_reconstruct<P, T>(kp, U, et, lane, scratch[wib]);
+      int fwt[3], nbt[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        fwt[k] = m.face[k * m.ld + et];
+        nbt[k] = m.nbr[k * m.ld + et];
+      }
+      const int rs = weno_reconstruct<P, T>(kp, U, et, fwt, nbt, lane, scratch[wib]);
       if (rs != ST_OK && lane == 0) {
         const int inst = m.n_inst > 1 ? m.inst[et] : 0;
         raise_status(ctl, &kp.ic[inst], rs, et);

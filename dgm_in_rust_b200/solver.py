@@ -131,7 +131,10 @@ def initial_state(mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints, hc
 def _launch_config(L, ctx) -> dict:
     cfg = (ctypes.c_int32 * 3)()
     L.dgm_get_launch_config(ctx, cfg)
-    return {"edge_threads": cfg[0], "edge_blocks": cfg[1], "element_threads": cfg[2]}
+    staged = ctypes.c_int32(0)
+    L.dgm_get_limiter_variant(ctx, ctypes.byref(staged), None)
+    return {"edge_threads": cfg[0], "edge_blocks": cfg[1], "element_threads": cfg[2],
+            "limiter_detector": "staged" if staged.value else "compact"}
 
 
 def _autotune(L, ctx, repeats: int) -> dict:
@@ -140,7 +143,9 @@ def _autotune(L, ctx, repeats: int) -> dict:
     if st != 0:
         raise DgmError(st, int(L.dgm_error_location(ctx)), "autotune")
     out = _launch_config(L, ctx)
-    out.update({"edge_us": best[0], "element_us": best[1]})
+    lim = (ctypes.c_double * 2)()
+    L.dgm_get_limiter_variant(ctx, None, lim)
+    out.update({"edge_us": best[0], "element_us": best[1], "limiter_compact_us": lim[0], "limiter_staged_us": lim[1]})
     return out
 
 
@@ -290,9 +295,15 @@ class SpatialDisc:
         self._check(self._lib.dgm_set_launch_config(self._ctx, int(edge_threads), int(edge_blocks),
                                                     int(element_threads)), "set_launch_config")
 
+    def set_limiter_detector(self, staged: bool) -> None:
+        """Pick the limiter's KXRCF detector form: staged loads (fewer memory round trips, more
+        registers) or compact; both give the same flags.  The autotuner picks one per context."""
+        self._check(self._lib.dgm_set_limiter_variant(self._ctx, 1 if staged else 0), "set_limiter_detector")
+
     def autotune(self, repeats: int = 20) -> dict:
-        """Time the candidate edge/element launch configurations on the resident state and keep
-        the fastest (a state must have been uploaded).  Returns the chosen configuration."""
+        """Time the candidate edge/element launch configurations and the two limiter detector
+        forms on the resident state and keep the fastest (a state must have been uploaded).
+        Returns the chosen configuration."""
         return _autotune(self._lib, self._ctx, repeats)
 
 

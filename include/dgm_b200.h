@@ -183,10 +183,19 @@ int32_t dgm_launch_phase(dgm_ctx* ctx, int32_t phase);
  * not depend on it.  No counterpart in the reference. */
 int32_t dgm_set_launch_config(dgm_ctx* ctx, int32_t edge_threads, int32_t edge_blocks, int32_t element_threads);
 int32_t dgm_get_launch_config(dgm_ctx* ctx, int32_t* config /* [3] as above */);
-/* Autotuner: times each candidate configuration of the edge and element passes on the resident
- * state (repeats launches each, CUDA events) and keeps the fastest; best_us (may be NULL)
- * receives the chosen edge and element times in microseconds.  Call after a state is uploaded. */
+/* Autotuner: times each candidate configuration of the edge and element passes, and both forms
+ * of the limiter's KXRCF detector, on the resident state (repeats launches each, CUDA events)
+ * and keeps the fastest; best_us (may be NULL) receives the chosen edge and element times in
+ * microseconds.  Call after a state is uploaded. */
 int32_t dgm_autotune(dgm_ctx* ctx, int32_t repeats, double* best_us /* [2] */);
+/* The limiter's detector form (modified_kxrcf, weno.rs:7-85, same arithmetic in both): 0 compact
+ * (walks the faces in turn: fewer registers, better for large batches), 1 staged (all loads of a
+ * round issued together: fewer memory round trips, better for small meshes).  The flags and
+ * results are the same.  No counterpart in the reference. */
+int32_t dgm_set_limiter_variant(dgm_ctx* ctx, int32_t staged);
+/* Current form, and the limiter times the last dgm_autotune measured for forms 0 and 1 (us;
+ * either pointer may be NULL). */
+int32_t dgm_get_limiter_variant(dgm_ctx* ctx, int32_t* staged, double* tuned_us /* [2] */);
 /* Launches of that kernel, and of all kernels, per time-march step. */
 int32_t dgm_phase_launches_per_step(dgm_ctx* ctx, int32_t phase);
 int32_t dgm_launches_per_step(dgm_ctx* ctx);

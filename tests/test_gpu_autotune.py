@@ -16,7 +16,7 @@ def _advance(mesh, init, order, precision, steps, config=None, tune=False):
         td.set_initial_on_device(init)
         if config is not None:
             sd.set_launch_config(*config)
-            assert tuple(sd.launch_config.values()) == config
+            assert tuple(sd.launch_config.values())[:3] == config
         if tune:
             chosen = sd.autotune(repeats=3)
             assert chosen["edge_us"] > 0 and chosen["element_us"] > 0
@@ -51,7 +51,10 @@ def test_launch_config_rejects_bad_values(built):
         for bad in [(0, 0, 256), (48, 0, 256), (512, 0, 256), (256, -1, 256), (256, 0, 288)]:
             with pytest.raises(DgmError):
                 s.spatial_disc.set_launch_config(*bad)
-        assert s.spatial_disc.launch_config == {"edge_threads": 256, "edge_blocks": 0, "element_threads": 256}
+        assert s.spatial_disc.launch_config == {"edge_threads": 256, "edge_blocks": 0, "element_threads": 256,
+                                                "limiter_detector": "compact"}
+        sd = s.spatial_disc
+        assert sd._lib.dgm_set_limiter_variant(sd.ctx, 2) == 7  # DGM_BAD_ARG
     finally:
         s.close()
 
@@ -76,3 +79,38 @@ def test_batch_autotune_keeps_results(built):
 
     for a, c in zip(run(False), run(True)):
         assert np.array_equal(a, c)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_limiter_detector_forms_agree(built, order, precision):
+    """The staged and compact KXRCF detectors flag the same cells, limit a perturbed state
+    identically and give the same time steps."""
+    mesh, init = instance_mesh(Instance(40, 20, 0.8, 1.25, order))
+    rng = np.random.default_rng(order)
+    out = []
+    for staged in (False, True):
+        s = build_solver(mesh, order, 1.4, 0.1, 1.0e30, 6, precision=precision)
+        try:
+            sd, td = s.spatial_disc, s.temporal_disc
+            sd.set_limiter_detector(staged)
+            assert sd.launch_config["limiter_detector"] == ("staged" if staged else "compact")
+            td.set_initial_on_device(init)
+            U = sd.new_state()
+            td.download(U)
+            if staged is False:
+                noise = 0.1 * rng.standard_normal(U[:, :, 1:].shape) * np.abs(U[:, :, :1])
+            Up = U.copy()
+            Up[:, :, 1:] += noise
+            n_limited = sd.apply_limiter(Up)
+            td.advance(6)
+            td.synchronize()
+            td.download(U)
+            out.append((Up, n_limited, U, td.current_time))
+        finally:
+            s.close()
+    (La, na, Ua, ta), (Lb, nb, Ub, tb) = out
+    assert na == nb and na > 0
+    assert np.array_equal(La, Lb)
+    assert ta == tb and np.array_equal(Ua, Ub)

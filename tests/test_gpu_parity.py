@@ -90,9 +90,12 @@ def test_limiter_parity(order, mesh):
     s.close()
 
 
-def test_limiter_heavy_sequential_dependencies():
-    """Many touching troubled cells in quad numbering: exercises long wave chains."""
+@pytest.mark.parametrize("staged", [False, True])
+def test_limiter_heavy_sequential_dependencies(staged):
+    """Many touching troubled cells in quad numbering: exercises long wave chains (both forms of
+    the KXRCF detector)."""
     s, o, U0 = pair(naca0012_ogrid(48, 24, order="quad"))
+    s.spatial_disc.set_limiter_detector(staged)
     U = perturbed(U0, 0.25, 5)
     Uo, Ug = U.copy(), U.copy()
     assert s.spatial_disc.apply_limiter(Ug) == o.apply_limiter(Uo)

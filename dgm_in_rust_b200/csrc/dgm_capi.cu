@@ -70,6 +70,7 @@ struct dgm_ctx {
   int graph_steps = 8;
   bool graphs_broken = false;
   bool limits_dirty = false;
+  bool dt_dirty = false;  // a host-driven time step left its minimum in the control blocks
   int64_t err_where = -1;
   int64_t last_troubled = 0;
   int last_waves = 0;
@@ -176,6 +177,14 @@ struct Ops {
     return DGM_OK;
   }
 
+  static int step_head(dgm_ctx* c, const T* U) {
+    const int threads = 256;
+    const int blocks = (int)std::max<int64_t>(1, (c->ne + threads - 1) / threads);
+    dgm::k_step_head<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U);
+    CK(cudaGetLastError());
+    return DGM_OK;
+  }
+
   static int time_step(dgm_ctx* c, const T* U) {
     const int threads = 256;
     const int blocks = (int)std::max<int64_t>(1, (c->ne + threads - 1) / threads);
@@ -210,12 +219,8 @@ struct Ops {
   static int step(dgm_ctx* c, T* Rout) {
     const int n = (int)c->inst.size();
     const int tb = 128, nblk = (n + tb - 1) / tb;
-    dgm::k_step_begin<<<nblk, tb, 0, c->stream>>>(c->ctl, c->ic, n);
-    CK(cudaGetLastError());
     int st;
-    if ((st = time_step(c, S(c->U)))) return st;
-    dgm::k_step_dt<<<nblk, tb, 0, c->stream>>>(c->ic, n);
-    CK(cudaGetLastError());
+    if ((st = step_head(c, S(c->U)))) return st;
     if ((st = rk3(c, Rout))) return st;
     dgm::k_step_end<<<nblk, tb, 0, c->stream>>>(c->ic, n);
     CK(cudaGetLastError());
@@ -426,10 +431,15 @@ int write_clock(dgm_ctx* c) {
     hi[i].cfl = c->inst[i].cfl;
     hi[i].status = c->inst[i].status;
     hi[i].err_where = c->inst[i].err_where;
+    const double start = 1.0e10;  // the time step's start value, temporal_disc.rs:59
+    std::memcpy(&hi[i].dt_bits, &start, sizeof(double));
   }
+  h.head_done = 0u;
   CK(cudaMemcpyAsync(c->ic, hi.data(), sizeof(InstCtl) * hi.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(&c->ctl->head_done, &h.head_done, sizeof(unsigned int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->limits_dirty = false;
+  c->dt_dirty = false;
   return DGM_OK;
 }
 
@@ -960,6 +970,7 @@ int32_t dgm_compute_time_step(dgm_ctx* c, const double* solutions, double* time_
   if ((st = read_control(c, &h, &hi))) return st;
   unsigned long long bits = hi[0].dt_bits;
   std::memcpy(time_step, &bits, sizeof(double));
+  c->dt_dirty = true;
   return collect_status(c);
 }
 
@@ -1033,7 +1044,7 @@ int32_t dgm_download_solutions(dgm_ctx* c, double* solutions) {
 int32_t dgm_advance(dgm_ctx* c, int64_t n_steps) {
   if (!c || n_steps < 0) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
-  if (c->limits_dirty) {
+  if (c->limits_dirty || c->dt_dirty) {
     int st = write_clock(c);
     if (st) return st;
   }
@@ -1043,7 +1054,7 @@ int32_t dgm_advance(dgm_ctx* c, int64_t n_steps) {
 int32_t dgm_advance_with_residual(dgm_ctx* c, int64_t n_steps) {
   if (!c || n_steps < 0) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
-  if (c->limits_dirty) {
+  if (c->limits_dirty || c->dt_dirty) {
     int st = write_clock(c);
     if (st) return st;
   }
@@ -1076,7 +1087,7 @@ int32_t dgm_launch_phase(dgm_ctx* c, int32_t phase) {
   return dispatch(c, [&](auto ops) {
     using O = decltype(ops);
     switch (phase) {
-      case 0: return O::time_step(c, O::S(c->U));
+      case 0: c->dt_dirty = true; return O::time_step(c, O::S(c->U));
       case 1: return O::edge_flux(c, O::S(c->U));
       case 2: return O::template element<2>(c, O::S(c->U), O::S(c->U), O::S(c->U2), nullptr, nullptr);
       default: return O::limiter(c, O::S(c->U2));
@@ -1238,7 +1249,7 @@ int32_t dgm_phase_launches_per_step(dgm_ctx* c, int32_t phase) {
 
 int32_t dgm_launches_per_step(dgm_ctx* c) {
   if (!c) return 0;
-  return 3 /* step control */ + 1 /* time step */ + 3 * (2 + (c->limiter ? 1 : 0));
+  return 1 /* step head: loop condition + time step */ + 1 /* step end */ + 3 * (2 + (c->limiter ? 1 : 0));
 }
 
 int64_t dgm_error_location(dgm_ctx* c) { return c ? c->err_where : -1; }

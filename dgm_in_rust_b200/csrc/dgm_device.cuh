@@ -110,6 +110,7 @@ struct Control {
   int unknown[2];              // per-wave count of unsettled cells (double-buffered)
   int wl_count[2];             // per-wave worklist length (double-buffered)
   unsigned int bar_count, bar_gen;  // grid barrier of the limiter kernel
+  unsigned int head_done;      // blocks of k_step_head that have finished (last one closes the step head)
 };
 
 // Gas constants, computed once on the host from hcr with the reference's expressions.
@@ -1094,8 +1095,9 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
       if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
       ++troubled_local;
     }
+    if (remaining == 0) break;  // no further wave: nothing reads what this phase wrote
     if (!grid_barrier(ctl, gridDim.x)) break;
-    if (remaining == 0 || wave > m.ne + 2) break;
+    if (wave > m.ne + 2) break;
   }
   if (lane == 0 && troubled_local) atomicAdd(&ctl->troubled, troubled_local);
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->waves = wave;
@@ -1144,23 +1146,84 @@ __global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KPara
   }
 }
 
-// Loop head of time_march (temporal_disc.rs:22), per instance: decide whether this step runs.
-__global__ void k_step_begin(Control* ctl, InstCtl* ic, int n_inst) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) ctl->troubled = 0;
-  if (i >= n_inst) return;
-  InstCtl& c = ic[i];
-  c.active = (c.status == 0 && c.step < c.final_step && c.t < c.final_time) ? 1 : 0;
-  c.dt_bits = (unsigned long long)__double_as_longlong(1.0e10);
+// Head of one time_march iteration (temporal_disc.rs:22-26) in one launch: the loop condition of
+// every instance, its CFL time step (compute_time_step, temporal_disc.rs:58-88, as k_time_step)
+// and the clamp to final_time.  Every thread evaluates the loop condition of its element's
+// instance from the clock it reads (nothing writes the clocks during this kernel); the last block
+// to finish (counted in Control::head_done) publishes `active` and the clamped dt.  dt_bits must
+// hold the bits of 1e10 (the reference's start value) on entry: the last block restores it after
+// reading the minimum, and the host restores it after host-driven time steps.
+__device__ __forceinline__ bool step_runs(const InstCtl& c) {
+  return c.status == 0 && c.step < c.final_step && c.t < c.final_time;
 }
-// temporal_disc.rs:23-26: the step's dt, clamped to reach final_time exactly.
-__global__ void k_step_dt(InstCtl* ic, int n_inst) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_inst || !ic[i].active) return;
-  double dt = __longlong_as_double((long long)ic[i].dt_bits);
-  if (ic[i].t + dt > ic[i].final_time) dt = ic[i].final_time - ic[i].t;
-  ic[i].dt = dt;
+
+template <int P, typename T>
+__global__ void __launch_bounds__(256) k_step_head(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB;
+  const MeshDev& m = kp.m;
+  InstCtl* ic = kp.ic;
+  Control* ctl = kp.ctl;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ec = e < m.ne ? e : m.ne - 1;
+  const int inst = m.n_inst > 1 ? m.inst[ec] : 0;
+  unsigned long long bits = 0x7ff0000000000000ull;
+  if (e < m.ne && step_runs(ic[inst])) {
+    double s[NEQ];
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) {
+      double a = 0.0;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) a += (double)ld_state(&U[(size_t)(v * NB + b) * m.ld + e]);
+      s[v] = a;
+    }
+    const double hcr = kp.gas.hcr;
+    const double rho = s[0];
+    const double u = s[1] / rho;
+    const double v = s[2] / rho;
+    const double p = (hcr - 1.0) * (s[3] - 0.5 * rho * (u * u + v * v));
+    const double c = sqrt(hcr * p / rho);
+    const double speed = sqrt(u * u + v * v) + c;
+    const double dt = ic[inst].cfl * m.hmin[e] / speed;
+    if (dt < 1.0e10) bits = (unsigned long long)__double_as_longlong(dt);  // NaN never passes
+  }
+  const int inst0 = __shfl_sync(0xffffffffu, inst, 0);
+  if (__all_sync(0xffffffffu, inst == inst0)) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+      bits = other < bits ? other : bits;
+    }
+    if ((threadIdx.x & 31) == 0 && bits != 0x7ff0000000000000ull) atomicMin(&ic[inst0].dt_bits, bits);
+  } else if (bits != 0x7ff0000000000000ull) {
+    atomicMin(&ic[inst].dt_bits, bits);
+  }
+  // the last block closes the head: loop condition and clamped dt of every instance
+  __shared__ bool s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&ctl->head_done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    ctl->head_done = 0u;
+    ctl->troubled = 0;
+  }
+  for (int i = threadIdx.x; i < m.n_inst; i += blockDim.x) {
+    InstCtl& c = ic[i];
+    const int act = step_runs(c) ? 1 : 0;
+    c.active = act;
+    const unsigned long long start = (unsigned long long)__double_as_longlong(1.0e10);
+    const unsigned long long mn = atomicExch(&c.dt_bits, start);
+    if (act) {
+      double dt = __longlong_as_double((long long)mn);
+      if (c.t + dt > c.final_time) dt = c.final_time - c.t;  // temporal_disc.rs:23-26
+      c.dt = dt;
+    }
+  }
 }
+
 // temporal_disc.rs:32-33
 __global__ void k_step_end(InstCtl* ic, int n_inst) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -235,8 +235,9 @@ def load_traffic():
 # ------------------------------------------------------------------------------------------
 def run_batched(args, local):
     """256 seeded instances (Ni uniform on {32..256}, Nj = Ni/2, Mach U[0.3,0.85], AoA U[-4,6] deg,
-    p in {1,2}): DOF-stage updates/s of (a) FP32 batches, (b) FP64 batches -- one batch context
-    per order, both groups on their own streams -- and (c) FP64 one instance at a time on a
+    p in {1,2}): DOF-stage updates/s of (a) FP32 batches, (b) FP32 batches with the basis
+    contractions on the tensor cores (split TF32 operands), (c) FP64 batches -- one batch context
+    per order, both groups on their own streams -- and (d) FP64 one instance at a time on a
     DOF-weighted sample of 32 instances.  Inputs exceed the L2 (no flush needed); device time by
     CUDA events."""
     import torch
@@ -300,14 +301,19 @@ def run_batched(args, local):
         return res["dof"] * 3 * K / (ms * 1e-3), ms / K, dev_bytes, acc
 
     v32, ms32, bytes32, acc32 = batched("fp32")
+    vtc, mstc, bytestc, acctc = batched("tf32x3")
     v64, ms64, bytes64, acc64 = batched("fp64")
-    dcl = [abs(acc32[k][0] - acc64[k][0]) for k in acc64]
-    dcd = [abs(acc32[k][1] - acc64[k][1]) for k in acc64]
-    errs = [field_rel_l2(acc32[k][2], acc64[k][2], acc64[k][3]) for k in acc64 if acc64[k][2] is not None]
-    res["fp32_vs_fp64_after_steps"] = {
-        "steps": W + K, "max_abs_delta_cl": max(dcl), "max_abs_delta_cd": max(dcd),
-        "density_rel_l2_max": max(errs), "density_rel_l2_median": float(np.median(errs)),
-        "density_sample": f"{len(errs)} instances (every 8th of each order group)"}
+
+    def versus(acc):
+        dcl = [abs(acc[k][0] - acc64[k][0]) for k in acc64]
+        dcd = [abs(acc[k][1] - acc64[k][1]) for k in acc64]
+        errs = [field_rel_l2(acc[k][2], acc64[k][2], acc64[k][3]) for k in acc64 if acc64[k][2] is not None]
+        return {"steps": W + K, "max_abs_delta_cl": max(dcl), "max_abs_delta_cd": max(dcd),
+                "density_rel_l2_max": max(errs), "density_rel_l2_median": float(np.median(errs)),
+                "density_sample": f"{len(errs)} instances (every 8th of each order group)"}
+
+    res["fp32_vs_fp64_after_steps"] = versus(acc32)
+    res["tf32x3_vs_fp64_after_steps"] = versus(acctc)
     # one at a time, FP64: a DOF-weighted sample (every 8th instance in DOF order)
     order = sorted(range(len(built)), key=lambda k: built[k][0].dofs)
     sample = [built[k] for k in order[::max(1, len(built) // 32)]]
@@ -329,7 +335,8 @@ def run_batched(args, local):
         s.close()
     v_single = tot_dof * 3 * K / (tot_ms * 1e-3)
     res.update({
-        "fp32_batched": v32, "fp64_batched": v64, "fp64_one_at_a_time": v_single,
+        "fp32_batched": v32, "tf32x3_batched": vtc, "fp64_batched": v64, "fp64_one_at_a_time": v_single,
+        "ms_per_step_tf32x3_batched": mstc,
         "ms_per_step_fp32_batched": ms32, "ms_per_step_fp64_batched": ms64,
         "device_bytes_fp32": bytes32, "device_bytes_fp64": bytes64,
         "speedup_fp32_batched_vs_fp64_one_at_a_time": v32 / v_single,
@@ -352,9 +359,11 @@ def field_rel_l2(a, b, w):
 def run_precision(args, local):
     """NACA 0012 O-grid 1024 x 512 (1,048,576 triangles), p = 3 (10 modes, 12-point triangle /
     4-point edge rules), M = 0.7, AoA = 2 deg, free-stream start, limiter on, CFL 0.1: the same
-    steps in FP64 and in FP32 (limiter, positivity checks, time step and reductions in FP64).
-    Reports relative L2 errors of the FP32 fields against FP64, C_L / C_D of both, and each
-    mode's DOF-stage updates/s (CUDA events on the library stream; the state exceeds L2)."""
+    steps in FP64, in FP32 (limiter, positivity checks, time step and reductions in FP64), and
+    in FP32 with the basis contractions on the tensor cores (tf32: TF32 operands; tf32x3: split
+    TF32 operands).  Reports relative L2 errors of each mode's fields against FP64, C_L / C_D,
+    and each mode's DOF-stage updates/s (CUDA events on the library stream; the state exceeds
+    L2)."""
     import torch
     from dgm_in_rust_b200 import build_solver, forces_to_coefficients
     from dgm_in_rust_b200.workloads import Instance, instance_mesh
@@ -364,8 +373,9 @@ def run_precision(args, local):
     res = {"workload": "naca0012_ogrid_1024x512_p3: 1,048,576 triangles, 10 modes, M=0.7, AoA=2deg, limiter on, "
                        f"CFL 0.1, free-stream start, {K} steps", "steps": K}
     out = {}
-    for prec in ("fp64", "fp32", "fp64_perturbed"):
-        s = build_solver(mesh, 3, HCR, CFL, 1.0e30, K, limiter=True, device=local, precision=prec[:4])
+    for prec in ("fp64", "fp32", "tf32", "tf32x3", "fp64_perturbed"):
+        s = build_solver(mesh, 3, HCR, CFL, 1.0e30, K, limiter=True, device=local,
+                         precision="fp64" if prec == "fp64_perturbed" else prec)
         td, sd = s.temporal_disc, s.spatial_disc
         td.set_initial_on_device(init)
         if prec == "fp64_perturbed":
@@ -403,6 +413,10 @@ def run_precision(args, local):
         n: float(np.linalg.norm(U32[:, v] - U64[:, v]) / np.linalg.norm(U64[:, v])) for v, n in enumerate(names)}
     res["abs_delta_cl"] = abs(cl32 - cl64)
     res["abs_delta_cd"] = abs(cd32 - cd64)
+    for prec in ("tf32", "tf32x3"):  # basis contractions on the tensor cores
+        Ut, clt, cdt, _ = out[prec]
+        res[f"{prec}_vs_fp64"] = {"rel_l2": {n: field_rel_l2(Ut[:, v], U64[:, v], w) for v, n in enumerate(names)},
+                                  "abs_delta_cl": abs(clt - cl64), "abs_delta_cd": abs(cdt - cd64)}
     res["fp64_conditioning_floor"] = {
         "perturbation": "initial state x (1 + 1e-13 N(0,1)), FP64", "abs_delta_cl": abs(clp - cl64),
         "abs_delta_cd": abs(cdp - cd64), "rel_l2_rho": field_rel_l2(Up[:, 0], U64[:, 0], w),

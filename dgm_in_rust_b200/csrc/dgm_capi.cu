@@ -15,6 +15,7 @@
 
 #include "dgm_b200.h"
 #include "dgm_device.cuh"
+#include "dgm_tc.cuh"
 
 using dgm::Control;
 using dgm::InstCtl;
@@ -38,7 +39,9 @@ struct dgm_ctx {
   int num_sms = 0;
   cudaStream_t stream = nullptr;
   int P = 0, nb = 0, nq = 0, ng = 0;
-  int prec = 0;  // 0: FP64 state, 1: FP32 state and bulk arithmetic
+  int prec = 0;       // storage: 0 FP64 state, 1 FP32 state and bulk arithmetic
+  int prec_mode = 0;  // dgm_params::precision (0 fp64, 1 fp32, 2 tf32, 3 tf32x3)
+  int tc_split = 0;   // element pass on the tensor cores: 0 no (FP32 FMA), 1 TF32, 3 3xTF32
   int64_t ne = 0, ld = 0, n_int = 0, n_bnd = 0, np = 0, max_inst_ne = 0;
   int limiter = 1;
   double hcr = 1.4;
@@ -147,8 +150,30 @@ struct Ops {
     return DGM_OK;
   }
 
+  template <int MODE, int SPLIT>
+  static int element_tc(dgm_ctx* c, const float* Uin, const float* Ubase, float* Uout, const float* Rin,
+                        float* Rout) {
+    auto kern = dgm::k_element_tc<P, MODE, SPLIT>;
+    const int smem = (int)dgm::tc::Plan<P, SPLIT>::bytes;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    // Residency is left to the hardware: registers and shared memory allow several CTAs per SM,
+    // and tensor memory at most 512 / 32 = 16 (the thread limit gives the same), so the grid is
+    // the tile count capped at 16 CTAs per SM; every CTA loops over its share of tiles.
+    const int64_t tiles = (c->ne + dgm::tc::kElems - 1) / dgm::tc::kElems;
+    const int64_t cap = (int64_t)(512 / dgm::tc::kTmemCols) * c->num_sms;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, cap));
+    kern<<<blocks, dgm::tc::kThreads, smem, c->stream>>>(kp_of<P, float>(c), Uin, Ubase,
+                                                         static_cast<const float*>(c->F), Uout, Rin, Rout);
+    CK(cudaGetLastError());
+    return DGM_OK;
+  }
+
   template <int MODE>
   static int element(dgm_ctx* c, const T* Uin, const T* Ubase, T* Uout, const T* Rin, T* Rout) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (c->tc_split == 1) return element_tc<MODE, 1>(c, Uin, Ubase, Uout, Rin, Rout);
+      if (c->tc_split == 3) return element_tc<MODE, 3>(c, Uin, Ubase, Uout, Rin, Rout);
+    }
     const int threads = c->elem_threads;  // warps of 8 elements, 4 threads (variables) per element
     const int per_block = threads / 4;
     const int blocks = (int)std::max<int64_t>(1, (c->ne + per_block - 1) / per_block);
@@ -715,7 +740,7 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* 
     *status = DGM_NO_DEVICE;
     return nullptr;
   }
-  if (!variant_ok(tables) || (params->precision != 0 && params->precision != 1)) {
+  if (!variant_ok(tables) || params->precision < 0 || params->precision > 3) {
     *status = DGM_BAD_ARG;
     return nullptr;
   }
@@ -730,7 +755,9 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* 
   c->nb = tables->n_basis;
   c->nq = tables->n_cell_gp;
   c->ng = tables->n_edge_gp;
-  c->prec = params->precision;
+  c->prec_mode = params->precision;
+  c->prec = params->precision == 0 ? 0 : 1;
+  c->tc_split = params->precision == 2 ? 1 : (params->precision == 3 ? 3 : 0);
   c->hcr = params->hcr;
   c->limiter = params->limiter ? 1 : 0;
   c->inst.resize(n_inst);
@@ -1276,6 +1303,6 @@ int32_t dgm_diagnostics(dgm_ctx* c, int32_t use_residual, double* out) {
   return DGM_OK;
 }
 
-int32_t dgm_precision(dgm_ctx* c) { return c ? c->prec : -1; }
+int32_t dgm_precision(dgm_ctx* c) { return c ? c->prec_mode : -1; }
 
 }  // extern "C"

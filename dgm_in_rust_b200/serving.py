@@ -86,7 +86,7 @@ def footprint_bytes(meshes: list, order: int, precision: str, limiter: bool = Tr
     its allocations (what dgm_device_bytes reports), following dgm_create's allocation list."""
     nb = (order + 1) * (order + 2) // 2
     ng = default_rules(order)[1]
-    eb = 4 if precision == "fp32" else 8
+    eb = 8 if precision == "fp64" else 4
     n = len(meshes)
     ne = sum(m.n_elements for m in meshes)
     ld = (ne + 31) // 32 * 32

@@ -197,7 +197,11 @@ def _tables_desc(basis: DubinerBasis, g: GaussPoints, keep: list) -> "_native.Ta
         dphi_cell_ref=f64(basis.dphis_cell_gps), mass_diag=f64(basis.mass_mat_diag))
 
 
-PRECISIONS = {"fp64": 0, "fp32": 1}
+# fp64: the reference's arithmetic.  fp32: FP32 state, contractions, fluxes and stage updates
+# (limiter, HLLC positivity checks, time step and diagnostics in FP64).  tf32 / tf32x3: as fp32,
+# with the element pass's two basis contractions on the tensor cores (TF32 operands, FP32
+# accumulation; tf32x3 splits each operand into a TF32 head and tail for FP32-level products).
+PRECISIONS = {"fp64": 0, "fp32": 1, "tf32": 2, "tf32x3": 3}
 
 
 class SpatialDisc:

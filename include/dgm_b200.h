@@ -101,7 +101,10 @@ typedef struct dgm_params {
   int32_t device;                   /* CUDA device ordinal                                  */
   /* 0 = FP64 throughout (the reference's arithmetic); 1 = FP32 state, contractions, fluxes and
    * stage updates, with the limiter, the HLLC positivity checks, the time step and the
-   * diagnostics kept in FP64.  No counterpart in the reference (FP64 only). */
+   * diagnostics kept in FP64; 2 = as 1 with the element pass's two basis contractions
+   * (basis -> quadrature points, quadrature and edge points -> basis) on the tensor cores
+   * (tcgen05, TF32 operands, FP32 accumulation); 3 = as 2 with each operand split into a TF32
+   * head and tail (three products: FP32-level accuracy).  No counterpart in the reference. */
   int32_t precision;
   int32_t _reserved;
 } dgm_params;

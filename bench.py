@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--serving-rate", type=float, default=20.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serving-max-steps", type=int, default=400)
     ap.add_argument("--serving-budget-gib", type=float, default=16.0)
+    ap.add_argument("--serving-max-active", type=int, default=2 << 20,
+                    help="elements of running requests above which new requests wait (work-in-flight cap)")
     ap.add_argument("--profile-case", choices=["c2", "c3"],
                     help="run a fixed launch sequence for ncu (no timing, no autotuning): c2 = the workload "
                          "above, c3 = the 1024 x 512 p = 3 O-grid (M 0.7, AoA 2 deg)")
@@ -454,7 +456,8 @@ def run_serving(args, local):
     reqs = requests_from_stream(request_stream(args.serving_requests, args.serving_rate, seed=seed))
     kw = dict(chunk_steps=32, tol=1e-6, max_steps=args.serving_max_steps)
     budget = int(args.serving_budget_gib * (1 << 30))
-    loop = ServingLoop(hbm_budget_bytes=budget, device=local, precision="fp32", **kw)
+    loop = ServingLoop(hbm_budget_bytes=budget, device=local, precision="fp32",
+                       max_active_elements=args.serving_max_active, **kw)
     t = time.perf_counter()
     served = loop.run(reqs, realtime=True)
     wall = time.perf_counter() - t
@@ -469,7 +472,8 @@ def run_serving(args, local):
                     f"{args.serving_max_steps} steps (the configuration's cap is 5000; bounded here so the "
                     f"default run stays within minutes); convergence checked at step 1 then every 32",
         "elements_total": int(sum(r.instance.elements for r in reqs)),
-        "hbm_budget_bytes": budget, "peak_resident_bytes": loop.peak_bytes, "cohorts": loop.cohorts_formed,
+        "hbm_budget_bytes": budget, "max_active_elements": args.serving_max_active,
+        "peak_resident_bytes": loop.peak_bytes, "cohorts": loop.cohorts_formed,
         "max_concurrent_requests": loop.max_concurrent, "scheduler": loop.stats,
         "fp32_serving": s32, "fp64_one_at_a_time": s64,
         "fp64_one_at_a_time_excluding_host_prep_dof_stage_per_s": gpu_only,

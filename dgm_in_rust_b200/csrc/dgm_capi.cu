@@ -9,8 +9,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "dgm_b200.h"
@@ -38,6 +40,7 @@ struct dgm_ctx {
   int device = 0;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;  // the device's context pool (held while the context lives)
   int P = 0, nb = 0, nq = 0, ng = 0;
   int prec = 0;       // storage: 0 FP64 state, 1 FP32 state and bulk arithmetic
   int prec_mode = 0;  // dgm_params::precision (0 fp64, 1 fp32, 2 tf32, 3 tf32x3)
@@ -93,23 +96,46 @@ const int64_t kGraphSteps = 8;
     }                                                                            \
   } while (0)
 
-template <class T>
-int dev_alloc(dgm_ctx* c, T** p, size_t count) {
-  void* ptr = nullptr;
-  const size_t nbytes = std::max<size_t>(count, 1) * sizeof(T);
-  if (cudaMalloc(&ptr, nbytes) != cudaSuccess) {
-    cudaGetLastError();
-    return DGM_OOM;
+// Device memory of contexts comes from one stream-ordered pool per device, owned by the library
+// and kept (release threshold: unlimited) while any context is alive: creating and destroying a
+// context then costs no cudaMalloc/cudaFree, and in particular no device-wide synchronisation
+// (cudaFree waits for every stream), so contexts created and retired while others run -- the
+// serving loop's cohorts -- do not stall them.  The pool is trimmed when the last context of the
+// device is destroyed.
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+int g_live[kMaxDevices] = {};
+
+cudaMemPool_t pool_acquire(int device) {
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if (device < 0 || device >= kMaxDevices) return nullptr;
+  if (!g_pool[device]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&g_pool[device], &props) != cudaSuccess) {
+      cudaGetLastError();
+      g_pool[device] = nullptr;
+      return nullptr;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(g_pool[device], cudaMemPoolAttrReleaseThreshold, &keep);
   }
-  c->allocs.push_back(ptr);
-  c->bytes += (int64_t)nbytes;
-  *p = static_cast<T*>(ptr);
-  return DGM_OK;
+  ++g_live[device];
+  return g_pool[device];
+}
+
+void pool_release(int device) {
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if (device < 0 || device >= kMaxDevices || !g_pool[device]) return;
+  if (--g_live[device] == 0) cudaMemPoolTrimTo(g_pool[device], 0);
 }
 
 int dev_alloc_bytes(dgm_ctx* c, void** p, size_t nbytes) {
   void* ptr = nullptr;
-  if (cudaMalloc(&ptr, std::max<size_t>(nbytes, 16)) != cudaSuccess) {
+  if (!c->pool || cudaMallocFromPoolAsync(&ptr, std::max<size_t>(nbytes, 16), c->pool, c->stream) != cudaSuccess) {
     cudaGetLastError();
     return DGM_OOM;
   }
@@ -120,10 +146,21 @@ int dev_alloc_bytes(dgm_ctx* c, void** p, size_t nbytes) {
 }
 
 template <class T>
+int dev_alloc(dgm_ctx* c, T** p, size_t count) {
+  void* ptr = nullptr;
+  const size_t nbytes = std::max<size_t>(count, 1) * sizeof(T);
+  int st = dev_alloc_bytes(c, &ptr, nbytes);
+  if (st) return st;
+  *p = static_cast<T*>(ptr);
+  return DGM_OK;
+}
+
+// Pageable source: cudaMemcpyAsync returns once the data is staged, so `h` may go out of scope.
+template <class T>
 int upload(dgm_ctx* c, T** p, const std::vector<T>& h) {
   int st = dev_alloc(c, p, h.size());
   if (st) return st;
-  if (!h.empty()) CK(cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (!h.empty()) CK(cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
   return DGM_OK;
 }
 
@@ -260,6 +297,15 @@ struct Ops {
     CK(cudaGetLastError());
     return DGM_OK;
   }
+  static int cell_fields(dgm_ctx* c, int64_t i, double* dst) {
+    const HostInst& h = c->inst[i];
+    const int threads = 256;
+    dgm::k_cell_fields<P, T><<<(int)((h.ne + threads - 1) / threads), threads, 0, c->stream>>>(
+        kp_of<P, T>(c), S(c->U), (int)h.elem_off, (int)h.ne, dst);
+    CK(cudaGetLastError());
+    return DGM_OK;
+  }
+
   static int weno_gram(dgm_ctx* c) {
     constexpr int NPAIR = V::NB * (V::NB + 1) / 2;
     const int64_t n = (int64_t)NPAIR * c->ne;
@@ -772,17 +818,18 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* 
     return (dgm_ctx*)nullptr;
   };
   if (cudaSetDevice(c->device) != cudaSuccess) return fail(DGM_NO_DEVICE);
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return fail(DGM_NO_DEVICE);
-  c->num_sms = prop.multiProcessorCount;
+  if (cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess)
+    return fail(DGM_NO_DEVICE);
   int coop = 0;
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
   if (!coop) return fail(DGM_NO_DEVICE);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  c->pool = pool_acquire(c->device);
+  if (!c->pool) return fail(DGM_CUDA_ERROR);
   int st;
   if ((st = dev_alloc(c, &c->ctl, 1)) || (st = dev_alloc(c, &c->ic, (size_t)n_inst))) return fail(st);
-  if (cudaMemset(c->ctl, 0, sizeof(Control)) != cudaSuccess) return fail(DGM_CUDA_ERROR);
-  if (cudaMemset(c->ic, 0, sizeof(InstCtl) * n_inst) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  if (cudaMemsetAsync(c->ctl, 0, sizeof(Control), c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  if (cudaMemsetAsync(c->ic, 0, sizeof(InstCtl) * n_inst, c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
   st = dispatch(c, [&](auto ops) { return decltype(ops)::fill_tables(c, tables); });
   if (st) return fail(st);
   MeshDev md;
@@ -799,13 +846,14 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* 
       (st = dev_alloc(c, &c->work, (size_t)c->ne)) || (st = dev_alloc(c, &c->d_diag, (size_t)n_inst * 8)))
     return fail(st);
   for (void* p : {c->U, c->U1, c->U2, c->R})
-    if (cudaMemset(p, 0, n_state * eb) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+    if (cudaMemsetAsync(p, 0, n_state * eb, c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
   if (c->limiter) {
     if ((st = dev_alloc(c, &c->gram, (size_t)(c->nb * (c->nb + 1) / 2) * c->ld))) return fail(st);
     if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::weno_gram(c); }))) return fail(st);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
   }
-  if (cudaMemset(c->status, 0, (size_t)c->ne * sizeof(unsigned int)) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  if (cudaMemsetAsync(c->status, 0, (size_t)c->ne * sizeof(unsigned int), c->stream) != cudaSuccess)
+    return fail(DGM_CUDA_ERROR);
   if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::occupancy(c); }))) return fail(st);
   c->graph_steps = (int)kGraphSteps;
   if ((st = write_clock(c))) return fail(st);
@@ -845,8 +893,12 @@ void dgm_destroy(dgm_ctx* c) {
   for (auto& row : c->graph)
     for (auto& g : row)
       if (g) cudaGraphExecDestroy(g);
-  for (void* p : c->allocs) cudaFree(p);
-  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream) {
+    for (void* p : c->allocs) cudaFreeAsync(p, c->stream);  // back to the pool, in stream order
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
+  if (c->pool) pool_release(c->device);
   delete c;
 }
 
@@ -1304,5 +1356,16 @@ int32_t dgm_diagnostics(dgm_ctx* c, int32_t use_residual, double* out) {
 }
 
 int32_t dgm_precision(dgm_ctx* c) { return c ? c->prec_mode : -1; }
+
+int32_t dgm_cell_fields(dgm_ctx* c, int32_t i, double* fields) {
+  if (!inst_ok(c, i) || !fields) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  // the FP64 staging buffer holds a whole instance's state (ne x 4 x NB >= ne x 4 doubles)
+  int st = dispatch(c, [&](auto ops) { return decltype(ops)::cell_fields(c, i, c->stage); });
+  if (st) return st;
+  CK(cudaMemcpyAsync(fields, c->stage, sizeof(double) * 4 * (size_t)c->inst[i].ne, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DGM_OK;
+}
 
 }  // extern "C"

@@ -1318,6 +1318,32 @@ __global__ void __launch_bounds__(256) k_diagnostics(const __grid_constant__ KPa
   }
 }
 
+// Cell fields of write_to_vtk (write_results.rs:33-61) for the elements [e0, e0 + ne): density,
+// x and y velocity and pressure from the mode-0 coefficients, in FP64 with the reference's
+// expressions and operation order (no contraction into FMAs): velocity = momentum / density,
+// pressure = (hcr - 1) (energy - 0.5 density (u^2 + v^2)).  out is [ne][4].
+template <int P, typename T>
+__global__ void k_cell_fields(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U, int e0, int ne,
+                              double* __restrict__ out) {
+  constexpr int NB = Variant<P>::NB;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  const int e = e0 + i;
+  const size_t ld = kp.m.ld;
+  const double density = (double)U[(size_t)(0 * NB) * ld + e];
+  const double x_momentum = (double)U[(size_t)(1 * NB) * ld + e];
+  const double y_momentum = (double)U[(size_t)(2 * NB) * ld + e];
+  const double energy = (double)U[(size_t)(3 * NB) * ld + e];
+  const double x_velocity = x_momentum / density;
+  const double y_velocity = y_momentum / density;
+  const double kinetic = __dadd_rn(__dmul_rn(x_velocity, x_velocity), __dmul_rn(y_velocity, y_velocity));
+  const double pressure = __dmul_rn(kp.gas.gm1, __dsub_rn(energy, __dmul_rn(__dmul_rn(0.5, density), kinetic)));
+  out[4 * i + 0] = density;
+  out[4 * i + 1] = x_velocity;
+  out[4 * i + 2] = y_velocity;
+  out[4 * i + 3] = pressure;
+}
+
 // Layout transposes between the reference's [element][variable][basis] (FP64) and the SoA
 // state in the storage type.
 template <int NB, typename T>

@@ -126,9 +126,10 @@ def _warm():
 
 
 class _Member:
-    def __init__(self, req: Request, index: int, ready_s: float):
+    def __init__(self, req: Request, index: int, ready_s: float, elements: int):
         self.req = req
         self.index = index
+        self.elements = elements
         self.ready_s = ready_s
         self.r0 = None
         self.drop = 1.0
@@ -143,7 +144,7 @@ class _Cohort:
                            device=device, precision=precision)
         for i, it in enumerate(items):
             self.batch.set_initial(i, it[2])
-        self.members = [_Member(it[0], i, it[3]) for i, it in enumerate(items)]
+        self.members = [_Member(it[0], i, it[3], it[1].n_elements) for i, it in enumerate(items)]
         self.admitted = now
         self.bytes = self.batch.device_bytes()
         self.checks = 0
@@ -160,14 +161,19 @@ class ServingLoop:
     ``precision`` is the batched contexts' precision ("fp32": FP32 bulk arithmetic with the
     limiter, positivity checks, time step and diagnostics in FP64; "fp64": the reference's
     arithmetic).  ``window_s`` is how long a new arrival may wait for others to share its
-    cohort while the GPU is busy (an idle GPU admits at once).  ``prep`` selects worker
+    cohort while the GPU is busy (an idle GPU admits at once).  ``max_active_elements`` caps the
+    work in flight: a request is admitted only while the elements of the running (not yet retired)
+    requests plus its own stay within the cap (a request larger than the cap runs alone).  Enough
+    elements to keep the GPU's launches full run at once; later arrivals wait in arrival order
+    instead of sharing the GPU with everything admitted before them, so early requests finish
+    early (first come, first served at the granularity of the cap).  ``prep`` selects worker
     processes ("process", started with spawn before the clock starts, like a server's standing
     pool) or threads ("thread") for mesh preparation."""
 
     def __init__(self, hbm_budget_bytes: int = 40 << 30, device: int = 0, precision: str = "fp32",
                  chunk_steps: int = 32, tol: float = 1e-6, max_steps: int = 5000, window_s: float = 0.002,
-                 max_cohort_elements: int = 4 << 20, prep_workers: int = 4, prep: str = "process",
-                 keep_states: bool = False):
+                 max_cohort_elements: int = 4 << 20, max_active_elements: int = 2 << 20, prep_workers: int = 4,
+                 prep: str = "process", keep_states: bool = False):
         if chunk_steps < 1 or max_steps < 1:
             raise ValueError("chunk_steps and max_steps must be positive")
         self.budget = int(hbm_budget_bytes)
@@ -178,6 +184,7 @@ class ServingLoop:
         self.max_steps = int(max_steps)
         self.window = float(window_s)
         self.max_cohort_elements = int(max_cohort_elements)
+        self.max_active_elements = int(max_active_elements)
         if prep not in ("process", "thread"):
             raise ValueError("prep must be 'process' or 'thread'")
         self.prep_workers = max(1, int(prep_workers))
@@ -276,12 +283,16 @@ class ServingLoop:
             return used
         take: list = []
         need_total = 0
+        running = sum(m.elements for co in active for m in co.members if not m.done)
         for item in waiting:
             need = footprint_bytes([item[1]], item[0].instance.order, self.precision)
             if (active or take) and used + need_total + need > self.budget:
                 break           # first-come first-served: nothing overtakes a request that waits for memory
+            if (running or take) and running + item[1].n_elements > self.max_active_elements:
+                break           # enough work in flight: later requests wait, in arrival order
             take.append(item)
             need_total += need
+            running += item[1].n_elements
         if not take:
             return used
         del waiting[:len(take)]

@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import ctypes
 import dataclasses
+import functools
 import math
 
 import numpy as np
@@ -277,6 +278,14 @@ class SpatialDisc:
         self._check(self._lib.dgm_apply_limiter(self._ctx, _native.dptr(solutions), ctypes.byref(n)), "apply_limiter")
         return int(n.value)
 
+    def cell_fields(self) -> np.ndarray:
+        """[ne, 4] density, x velocity, y velocity, pressure of the resident state's mode-0
+        coefficients, computed on the device with write_to_vtk's expressions
+        (src/io/write_results.rs:33-61)."""
+        out = np.zeros((self.ne, 4))
+        self._check(self._lib.dgm_cell_fields(self._ctx, 0, _native.dptr(out)), "cell_fields")
+        return out
+
     def diagnostics(self, use_residual: bool = False) -> np.ndarray:
         """[8]: integrals of rho, rho u, rho v, rho E; wall force Fx, Fy; sum of squared density
         residual coefficients (last residual written); element count.  FP64, deterministic."""
@@ -413,16 +422,31 @@ class Solver:
     def solve(self) -> None:
         self.temporal_disc.time_march(self.spatial_disc, self.residuals, self.solutions)
 
+    def write_results(self, root: str = "outputfiles/solutions") -> str:
+        """write_to_vtk after the time loop (temporal_disc.rs:56, write_results.rs:8-93): the
+        resident state's cell fields, computed on the device, to root/step=<current_step>.vtk."""
+        from .output import solution_path, write_to_vtk
+        return write_to_vtk(solution_path(self.temporal_disc.current_step, root), self.mesh,
+                            self.spatial_disc.cell_fields())
+
     def close(self) -> None:
         self.spatial_disc.close()
+
+
+@functools.lru_cache(maxsize=None)
+def default_tables(order: int):
+    """(GaussPoints, DubinerBasis) of ``order`` with the default rules, built once per process
+    (the tables are read-only once built; p = 3 takes ~0.1 s to expand)."""
+    nq, ng = default_rules(order)
+    g = GaussPoints(nq, ng)
+    return g, DubinerBasis(order, g)
 
 
 def build_solver(mesh: Mesh, order: int, hcr: float, cfl: float, final_time: float, final_step: int,
                  limiter: bool = True, device: int = 0, precision: str = "fp64") -> Solver:
     """Convenience: tables for ``order`` with the default rules, then a Solver."""
     nq, ng = default_rules(order)
-    g = GaussPoints(nq, ng)
-    b = DubinerBasis(order, g)
+    g, b = default_tables(order)
     sp = SolverParameters(cfl=cfl, final_time=final_time, final_step=final_step, order_of_polynomials=order,
                           number_of_cell_gp=nq, number_of_edge_gp=ng)
     return Solver(mesh, b, g, FlowParameters(hcr=hcr), sp, limiter=limiter, device=device, precision=precision)
@@ -445,9 +469,7 @@ class Batch:
 
     def __init__(self, meshes: list, order: int, hcr: float, cfls, final_times, final_steps,
                  limiter: bool = True, device: int = 0, precision: str = "fp64"):
-        nq, ng = default_rules(order)
-        self.gauss_points = GaussPoints(nq, ng)
-        self.basis = DubinerBasis(order, self.gauss_points)
+        self.gauss_points, self.basis = default_tables(order)
         self.meshes = list(meshes)
         n = len(self.meshes)
         keep: list = []
@@ -539,6 +561,12 @@ class Batch:
                      final_step: int) -> None:
         self._check(self._lib.dgm_instance_set(self._ctx, i, float(current_time), int(current_step),
                                                float(final_time), int(final_step)), "set_instance")
+
+    def cell_fields(self, i: int) -> np.ndarray:
+        """[ne_i, 4] write_to_vtk cell fields of instance i (see SpatialDisc.cell_fields)."""
+        out = np.zeros((self.meshes[i].n_elements, 4))
+        self._check(self._lib.dgm_cell_fields(self._ctx, i, _native.dptr(out)), "cell_fields")
+        return out
 
     def diagnostics(self, use_residual: bool = False) -> np.ndarray:
         """[n, 8]: integrals of rho, rho u, rho v, rho E; wall force Fx, Fy; sum of squared density

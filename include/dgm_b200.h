@@ -244,6 +244,11 @@ int32_t dgm_advance_with_residual(dgm_ctx* ctx, int64_t n_steps);
  * No counterpart in the reference (it computes no forces or norms). */
 int32_t dgm_diagnostics(dgm_ctx* ctx, int32_t use_residual, double* out);
 
+/* Cell fields of write_to_vtk (src/io/write_results.rs:33-61) for instance i of the resident
+ * state: fields[e][0..4] = density, x velocity, y velocity, pressure from each element's mode-0
+ * coefficients, computed on the device in FP64 with the reference's expressions (bit-identical
+ * to them).  The host writes the file (dgm_in_rust_b200.output.write_to_vtk). */
+int32_t dgm_cell_fields(dgm_ctx* ctx, int32_t instance, double* fields /* [ne][4] */);
 /* The context's precision mode (dgm_params::precision). */
 int32_t dgm_precision(dgm_ctx* ctx);
 

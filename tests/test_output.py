@@ -1,0 +1,81 @@
+"""Result output in the reference's VTK format (src/io/write_results.rs:8-93).
+
+CPU: the text layout against the reference's own output file structure (a legacy ASCII file of
+vtkio: empty title, one-line data blocks, one cell type per line, empty POINT_DATA) and Rust's
+f64 formatting.  GPU: the device cell fields against the reference's expressions evaluated in
+numpy on the downloaded state (bitwise), and a written file read back.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import airfoil_raw
+from dgm_in_rust_b200 import InitialSolution, build_solver, freestream_quantity, naca0012_ogrid, process_mesh
+from dgm_in_rust_b200.output import format_f64, solution_path, vtk_text, write_to_vtk
+
+
+def test_rust_f64_display():
+    cases = [(1.0, "1"), (-20.0, "-20"), (0.141414, "0.141414"),
+             (9.833257050678418e-18, "0.000000000000000009833257050678418"), (1e20, "100000000000000000000"),
+             (0.1 + 0.2, "0.30000000000000004"), (float("nan"), "NaN"), (float("inf"), "inf"), (-0.0, "-0"),
+             (0.0, "0")]
+    for x, s in cases:
+        assert format_f64(x) == s, (x, format_f64(x))
+
+
+def test_vtk_layout_matches_reference_structure():
+    v = np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0], [1.0, 1.0]])
+    t = np.array([[0, 1, 2], [1, 3, 2]])
+    f = np.array([[1.0, 0.5, 0.0, 0.7142857142857143], [1.25, -0.5, 0.25, 1.0]])
+    lines = vtk_text(v, t, f).split("\n")
+    assert lines[:6] == ["# vtk DataFile Version 2.0", "", "ASCII", "", "DATASET UNSTRUCTURED_GRID", "POINTS 4 double"]
+    assert lines[6] == "0 0 0 1 0 0 0 1 0 1 1 0"
+    assert lines[7:12] == ["", "CELLS 2 8", "3 0 1 2 3 1 3 2", "", "CELL_TYPES 2"]
+    assert lines[12:14] == ["5", "5"]
+    assert lines[14:20] == ["", "", "POINT_DATA 4", "", "CELL_DATA 2", ""]
+    assert lines[20:23] == ["SCALARS Density double 1", "LOOKUP_TABLE default", "1 1.25"]
+    assert lines[23:26] == ["", "VECTORS Velocity double", "0.5 0 0 -0.5 0.25 0"]
+    assert lines[26:30] == ["", "SCALARS Pressure double 1", "LOOKUP_TABLE default", "0.7142857142857143 1"]
+    assert lines[30:] == ["", ""]
+
+
+def test_section_sizes_on_the_reference_mesh(tmp_path):
+    raw = airfoil_raw()
+    mesh = process_mesh(raw, freestream_quantity(0.8, 1.5, 1.0, 1e5, 1.4), 1.4)
+    ne, nv = mesh.n_elements, mesh.vertices.shape[0]
+    path = write_to_vtk(solution_path(20, str(tmp_path / "outputfiles" / "solutions")), mesh, np.ones((ne, 4)))
+    assert path.endswith(os.path.join("solutions", "step=20.vtk"))
+    lines = open(path).read().split("\n")
+    # the reference's outputfiles/mesh.vtk for this mesh: POINTS 1961, CELLS 3738 14952, 5883 point
+    # values and 14952 cell entries on one line each, POINT_DATA 1961, CELL_DATA 3738
+    assert (nv, ne) == (1961, 3738)
+    assert lines[5] == "POINTS 1961 double" and len(lines[6].split()) == 5883
+    assert lines[8] == "CELLS 3738 14952" and len(lines[9].split()) == 14952
+    assert lines[11] == "CELL_TYPES 3738" and lines[12:12 + ne] == ["5"] * ne
+    assert lines[12 + ne + 2] == "POINT_DATA 1961" and lines[12 + ne + 4] == "CELL_DATA 3738"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_device_cell_fields_match_reference_expressions(built, tmp_path, precision):
+    raw = naca0012_ogrid(32, 16)
+    mesh = process_mesh(raw, freestream_quantity(0.8, 1.25, 1.0, 1.0 / 1.4, 1.4), 1.4)
+    s = build_solver(mesh, 2, 1.4, 0.1, 1.0e30, 6, precision=precision)
+    td, sd = s.temporal_disc, s.spatial_disc
+    td.set_initial_on_device(InitialSolution(1.0, 1.25, 0.8, 1.0 / 1.4))
+    td.advance(6)
+    td.synchronize()
+    U = sd.new_state()
+    td.download(U)
+    f = sd.cell_fields()
+    rho, mx, my, en = U[:, 0, 0], U[:, 1, 0], U[:, 2, 0], U[:, 3, 0]
+    u, v = mx / rho, my / rho
+    p = (1.4 - 1.0) * (en - 0.5 * rho * (u * u + v * v))
+    assert np.array_equal(f, np.stack([rho, u, v, p], axis=1))
+    path = s.write_results(str(tmp_path / "solutions"))
+    assert path.endswith("step=6.vtk")
+    lines = open(path).read().split("\n")
+    k = lines.index("SCALARS Density double 1")
+    assert np.array_equal(np.array([float(x) for x in lines[k + 2].split()]), rho)
+    s.close()

@@ -232,3 +232,22 @@ def test_one_at_a_time_fifo_latency(built):
     assert busy > prep > 0 and all(r.steps == 17 for r in res)
     for a, b in zip(res, res[1:]):
         assert b.admitted_s >= a.finished_s - 1e-12
+
+
+def test_active_work_cap_admits_in_order(fake_batch):
+    """With room for two requests' elements, the third waits until one retires; arrival order is
+    kept and no more than the cap runs at once."""
+    reqs = _reqs([(16, 1), (16, 1), (16, 1), (16, 1)], gap=0.01)
+    ne = instance_mesh(reqs[0].instance)[0].n_elements
+    FakeBatch.lag = 200
+    try:
+        loop = ServingLoop(prep="thread", chunk_steps=64, tol=1e-3, max_steps=100, window_s=0.0,
+                           max_active_elements=2 * ne)
+        res = loop.run(reqs, realtime=True)
+    finally:
+        FakeBatch.lag = 2
+    assert len(res) == 4 and all(r.converged for r in res)
+    assert loop.max_concurrent <= 2
+    admitted = [r.admitted_s for r in res]
+    assert admitted == sorted(admitted)
+    assert min(res[2].admitted_s, res[3].admitted_s) >= min(res[0].finished_s, res[1].finished_s)

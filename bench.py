@@ -65,8 +65,9 @@ def parse():
                     help="run a fixed launch sequence for ncu (no timing, no autotuning): c2 = the workload "
                          "above, c3 = the 1024 x 512 p = 3 O-grid (M 0.7, AoA 2 deg)")
     ap.add_argument("--precision", choices=["fp64", "fp32", "tf32", "tf32x3"], default="fp64")
-    ap.add_argument("--launch", default="128,2368,128,1",
-                    help="edge threads, edge blocks, element threads, staged limiter detector (profile case)")
+    ap.add_argument("--launch", default="128,2368,128,1,0",
+                    help="edge threads, edge blocks, element threads, staged limiter detector, lane-pair edge "
+                         "pass (profile case; the last value may be left out: 0)")
     return ap.parse_args()
 
 
@@ -671,9 +672,11 @@ def run_profile_case(args):
     mesh, init = instance_mesh(inst)
     s = build_solver(mesh, inst.order, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, precision=args.precision)
     sd, td = s.spatial_disc, s.temporal_disc
-    e_t, e_b, l_t, staged = (int(x) for x in args.launch.split(","))
+    vals = [int(x) for x in args.launch.split(",")] + [0]
+    e_t, e_b, l_t, staged, pair = vals[:5]
     sd.set_launch_config(e_t, e_b, l_t)
     sd.set_limiter_detector(bool(staged))
+    sd.set_edge_form(bool(pair))
     td.set_initial_on_device(init)
     td.advance(args.warmup + args.steps)
     td.synchronize()

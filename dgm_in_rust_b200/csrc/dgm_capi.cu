@@ -67,6 +67,7 @@ struct dgm_ctx {
   int64_t bytes = 0;
   int coop_blocks[2] = {1, 1};  // co-resident limiter blocks of the compact / staged detector
   int lim_staged = 0;            // limiter detector variant (dgm_set_limiter_variant / autotune)
+  int edge_pair = 0;             // edge pass form: 0 thread per (slot, point), 1 lane pair per slot
   float lim_us[2] = {0.f, 0.f};  // last autotuned limiter times, compact / staged
   // launch configuration of the edge and element passes (dgm_set_launch_config / dgm_autotune):
   // edge_blocks = 0 launches one thread per (slot, Gauss point), else a grid-stride grid
@@ -178,11 +179,18 @@ struct Ops {
   static T* S(void* p) { return static_cast<T*>(p); }
 
   static int edge_flux(dgm_ctx* c, const T* U) {
-    const int64_t total = (c->n_int + c->n_bnd) * V::NG;
     const int threads = c->edge_threads;
-    const int64_t full = std::max<int64_t>(1, (total + threads - 1) / threads);
-    const int blocks = (int)(c->edge_blocks > 0 ? std::min<int64_t>(c->edge_blocks, full) : full);
-    dgm::k_edge_flux<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, S(c->F));
+    if (c->edge_pair) {  // a warp covers 16 slots per iteration
+      const int64_t warps = (c->n_int + c->n_bnd + 15) / 16;
+      const int64_t full = std::max<int64_t>(1, (warps * 32 + threads - 1) / threads);
+      const int blocks = (int)(c->edge_blocks > 0 ? std::min<int64_t>(c->edge_blocks, full) : full);
+      dgm::k_edge_flux_pair<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, S(c->F));
+    } else {
+      const int64_t total = (c->n_int + c->n_bnd) * V::NG;
+      const int64_t full = std::max<int64_t>(1, (total + threads - 1) / threads);
+      const int blocks = (int)(c->edge_blocks > 0 ? std::min<int64_t>(c->edge_blocks, full) : full);
+      dgm::k_edge_flux<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, S(c->F));
+    }
     CK(cudaGetLastError());
     return DGM_OK;
   }
@@ -1197,6 +1205,17 @@ int32_t dgm_set_limiter_variant(dgm_ctx* c, int32_t staged) {
   return DGM_OK;
 }
 
+int32_t dgm_set_edge_variant(dgm_ctx* c, int32_t pair) {
+  if (!c || (pair != 0 && pair != 1)) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  CK(cudaStreamSynchronize(c->stream));
+  c->edge_pair = pair;
+  reset_graphs(c);
+  return DGM_OK;
+}
+
+int32_t dgm_get_edge_variant(dgm_ctx* c) { return c ? c->edge_pair : -1; }
+
 int32_t dgm_get_limiter_variant(dgm_ctx* c, int32_t* staged, double* tuned_us) {
   if (!c) return DGM_BAD_ARG;
   if (staged) *staged = c->lim_staged;
@@ -1230,8 +1249,11 @@ int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
     return DGM_CUDA_ERROR;
   }
   const int sms = c->num_sms;
-  const int edge_cand[][2] = {{256, 0}, {128, 0}, {64, 0}, {256, 4 * sms}, {256, 8 * sms}, {128, 8 * sms},
-                              {128, 16 * sms}};
+  // (form, threads, blocks): per-point and lane-pair edge passes, one work item per thread or a
+  // grid-stride grid of 4-16 blocks per SM
+  const int edge_cand[][3] = {{0, 256, 0},        {0, 128, 0},        {0, 64, 0},         {0, 256, 4 * sms},
+                              {0, 256, 8 * sms},  {0, 128, 8 * sms},  {0, 128, 16 * sms}, {1, 256, 0},
+                              {1, 128, 0},        {1, 64, 0},         {1, 128, 8 * sms},  {1, 128, 16 * sms}};
   const int elem_cand[] = {256, 128, 64};
   auto time_phase = [&](int phase, float* us) -> int {
     for (int w = 0; w < 2; ++w) {
@@ -1259,7 +1281,7 @@ int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
     return DGM_OK;
   };
   float best_edge = 1e30f, best_elem = 1e30f;
-  int be_t = c->edge_threads, be_b = c->edge_blocks, bl_t = c->elem_threads;
+  int be_t = c->edge_threads, be_b = c->edge_blocks, bl_t = c->elem_threads, be_f = c->edge_pair;
   // limiter detector variant: each timed launch limits the same stage buffer, rebuilt by an edge
   // and an element pass before it (only the limiter sits between the events)
   auto time_limiter = [&](float* us) -> int {
@@ -1291,11 +1313,12 @@ int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
     c->lim_staged = (!st && c->lim_us[1] < c->lim_us[0]) ? 1 : 0;
   }
   for (auto& cand : edge_cand) {
-    c->edge_threads = cand[0];
-    c->edge_blocks = cand[1];
+    c->edge_pair = cand[0];
+    c->edge_threads = cand[1];
+    c->edge_blocks = cand[2];
     float us;
     if ((st = time_phase(1, &us))) break;
-    if (us < best_edge) best_edge = us, be_t = cand[0], be_b = cand[1];
+    if (us < best_edge) best_edge = us, be_f = cand[0], be_t = cand[1], be_b = cand[2];
   }
   for (int t : elem_cand) {
     if (st) break;
@@ -1306,6 +1329,7 @@ int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  c->edge_pair = be_f;
   c->edge_threads = be_t;
   c->edge_blocks = be_b;
   c->elem_threads = bl_t;

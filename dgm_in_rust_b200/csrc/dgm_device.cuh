@@ -319,6 +319,74 @@ __device__ __forceinline__ double phys_deriv(const double (&r)[NK], double xx, d
   return 0.0;
 }
 
+// Boundary flux at one Gauss point of a boundary slot, from the interior trace lv (times
+// nothing: the caller scales by half the edge length).  Slip wall: the pressure flux
+// [0, p nx, p ny, 0] (boundary_condition.rs:31-47); far field: characteristic upwinding between
+// the interior trace and the patch's free stream, then the physical normal flux of the blended
+// state (boundary_condition.rs:48-94).  (nx, ny) is the element's outward normal.
+template <typename T>
+__device__ __forceinline__ void boundary_flux(const T lv[4], int info, T nx, T ny, const MeshDev& m, const Gas& gas,
+                                              T out[4]) {
+  const T gm1 = T(gas.gm1);
+  if (((info >> 2) & 1) == 0) {
+    const T pressure = gm1 * (lv[3] - T(0.5) * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+    out[0] = T(0);
+    out[1] = pressure * nx;
+    out[2] = pressure * ny;
+    out[3] = T(0);
+    return;
+  }
+  const double4 bq = m.patch_q[info >> 3];
+  const T bc[4] = {T(bq.x), T(bq.y), T(bq.z), T(bq.w)};
+  const T u = lv[1] / lv[0];
+  const T v = lv[2] / lv[0];
+  const T p = gm1 * (lv[3] - T(0.5) * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+  const T c = sqrt(T(gas.hcr) * p / lv[0]);
+  const T vn = u * nx + v * ny;
+  T Lm[4][4], Rm[4][4];
+  eigenmatrix<T>(lv, nx, ny, gas, Lm, Rm);
+  const T lam[4] = {vn - c, vn, vn, vn + c};
+  T mix[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    T alpha = T(0), beta = T(0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      alpha += Lm[i][j] * lv[j];
+      beta += Lm[i][j] * bc[j];
+    }
+    mix[i] = lam[i] >= T(0) ? alpha : beta;
+  }
+  T q[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    T sum = T(0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sum += Rm[i][j] * mix[j];
+    q[i] = sum;
+  }
+  const T un = q[1] / q[0];
+  const T vv = q[2] / q[0];
+  const T vn_new = un * nx + vv * ny;
+  const T p_new = gm1 * (q[3] - T(0.5) * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+  const T h_new = q[3] + p_new;
+  out[0] = q[0] * vn_new;
+  out[1] = q[1] * vn_new + p_new * nx;
+  out[2] = q[2] * vn_new + p_new * ny;
+  out[3] = h_new * vn_new;
+}
+
+template <typename T>
+__device__ __forceinline__ void store_flux(T* F, size_t s, int NG, int g, const T out[4]) {
+  T* dst = &F[(s * NG + g) * 4];
+  if constexpr (std::is_same<T, double>::value) {
+    reinterpret_cast<double2*>(dst)[0] = make_double2(out[0], out[1]);
+    reinterpret_cast<double2*>(dst)[1] = make_double2(out[2], out[3]);
+  } else {
+    reinterpret_cast<float4*>(dst)[0] = make_float4(out[0], out[1], out[2], out[3]);
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Edge pass: one thread per (edge slot, Gauss point).  Internal slots: traces of both
 // elements + HLLC (integrate_over_edges_euler, spatial_disc.rs:161-211).  Boundary slots:
@@ -380,65 +448,101 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
         lv[v] = a;
       }
       const double4 geo = m.be_geo[sb];
-      const T nx = T(geo.x), ny = T(geo.y);
-      const T gm1 = T(gas.gm1);
-      if (((info >> 2) & 1) == 0) {
-        // slip wall, boundary_condition.rs:31-47
-        const T pressure = gm1 * (lv[3] - T(0.5) * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
-        out[0] = T(0);
-        out[1] = pressure * nx;
-        out[2] = pressure * ny;
-        out[3] = T(0);
-      } else {
-        // characteristic far field, boundary_condition.rs:48-94
-        const double4 bq = m.patch_q[info >> 3];
-        const T bc[4] = {T(bq.x), T(bq.y), T(bq.z), T(bq.w)};
-        const T u = lv[1] / lv[0];
-        const T v = lv[2] / lv[0];
-        const T p = gm1 * (lv[3] - T(0.5) * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
-        const T c = sqrt(T(gas.hcr) * p / lv[0]);
-        const T vn = u * nx + v * ny;
-        T Lm[4][4], Rm[4][4];
-        eigenmatrix<T>(lv, nx, ny, gas, Lm, Rm);
-        const T lam[4] = {vn - c, vn, vn, vn + c};
-        T mix[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          T alpha = T(0), beta = T(0);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            alpha += Lm[i][j] * lv[j];
-            beta += Lm[i][j] * bc[j];
-          }
-          mix[i] = lam[i] >= T(0) ? alpha : beta;
-        }
-        T q[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          T sum = T(0);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) sum += Rm[i][j] * mix[j];
-          q[i] = sum;
-        }
-        const T un = q[1] / q[0];
-        const T vv = q[2] / q[0];
-        const T vn_new = un * nx + vv * ny;
-        const T p_new = gm1 * (q[3] - T(0.5) * (q[1] * q[1] + q[2] * q[2]) / q[0]);
-        const T h_new = q[3] + p_new;
-        out[0] = q[0] * vn_new;
-        out[1] = q[1] * vn_new + p_new * nx;
-        out[2] = q[2] * vn_new + p_new * ny;
-        out[3] = h_new * vn_new;
-      }
+      boundary_flux<T>(lv, info, T(geo.x), T(geo.y), m, gas, out);
 #pragma unroll
       for (int v = 0; v < NEQ; ++v) out[v] *= T(geo.z);
     }
-    T* dst = &F[((size_t)s * NG + g) * 4];
-    if constexpr (std::is_same<T, double>::value) {
-      reinterpret_cast<double2*>(dst)[0] = make_double2(out[0], out[1]);
-      reinterpret_cast<double2*>(dst)[1] = make_double2(out[2], out[3]);
-    } else {
-      reinterpret_cast<float4*>(dst)[0] = make_float4(out[0], out[1], out[2], out[3]);
+    store_flux<T>(F, (size_t)s, NG, g, out);
+  }
+}
+
+// The same edge pass with two lanes per edge slot, one per side: each lane loads its element's
+// modes once, evaluates the traces at all NG points (the right side at the reversed points,
+// spatial_disc.rs:185), the pair swaps traces with shuffles, and the two lanes split the points
+// for HLLC / the boundary flux.  Each element's state is loaded once per slot instead of once per
+// point; every trace and flux is the same expression in the same order as in k_edge_flux, so the
+// results are bitwise identical.  A warp covers 16 consecutive slots per iteration.
+template <int P, typename T>
+__global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant__ KParams<P, T> kp,
+                                                           const T* __restrict__ U, T* __restrict__ F) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NG = V::NG;
+  constexpr int G0 = (NG + 1) / 2;  // points of the left lane: [0, G0); right lane: [G0, NG)
+  __shared__ T s_pe[3 * NG * NB];
+  for (int i = threadIdx.x; i < 3 * NG * NB; i += blockDim.x) s_pe[i] = (&kp.t.phi_edge[0][0][0])[i];
+  __syncthreads();
+  const MeshDev& m = kp.m;
+  const Gas& gas = kp.gas;
+  const int total = m.n_int + m.n_bnd;
+  const int lane = threadIdx.x & 31, side = lane & 1;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int base = gwarp * 16; base < total; base += nwarps * 16) {
+    const int s = base + (lane >> 1);
+    bool valid = s < total, internal = false, has = false;
+    int e = 0, k = 0, inst = 0, info = 0;
+    if (valid) {
+      if (s < m.n_int) {
+        internal = true;
+        const int2 lr = m.ie_lr[s];
+        const int ic = m.ie_ic[s];
+        e = side ? lr.y : lr.x;
+        k = side ? (ic >> 2) : (ic & 3);
+        inst = m.n_inst > 1 ? m.inst[lr.x] : 0;
+        has = true;
+      } else {
+        const int sb = s - m.n_int;
+        e = m.be_elem[sb];
+        info = m.be_info[sb];
+        k = info & 3;
+        inst = m.n_inst > 1 ? m.inst[e] : 0;
+        has = side == 0;
+      }
+      if (!kp.ic[inst].active) valid = has = false;
+    }
+    T tr[NEQ][NG];
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v) {
+      T u[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) u[b] = has ? ld_state(&U[(size_t)(v * NB + b) * m.ld + e]) : T(0);
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        const T* pe = &s_pe[(k * NG + (side ? NG - 1 - g : g)) * NB];
+        T a = T(0);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) a += u[b] * pe[b];
+        tr[v][g] = a;
+      }
+    }
+    T ot[NEQ][NG];
+#pragma unroll
+    for (int v = 0; v < NEQ; ++v)
+#pragma unroll
+      for (int g = 0; g < NG; ++g) ot[v][g] = __shfl_xor_sync(0xffffffffu, tr[v][g], 1);
+    if (!valid) continue;
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+      if ((g < G0) != (side == 0)) continue;
+      T lv[4], rv[4], out[4];
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) {
+        lv[v] = side ? ot[v][g] : tr[v][g];
+        rv[v] = side ? tr[v][g] : ot[v][g];
+      }
+      if (internal) {
+        const double4 geo = m.ie_geo[s];
+        const int st = hllc<T>(lv, rv, T(geo.x), T(geo.y), gas, out);
+        if (st != ST_OK) raise_status(kp.ctl, &kp.ic[inst], st, m.slot_ref[s]);
+#pragma unroll
+        for (int v = 0; v < NEQ; ++v) out[v] *= T(geo.z);
+      } else {
+        const double4 geo = m.be_geo[s - m.n_int];
+        boundary_flux<T>(lv, info, T(geo.x), T(geo.y), m, gas, out);
+#pragma unroll
+        for (int v = 0; v < NEQ; ++v) out[v] *= T(geo.z);
+      }
+      store_flux<T>(F, (size_t)s, NG, g, out);
     }
   }
 }

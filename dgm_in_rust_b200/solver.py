@@ -135,7 +135,8 @@ def _launch_config(L, ctx) -> dict:
     staged = ctypes.c_int32(0)
     L.dgm_get_limiter_variant(ctx, ctypes.byref(staged), None)
     return {"edge_threads": cfg[0], "edge_blocks": cfg[1], "element_threads": cfg[2],
-            "limiter_detector": "staged" if staged.value else "compact"}
+            "limiter_detector": "staged" if staged.value else "compact",
+            "edge_form": "pair" if L.dgm_get_edge_variant(ctx) == 1 else "point"}
 
 
 def _autotune(L, ctx, repeats: int) -> dict:
@@ -307,6 +308,11 @@ class SpatialDisc:
     def set_launch_config(self, edge_threads: int, edge_blocks: int, element_threads: int) -> None:
         self._check(self._lib.dgm_set_launch_config(self._ctx, int(edge_threads), int(edge_blocks),
                                                     int(element_threads)), "set_launch_config")
+
+    def set_edge_form(self, pair: bool) -> None:
+        """Pick the edge pass's form: a lane pair per edge slot (each side's state loaded once)
+        or a thread per (slot, Gauss point); both give bitwise identical fluxes."""
+        self._check(self._lib.dgm_set_edge_variant(self._ctx, 1 if pair else 0), "set_edge_form")
 
     def set_limiter_detector(self, staged: bool) -> None:
         """Pick the limiter's KXRCF detector form: staged loads (fewer memory round trips, more

@@ -297,12 +297,15 @@ struct Ops {
     return DGM_OK;
   }
 
-  static int to_soa(dgm_ctx* c, const double* src_aos, void* dst, int64_t elem_off, int64_t ne) {
-    const int64_t n = ne * NEQ * V::NB;
+  // FP64 device array in the reference layout -> the state (FP32 contexts; FP64 copies directly)
+  static int to_storage(dgm_ctx* c, const double* src, void* dst, int64_t elem_off, int64_t ne) {
+    const long long n = (long long)ne * NEQ * V::NB;
     const int threads = 256;
-    dgm::k_aos_to_soa<V::NB, T><<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(
-        src_aos, S(dst) + elem_off, (int)ne, (int)c->ld);
-    CK(cudaGetLastError());
+    if constexpr (std::is_same<T, float>::value) {
+      dgm::k_f64_to_f32<<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(
+          src, S(dst) + elem_off * NEQ * V::NB, n);
+      CK(cudaGetLastError());
+    }
     return DGM_OK;
   }
   static int cell_fields(dgm_ctx* c, int64_t i, double* dst) {
@@ -339,12 +342,14 @@ struct Ops {
     CK(cudaGetLastError());
     return DGM_OK;
   }
-  static int to_aos(dgm_ctx* c, const void* src, double* dst_aos, int64_t elem_off, int64_t ne) {
-    const int64_t n = ne * NEQ * V::NB;
+  static int from_storage(dgm_ctx* c, const void* src, double* dst, int64_t elem_off, int64_t ne) {
+    const long long n = (long long)ne * NEQ * V::NB;
     const int threads = 256;
-    dgm::k_soa_to_aos<V::NB, T><<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(
-        static_cast<const T*>(src) + elem_off, dst_aos, (int)ne, (int)c->ld);
-    CK(cudaGetLastError());
+    if constexpr (std::is_same<T, float>::value) {
+      dgm::k_f32_to_f64<<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(
+          static_cast<const float*>(src) + elem_off * NEQ * V::NB, dst, n);
+      CK(cudaGetLastError());
+    }
     return DGM_OK;
   }
 
@@ -479,20 +484,33 @@ int set_active(dgm_ctx* c, double dt, bool set_dt) {
 }
 
 // Host state ([element][variable][basis], FP64) of instance i -> device SoA array dst.
+// Host state ([element][variable][basis], FP64) of instance i -> device state array dst: the
+// device layout is the same element-major order, so an FP64 state is one copy; an FP32 state goes
+// through the FP64 staging buffer and a conversion.
 int upload_state(dgm_ctx* c, int64_t i, const double* host, void* dst) {
   const HostInst& h = c->inst[i];
   const size_t n = (size_t)h.ne * NEQ * c->nb;
+  if (c->prec == 0) {
+    CK(cudaMemcpyAsync(static_cast<double*>(dst) + (size_t)h.elem_off * NEQ * c->nb, host, n * sizeof(double),
+                       cudaMemcpyHostToDevice, c->stream));
+    return DGM_OK;
+  }
   CK(cudaMemcpyAsync(c->stage, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  return dispatch(c, [&](auto ops) { return decltype(ops)::to_soa(c, c->stage, dst, h.elem_off, h.ne); });
+  return dispatch(c, [&](auto ops) { return decltype(ops)::to_storage(c, c->stage, dst, h.elem_off, h.ne); });
 }
 
 int download_state(dgm_ctx* c, int64_t i, const void* src, double* host) {
   const HostInst& h = c->inst[i];
   const size_t n = (size_t)h.ne * NEQ * c->nb;
-  int st = dispatch(c, [&](auto ops) { return decltype(ops)::to_aos(c, src, c->stage, h.elem_off, h.ne); });
-  if (st) return st;
-  CK(cudaMemcpyAsync(host, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));  // the staging buffer is reused by the next copy
+  if (c->prec == 0) {
+    CK(cudaMemcpyAsync(host, static_cast<const double*>(src) + (size_t)h.elem_off * NEQ * c->nb, n * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    int st = dispatch(c, [&](auto ops) { return decltype(ops)::from_storage(c, src, c->stage, h.elem_off, h.ne); });
+    if (st) return st;
+    CK(cudaMemcpyAsync(host, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));  // the host reads the array; the staging buffer is reused
   return DGM_OK;
 }
 

@@ -5,8 +5,11 @@
 // instances; each instance has its own time-march control (time, dt, step, loop bounds, status).
 //
 // Data layout in HBM:
-//   state      U[v*NB + b][ld]        SoA in the storage type T (double or float), v = conserved
-//                                      variable, b = Dubiner mode, ld = element count padded to 32
+//   state      U[e][v][b]             element-major in the storage type T (double or float), the
+//                                      reference's own [element][variable][basis] order: an
+//                                      element's 4 NB coefficients are contiguous (48 to 320 bytes,
+//                                      a multiple of 16), read with 16-byte loads; padded to ld
+//                                      elements (element count rounded up to 32)
 //   geometry   jac[ne], dinv[4][ld]   (dxi/dx, dxi/dy, deta/dx, deta/dy), hmin[ne], h15[ne]
 //   faces      face[3][ld]            (edge slot << 1) | side, side 1 = element is the edge's
 //                                      right element; slots [0, n_int) are internal edges,
@@ -142,6 +145,80 @@ __device__ __forceinline__ void raise_status(Control* ctl, InstCtl* ic, int code
 
 template <typename T>
 __device__ __forceinline__ T ld_state(const T* p) { return __ldcg(p); }
+
+// Index of coefficient (v, b) of element e in an element-major state array.
+template <int NB>
+__host__ __device__ __forceinline__ size_t sx(int e, int v, int b) {
+  return (size_t)e * (NEQ * NB) + (size_t)(v * NB + b);
+}
+
+// The NB modes of variable VAR of element e (L2 loads), converted to FP64, with the widest loads
+// the block's alignment allows (its byte offset in the 16-byte aligned record is known at compile
+// time): 16-byte loads for the density block and most others, 8- or 4-byte ones otherwise.
+template <int NB, typename T, int VAR>
+__device__ __forceinline__ void load_var_modes(const T* __restrict__ U, int e, double (&out)[NB]) {
+  constexpr int OFF = VAR * NB * (int)sizeof(T);  // byte offset of the block in the record
+  constexpr int ALIGN = (OFF % 16 == 0) ? 16 : (OFF % 8 == 0) ? 8 : 4;
+  const T* p = U + (size_t)e * (NEQ * NB) + VAR * NB;
+  if constexpr (std::is_same<T, double>::value && ALIGN == 16) {
+#pragma unroll
+    for (int i = 0; i < NB / 2; ++i) {
+      const double2 x = __ldcg(reinterpret_cast<const double2*>(p) + i);
+      out[2 * i] = x.x;
+      out[2 * i + 1] = x.y;
+    }
+    if constexpr (NB % 2) out[NB - 1] = __ldcg(p + NB - 1);
+  } else if constexpr (std::is_same<T, float>::value && ALIGN == 16) {
+#pragma unroll
+    for (int i = 0; i < NB / 4; ++i) {
+      const float4 x = __ldcg(reinterpret_cast<const float4*>(p) + i);
+      out[4 * i] = x.x;
+      out[4 * i + 1] = x.y;
+      out[4 * i + 2] = x.z;
+      out[4 * i + 3] = x.w;
+    }
+#pragma unroll
+    for (int i = NB / 4 * 4; i < NB; ++i) out[i] = __ldcg(p + i);
+  } else if constexpr (std::is_same<T, float>::value && ALIGN == 8) {
+#pragma unroll
+    for (int i = 0; i < NB / 2; ++i) {
+      const float2 x = __ldcg(reinterpret_cast<const float2*>(p) + i);
+      out[2 * i] = x.x;
+      out[2 * i + 1] = x.y;
+    }
+    if constexpr (NB % 2) out[NB - 1] = __ldcg(p + NB - 1);
+  } else {
+#pragma unroll
+    for (int i = 0; i < NB; ++i) out[i] = (double)__ldcg(p + i);
+  }
+}
+
+// All 4 NB coefficients of element e with 16-byte loads (the record is 16-byte aligned for every
+// order and storage type).  L1 = true caches in L1 (for arrays no thread writes during the
+// kernel); otherwise the loads go to L2 only.
+template <int NB, typename T, bool L1 = false>
+__device__ __forceinline__ void load_elem(const T* __restrict__ U, int e, T (&u)[NEQ * NB]) {
+  constexpr int N = NEQ * NB;
+  if constexpr (std::is_same<T, double>::value) {
+    const double2* p = reinterpret_cast<const double2*>(U + (size_t)e * N);
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const double2 x = L1 ? p[i] : __ldcg(p + i);
+      u[2 * i] = x.x;
+      u[2 * i + 1] = x.y;
+    }
+  } else {
+    const float4* p = reinterpret_cast<const float4*>(U + (size_t)e * N);
+#pragma unroll
+    for (int i = 0; i < N / 4; ++i) {
+      const float4 x = L1 ? p[i] : __ldcg(p + i);
+      u[4 * i] = x.x;
+      u[4 * i + 1] = x.y;
+      u[4 * i + 2] = x.z;
+      u[4 * i + 3] = x.w;
+    }
+  }
+}
 
 // flux::flux, flux.rs:154-169 (one reciprocal of the density instead of three divisions)
 template <typename T>
@@ -415,14 +492,17 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
       const int ic = m.ie_ic[s];
       const T* pl = &s_pe[((ic & 3) * NG + g) * NB];
       const T* pr = &s_pe[((ic >> 2) * NG + (NG - 1 - g)) * NB];
+      T ul[NEQ * NB], ur[NEQ * NB];
+      load_elem<NB, T>(U, lr.x, ul);
+      load_elem<NB, T>(U, lr.y, ur);
       T lv[4], rv[4];
 #pragma unroll
       for (int v = 0; v < NEQ; ++v) {
         T a = T(0), c = T(0);
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-          a += ld_state(&U[(size_t)(v * NB + b) * m.ld + lr.x]) * pl[b];
-          c += ld_state(&U[(size_t)(v * NB + b) * m.ld + lr.y]) * pr[b];
+          a += ul[v * NB + b] * pl[b];
+          c += ur[v * NB + b] * pr[b];
         }
         lv[v] = a;
         rv[v] = c;
@@ -439,12 +519,14 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
       if (!kp.ic[inst].active) continue;
       const int info = m.be_info[sb];
       const T* pe = &s_pe[((info & 3) * NG + g) * NB];
+      T ue[NEQ * NB];
+      load_elem<NB, T>(U, e, ue);
       T lv[4];
 #pragma unroll
       for (int v = 0; v < NEQ; ++v) {
         T a = T(0);
 #pragma unroll
-        for (int b = 0; b < NB; ++b) a += ld_state(&U[(size_t)(v * NB + b) * m.ld + e]) * pe[b];
+        for (int b = 0; b < NB; ++b) a += ue[v * NB + b] * pe[b];
         lv[v] = a;
       }
       const double4 geo = m.be_geo[sb];
@@ -500,18 +582,22 @@ __global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant
       }
       if (!kp.ic[inst].active) valid = has = false;
     }
+    T u[NEQ * NB];
+    if (has) {
+      load_elem<NB, T>(U, e, u);
+    } else {
+#pragma unroll
+      for (int i = 0; i < NEQ * NB; ++i) u[i] = T(0);
+    }
     T tr[NEQ][NG];
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
-      T u[NB];
-#pragma unroll
-      for (int b = 0; b < NB; ++b) u[b] = has ? ld_state(&U[(size_t)(v * NB + b) * m.ld + e]) : T(0);
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
         const T* pe = &s_pe[(k * NG + (side ? NG - 1 - g : g)) * NB];
         T a = T(0);
 #pragma unroll
-        for (int b = 0; b < NB; ++b) a += u[b] * pe[b];
+        for (int b = 0; b < NB; ++b) a += u[v * NB + b] * pe[b];
         tr[v][g] = a;
       }
     }
@@ -558,15 +644,65 @@ __global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant
 //   MODE 3: out = 1/3 Ubase + 2/3 (Uin + dt R)
 // Four threads per element, one per conserved variable: lane = v * 8 + i within a warp that
 // covers 8 elements.  The quadrature-point states are exchanged with shuffles, so a thread
-// holds only its variable's NB modes and residuals, and each (v, b) load of the 8 elements is
-// one contiguous run.  Elements of instances that are not stepping are left untouched.
+// holds only its variable's NB modes and residuals.  The warp's 8 element records are one
+// contiguous block of the element-major arrays: it moves them between global and shared memory
+// with 16-byte accesses (coalesced), and each thread reads and writes its variable's modes in
+// shared memory.  Elements of instances that are not stepping are left untouched (their records
+// are not stored).
 // ------------------------------------------------------------------------------------------
+constexpr int kElemMaxWarps = 8;  // element pass: at most 256 threads per block
+
+// Element records staged in shared memory are padded to an odd number of 16-byte units:
+// consecutive lanes reading the same coefficient of their own records then spread over the banks
+// (2-way conflicts for FP64, 4-way for FP32, the least 16-byte granularity allows; unpadded
+// records of 48-320 bytes map most lanes to the same few banks).
+template <int NB, typename T>
+struct Staged {
+  static constexpr int kRecBytes = NEQ * NB * (int)sizeof(T);
+  static constexpr int kStrideBytes = kRecBytes + ((kRecBytes / 16) % 2 == 0 ? 16 : 32);
+  static constexpr int kStride = kStrideBytes / (int)sizeof(T);  // record stride in T
+  static constexpr int kCpr = kRecBytes / 16;                          // 16-byte chunks per record
+  static_assert(kRecBytes % 16 == 0, "element records are a multiple of 16 bytes");
+};
+
+// Copies the NR element records starting at e0 (always inside the arrays, which are padded to a
+// multiple of 32 elements, with e0 a multiple of NR) into the warp's shared buffer (record r at
+// sbuf + r * Staged::kStride), with coalesced 16-byte loads through L2.
+template <int NB, typename T, int NR = 8>
+__device__ __forceinline__ void warp_load_records(const T* __restrict__ src, int e0, T* sbuf, int lane) {
+  using S = Staged<NB, T>;
+  constexpr int C = NR * S::kCpr;
+  const uint4* g = reinterpret_cast<const uint4*>(src + (size_t)e0 * NEQ * NB);
+  __syncwarp();
+#pragma unroll
+  for (int c = lane; c < C; c += 32)
+    *reinterpret_cast<uint4*>(sbuf + (c / S::kCpr) * S::kStride + (c % S::kCpr) * (16 / (int)sizeof(T))) = __ldcg(g + c);
+  __syncwarp();
+}
+
+// Stores the warp's shared buffer to the 8 element records starting at e0, skipping the records
+// of elements whose bit in `keep` is clear.
+template <int NB, typename T>
+__device__ __forceinline__ void warp_store_records(T* dst, int e0, const T* sbuf, unsigned int keep, int lane) {
+  using S = Staged<NB, T>;
+  constexpr int C = 8 * S::kCpr;
+  uint4* g = reinterpret_cast<uint4*>(dst + (size_t)e0 * NEQ * NB);
+  __syncwarp();
+#pragma unroll
+  for (int c = lane; c < C; c += 32)
+    if ((keep >> (c / S::kCpr)) & 1u)
+      g[c] = *reinterpret_cast<const uint4*>(sbuf + (c / S::kCpr) * S::kStride + (c % S::kCpr) * (16 / (int)sizeof(T)));
+  __syncwarp();
+}
+
 template <int P, typename T, int MODE>
 __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KParams<P, T> kp,
                                                     const T* __restrict__ Uin, const T* Ubase,
                                                     const T* __restrict__ F, T* Uout, const T* Rin, T* Rout) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NQ = V::NQ, NG = V::NG;
+  constexpr int STRIDE = Staged<NB, T>::kStride;
+  __shared__ __align__(16) T s_rec[kElemMaxWarps][8 * STRIDE];
   Control* ctl = kp.ctl;
   if (blockIdx.x == 0 && threadIdx.x == 0) {  // counters of the limiter pass that follows
     ctl->t0_count = 0;
@@ -576,16 +712,21 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
   const MeshDev& m = kp.m;
   const int lane = threadIdx.x & 31;
   const int var = lane >> 3, i = lane & 7;
-  const int e_raw = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 8 + i;
-  if ((e_raw & ~7) >= m.ne) return;  // whole warp past the end
+  const int e0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 8;
+  const int e_raw = e0 + i;
+  if (e0 >= m.ne) return;  // whole warp past the end
   const int e = e_raw < m.ne ? e_raw : m.ne - 1;
   const int inst = m.n_inst > 1 ? m.inst[e] : 0;
   const bool valid = e_raw < m.ne && kp.ic[inst].active;
+  const unsigned int keep = __ballot_sync(0xffffffffu, valid) & 0xffu;  // lanes 0-7: var 0 of each element
   const size_t ld = m.ld;
+  T* sbuf = s_rec[threadIdx.x >> 5];
+  T* mine_rec = sbuf + i * STRIDE + var * NB;
+  warp_load_records<NB, T>(Uin, e0, sbuf, lane);
   T u[NB], r[NB];
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
-    u[b] = ld_state(&Uin[(var * NB + b) * ld + e]);
+    u[b] = mine_rec[b];
     r[b] = T(0);
   }
   const T J = T(m.jac[e]);
@@ -625,23 +766,43 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
       for (int b = 0; b < NB; ++b) r[b] += fv * kp.t.phi_edge[k][gp][b];
     }
   }
-  if (!valid) return;
+  if (!keep) return;  // no element of this warp is stepping
   const T dt = T(kp.ic[inst].dt);
   const T inv_half_j = T(1) / (T(0.5) * J);
+  if constexpr (MODE == 0) {  // compute_residuals adds to the residual it is given
+    warp_load_records<NB, T>(Rin, e0, sbuf, lane);
 #pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    const size_t idx = (var * NB + b) * ld + e;
-    T rr = r[b];
-    if constexpr (MODE == 0) rr = Rin[idx] + rr;
-    rr = rr * kp.t.inv_mass[b] * inv_half_j;  // divide_residual_by_mass_mat_diag
-    if (Rout) Rout[idx] = rr;
-    if constexpr (MODE == 1) {
-      Uout[idx] = u[b] + dt * rr;
-    } else if constexpr (MODE == 2) {
-      Uout[idx] = T(0.75) * Ubase[idx] + T(0.25) * (u[b] + dt * rr);
-    } else if constexpr (MODE == 3) {
-      Uout[idx] = T(1.0 / 3.0) * Ubase[idx] + T(2.0 / 3.0) * (u[b] + dt * rr);
+    for (int b = 0; b < NB; ++b) r[b] = mine_rec[b] + r[b];
+  }
+#pragma unroll
+  for (int b = 0; b < NB; ++b) r[b] = r[b] * kp.t.inv_mass[b] * inv_half_j;  // divide_residual_by_mass_mat_diag
+  if (Rout) {
+#pragma unroll
+    for (int b = 0; b < NB; ++b) mine_rec[b] = r[b];
+    warp_store_records<NB, T>(Rout, e0, sbuf, keep, lane);
+  }
+  if constexpr (MODE != 0) {
+    T base[NB];
+    if constexpr (MODE >= 2) {
+      warp_load_records<NB, T>(Ubase, e0, sbuf, lane);
+#pragma unroll
+      for (int b = 0; b < NB; ++b) base[b] = mine_rec[b];
+      __syncwarp();
     }
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const T rr = r[b];
+      T out;
+      if constexpr (MODE == 1) {
+        out = u[b] + dt * rr;
+      } else if constexpr (MODE == 2) {
+        out = T(0.75) * base[b] + T(0.25) * (u[b] + dt * rr);
+      } else {
+        out = T(1.0 / 3.0) * base[b] + T(2.0 / 3.0) * (u[b] + dt * rr);
+      }
+      mine_rec[b] = out;
+    }
+    warp_store_records<NB, T>(Uout, e0, sbuf, keep, lane);
   }
 }
 
@@ -649,9 +810,11 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
 // modified_kxrcf, weno.rs:7-85, for element e on state U (FP64 arithmetic).  Keeps the
 // reference's exterior-trace indexing: the neighbour's modes are evaluated with this element's
 // own local edge index k (weno.rs:21-27 pick in_cell_indices[side], always this element's).
+// `own` is e's record (the limiter stages its warp's records in shared memory); the
+// neighbours' modes are read from U through L2.
 // ------------------------------------------------------------------------------------------
 template <int P, typename T>
-__device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restrict__ U, int e) {
+__device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restrict__ U, int e, const T* own) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
   const MeshDev& m = kp.m;
@@ -673,8 +836,8 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
       double rho = 0.0, rho_e = 0.0;
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        rho += (double)ld_state(&U[(0 * NB + b) * ld + e]) * kp.d.phi_edge[k][g][b];
-        rho_e += (double)ld_state(&U[(3 * NB + b) * ld + e]) * kp.d.phi_edge[k][g][b];
+        rho += (double)own[0 * NB + b] * kp.d.phi_edge[k][g][b];
+        rho_e += (double)own[3 * NB + b] * kp.d.phi_edge[k][g][b];
       }
       own_rho[g] = rho;
       own_rhoe[g] = rho_e;
@@ -685,19 +848,22 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
     double rho_u = 0.0, rho_v = 0.0;
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      rho_u += (double)ld_state(&U[(1 * NB + b) * ld + e]) * kp.d.phi_edge[k][cg][b];
-      rho_v += (double)ld_state(&U[(2 * NB + b) * ld + e]) * kp.d.phi_edge[k][cg][b];
+      rho_u += (double)own[1 * NB + b] * kp.d.phi_edge[k][cg][b];
+      rho_v += (double)own[2 * NB + b] * kp.d.phi_edge[k][cg][b];
     }
     if (rho_u * nx + rho_v * ny < 0.0) {
       double rho_jump = 0.0, rho_e_jump = 0.0;
       const double jd = geo.w;
+      double nrho[NB], nrhoe[NB];
+      load_var_modes<NB, T, 0>(U, nb, nrho);
+      load_var_modes<NB, T, 3>(U, nb, nrhoe);
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
         double er = 0.0, ere = 0.0;
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-          er += (double)ld_state(&U[(0 * NB + b) * ld + nb]) * kp.d.phi_edge[k][NG - 1 - g][b];
-          ere += (double)ld_state(&U[(3 * NB + b) * ld + nb]) * kp.d.phi_edge[k][NG - 1 - g][b];
+          er += nrho[b] * kp.d.phi_edge[k][NG - 1 - g][b];
+          ere += nrhoe[b] * kp.d.phi_edge[k][NG - 1 - g][b];
         }
         rho_jump += 0.5 * jd * kp.d.edge_w[g] * (own_rho[g] - er);
         rho_e_jump += 0.5 * jd * kp.d.edge_w[g] * (own_rhoe[g] - ere);
@@ -720,7 +886,8 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
 // a pass is latency-bound (small meshes), slower when occupancy matters (large batches); the
 // autotuner picks one per context.  Same arithmetic in the same order, so the same flags.
 template <int P, typename T>
-__device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* __restrict__ U, int e) {
+__device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* __restrict__ U, int e,
+                                             const T* own_rec) {
   int fw[3], nb[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -730,12 +897,11 @@ __device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* _
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
   const MeshDev& m = kp.m;
-  const size_t ld = m.ld;
   double own[NEQ][NB];
 #pragma unroll
   for (int v = 0; v < NEQ; ++v)
 #pragma unroll
-    for (int b = 0; b < NB; ++b) own[v][b] = (double)ld_state(&U[(v * NB + b) * ld + e]);
+    for (int b = 0; b < NB; ++b) own[v][b] = (double)own_rec[v * NB + b];
   double nx[3], ny[3], jd[3];
   bool interior[3];
 #pragma unroll
@@ -766,8 +932,8 @@ __device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* _
   for (int k = 0; k < 3; ++k)
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      ext_rho[k][b] = inflow[k] ? (double)ld_state(&U[(0 * NB + b) * ld + nb[k]]) : 0.0;
-      ext_rhoe[k][b] = inflow[k] ? (double)ld_state(&U[(3 * NB + b) * ld + nb[k]]) : 0.0;
+      ext_rho[k][b] = inflow[k] ? (double)ld_state(&U[sx<NB>(nb[k], 0, b)]) : 0.0;
+      ext_rhoe[k][b] = inflow[k] ? (double)ld_state(&U[sx<NB>(nb[k], 3, b)]) : 0.0;
     }
   double density_jump = 0.0, total_energy_jump = 0.0, surface = 0.0;
   double min_density = 1.0e10, min_total_energy = 1.0e10;
@@ -921,10 +1087,10 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __re
     const int i = lane + 32 * it;
     const bool ok = i < NEQ * NB;
     const int b = i % NB;
-    own[it] = ok ? (double)ld_state(&U[(size_t)i * ld + e]) : 0.0;
+    own[it] = ok ? (double)ld_state(&U[(size_t)e * (NEQ * NB) + i]) : 0.0;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-      nbv[it][k] = (ok && interior[k] && b > 0) ? (double)ld_state(&U[(size_t)i * ld + nbrs[k]]) : 0.0;
+      nbv[it][k] = (ok && interior[k] && b > 0) ? (double)ld_state(&U[(size_t)nbrs[k] * (NEQ * NB) + i]) : 0.0;
   }
 #pragma unroll
   for (int it = 0; it < NQL; ++it) {
@@ -1045,7 +1211,7 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __re
       for (int k = 0; k < NEQ; ++k) sum += S.R[f][r][k] * S.pol_new[f][k][b];
       recon = recon + sum * Jn[f] * 0.5;
     }
-    U[(r * NB + b) * ld + e] = T(recon * inv_area);
+    U[sx<NB>(e, r, b)] = T(recon * inv_area);
   }
   __syncwarp();
   return ST_OK;
@@ -1108,8 +1274,16 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
                                                                 int* __restrict__ work) {
   Control* ctl = kp.ctl;
   const MeshDev& m = kp.m;
-  __shared__ WenoScratch<P> scratch[kLimiterWarps];
+  // per warp: the WENO scratch in phase B, the batch's 32 element records in phase A
+  constexpr int STRIDE = Staged<Variant<P>::NB, T>::kStride;
+  constexpr size_t kWarpNeed = (sizeof(WenoScratch<P>) > 32 * STRIDE * sizeof(T) ? sizeof(WenoScratch<P>)
+                                                                                   : 32 * STRIDE * sizeof(T));
+  constexpr size_t kWarpBytes = (kWarpNeed + 127) / 128 * 128;  // every warp's buffer 16-byte aligned
+  static_assert(kWarpBytes % 16 == 0, "16-byte record copies need 16-byte aligned warp buffers");
+  __shared__ __align__(128) unsigned char s_warp[kLimiterWarps][kWarpBytes];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  WenoScratch<P>* scratch_w = reinterpret_cast<WenoScratch<P>*>(s_warp[wib]);
+  T* recs = reinterpret_cast<T*>(s_warp[wib]);
   const int gwarp = blockIdx.x * kLimiterWarps + wib;
   const int nwarps = gridDim.x * kLimiterWarps;
   int troubled_local = 0;
@@ -1119,25 +1293,21 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
     int unknown_local = 0, flagged_local = 0;
     for (int base = gwarp * 32; base < m.ne; base += nwarps * 32) {
       const int e = base + lane;
-      bool pending = false, ready = false, trouble = false;
+      bool pending = false, ready = false, trouble = false, need = false, any_mod = false;
       if (e < m.ne) {
-        bool flag0 = false;
         if (wave == 1) {
           const int inst = m.n_inst > 1 ? m.inst[e] : 0;
           if (kp.ic[inst].active) {
-            flag0 = STAGED ? kxrcf_staged<P, T>(kp, U, e) : kxrcf<P, T>(kp, U, e);
+            need = true;  // the parallel flag t0 of every stepping element
             pending = true;
           } else {
             ready = true;  // not stepping: settles clean, never read as rewritten
           }
-          t0[e] = flag0 ? 1 : 0;
-          flagged_local += flag0 ? 1 : 0;
         } else {
           pending = (__ldcg(&status[e]) & 3u) == 0u;
         }
         if (pending) {
           ready = true;
-          bool any_mod = false;
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
             const int nb = m.nbr[k * m.ld + e];
@@ -1151,8 +1321,31 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
               }
             }
           }
-          if (ready) trouble = (wave == 1) ? flag0 : (any_mod ? (STAGED ? kxrcf_staged<P, T>(kp, U, e) : kxrcf<P, T>(kp, U, e)) : (t0[e] != 0));
+          if (wave > 1 && ready && any_mod) need = true;  // a lower neighbour was rewritten
         }
+      }
+      // modified_kxrcf of the lanes that need it.  Wave 1 evaluates every element: the batch's 32
+      // records (contiguous) are staged in shared memory with coalesced 16-byte loads through L2.
+      // Later waves re-evaluate only the few elements next to rewritten cells, each reading its own
+      // record directly (it is still pending, so nothing has rewritten it in this pass)
+      bool flag = false;
+      if (wave == 1) {
+        if (__any_sync(0xffffffffu, need)) {
+          warp_load_records<Variant<P>::NB, T, 32>(U, base, recs, lane);
+          if (need)
+            flag = STAGED ? kxrcf_staged<P, T>(kp, U, e, recs + lane * STRIDE)
+                          : kxrcf<P, T>(kp, U, e, recs + lane * STRIDE);
+        }
+      } else if (need) {
+        const T* own = U + (size_t)e * (NEQ * Variant<P>::NB);
+        flag = STAGED ? kxrcf_staged<P, T>(kp, U, e, own) : kxrcf<P, T>(kp, U, e, own);
+      }
+      if (e < m.ne) {
+        if (wave == 1) {
+          t0[e] = flag ? 1 : 0;
+          flagged_local += flag ? 1 : 0;
+        }
+        if (pending && ready) trouble = (wave == 1 || any_mod) ? flag : (t0[e] != 0);
         if (wave == 1 && !ready) status[e] = 0u;
         if (ready && !trouble) status[e] = ((unsigned int)wave << 2) | 1u;
       }
@@ -1190,7 +1383,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
         fwt[k] = m.face[k * m.ld + et];
         nbt[k] = m.nbr[k * m.ld + et];
       }
-      const int rs = weno_reconstruct<P, T>(kp, U, et, fwt, nbt, lane, scratch[wib]);
+      const int rs = weno_reconstruct<P, T>(kp, U, et, fwt, nbt, lane, *scratch_w);
       if (rs != ST_OK && lane == 0) {
         const int inst = m.n_inst > 1 ? m.inst[et] : 0;
         raise_status(ctl, &kp.ic[inst], rs, et);
@@ -1219,12 +1412,14 @@ __global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KPara
   const int inst = m.n_inst > 1 ? m.inst[ec] : 0;
   unsigned long long bits = 0x7ff0000000000000ull;  // +inf never wins against 1e10
   if (e < m.ne && kp.ic[inst].active) {
+    T rec[NEQ * NB];
+    load_elem<NB, T, true>(U, e, rec);
     double s[NEQ];
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
       double a = 0.0;
 #pragma unroll
-      for (int b = 0; b < NB; ++b) a += (double)ld_state(&U[(size_t)(v * NB + b) * m.ld + e]);
+      for (int b = 0; b < NB; ++b) a += (double)rec[v * NB + b];
       s[v] = a;
     }
     const double hcr = kp.gas.hcr;
@@ -1273,12 +1468,14 @@ __global__ void __launch_bounds__(256) k_step_head(const __grid_constant__ KPara
   const int inst = m.n_inst > 1 ? m.inst[ec] : 0;
   unsigned long long bits = 0x7ff0000000000000ull;
   if (e < m.ne && step_runs(ic[inst])) {
+    T rec[NEQ * NB];
+    load_elem<NB, T, true>(U, e, rec);
     double s[NEQ];
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
       double a = 0.0;
 #pragma unroll
-      for (int b = 0; b < NB; ++b) a += (double)ld_state(&U[(size_t)(v * NB + b) * m.ld + e]);
+      for (int b = 0; b < NB; ++b) a += (double)rec[v * NB + b];
       s[v] = a;
     }
     const double hcr = kp.gas.hcr;
@@ -1376,11 +1573,11 @@ __global__ void __launch_bounds__(256) k_diagnostics(const __grid_constant__ KPa
   for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
     const double area = 0.5 * m.jac[e] * wsum;
 #pragma unroll
-    for (int v = 0; v < NEQ; ++v) acc[v] += area * (double)U[(size_t)(v * NB) * m.ld + e];
+    for (int v = 0; v < NEQ; ++v) acc[v] += area * (double)U[sx<NB>(e, v, 0)];
     if (R) {
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        const double r = (double)R[(size_t)b * m.ld + e];
+        const double r = (double)R[sx<NB>(e, 0, b)];
         acc[6] += r * r;
       }
     }
@@ -1397,7 +1594,7 @@ __global__ void __launch_bounds__(256) k_diagnostics(const __grid_constant__ KPa
       for (int v = 0; v < NEQ; ++v) {
         double a = 0.0;
 #pragma unroll
-        for (int b = 0; b < NB; ++b) a += (double)U[(size_t)(v * NB + b) * m.ld + e] * kp.d.phi_edge[k][g][b];
+        for (int b = 0; b < NB; ++b) a += (double)U[sx<NB>(e, v, b)] * kp.d.phi_edge[k][g][b];
         q[v] = a;
       }
       const double p = kp.gas.gm1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
@@ -1433,11 +1630,10 @@ __global__ void k_cell_fields(const __grid_constant__ KParams<P, T> kp, const T*
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne) return;
   const int e = e0 + i;
-  const size_t ld = kp.m.ld;
-  const double density = (double)U[(size_t)(0 * NB) * ld + e];
-  const double x_momentum = (double)U[(size_t)(1 * NB) * ld + e];
-  const double y_momentum = (double)U[(size_t)(2 * NB) * ld + e];
-  const double energy = (double)U[(size_t)(3 * NB) * ld + e];
+  const double density = (double)U[sx<NB>(e, 0, 0)];
+  const double x_momentum = (double)U[sx<NB>(e, 1, 0)];
+  const double y_momentum = (double)U[sx<NB>(e, 2, 0)];
+  const double energy = (double)U[sx<NB>(e, 3, 0)];
   const double x_velocity = x_momentum / density;
   const double y_velocity = y_momentum / density;
   const double kinetic = __dadd_rn(__dmul_rn(x_velocity, x_velocity), __dmul_rn(y_velocity, y_velocity));
@@ -1448,23 +1644,15 @@ __global__ void k_cell_fields(const __grid_constant__ KParams<P, T> kp, const T*
   out[4 * i + 3] = pressure;
 }
 
-// Layout transposes between the reference's [element][variable][basis] (FP64) and the SoA
-// state in the storage type.
-template <int NB, typename T>
-__global__ void k_aos_to_soa(const double* __restrict__ src, T* __restrict__ dst, int ne, int ld) {
+// Conversions between the reference's FP64 arrays and an FP32 state (same element-major
+// layout; FP64 states are copied directly).
+__global__ void k_f64_to_f32(const double* __restrict__ src, float* __restrict__ dst, long long n) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)ne * NEQ * NB) return;
-  const int e = (int)(i / (NEQ * NB));
-  const int c = (int)(i - (long long)e * NEQ * NB);
-  dst[(size_t)c * ld + e] = T(src[i]);
+  if (i < n) dst[i] = (float)src[i];
 }
-template <int NB, typename T>
-__global__ void k_soa_to_aos(const T* __restrict__ src, double* __restrict__ dst, int ne, int ld) {
+__global__ void k_f32_to_f64(const float* __restrict__ src, double* __restrict__ dst, long long n) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)ne * NEQ * NB) return;
-  const int e = (int)(i / (NEQ * NB));
-  const int c = (int)(i - (long long)e * NEQ * NB);
-  dst[i] = (double)src[(size_t)c * ld + e];
+  if (i < n) dst[i] = (double)src[i];
 }
 
 // Initial L2 projection of a uniform state onto the basis (Solver::set_initial_solution,
@@ -1497,7 +1685,7 @@ __global__ void k_project_uniform(const __grid_constant__ Projection<P> pr, cons
 #pragma unroll
       for (int g = 0; g < V::NQ; ++g)
         acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(__dmul_rn(hj, pr.w[g]), pr.q[v]), pr.phi[g][b]));
-      U[(size_t)(v * V::NB + b) * ld + e] = T(acc / __dmul_rn(__dmul_rn(pr.mass[b], 0.5), J));
+      U[sx<V::NB>(e, v, b)] = T(acc / __dmul_rn(__dmul_rn(pr.mass[b], 0.5), J));
     }
   }
 }

@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(tc::kThreads, 8) k_element_tc(const __grid_con
     const bool valid = e_raw < m.ne && kp.ic[inst].active;
     float u[NB];
 #pragma unroll
-    for (int b = 0; b < NB; ++b) u[b] = ld_state(&Uin[(var * NB + b) * ld + e]);
+    for (int b = 0; b < NB; ++b) u[b] = ld_state(&Uin[sx<NB>(e, var, b)]);
     // geometry and the faces' edge fluxes: loaded now, used after the first contraction
     const float J = (float)m.jac[e];
     const float xx = (float)m.dinv[0 * ld + e], xy = (float)m.dinv[1 * ld + e], ex = (float)m.dinv[2 * ld + e],
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(tc::kThreads, 8) k_element_tc(const __grid_con
       const float inv_half_j = 1.f / (0.5f * J);
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        const size_t idx = (var * NB + b) * ld + e;
+        const size_t idx = sx<NB>(e, var, b);
         float rr = r[b];
         if constexpr (MODE == 0) rr = Rin[idx] + rr;
         rr = rr * kp.t.inv_mass[b] * inv_half_j;

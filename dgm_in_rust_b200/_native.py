@@ -161,6 +161,8 @@ def lib() -> ctypes.CDLL:
     L.dgm_set_edge_variant.argtypes = [vp, ctypes.c_int32]
     L.dgm_get_edge_variant.argtypes = [vp]
     L.dgm_get_limiter_variant.argtypes = [vp, P_I32, P_D]
+    L.dgm_set_limiter_schedule.argtypes = [vp, ctypes.c_int32]
+    L.dgm_get_limiter_schedule.argtypes = [vp, P_I32, P_D]
     L.dgm_instance_set_initial.argtypes = [vp, ctypes.c_int32] + [ctypes.c_double] * 4
     L.dgm_diagnostics.argtypes = [vp, ctypes.c_int32, P_D]
     L.dgm_precision.argtypes = [vp]
@@ -188,8 +190,8 @@ def lib() -> ctypes.CDLL:
                  "dgm_instance_download_residual", "dgm_instance_state", "dgm_instance_set",
                  "dgm_advance_with_residual", "dgm_diagnostics", "dgm_precision", "dgm_set_initial_solution",
                  "dgm_instance_set_initial", "dgm_set_launch_config", "dgm_get_launch_config", "dgm_autotune",
-                 "dgm_set_limiter_variant", "dgm_get_limiter_variant", "dgm_cell_fields", "dgm_set_edge_variant",
-                 "dgm_get_edge_variant"):
+                 "dgm_set_limiter_variant", "dgm_get_limiter_variant", "dgm_set_limiter_schedule",
+                 "dgm_get_limiter_schedule", "dgm_cell_fields", "dgm_set_edge_variant", "dgm_get_edge_variant"):
         getattr(L, name).restype = ctypes.c_int32
     _lib = L
     return L

@@ -65,10 +65,11 @@ struct dgm_ctx {
   InstCtl* ic = nullptr;
   std::vector<void*> allocs;
   int64_t bytes = 0;
-  int coop_blocks[2] = {1, 1};  // co-resident limiter blocks of the compact / staged detector
+  int coop_blocks[2][2] = {{1, 1}, {1, 1}};  // co-resident limiter blocks [detector][schedule]
   int lim_staged = 0;            // limiter detector variant (dgm_set_limiter_variant / autotune)
+  int lim_queue = 0;             // limiter schedule (dgm_set_limiter_schedule / autotune)
   int edge_pair = 0;             // edge pass form: 0 thread per (slot, point), 1 lane pair per slot
-  float lim_us[2] = {0.f, 0.f};  // last autotuned limiter times, compact / staged
+  float lim_us[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // last autotuned limiter times [detector][schedule]
   // launch configuration of the edge and element passes (dgm_set_launch_config / dgm_autotune):
   // edge_blocks = 0 launches one thread per (slot, Gauss point), else a grid-stride grid
   int edge_threads = 256, edge_blocks = 0, elem_threads = 256;
@@ -231,7 +232,7 @@ struct Ops {
   static int limiter(dgm_ctx* c, T* U) {
     if (!c->limiter) return DGM_OK;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(c->coop_blocks[c->lim_staged]);
+    cfg.gridDim = dim3(c->coop_blocks[c->lim_staged][c->lim_queue]);
     cfg.blockDim = dim3(dgm::kLimiterWarps * 32);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = c->stream;
@@ -240,10 +241,10 @@ struct Ops {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (c->lim_staged)
-      CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter<P, T, true>, kp_of<P, T>(c), U, c->t0, c->status, c->work));
-    else
-      CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter<P, T, false>, kp_of<P, T>(c), U, c->t0, c->status, c->work));
+    auto kern = dgm::k_limiter<P, T, false, false>;
+    if (c->lim_staged) kern = c->lim_queue ? dgm::k_limiter<P, T, true, true> : dgm::k_limiter<P, T, true, false>;
+    else if (c->lim_queue) kern = dgm::k_limiter<P, T, false, true>;
+    CK(cudaLaunchKernelEx(&cfg, kern, kp_of<P, T>(c), U, c->t0, c->status, c->work));
     return DGM_OK;
   }
 
@@ -354,12 +355,16 @@ struct Ops {
   }
 
   static int occupancy(dgm_ctx* c) {
-    int per_sm[2] = {0, 0};
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], dgm::k_limiter<P, T, false>, dgm::kLimiterWarps * 32, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], dgm::k_limiter<P, T, true>, dgm::kLimiterWarps * 32, 0));
+    int per_sm[2][2] = {{0, 0}, {0, 0}};
+    const int threads = dgm::kLimiterWarps * 32;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0][0], dgm::k_limiter<P, T, false, false>, threads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0][1], dgm::k_limiter<P, T, false, true>, threads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1][0], dgm::k_limiter<P, T, true, false>, threads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1][1], dgm::k_limiter<P, T, true, true>, threads, 0));
     const int64_t want = std::max<int64_t>(1, (c->ne + 32 * dgm::kLimiterWarps - 1) / (32 * dgm::kLimiterWarps));
     for (int v = 0; v < 2; ++v)
-      c->coop_blocks[v] = (int)std::min<int64_t>((int64_t)std::max(1, per_sm[v]) * c->num_sms, want);
+      for (int q = 0; q < 2; ++q)
+        c->coop_blocks[v][q] = (int)std::min<int64_t>((int64_t)std::max(1, per_sm[v][q]) * c->num_sms, want);
     return DGM_OK;
   }
 
@@ -468,6 +473,12 @@ int collect_status(dgm_ctx* c) {
     c->err_where = h.err_where;
     const int zero = 0;
     CK(cudaMemcpyAsync(&c->ctl->status, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    if (h.status == dgm::ST_TIMEOUT) {
+      // a limiter pass that gave up may have left queue slots and counters behind
+      CK(cudaMemsetAsync(c->work, 0, sizeof(int) * std::max<int64_t>(c->ne, 1), c->stream));
+      CK(cudaMemsetAsync(&c->ctl->lim_exit, 0, sizeof(unsigned int), c->stream));
+      CK(cudaMemsetAsync(&c->ctl->lq[0], 0, sizeof(c->ctl->lq), c->stream));
+    }
     for (size_t i = 0; i < c->inst.size(); ++i)
       if (hi[i].status) CK(cudaMemcpyAsync(&c->ic[i].status, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -873,6 +884,9 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* 
     return fail(st);
   for (void* p : {c->U, c->U1, c->U2, c->R})
     if (cudaMemsetAsync(p, 0, n_state * eb, c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  // the limiter's queue slots are zero between passes (each consumer clears its slot)
+  if (cudaMemsetAsync(c->work, 0, sizeof(int) * std::max<int64_t>(c->ne, 1), c->stream) != cudaSuccess)
+    return fail(DGM_CUDA_ERROR);
   if (c->limiter) {
     if ((st = dev_alloc(c, &c->gram, (size_t)(c->nb * (c->nb + 1) / 2) * c->ld))) return fail(st);
     if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::weno_gram(c); }))) return fail(st);
@@ -1223,6 +1237,33 @@ int32_t dgm_set_limiter_variant(dgm_ctx* c, int32_t staged) {
   return DGM_OK;
 }
 
+// The queue schedule needs the worklist all zero when a pass starts (its consumers clear what
+// they take); the barrier schedule leaves its entries behind, so a switch to the queue clears it.
+static int set_schedule(dgm_ctx* c, int queue) {
+  if (queue && !c->lim_queue)
+    CK(cudaMemsetAsync(c->work, 0, sizeof(int) * std::max<int64_t>(c->ne, 1), c->stream));
+  c->lim_queue = queue;
+  return DGM_OK;
+}
+
+int32_t dgm_set_limiter_schedule(dgm_ctx* c, int32_t queue) {
+  if (!c || (queue != 0 && queue != 1)) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  CK(cudaStreamSynchronize(c->stream));
+  int st = set_schedule(c, queue);
+  if (st) return st;
+  reset_graphs(c);
+  return DGM_OK;
+}
+
+int32_t dgm_get_limiter_schedule(dgm_ctx* c, int32_t* queue, double* tuned_us) {
+  if (!c) return DGM_BAD_ARG;
+  if (queue) *queue = c->lim_queue;
+  if (tuned_us)
+    for (int q = 0; q < 2; ++q) tuned_us[q] = std::min(c->lim_us[0][q], c->lim_us[1][q]);
+  return DGM_OK;
+}
+
 int32_t dgm_set_edge_variant(dgm_ctx* c, int32_t pair) {
   if (!c || (pair != 0 && pair != 1)) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
@@ -1237,10 +1278,8 @@ int32_t dgm_get_edge_variant(dgm_ctx* c) { return c ? c->edge_pair : -1; }
 int32_t dgm_get_limiter_variant(dgm_ctx* c, int32_t* staged, double* tuned_us) {
   if (!c) return DGM_BAD_ARG;
   if (staged) *staged = c->lim_staged;
-  if (tuned_us) {
-    tuned_us[0] = c->lim_us[0];
-    tuned_us[1] = c->lim_us[1];
-  }
+  if (tuned_us)
+    for (int v = 0; v < 2; ++v) tuned_us[v] = std::min(c->lim_us[v][0], c->lim_us[v][1]);
   return DGM_OK;
 }
 
@@ -1324,11 +1363,16 @@ int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
     return DGM_OK;
   };
   if (c->limiter) {
-    for (int v = 0; v < 2 && !st; ++v) {
-      c->lim_staged = v;
-      st = time_limiter(&c->lim_us[v]);
-    }
-    c->lim_staged = (!st && c->lim_us[1] < c->lim_us[0]) ? 1 : 0;
+    int bv = 0, bq = 0;
+    for (int v = 0; v < 2 && !st; ++v)
+      for (int q = 0; q < 2 && !st; ++q) {
+        c->lim_staged = v;
+        st = set_schedule(c, q);
+        if (!st) st = time_limiter(&c->lim_us[v][q]);
+        if (!st && c->lim_us[v][q] < c->lim_us[bv][bq]) bv = v, bq = q;
+      }
+    c->lim_staged = bv;
+    if (!st) st = set_schedule(c, bq);
   }
   for (auto& cand : edge_cand) {
     c->edge_pair = cand[0];

@@ -102,6 +102,27 @@ struct InstCtl {
   long long err_where;         // edge / element of that error
 };
 
+// Counters of one limiter wave, each on its own 128-byte line so that polling one does not slow
+// the atomics on another: cells enlisted for reconstruction (tail), tickets handed to
+// reconstructing warps (head), warps that finished the wave's scan (scanned) and cells left for a
+// later wave (unknown).
+struct alignas(128) LimQueue {
+  int tail;
+  int _pad0[31];
+  int head;
+  int _pad1[31];
+  int scanned;
+  int unknown;
+  int _pad2[30];
+};
+
+__host__ __device__ __forceinline__ void reset_queue(LimQueue& q) {
+  q.tail = 0;
+  q.head = 0;
+  q.scanned = 0;
+  q.unknown = 0;
+}
+
 // Context-wide control block: first error, limiter counters, grid barrier.
 struct Control {
   int status;                  // first error raised on the device (any instance)
@@ -110,10 +131,12 @@ struct Control {
   int t0_count;                // cells flagged by the parallel KXRCF pass
   int troubled;                // cells limited since the last step start
   int waves;                   // limiter waves of the last pass
-  int unknown[2];              // per-wave count of unsettled cells (double-buffered)
-  int wl_count[2];             // per-wave worklist length (double-buffered)
+  int unknown[2];              // barrier schedule: per-wave count of unsettled cells (double-buffered)
+  int wl_count[2];             // barrier schedule: per-wave worklist length (double-buffered)
   unsigned int bar_count, bar_gen;  // grid barrier of the limiter kernel
   unsigned int head_done;      // blocks of k_step_head that have finished (last one closes the step head)
+  unsigned int lim_exit;       // queue schedule: blocks that have left the pass (the last one resets the queues)
+  LimQueue lq[3];              // queue schedule: per-wave queues, wave w uses lq[w % 3]
 };
 
 // Gas constants, computed once on the host from hcr with the reference's expressions.
@@ -708,6 +731,8 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
     ctl->t0_count = 0;
     ctl->unknown[0] = ctl->unknown[1] = 0;
     ctl->wl_count[0] = ctl->wl_count[1] = 0;
+    ctl->lim_exit = 0u;
+    for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
   }
   const MeshDev& m = kp.m;
   const int lane = threadIdx.x & 31;
@@ -1250,6 +1275,64 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int nblocks)
 
 constexpr int kLimiterWarps = 4;
 
+// Release/acquire fence at GPU scope: orders this thread's earlier accesses before its later ones
+// as seen by other blocks (what the limiter's queue hand-offs need; lighter than a sequentially
+// consistent __threadfence).
+__device__ __forceinline__ void fence_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Queue schedule.  Lane 0 of a reconstructing warp: returns the next cell enlisted in a wave's
+// queue, or -1 once
+// every warp has finished the wave's scan and every enlisted cell has been taken.  The warp first
+// waits, reading only, until the queue shows an untaken slot (so idle warps take no ticket and do
+// not queue up on the ticket counter), then takes a ticket.  A ticket inside the queue whose slot
+// is not yet written waits for its producer, which has reserved it; a ticket that overshot the
+// queue waits until the queue grows past it or closes.  Slots hold cell + 1 and are cleared by
+// their consumer, so the whole queue is zero again when a pass ends.  Every wait is bounded.
+__device__ __forceinline__ int limiter_ticket(Control* ctl, LimQueue* q, int* __restrict__ work, int cap,
+                                              int nwarps) {
+  volatile int* tail = &q->tail;
+  volatile int* head = &q->head;
+  volatile int* scanned = &q->scanned;
+  constexpr long long kSpin = 1ll << 23;
+  unsigned int ns = 64;
+  long long it = 0;
+  for (;; ++it) {
+    if (*head < *tail) break;
+    if (*scanned >= nwarps) {
+      fence_gpu();
+      if (*head >= *tail) return -1;
+      break;
+    }
+    if (it > kSpin) goto timeout;
+    __nanosleep(ns);
+    ns = ns < 1024u ? 2u * ns : 1024u;
+  }
+  {
+    const int i = atomicAdd(&q->head, 1);
+    ns = 32;
+    for (; it <= 2 * kSpin; ++it) {
+      if (i < cap) {
+        volatile int* slot = work + i;
+        const int v = *slot;
+        if (v != 0) {
+          *slot = 0;
+          return v - 1;
+        }
+      }
+      if (*scanned >= nwarps) {
+        fence_gpu();
+        if (i >= *tail) return -1;
+        ns = 32;  // reserved by a producer: its store is on the way
+      }
+      __nanosleep(ns);
+      ns = ns < 1024u ? 2u * ns : 1024u;
+    }
+  }
+timeout:
+  if (atomicCAS(&ctl->status, 0, ST_TIMEOUT) == 0) ctl->err_where = -1;
+  return -1;
+}
+
 // The limiter (apply_limiter -> weno, limiter.rs:7, weno.rs:86-269), exact in the reference's
 // sequential, in-place element order, run in parallel waves:
 //   * an element settles in wave w once every lower-index neighbour settled in an earlier
@@ -1260,21 +1343,29 @@ constexpr int kLimiterWarps = 4;
 //     neighbours -- again what the sequential loop reads;
 //   * elements that settle in the same wave never read one another, so in-place writes are
 //     race free.
-// Wave 1 also evaluates modified_kxrcf on every element (the parallel flags t0).  Each wave:
-// (A) every warp scans 32 elements at a time, settles the clean ready ones and appends the
-// troubled ready ones to a worklist; grid barrier; (B) one warp per worklist element
-// reconstructs; grid barrier.  Status word: (wave << 2) | kind, kind 1 clean, 2 limited.
-// Wave count = longest chain of increasing-index neighbours through unsettled elements: 2 on
-// the O-grid's 2-colour numbering.  Instances never share neighbours, so one pass limits all of
-// them; elements of instances that are not stepping settle clean without evaluation.
-template <int P, typename T, bool STAGED>
+// Wave 1 also evaluates modified_kxrcf on every element (the parallel flags t0).  In each wave
+// every warp scans 32 elements at a time, settles the clean ready ones and enlists the troubled
+// ready ones in the wave's queue; the enlisted elements are then reconstructed, one per warp.
+// Two schedules, same results bit for bit:
+//   * QUEUE = false: a grid barrier separates the scan from the reconstruction, warps take the
+//     worklist's entries in a fixed stride (the entries stay behind after the pass);
+//   * QUEUE = true: a warp that has finished its scan takes tickets from the queue and
+//     reconstructs while other warps still scan.  That overlap is safe: a reconstruction in wave
+//     w rewrites an element all of whose lower neighbours settled before wave w, so the only
+//     concurrent reads of it are wave-1 flags of its higher neighbours, and those flags are never
+//     used (a higher neighbour of a rewritten element is re-evaluated in a later wave).
+// A grid barrier ends every wave but the last.  Status word: (wave << 2) | kind, kind 1 clean,
+// 2 limited.  Wave count = longest chain of increasing-index neighbours through unsettled
+// elements: 2 on the O-grid's 2-colour numbering.  Instances never share neighbours, so one pass
+// limits all of them; elements of instances that are not stepping settle clean without evaluation.
+template <int P, typename T, bool STAGED, bool QUEUE>
 __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_constant__ KParams<P, T> kp,
                                                                 T* __restrict__ U, unsigned char* __restrict__ t0,
                                                                 unsigned int* __restrict__ status,
                                                                 int* __restrict__ work) {
   Control* ctl = kp.ctl;
   const MeshDev& m = kp.m;
-  // per warp: the WENO scratch in phase B, the batch's 32 element records in phase A
+  // per warp: the WENO scratch while reconstructing, the batch's 32 element records while scanning
   constexpr int STRIDE = Staged<Variant<P>::NB, T>::kStride;
   constexpr size_t kWarpNeed = (sizeof(WenoScratch<P>) > 32 * STRIDE * sizeof(T) ? sizeof(WenoScratch<P>)
                                                                                    : 32 * STRIDE * sizeof(T));
@@ -1289,7 +1380,10 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
   int troubled_local = 0;
   int wave = 1;
   for (;; ++wave) {
-    // ---- phase A: readiness scan, settle clean elements, enlist troubled ones ----
+    LimQueue* q = &ctl->lq[wave % 3];
+    // the queue of wave w + 1 was last used by wave w - 2, whose readers all passed a barrier since
+    if (QUEUE && wave >= 2 && blockIdx.x == 0 && threadIdx.x == 0) reset_queue(ctl->lq[(wave + 1) % 3]);
+    // ---- scan: readiness, settle clean elements, enlist troubled ones ----
     int unknown_local = 0, flagged_local = 0;
     for (int base = gwarp * 32; base < m.ne; base += nwarps * 32) {
       const int e = base + lane;
@@ -1352,9 +1446,9 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
       const unsigned int tb = __ballot_sync(0xffffffffu, ready && trouble);
       if (tb) {
         int slot0 = 0;
-        if (lane == 0) slot0 = atomicAdd(&ctl->wl_count[wave & 1], __popc(tb));
+        if (lane == 0) slot0 = atomicAdd(QUEUE ? &q->tail : &ctl->wl_count[wave & 1], __popc(tb));
         slot0 = __shfl_sync(0xffffffffu, slot0, 0);
-        if (ready && trouble) work[slot0 + __popc(tb & ((1u << lane) - 1u))] = e;
+        if (ready && trouble) work[slot0 + __popc(tb & ((1u << lane) - 1u))] = QUEUE ? e + 1 : e;
       }
       unknown_local += (pending && !ready) ? 1 : 0;
     }
@@ -1363,20 +1457,8 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
       unknown_local += __shfl_xor_sync(0xffffffffu, unknown_local, o);
       flagged_local += __shfl_xor_sync(0xffffffffu, flagged_local, o);
     }
-    if (lane == 0 && unknown_local) atomicAdd(&ctl->unknown[wave & 1], unknown_local);
-    if (lane == 0 && flagged_local) atomicAdd(&ctl->t0_count, flagged_local);
-    if (!grid_barrier(ctl, gridDim.x)) break;
-    if (wave == 1 && *((volatile int*)&ctl->t0_count) == 0) break;  // nothing to limit
-    const int n_work = *((volatile int*)&ctl->wl_count[wave & 1]);
-    const int remaining = *((volatile int*)&ctl->unknown[wave & 1]);
-    // the other parity's counters were last read before the previous wave's second barrier
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      ctl->wl_count[(wave + 1) & 1] = 0;
-      ctl->unknown[(wave + 1) & 1] = 0;
-    }
-    // ---- phase B: reconstruct the enlisted elements, one warp each ----
-    for (int i = gwarp; i < n_work; i += nwarps) {
-      const int et = __ldcg(&work[i]);
+    // reconstruction of one enlisted element by the whole warp
+    auto reconstruct = [&](int et) {
       int fwt[3], nbt[3];
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
@@ -1388,16 +1470,83 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
         const int inst = m.n_inst > 1 ? m.inst[et] : 0;
         raise_status(ctl, &kp.ic[inst], rs, et);
       }
-      __threadfence();
-      if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
-      ++troubled_local;
+    };
+    if (!QUEUE) {
+      if (lane == 0 && unknown_local) atomicAdd(&ctl->unknown[wave & 1], unknown_local);
+      if (lane == 0 && flagged_local) atomicAdd(&ctl->t0_count, flagged_local);
+      if (!grid_barrier(ctl, gridDim.x)) break;
+      if (wave == 1 && *((volatile int*)&ctl->t0_count) == 0) break;  // nothing to limit
+      const int n_work = *((volatile int*)&ctl->wl_count[wave & 1]);
+      const int remaining = *((volatile int*)&ctl->unknown[wave & 1]);
+      // the other parity's counters were last read before the previous wave's second barrier
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->wl_count[(wave + 1) & 1] = 0;
+        ctl->unknown[(wave + 1) & 1] = 0;
+      }
+      // ---- reconstruct the enlisted elements, one warp each, in a fixed stride ----
+      for (int i = gwarp; i < n_work; i += nwarps) {
+        const int et = __ldcg(&work[i]);
+        reconstruct(et);
+        __threadfence();
+        if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
+        ++troubled_local;
+      }
+      if (remaining == 0) break;  // no further wave: nothing reads what this phase wrote
+    } else {
+      __syncwarp();
+      if (lane == 0) {
+        if (unknown_local) atomicAdd(&q->unknown, unknown_local);
+        if (flagged_local) atomicAdd(&ctl->t0_count, flagged_local);
+        fence_gpu();  // the counts before the report that this warp's scan is done
+        atomicAdd(&q->scanned, 1);
+      }
+      // ---- reconstruct enlisted elements from the queue while other warps still scan ----
+      for (;;) {
+        int et = -1;
+        if (lane == 0) et = limiter_ticket(ctl, q, work, m.ne, nwarps);
+        et = __shfl_sync(0xffffffffu, et, 0);
+        if (et < 0) break;
+        reconstruct(et);
+        // no fence: nothing reads this element or its status before the wave's barrier
+        if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
+        ++troubled_local;
+      }
+      // every warp's scan has been reported (the ticket loop ends only then): the counts are final
+      int remaining = 0, flagged = 0;
+      if (lane == 0) {
+        fence_gpu();
+        remaining = *((volatile int*)&q->unknown);
+        flagged = *((volatile int*)&ctl->t0_count);
+      }
+      remaining = __shfl_sync(0xffffffffu, remaining, 0);
+      flagged = __shfl_sync(0xffffffffu, flagged, 0);
+      if (wave == 1 && flagged == 0) break;  // nothing flagged: no element is limited
+      if (remaining == 0) break;             // no further wave: nothing reads what this one wrote
     }
-    if (remaining == 0) break;  // no further wave: nothing reads what this phase wrote
     if (!grid_barrier(ctl, gridDim.x)) break;
     if (wave > m.ne + 2) break;
   }
-  if (lane == 0 && troubled_local) atomicAdd(&ctl->troubled, troubled_local);
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->waves = wave;
+  if (!QUEUE) {
+    if (lane == 0 && troubled_local) atomicAdd(&ctl->troubled, troubled_local);
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->waves = wave;
+    return;
+  }
+  // queue schedule: the last block to leave resets the queues for the next pass
+  __shared__ int s_troubled;
+  if (threadIdx.x == 0) s_troubled = 0;
+  __syncthreads();
+  if (lane == 0 && troubled_local) atomicAdd_block(&s_troubled, troubled_local);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_troubled) atomicAdd(&ctl->troubled, s_troubled);
+    fence_gpu();
+    if (atomicAdd(&ctl->lim_exit, 1u) == gridDim.x - 1u) {
+      for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
+      ctl->t0_count = 0;
+      ctl->waves = wave;
+      ctl->lim_exit = 0u;
+    }
+  }
 }
 
 // compute_time_step, temporal_disc.rs:58-88: each instance's minimum over its elements
@@ -1541,6 +1690,8 @@ __global__ void k_set_active(Control* ctl, InstCtl* ic, int n_inst, double dt, i
     ctl->t0_count = 0;
     ctl->unknown[0] = ctl->unknown[1] = 0;
     ctl->wl_count[0] = ctl->wl_count[1] = 0;
+    ctl->lim_exit = 0u;
+    for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
   }
   if (i >= n_inst) return;
   ic[i].active = 1;

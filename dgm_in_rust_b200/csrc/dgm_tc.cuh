@@ -199,8 +199,8 @@ __global__ void __launch_bounds__(tc::kThreads, 8) k_element_tc(const __grid_con
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   if (blockIdx.x == 0 && t == 0) {  // counters of the limiter pass that follows
     ctl->t0_count = 0;
-    ctl->unknown[0] = ctl->unknown[1] = 0;
-    ctl->wl_count[0] = ctl->wl_count[1] = 0;
+    ctl->lim_exit = 0u;
+    for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
   }
   // constant operands: B1[q][b] = phi_cell, B2[b][k] = [dxi | deta | phi_edge] (zero padded)
   for (int i = t; i < tc::kN * K1; i += tc::kThreads) {

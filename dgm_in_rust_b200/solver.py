@@ -132,10 +132,12 @@ def initial_state(mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints, hc
 def _launch_config(L, ctx) -> dict:
     cfg = (ctypes.c_int32 * 3)()
     L.dgm_get_launch_config(ctx, cfg)
-    staged = ctypes.c_int32(0)
+    staged, queue = ctypes.c_int32(0), ctypes.c_int32(0)
     L.dgm_get_limiter_variant(ctx, ctypes.byref(staged), None)
+    L.dgm_get_limiter_schedule(ctx, ctypes.byref(queue), None)
     return {"edge_threads": cfg[0], "edge_blocks": cfg[1], "element_threads": cfg[2],
             "limiter_detector": "staged" if staged.value else "compact",
+            "limiter_schedule": "queue" if queue.value else "barrier",
             "edge_form": "pair" if L.dgm_get_edge_variant(ctx) == 1 else "point"}
 
 
@@ -145,9 +147,11 @@ def _autotune(L, ctx, repeats: int) -> dict:
     if st != 0:
         raise DgmError(st, int(L.dgm_error_location(ctx)), "autotune")
     out = _launch_config(L, ctx)
-    lim = (ctypes.c_double * 2)()
+    lim, sched = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
     L.dgm_get_limiter_variant(ctx, None, lim)
-    out.update({"edge_us": best[0], "element_us": best[1], "limiter_compact_us": lim[0], "limiter_staged_us": lim[1]})
+    L.dgm_get_limiter_schedule(ctx, None, sched)
+    out.update({"edge_us": best[0], "element_us": best[1], "limiter_compact_us": lim[0], "limiter_staged_us": lim[1],
+                "limiter_barrier_us": sched[0], "limiter_queue_us": sched[1]})
     return out
 
 
@@ -319,9 +323,15 @@ class SpatialDisc:
         registers) or compact; both give the same flags.  The autotuner picks one per context."""
         self._check(self._lib.dgm_set_limiter_variant(self._ctx, 1 if staged else 0), "set_limiter_detector")
 
+    def set_limiter_schedule(self, queue: bool) -> None:
+        """Pick the limiter's schedule: a grid barrier between each wave's scan and its
+        reconstructions, or a queue that lets finished scanners reconstruct while others still
+        scan; both give bitwise identical results.  The autotuner picks one per context."""
+        self._check(self._lib.dgm_set_limiter_schedule(self._ctx, 1 if queue else 0), "set_limiter_schedule")
+
     def autotune(self, repeats: int = 20) -> dict:
-        """Time the candidate edge/element launch configurations and the two limiter detector
-        forms on the resident state and keep the fastest (a state must have been uploaded).
+        """Time the candidate edge/element launch configurations and the limiter's detector forms
+        and schedules on the resident state and keep the fastest (a state must have been uploaded).
         Returns the chosen configuration."""
         return _autotune(self._lib, self._ctx, repeats)
 

@@ -201,9 +201,18 @@ int32_t dgm_get_edge_variant(dgm_ctx* ctx);
  * round issued together: fewer memory round trips, better for small meshes).  The flags and
  * results are the same.  No counterpart in the reference. */
 int32_t dgm_set_limiter_variant(dgm_ctx* ctx, int32_t staged);
-/* Current form, and the limiter times the last dgm_autotune measured for forms 0 and 1 (us;
- * either pointer may be NULL). */
+/* Current form, and the limiter times the last dgm_autotune measured for forms 0 and 1 at their
+ * faster schedule (us; either pointer may be NULL). */
 int32_t dgm_get_limiter_variant(dgm_ctx* ctx, int32_t* staged, double* tuned_us /* [2] */);
+/* The limiter's schedule (same results bit for bit): 0 barrier (each wave scans every element,
+ * passes a grid barrier, then reconstructs the troubled elements it enlisted), 1 queue (warps that
+ * have finished the scan already reconstruct enlisted elements while others still scan; no barrier
+ * between the two halves of a wave; better when many elements are limited).  No counterpart in
+ * the reference. */
+int32_t dgm_set_limiter_schedule(dgm_ctx* ctx, int32_t queue);
+/* Current schedule, and the best limiter times the last dgm_autotune measured with schedules 0
+ * and 1 (us; either pointer may be NULL). */
+int32_t dgm_get_limiter_schedule(dgm_ctx* ctx, int32_t* queue, double* tuned_us /* [2] */);
 /* Launches of that kernel, and of all kernels, per time-march step. */
 int32_t dgm_phase_launches_per_step(dgm_ctx* ctx, int32_t phase);
 int32_t dgm_launches_per_step(dgm_ctx* ctx);

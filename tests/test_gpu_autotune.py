@@ -62,9 +62,11 @@ def test_launch_config_rejects_bad_values(built):
             with pytest.raises(DgmError):
                 s.spatial_disc.set_launch_config(*bad)
         assert s.spatial_disc.launch_config == {"edge_threads": 256, "edge_blocks": 0, "element_threads": 256,
-                                                "limiter_detector": "compact", "edge_form": "point"}
+                                                "limiter_detector": "compact", "limiter_schedule": "barrier",
+                                                "edge_form": "point"}
         sd = s.spatial_disc
         assert sd._lib.dgm_set_limiter_variant(sd.ctx, 2) == 7  # DGM_BAD_ARG
+        assert sd._lib.dgm_set_limiter_schedule(sd.ctx, 2) == 7
     finally:
         s.close()
 
@@ -95,21 +97,23 @@ def test_batch_autotune_keeps_results(built):
 @pytest.mark.parametrize("order", [1, 2, 3])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_limiter_detector_forms_agree(built, order, precision):
-    """The staged and compact KXRCF detectors flag the same cells, limit a perturbed state
-    identically and give the same time steps."""
+    """The staged and compact KXRCF detectors, each under the barrier and the queue schedule,
+    flag the same cells, limit a perturbed state identically and give the same time steps."""
     mesh, init = instance_mesh(Instance(40, 20, 0.8, 1.25, order))
     rng = np.random.default_rng(order)
     out = []
-    for staged in (False, True):
+    for staged, queue in ((False, False), (True, False), (False, True), (True, True)):
         s = build_solver(mesh, order, 1.4, 0.1, 1.0e30, 6, precision=precision)
         try:
             sd, td = s.spatial_disc, s.temporal_disc
             sd.set_limiter_detector(staged)
+            sd.set_limiter_schedule(queue)
             assert sd.launch_config["limiter_detector"] == ("staged" if staged else "compact")
+            assert sd.launch_config["limiter_schedule"] == ("queue" if queue else "barrier")
             td.set_initial_on_device(init)
             U = sd.new_state()
             td.download(U)
-            if staged is False:
+            if not out:
                 noise = 0.1 * rng.standard_normal(U[:, :, 1:].shape) * np.abs(U[:, :, :1])
             Up = U.copy()
             Up[:, :, 1:] += noise
@@ -120,7 +124,43 @@ def test_limiter_detector_forms_agree(built, order, precision):
             out.append((Up, n_limited, U, td.current_time))
         finally:
             s.close()
-    (La, na, Ua, ta), (Lb, nb, Ub, tb) = out
+    La, na, Ua, ta = out[0]
+    assert na > 0
+    for Lb, nb, Ub, tb in out[1:]:
+        assert na == nb
+        assert np.array_equal(La, Lb)
+        assert ta == tb and np.array_equal(Ua, Ub)
+
+
+@pytest.mark.gpu
+def test_limiter_schedule_switch_keeps_results(built):
+    """Limiting under the barrier schedule, then switching the same context to the queue schedule
+    (whose worklist must start empty) gives the results of a context that used only the queue."""
+    mesh, init = instance_mesh(Instance(48, 24, 0.8, 1.25, 2))
+    rng = np.random.default_rng(11)
+    out = []
+    for switch in (False, True):
+        s = build_solver(mesh, 2, 1.4, 0.1, 1.0e30, 10, precision="fp64")
+        try:
+            sd, td = s.spatial_disc, s.temporal_disc
+            td.set_initial_on_device(init)
+            U = sd.new_state()
+            td.download(U)
+            if not out:
+                noise = 0.1 * rng.standard_normal(U[:, :, 1:].shape) * np.abs(U[:, :, :1])
+            Up = U.copy()
+            Up[:, :, 1:] += noise
+            if switch:
+                sd.set_limiter_schedule(False)
+                assert sd.apply_limiter(Up.copy()) > 0  # leaves worklist entries behind
+            sd.set_limiter_schedule(True)
+            n_limited = sd.apply_limiter(Up)
+            td.advance(5)
+            td.synchronize()
+            td.download(U)
+            out.append((Up, n_limited, U))
+        finally:
+            s.close()
+    (La, na, Ua), (Lb, nb, Ub) = out
     assert na == nb and na > 0
-    assert np.array_equal(La, Lb)
-    assert ta == tb and np.array_equal(Ua, Ub)
+    assert np.array_equal(La, Lb) and np.array_equal(Ua, Ub)

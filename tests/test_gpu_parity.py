@@ -73,10 +73,12 @@ def test_residual_accumulates_into_input():
     s.close()
 
 
+@pytest.mark.parametrize("queue", [False, True])
 @pytest.mark.parametrize("order", [1, 2, 3])
 @pytest.mark.parametrize("mesh", sorted(MESHES))
-def test_limiter_parity(order, mesh):
+def test_limiter_parity(order, mesh, queue):
     s, o, U0 = pair(MESHES[mesh](), order=order)
+    s.spatial_disc.set_limiter_schedule(queue)
     U = perturbed(U0, 0.1, 4)
     Uo, Ug = U.copy(), U.copy()
     no = o.apply_limiter(Uo)
@@ -90,12 +92,14 @@ def test_limiter_parity(order, mesh):
     s.close()
 
 
+@pytest.mark.parametrize("queue", [False, True])
 @pytest.mark.parametrize("staged", [False, True])
-def test_limiter_heavy_sequential_dependencies(staged):
+def test_limiter_heavy_sequential_dependencies(staged, queue):
     """Many touching troubled cells in quad numbering: exercises long wave chains (both forms of
-    the KXRCF detector)."""
+    the KXRCF detector, both schedules)."""
     s, o, U0 = pair(naca0012_ogrid(48, 24, order="quad"))
     s.spatial_disc.set_limiter_detector(staged)
+    s.spatial_disc.set_limiter_schedule(queue)
     U = perturbed(U0, 0.25, 5)
     Uo, Ug = U.copy(), U.copy()
     assert s.spatial_disc.apply_limiter(Ug) == o.apply_limiter(Uo)

@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "fp32", "tf32", "tf32x3"], default="fp64")
     ap.add_argument("--launch", default="128,2368,128,1,0",
                     help="edge threads, edge blocks, element threads, staged limiter detector, lane-pair edge "
-                         "pass (profile case; the last value may be left out: 0)")
+                         "pass, queue limiter schedule (profile case; the last two may be left out: 0)")
     return ap.parse_args()
 
 
@@ -387,11 +387,25 @@ def run_precision(args, local):
     mesh, init = instance_mesh(inst)
     res = {"workload": "naca0012_ogrid_1024x512_p3: 1,048,576 triangles, 10 modes, M=0.7, AoA=2deg, limiter on, "
                        f"CFL 0.1, free-stream start, {K} steps", "steps": K}
-    out = {}
+    out, tuned = {}, {}
     for prec in ("fp64", "fp32", "tf32", "tf32x3", "fp64_perturbed"):
-        s = build_solver(mesh, 3, HCR, CFL, 1.0e30, K, limiter=True, device=local,
-                         precision="fp64" if prec == "fp64_perturbed" else prec)
+        mode = "fp64" if prec == "fp64_perturbed" else prec
+        if mode not in tuned:
+            # launch configuration of this mode, tuned on a developed state (a separate context
+            # advanced 20 steps), so that the timed run below starts from the free stream
+            t = build_solver(mesh, 3, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, device=local, precision=mode)
+            t.temporal_disc.set_initial_on_device(init)
+            t.temporal_disc.advance(20)
+            t.temporal_disc.synchronize()
+            tuned[mode] = t.spatial_disc.autotune(repeats=5)
+            t.close()
+        s = build_solver(mesh, 3, HCR, CFL, 1.0e30, K, limiter=True, device=local, precision=mode)
         td, sd = s.temporal_disc, s.spatial_disc
+        cfg = tuned[mode]
+        sd.set_launch_config(cfg["edge_threads"], cfg["edge_blocks"], cfg["element_threads"])
+        sd.set_edge_form(cfg["edge_form"] == "pair")
+        sd.set_limiter_detector(cfg["limiter_detector"] == "staged")
+        sd.set_limiter_schedule(cfg["limiter_schedule"] == "queue")
         td.set_initial_on_device(init)
         if prec == "fp64_perturbed":
             # conditioning floor: the FP64 solve from an initial state perturbed by 1e-13 (relative,
@@ -416,7 +430,9 @@ def run_precision(args, local):
         out[prec] = (U, cl, cd, d)
         res[prec] = {"dof_stage_updates_per_s": inst.dofs * 3 * td.current_step / (ms * 1e-3),
                      "ms_per_step": ms / max(td.current_step, 1), "steps_done": td.current_step,
-                     "time": td.current_time, "cl": cl, "cd": cd, "troubled_cells_last_stage": troubled}
+                     "time": td.current_time, "cl": cl, "cd": cd, "troubled_cells_last_stage": troubled,
+                     "launch": {k: cfg[k] for k in ("edge_threads", "edge_blocks", "element_threads", "edge_form",
+                                                    "limiter_detector", "limiter_schedule")}}
         w_basis = s.basis.mass_mat_diag
         s.close()
     (U32, cl32, cd32, _), (U64, cl64, cd64, _) = out["fp32"], out["fp64"]
@@ -672,10 +688,11 @@ def run_profile_case(args):
     mesh, init = instance_mesh(inst)
     s = build_solver(mesh, inst.order, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, precision=args.precision)
     sd, td = s.spatial_disc, s.temporal_disc
-    vals = [int(x) for x in args.launch.split(",")] + [0]
-    e_t, e_b, l_t, staged, pair = vals[:5]
+    vals = [int(x) for x in args.launch.split(",")] + [0, 0]
+    e_t, e_b, l_t, staged, pair, queue = vals[:6]
     sd.set_launch_config(e_t, e_b, l_t)
     sd.set_limiter_detector(bool(staged))
+    sd.set_limiter_schedule(bool(queue))
     sd.set_edge_form(bool(pair))
     td.set_initial_on_device(init)
     td.advance(args.warmup + args.steps)

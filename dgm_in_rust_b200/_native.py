@@ -182,6 +182,14 @@ def lib() -> ctypes.CDLL:
     L.dgm_status_string.restype = ctypes.c_char_p
     L.dgm_version.argtypes = []
     L.dgm_version.restype = ctypes.c_char_p
+    L.dgm_mesh_process.argtypes = [ctypes.c_int64, P_D, ctypes.c_int64, P_I64, ctypes.c_int64, P_I64, P_I32]
+    L.dgm_mesh_process.restype = vp
+    L.dgm_mesh_counts.argtypes = [vp, P_I64, P_I64, P_I64]
+    L.dgm_mesh_counts.restype = ctypes.c_int32
+    L.dgm_mesh_fetch.argtypes = [vp, P_I64, P_I64, P_D, P_D, P_D, P_I64, P_I64, P_I64, P_D, P_D, P_I64, P_I64, P_I64]
+    L.dgm_mesh_fetch.restype = ctypes.c_int32
+    L.dgm_mesh_free.argtypes = [vp]
+    L.dgm_mesh_free.restype = None
     for name in ("dgm_compute_residuals", "dgm_apply_limiter", "dgm_compute_time_step", "dgm_rk3",
                  "dgm_time_march", "dgm_get_clock", "dgm_set_clock", "dgm_upload_solutions",
                  "dgm_download_solutions", "dgm_advance", "dgm_synchronize", "dgm_query", "dgm_limiter_stats",

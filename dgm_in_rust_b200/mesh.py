@@ -1,6 +1,7 @@
 """Mesh ingest and preprocessing (host side, once per solve).
 
-Restates, vectorised with numpy, the reference's mesh pipeline:
+Restates the reference's mesh pipeline (the parser and the O-grid generator in numpy, the edge
+numbering and geometry natively in the library):
 
 * ``GmshParser.parse``   -- src/io/mesh_parser.rs:28-158 (gmsh 4.1 ASCII line state machine)
 * ``process_mesh``       -- src/initialization.rs:112-261 (edge numbering, left/right rule,
@@ -20,6 +21,7 @@ Conventions that the device kernels rely on (all from the reference):
 """
 from __future__ import annotations
 
+import ctypes
 import dataclasses
 import math
 from typing import Sequence
@@ -193,37 +195,18 @@ class Mesh:
         return np.stack([(y3 - y1) / J, -(x3 - x1) / J, -(y2 - y1) / J, (x2 - x1) / J], axis=1)
 
 
-def _assign_sequential(e_base, tris, edge_ids, edge_vertices, edge_elements, edge_in_cell):
-    """The reference's element->edge assignment loop (initialization.rs:181-201), used only when
-    a mesh has repeated (edge, side) writes and the vectorised path would be ambiguous."""
-    internal = np.ones(tris.shape[0], dtype=bool)
-    for t in range(tris.shape[0]):
-        e = e_base + t
-        for k in range(3):
-            d = edge_ids[t, k]
-            if edge_elements[d, 1] == -1:
-                edge_elements[d, 0] = e
-                edge_in_cell[d, 0] = k
-                internal[t] = False
-            elif tris[t, k] == edge_vertices[d, 0]:
-                edge_elements[d, 0] = e
-                edge_in_cell[d, 0] = k
-            else:
-                edge_elements[d, 1] = e
-                edge_in_cell[d, 1] = k
-    return internal
-
-
 def process_mesh(raw: RawMesh, freestream: np.ndarray, hcr: float) -> Mesh:
     """process_mesh (initialization.rs:112-261) followed by the Mesh::compute_* geometry of
     initialize_mesh_basis_gauss_params (initialization.rs:59-65).
 
-    ``freestream`` is the far-field BoundaryQuantity (rho, u, v, p) given to every "Farfield"
-    block; "Wall" blocks get none; any other name is rejected like the reference's panic.
+    The edge numbering, element-edge assignment, geometry and neighbours are computed natively
+    by the library (dgm_mesh_process: one pass, linear in the mesh size).  ``freestream`` is the
+    far-field BoundaryQuantity (rho, u, v, p) given to every "Farfield" block; "Wall" blocks get
+    none; any other name is rejected like the reference's panic.
     """
+    from . import _native
     xy = np.ascontiguousarray(raw.vertices, dtype=np.float64)
     nv = xy.shape[0]
-    key_of = lambda pairs: np.minimum(pairs[:, 0], pairs[:, 1]) * nv + np.maximum(pairs[:, 0], pairs[:, 1])
     ev_list, ep_list, ptype, pq = [], [], [], []
     for blk in raw.edge_blocks:
         name = blk.physical_name.lower()
@@ -237,108 +220,38 @@ def process_mesh(raw: RawMesh, freestream: np.ndarray, hcr: float) -> Mesh:
             raise ValueError("Boundary type not implemented")
         ev_list.append(np.asarray(blk.node_pairs, dtype=np.int64).reshape(-1, 2))
         ep_list.append(np.full(len(blk.node_pairs), len(ptype) - 1, dtype=np.int64))
-    bverts = np.concatenate(ev_list) if ev_list else np.zeros((0, 2), np.int64)
+    bverts = np.ascontiguousarray(np.concatenate(ev_list) if ev_list else np.zeros((0, 2), np.int64))
     bpatch = np.concatenate(ep_list) if ep_list else np.zeros(0, np.int64)
     nbd = bverts.shape[0]
-    # edge map: unordered node pair -> edge id (lookups try (a,b) then (b,a))
-    emap_keys = key_of(bverts) if nbd else np.zeros(0, np.int64)
-    emap_ids = np.arange(nbd, dtype=np.int64)
-    if nbd:  # a repeated pair maps to its last insertion
-        order = np.argsort(emap_keys, kind="stable")
-        k_sorted = emap_keys[order]
-        last = np.r_[k_sorted[1:] != k_sorted[:-1], True]
-        emap_keys, emap_ids = k_sorted[last], emap_ids[order][last]
-    edge_vertices = [bverts]
-    n_edges = nbd
-    internal_edges = []
-    elem_vertices, elem_edges, internal_flags = [], [], []
-    # grow-only arrays for ielements / in_cell_indices
-    cap = nbd + 3 * sum(b.shape[0] for b in raw.element_blocks)
-    edge_elements = np.zeros((cap, 2), np.int64)
-    edge_in_cell = np.zeros((cap, 2), np.int64)
-    edge_elements[:nbd] = (0, -1)
-    edge_in_cell[:nbd] = (0, -1)
-    e_base = 0
-    for tris in raw.element_blocks:
-        tris = np.asarray(tris, dtype=np.int64).reshape(-1, 3)
-        nt = tris.shape[0]
-        pairs = np.stack([tris, np.roll(tris, -1, axis=1)], axis=2).reshape(-1, 2)  # (v_i, v_{i+1})
-        keys = key_of(pairs)
-        pos = np.searchsorted(emap_keys, keys)
-        pos_c = np.minimum(pos, max(len(emap_keys) - 1, 0))
-        found = (len(emap_keys) > 0) & (emap_keys[pos_c] == keys) if len(emap_keys) else np.zeros(len(keys), bool)
-        # new internal edges, numbered by first appearance
-        new_keys, first_idx = np.unique(keys[~found], return_index=True)
-        cand = np.nonzero(~found)[0]
-        first_pos = cand[first_idx]
-        order = np.argsort(first_pos, kind="stable")
-        new_keys, first_pos = new_keys[order], first_pos[order]
-        new_ids = n_edges + np.arange(len(new_keys), dtype=np.int64)
-        edge_vertices.append(pairs[first_pos])
-        internal_edges.append(new_ids)
-        edge_elements[n_edges:n_edges + len(new_keys)] = 0
-        edge_in_cell[n_edges:n_edges + len(new_keys)] = 0
-        n_edges += len(new_keys)
-        all_keys = np.concatenate([emap_keys, new_keys])
-        all_ids = np.concatenate([emap_ids, new_ids])
-        srt = np.argsort(all_keys, kind="stable")
-        emap_keys, emap_ids = all_keys[srt], all_ids[srt]
-        ids = emap_ids[np.searchsorted(emap_keys, keys)].reshape(nt, 3)
-        ev_all = np.concatenate(edge_vertices)
-        # assignment (initialization.rs:181-201)
-        elem_idx = e_base + np.repeat(np.arange(nt, dtype=np.int64), 3)
-        kk = np.tile(np.arange(3, dtype=np.int64), nt)
-        flat = ids.reshape(-1)
-        is_bnd = flat < nbd
-        same = pairs[:, 0] == ev_all[flat, 0]
-        left = is_bnd | same
-        tgt_side = np.where(left, 0, 1)
-        slot = flat * 2 + tgt_side
-        if len(np.unique(slot)) != len(slot):
-            internal = _assign_sequential(e_base, tris, ids, ev_all, edge_elements, edge_in_cell)
-        else:
-            edge_elements[flat, tgt_side] = elem_idx
-            edge_in_cell[flat, tgt_side] = kk
-            internal = ~is_bnd.reshape(nt, 3).any(axis=1)
-        elem_vertices.append(tris)
-        elem_edges.append(ids)
-        internal_flags.append(internal)
-        e_base += nt
-    edge_vertices = np.concatenate(edge_vertices)
-    edge_elements = edge_elements[:n_edges].copy()
-    edge_in_cell = edge_in_cell[:n_edges].copy()
-    edge_patch = np.full(n_edges, -1, np.int64)
-    edge_patch[:nbd] = bpatch
-    elem_vertices = np.concatenate(elem_vertices) if elem_vertices else np.zeros((0, 3), np.int64)
-    elem_edges = np.concatenate(elem_edges) if elem_edges else np.zeros((0, 3), np.int64)
-    internal_flags = np.concatenate(internal_flags) if internal_flags else np.zeros(0, bool)
+    blocks = [np.asarray(t, dtype=np.int64).reshape(-1, 3) for t in raw.element_blocks]
+    elem_vertices = np.ascontiguousarray(np.concatenate(blocks) if blocks else np.zeros((0, 3), np.int64))
     ne = elem_vertices.shape[0]
 
-    # ---- geometry, mesh.rs:15-84 (same operation order as the reference) ----
-    x, y = xy[:, 0], xy[:, 1]
-    ex1, ex2 = x[edge_vertices[:, 0]], x[edge_vertices[:, 1]]
-    ey1, ey2 = y[edge_vertices[:, 0]], y[edge_vertices[:, 1]]
-    edx, edy = ex2 - ex1, ey2 - ey1
-    edge_jac = np.sqrt(edx * edx + edy * edy)
-    edge_normal = np.stack([edy / edge_jac, -edx / edge_jac], axis=1)
-    x1, x2, x3 = x[elem_vertices[:, 0]], x[elem_vertices[:, 1]], x[elem_vertices[:, 2]]
-    y1, y2, y3 = y[elem_vertices[:, 0]], y[elem_vertices[:, 1]], y[elem_vertices[:, 2]]
-    jac = (x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1)
-    a = np.sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1))
-    b = np.sqrt((x3 - x2) * (x3 - x2) + (y3 - y2) * (y3 - y2))
-    c = np.sqrt((x1 - x3) * (x1 - x3) + (y1 - y3) * (y1 - y3))
-    s = (a + b + c) / 2.0
-    with np.errstate(invalid="ignore", divide="ignore"):
-        circ = a * b * c / (4.0 * np.sqrt(s * (s - a) * (s - b) * (s - c)))
-        surface = 0.5 * jac
-        hmin = np.fmin(np.fmin(2.0 * surface / a, 2.0 * surface / b), 2.0 * surface / c)
-    # set_neighbours, mesh.rs:133-147
-    nbr = np.full((ne, 3), -1, np.int64)
-    d = elem_edges
-    bnd = edge_elements[d, 1] == -1
-    same = elem_vertices == edge_vertices[d, 0]
-    other = np.where(same, edge_elements[d, 1], edge_elements[d, 0])
-    nbr[~bnd] = other[~bnd]
+    L = _native.lib()
+    st = ctypes.c_int32(0)
+    h = L.dgm_mesh_process(nv, _native.dptr(xy), nbd, _native.iptr(bverts), ne, _native.iptr(elem_vertices),
+                           ctypes.byref(st))
+    if not h:
+        raise _native.DgmError(st.value, what="process_mesh")
+    try:
+        ned, nie, nil = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+        L.dgm_mesh_counts(h, ctypes.byref(ned), ctypes.byref(nie), ctypes.byref(nil))
+        ned, nie, nil = ned.value, nie.value, nil.value
+        elem_edges, nbr = np.empty((ne, 3), np.int64), np.empty((ne, 3), np.int64)
+        jac, circ, hmin = np.empty(ne), np.empty(ne), np.empty(ne)
+        edge_elements, edge_vertices = np.empty((ned, 2), np.int64), np.empty((ned, 2), np.int64)
+        edge_in_cell, edge_jac, edge_normal = np.empty((ned, 2), np.int64), np.empty(ned), np.empty((ned, 2))
+        internal_edges, internal_el = np.empty(nie, np.int64), np.empty(nil, np.int64)
+        boundary_el = np.empty(ne - nil, np.int64)
+        P = _native.iptr
+        D = _native.dptr
+        L.dgm_mesh_fetch(h, P(elem_edges), P(nbr), D(jac), D(circ), D(hmin), P(edge_elements), P(edge_vertices),
+                         P(edge_in_cell), D(edge_jac), D(edge_normal), P(internal_edges), P(internal_el),
+                         P(boundary_el))
+    finally:
+        L.dgm_mesh_free(h)
+    edge_patch = np.full(ned, -1, np.int64)
+    edge_patch[:nbd] = bpatch
     return Mesh(
         vertices=xy,
         elem_vertices=elem_vertices,
@@ -355,9 +268,9 @@ def process_mesh(raw: RawMesh, freestream: np.ndarray, hcr: float) -> Mesh:
         edge_patch=edge_patch,
         patch_type=np.array(ptype, dtype=np.int32),
         patch_quantity=np.array(pq, dtype=np.float64).reshape(-1, 4),
-        internal_edge_indices=np.concatenate(internal_edges) if internal_edges else np.zeros(0, np.int64),
-        internal_element_indices=np.nonzero(internal_flags)[0].astype(np.int64),
-        boundary_element_indices=np.nonzero(~internal_flags)[0].astype(np.int64),
+        internal_edge_indices=internal_edges,
+        internal_element_indices=internal_el,
+        boundary_element_indices=boundary_el,
     )
 
 

@@ -72,6 +72,32 @@ typedef struct dgm_mesh_desc {
   const int64_t* boundary_elements; /* Mesh::boundary_element_indices                       */
 } dgm_mesh_desc;
 
+/* Host mesh preprocessing, native (no device memory, no GPU needed): process_mesh
+ * (initialization.rs:112-261) and the Mesh::compute_* geometry (mesh.rs:15-147) in one pass that
+ * is linear in the mesh size, producing the arrays of dgm_mesh_desc bit for bit as the reference
+ * computes them.  Input: what GmshParser::parse (mesh_parser.rs:28-158) returns -- vertices, the
+ * node pairs of every boundary line block concatenated in block order, and the triangles of every
+ * surface block concatenated in block order, all 0-based.  dgm_mesh_process returns a handle
+ * (NULL with *status set on failure: DGM_BAD_ARG for a node index out of range); dgm_mesh_counts
+ * gives the array sizes (edges, internal edges, internal elements; the boundary elements are the
+ * rest); dgm_mesh_fetch copies the arrays into caller-allocated buffers (any pointer may be NULL);
+ * dgm_mesh_free releases the handle.  Patch types and quantities stay with the caller (one per
+ * boundary block). */
+typedef struct dgm_mesh_build dgm_mesh_build;
+dgm_mesh_build* dgm_mesh_process(int64_t n_vertices, const double* vertex_xy, int64_t n_boundary_edges,
+                                 const int64_t* boundary_pairs /* [n_boundary_edges][2] */, int64_t n_elements,
+                                 const int64_t* elem_vertices /* [n_elements][3] */, int32_t* status);
+int32_t dgm_mesh_counts(const dgm_mesh_build* m, int64_t* n_edges, int64_t* n_internal_edges,
+                        int64_t* n_internal_elements);
+int32_t dgm_mesh_fetch(const dgm_mesh_build* m, int64_t* elem_edges /* [ne][3] */,
+                       int64_t* elem_neighbours /* [ne][3] */, double* elem_jacob_det /* [ne] */,
+                       double* elem_circumradius /* [ne] */, double* elem_minimum_height /* [ne] */,
+                       int64_t* edge_elements /* [n_edges][2] */, int64_t* edge_vertices /* [n_edges][2] */,
+                       int64_t* edge_in_cell /* [n_edges][2] */, double* edge_jacob_det /* [n_edges] */,
+                       double* edge_normal /* [n_edges][2] */, int64_t* internal_edges,
+                       int64_t* internal_elements, int64_t* boundary_elements);
+void dgm_mesh_free(dgm_mesh_build* m);
+
 /* Basis and quadrature tables: DubinerBasis (basis_function.rs:6-13) and GaussPoints
  * (gauss_point.rs:4-11).  Supported (order, cell rule, edge rule): (1,3,2), (2,6,3), (3,12,4). */
 typedef struct dgm_tables_desc {

@@ -18,9 +18,10 @@ def rel_l2(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
 
 
-@pytest.fixture(scope="session")
+@pytest.fixture(scope="session", autouse=True)
 def built():
-    """Compile the CUDA library (nvcc cross-compiles without a GPU) and the oracle."""
+    """Compile the CUDA library (nvcc cross-compiles without a GPU; it also holds the native
+    mesh preprocessing every test uses) and the oracle."""
     from dgm_in_rust_b200.build import build
     from oracle.oracle import build as build_oracle
     build()

@@ -50,6 +50,37 @@ def test_process_mesh_matches_oracle_airfoil():
     assert (m.elem_jacob_det > 0).all()  # every airfoil.msh triangle is counter-clockwise
 
 
+def test_process_mesh_multiblock_repeated_pairs_matches_oracle():
+    """Two triangle blocks and a boundary pair listed twice (reversed, in a second wall block):
+    the edge numbering runs over the blocks in order and the repeated pair maps to its last
+    listing, as the reference's HashMap insert does."""
+    from dgm_in_rust_b200.mesh import EdgeBlock, RawMesh
+    r = naca0012_ogrid(16, 8)
+    t = r.element_blocks[0]
+    wall, far = r.edge_blocks
+    raw = RawMesh(r.vertices, [EdgeBlock(wall.node_pairs, "Wall"), EdgeBlock(wall.node_pairs[:3][:, ::-1].copy(), "Wall"),
+                               EdgeBlock(far.node_pairs, "Farfield")], [t[:100].copy(), t[100:].copy()])
+    m = process_mesh(raw, _fs_q(FS), 1.4)
+    _check_mesh_equal(Oracle(raw=raw, order=2, freestream=FS), m)
+    assert m.edge_elements[0, 0] == 0 and m.edge_elements[0, 1] == -1  # first listing never found
+
+
+def test_process_mesh_larger_ogrid_matches_oracle():
+    raw = naca0012_ogrid(128, 64, order="quad")
+    m = process_mesh(raw, _fs_q(FS), 1.4)
+    _check_mesh_equal(Oracle(raw=raw, order=2, freestream=FS), m)
+
+
+def test_process_mesh_rejects_bad_node_index():
+    from dgm_in_rust_b200.mesh import RawMesh
+    r = naca0012_ogrid(8, 4)
+    t = r.element_blocks[0].copy()
+    t[5, 1] = r.vertices.shape[0]
+    with pytest.raises(DgmError) as err:
+        process_mesh(RawMesh(r.vertices, r.edge_blocks, [t]), _fs_q(FS), 1.4)
+    assert err.value.status == 7  # DGM_BAD_ARG
+
+
 @pytest.mark.parametrize("order", [1, 2, 3])
 def test_tables_match_oracle(order):
     nq, ng = default_rules(order)

@@ -190,6 +190,20 @@ def lib() -> ctypes.CDLL:
     L.dgm_mesh_fetch.restype = ctypes.c_int32
     L.dgm_mesh_free.argtypes = [vp]
     L.dgm_mesh_free.restype = None
+    L.dgm_gmsh_parse.argtypes = [ctypes.c_char_p, P_I32]
+    L.dgm_gmsh_parse.restype = vp
+    L.dgm_gmsh_counts.argtypes = [vp, P_I64, P_I32, P_I32]
+    L.dgm_gmsh_counts.restype = ctypes.c_int32
+    L.dgm_gmsh_vertices.argtypes = [vp, P_D]
+    L.dgm_gmsh_vertices.restype = ctypes.c_int32
+    L.dgm_gmsh_block_size.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
+    L.dgm_gmsh_block_size.restype = ctypes.c_int64
+    L.dgm_gmsh_block_name.argtypes = [vp, ctypes.c_int32]
+    L.dgm_gmsh_block_name.restype = ctypes.c_char_p
+    L.dgm_gmsh_block.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, P_I64]
+    L.dgm_gmsh_block.restype = ctypes.c_int32
+    L.dgm_gmsh_free.argtypes = [vp]
+    L.dgm_gmsh_free.restype = None
     for name in ("dgm_compute_residuals", "dgm_apply_limiter", "dgm_compute_time_step", "dgm_rk3",
                  "dgm_time_march", "dgm_get_clock", "dgm_set_clock", "dgm_upload_solutions",
                  "dgm_download_solutions", "dgm_advance", "dgm_synchronize", "dgm_query", "dgm_limiter_stats",

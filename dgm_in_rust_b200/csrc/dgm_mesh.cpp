@@ -1,4 +1,5 @@
-// Host mesh preprocessing, native: process_mesh (src/initialization.rs:112-261) followed by the
+// Host mesh ingest, native: the gmsh 4.1 ASCII reader GmshParser::parse
+// (src/io/mesh_parser.rs:28-158), and process_mesh (src/initialization.rs:112-261) followed by the
 // Mesh::compute_* geometry (src/mesh.rs:15-147), in passes linear in the mesh size.
 //
 // Conventions (all the reference's; the device kernels rely on them):
@@ -16,11 +17,17 @@
 //     for bit those of the reference's f64 code.
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "dgm_b200.h"
+
+struct dgm_gmsh;
 
 struct dgm_mesh_build {
   int64_t ne = 0, ned = 0;
@@ -177,6 +184,170 @@ int build(dgm_mesh_build& m, int64_t nv, const double* xy, int64_t nbd, const in
   return DGM_OK;
 }
 
+// ---- GmshParser::parse (mesh_parser.rs:28-158): the reference's line state machine ----
+// Lines end at '\n' with one '\r' before it dropped (BufRead::lines); tokens are split at ASCII
+// white space; integers are unsigned decimals (an optional '+'), reals whatever f64::from_str
+// reads.  Where the reference unwraps a failed parse or lookup (a panic), this returns
+// DGM_BAD_ARG.
+struct GmshData {
+  std::vector<double> xy;
+  std::vector<std::string> edge_names;
+  std::vector<std::vector<int64_t>> edge_pairs, elem_nodes;
+};
+
+bool parse_usize(const char* t, int64_t& out) {
+  if (*t == '+') ++t;
+  if (!*t) return false;
+  uint64_t v = 0;
+  for (; *t; ++t) {
+    if (*t < '0' || *t > '9') return false;
+    if (v > (UINT64_MAX - 9) / 10) return false;
+    v = 10 * v + (uint64_t)(*t - '0');
+  }
+  if (v > (uint64_t)INT64_MAX) return false;
+  out = (int64_t)v;
+  return true;
+}
+
+bool parse_f64(const char* t, double& out) {
+  // f64::from_str takes decimal and exponent forms, inf/infinity/nan, an optional sign; strtod
+  // also reads hexadecimal forms, which f64::from_str rejects
+  const char* u = (*t == '+' || *t == '-') ? t + 1 : t;
+  if (u[0] == '0' && (u[1] == 'x' || u[1] == 'X')) return false;
+  char* end = nullptr;
+  out = std::strtod(t, &end);
+  return end != t && *end == '\0';
+}
+
+bool is_ws(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f'; }
+
+int parse_gmsh(const char* path, GmshData& g) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return DGM_BAD_ARG;
+  std::vector<char> buf;
+  if (std::fseek(f, 0, SEEK_END) == 0) {
+    const long n = std::ftell(f);
+    if (n > 0) buf.resize((size_t)n);
+    std::fseek(f, 0, SEEK_SET);
+  }
+  const size_t got = buf.empty() ? 0 : std::fread(buf.data(), 1, buf.size(), f);
+  std::fclose(f);
+  if (got != buf.size()) return DGM_BAD_ARG;
+  if (buf.empty() || buf.back() != '\n') buf.push_back('\n');  // a last line without a newline
+  enum St { Standby, FirstPhys, Phys, FirstEnt, Ent, FirstNodes, Nodes, FirstElems, FirstBlock, EdgeBlock, ElemBlock };
+  St st = Standby;
+  std::map<int64_t, std::string> phys_names;
+  std::map<int64_t, int64_t> ent_to_phys;
+  int64_t line_count = 0, max_line_count = 0;
+  std::vector<char*> tok;
+  char* p = buf.data();
+  char* const end = buf.data() + buf.size();
+  while (p < end) {
+    char* nl = static_cast<char*>(std::memchr(p, '\n', (size_t)(end - p)));
+    if (!nl) break;
+    char* line = p;
+    char* lend = nl;
+    p = nl + 1;
+    if (lend > line && lend[-1] == '\r') --lend;
+    *lend = '\0';
+    const size_t len = (size_t)(lend - line);
+    auto starts = [&](const char* pre) { const size_t n = std::strlen(pre); return len >= n && std::memcmp(line, pre, n) == 0; };
+    if (starts("$End")) { st = Standby; continue; }
+    if (starts("$PhysicalNames")) { st = FirstPhys; continue; }
+    if (starts("$Entities")) { st = FirstEnt; continue; }
+    if (starts("$Nodes")) { st = FirstNodes; continue; }
+    if (starts("$Elements")) { st = FirstElems; continue; }
+    if (st == Standby) continue;
+    if (st == FirstPhys) { st = Phys; continue; }
+    if (st == FirstEnt) { st = Ent; continue; }
+    if (st == FirstElems) { st = FirstBlock; continue; }
+    tok.clear();
+    for (char* c = line; c < lend;) {
+      while (c < lend && is_ws(*c)) ++c;
+      if (c >= lend) break;
+      tok.push_back(c);
+      while (c < lend && !is_ws(*c)) ++c;
+      *c = '\0';
+      ++c;
+    }
+    int64_t a = 0, b = 0, c3 = 0;
+    switch (st) {
+      case Phys:
+        if (tok.size() == 3) {
+          if (!parse_usize(tok[1], a)) return DGM_BAD_ARG;
+          const char* s0 = tok[2];
+          const char* s1 = s0 + std::strlen(s0);
+          while (s0 < s1 && *s0 == '"') ++s0;
+          while (s1 > s0 && s1[-1] == '"') --s1;
+          phys_names[a] = std::string(s0, s1);
+        }
+        break;
+      case Ent:
+        if (tok.size() >= 11) {
+          if (!parse_usize(tok[0], a) || !parse_usize(tok[8], b)) return DGM_BAD_ARG;
+          ent_to_phys[a] = b;
+        }
+        break;
+      case FirstNodes:
+        if (tok.size() < 2 || !parse_usize(tok[1], a)) return DGM_BAD_ARG;
+        g.xy.reserve((size_t)(2 * std::min<int64_t>(a, (int64_t)1 << 32)));
+        st = Nodes;
+        break;
+      case Nodes:
+        if (tok.size() == 3) {
+          double x, y;
+          if (!parse_f64(tok[0], x) || !parse_f64(tok[1], y)) return DGM_BAD_ARG;
+          g.xy.push_back(x);
+          g.xy.push_back(y);
+        }
+        break;
+      case FirstBlock: {
+        int64_t dim, tag, num;
+        if (tok.size() < 4 || !parse_usize(tok[0], dim) || !parse_usize(tok[1], tag) || !parse_usize(tok[3], num))
+          return DGM_BAD_ARG;
+        auto ip = ent_to_phys.find(tag);
+        if (ip == ent_to_phys.end()) return DGM_BAD_ARG;
+        auto in = phys_names.find(ip->second);
+        if (in == phys_names.end()) return DGM_BAD_ARG;
+        if (dim == 1) {
+          g.edge_names.push_back(in->second);
+          g.edge_pairs.emplace_back();
+          g.edge_pairs.back().reserve((size_t)(2 * std::min<int64_t>(num, (int64_t)1 << 30)));
+          st = EdgeBlock;
+        }
+        if (dim == 2) {
+          g.elem_nodes.emplace_back();
+          g.elem_nodes.back().reserve((size_t)(3 * std::min<int64_t>(num, (int64_t)1 << 30)));
+          st = ElemBlock;
+        }
+        line_count = 0;
+        max_line_count = num;
+        break;
+      }
+      case EdgeBlock:
+        ++line_count;
+        if (tok.size() < 3 || !parse_usize(tok[1], a) || !parse_usize(tok[2], b) || a < 1 || b < 1) return DGM_BAD_ARG;
+        g.edge_pairs.back().push_back(a - 1);
+        g.edge_pairs.back().push_back(b - 1);
+        if (line_count == max_line_count) st = FirstBlock;
+        break;
+      case ElemBlock:
+        ++line_count;
+        if (tok.size() < 4 || !parse_usize(tok[1], a) || !parse_usize(tok[2], b) || !parse_usize(tok[3], c3) ||
+            a < 1 || b < 1 || c3 < 1)
+          return DGM_BAD_ARG;
+        g.elem_nodes.back().push_back(a - 1);
+        g.elem_nodes.back().push_back(b - 1);
+        g.elem_nodes.back().push_back(c3 - 1);
+        if (line_count == max_line_count) st = FirstBlock;
+        break;
+      default:
+        break;
+    }
+  }
+  return DGM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -244,5 +415,66 @@ int32_t dgm_mesh_fetch(const dgm_mesh_build* m, int64_t* elem_edges, int64_t* el
 }
 
 void dgm_mesh_free(dgm_mesh_build* m) { delete m; }
+
+dgm_gmsh* dgm_gmsh_parse(const char* path, int32_t* status) {
+  int32_t st = DGM_BAD_ARG;
+  dgm_gmsh* g = nullptr;
+  if (path) {
+    auto* d = new (std::nothrow) GmshData();
+    if (!d) {
+      st = DGM_OOM;
+    } else {
+      try {
+        st = parse_gmsh(path, *d);
+      } catch (const std::bad_alloc&) {
+        st = DGM_OOM;
+      }
+      if (st == DGM_OK) g = reinterpret_cast<dgm_gmsh*>(d);
+      else delete d;
+    }
+  }
+  if (status) *status = st;
+  return g;
+}
+
+int32_t dgm_gmsh_counts(const dgm_gmsh* h, int64_t* n_vertices, int32_t* n_edge_blocks, int32_t* n_elem_blocks) {
+  if (!h) return DGM_BAD_ARG;
+  const GmshData& g = *reinterpret_cast<const GmshData*>(h);
+  if (n_vertices) *n_vertices = (int64_t)(g.xy.size() / 2);
+  if (n_edge_blocks) *n_edge_blocks = (int32_t)g.edge_pairs.size();
+  if (n_elem_blocks) *n_elem_blocks = (int32_t)g.elem_nodes.size();
+  return DGM_OK;
+}
+
+int32_t dgm_gmsh_vertices(const dgm_gmsh* h, double* xy) {
+  if (!h || !xy) return DGM_BAD_ARG;
+  const GmshData& g = *reinterpret_cast<const GmshData*>(h);
+  if (!g.xy.empty()) std::memcpy(xy, g.xy.data(), g.xy.size() * sizeof(double));
+  return DGM_OK;
+}
+
+int64_t dgm_gmsh_block_size(const dgm_gmsh* h, int32_t dim, int32_t i) {
+  if (!h) return -1;
+  const GmshData& g = *reinterpret_cast<const GmshData*>(h);
+  if (dim == 1 && i >= 0 && (size_t)i < g.edge_pairs.size()) return (int64_t)(g.edge_pairs[(size_t)i].size() / 2);
+  if (dim == 2 && i >= 0 && (size_t)i < g.elem_nodes.size()) return (int64_t)(g.elem_nodes[(size_t)i].size() / 3);
+  return -1;
+}
+
+const char* dgm_gmsh_block_name(const dgm_gmsh* h, int32_t i) {
+  if (!h) return nullptr;
+  const GmshData& g = *reinterpret_cast<const GmshData*>(h);
+  return (i >= 0 && (size_t)i < g.edge_names.size()) ? g.edge_names[(size_t)i].c_str() : nullptr;
+}
+
+int32_t dgm_gmsh_block(const dgm_gmsh* h, int32_t dim, int32_t i, int64_t* nodes) {
+  if (!h || !nodes || dgm_gmsh_block_size(h, dim, i) < 0) return DGM_BAD_ARG;
+  const GmshData& g = *reinterpret_cast<const GmshData*>(h);
+  const std::vector<int64_t>& v = dim == 1 ? g.edge_pairs[(size_t)i] : g.elem_nodes[(size_t)i];
+  if (!v.empty()) std::memcpy(nodes, v.data(), v.size() * sizeof(int64_t));
+  return DGM_OK;
+}
+
+void dgm_gmsh_free(dgm_gmsh* h) { delete reinterpret_cast<GmshData*>(h); }
 
 }  // extern "C"

@@ -1,7 +1,7 @@
 """Mesh ingest and preprocessing (host side, once per solve).
 
-Restates the reference's mesh pipeline (the parser and the O-grid generator in numpy, the edge
-numbering and geometry natively in the library):
+Restates the reference's mesh pipeline (the gmsh reader, the edge numbering and the geometry run
+natively in the library; the O-grid generator and the gmsh writer are numpy):
 
 * ``GmshParser.parse``   -- src/io/mesh_parser.rs:28-158 (gmsh 4.1 ASCII line state machine)
 * ``process_mesh``       -- src/initialization.rs:112-261 (edge numbering, left/right rule,
@@ -65,86 +65,44 @@ class RawMesh:
 
 
 class GmshParser:
-    """gmsh 4.1 ASCII reader with the reference's state machine (mesh_parser.rs:28-158).
+    """gmsh 4.1 ASCII reader with the reference's state machine (mesh_parser.rs:28-158), run
+    natively by the library (dgm_gmsh_parse).
 
     Quirks kept: every 3-token line inside $Nodes is a coordinate line (node tags are taken as
     file order); an entity is registered only from lines with at least 11 tokens (curves and
-    surfaces); element blocks of dimension other than 1 or 2 are not expected.
+    surfaces); element blocks of dimension other than 1 or 2 are not expected.  Where the
+    reference panics (a missing file, a malformed number, an entity without a physical name) this
+    raises DgmError (DGM_BAD_ARG).
     """
 
     @staticmethod
     def parse(filename: str) -> RawMesh:
-        physical_names: dict[int, str] = {}
-        ent_to_phys: dict[int, int] = {}
-        xy: list[float] = []
-        edge_blocks: list[tuple[list[int], str]] = []
-        elem_blocks: list[list[int]] = []
-        state = "standby"
-        line_count = max_line_count = 0
-        with open(filename, "r") as f:
-            for raw in f:
-                line = raw.rstrip("\r\n")
-                if line.startswith("$End"):
-                    state = "standby"
-                    continue
-                if line.startswith("$PhysicalNames"):
-                    state = "first_phys"
-                    continue
-                if line.startswith("$Entities"):
-                    state = "first_ent"
-                    continue
-                if line.startswith("$Nodes"):
-                    state = "first_nodes"
-                    continue
-                if line.startswith("$Elements"):
-                    state = "first_elems"
-                    continue
-                v = line.split()
-                if state == "standby":
-                    continue
-                if state == "first_phys":
-                    state = "phys"
-                elif state == "phys":
-                    if len(v) == 3:
-                        physical_names[int(v[1])] = v[2].strip('"')
-                elif state == "first_ent":
-                    state = "ent"
-                elif state == "ent":
-                    if len(v) >= 11:
-                        ent_to_phys[int(v[0])] = int(v[8])
-                elif state == "first_nodes":
-                    state = "nodes"
-                elif state == "nodes":
-                    if len(v) == 3:
-                        xy.append(float(v[0]))
-                        xy.append(float(v[1]))
-                elif state == "first_elems":
-                    state = "first_block"
-                elif state == "first_block":
-                    dim, tag, num = int(v[0]), int(v[1]), int(v[3])
-                    name = physical_names[ent_to_phys[tag]]
-                    if dim == 1:
-                        edge_blocks.append(([], name))
-                        state = "edge_block"
-                    if dim == 2:
-                        elem_blocks.append([])
-                        state = "elem_block"
-                    line_count, max_line_count = 0, num
-                elif state == "edge_block":
-                    line_count += 1
-                    edge_blocks[-1][0].extend((int(v[1]) - 1, int(v[2]) - 1))
-                    if line_count == max_line_count:
-                        state = "first_block"
-                elif state == "elem_block":
-                    line_count += 1
-                    elem_blocks[-1].extend((int(v[1]) - 1, int(v[2]) - 1, int(v[3]) - 1))
-                    if line_count == max_line_count:
-                        state = "first_block"
-        return RawMesh(
-            vertices=np.array(xy, dtype=np.float64).reshape(-1, 2),
-            edge_blocks=[EdgeBlock(np.array(p, dtype=np.int64).reshape(-1, 2), n) for p, n in edge_blocks],
-            element_blocks=[np.array(b, dtype=np.int64).reshape(-1, 3) for b in elem_blocks],
-        )
+        from . import _native
+        L = _native.lib()
+        st = ctypes.c_int32(0)
+        h = L.dgm_gmsh_parse(str(filename).encode(), ctypes.byref(st))
+        if not h:
+            raise _native.DgmError(st.value, what=f"GmshParser.parse({filename})")
+        try:
+            nv, neb, nel = ctypes.c_int64(0), ctypes.c_int32(0), ctypes.c_int32(0)
+            L.dgm_gmsh_counts(h, ctypes.byref(nv), ctypes.byref(neb), ctypes.byref(nel))
+            xy = np.empty((nv.value, 2))
+            if nv.value:
+                L.dgm_gmsh_vertices(h, _native.dptr(xy))
+            edge_blocks, elem_blocks = [], []
+            for i in range(neb.value):
+                pairs = np.empty((L.dgm_gmsh_block_size(h, 1, i), 2), np.int64)
+                if pairs.size:
+                    L.dgm_gmsh_block(h, 1, i, _native.iptr(pairs))
+                edge_blocks.append(EdgeBlock(pairs, L.dgm_gmsh_block_name(h, i).decode()))
+            for i in range(nel.value):
+                tris = np.empty((L.dgm_gmsh_block_size(h, 2, i), 3), np.int64)
+                if tris.size:
+                    L.dgm_gmsh_block(h, 2, i, _native.iptr(tris))
+                elem_blocks.append(tris)
+        finally:
+            L.dgm_gmsh_free(h)
+        return RawMesh(vertices=xy, edge_blocks=edge_blocks, element_blocks=elem_blocks)
 
 
 def freestream_quantity(mach: float, aoa_deg: float, rho: float, p: float, hcr: float) -> np.ndarray:

@@ -98,6 +98,23 @@ int32_t dgm_mesh_fetch(const dgm_mesh_build* m, int64_t* elem_edges /* [ne][3] *
                        int64_t* internal_elements, int64_t* boundary_elements);
 void dgm_mesh_free(dgm_mesh_build* m);
 
+/* gmsh 4.1 ASCII reader with the reference's line state machine (GmshParser::parse,
+ * mesh_parser.rs:28-158), native.  dgm_gmsh_parse reads the file (NULL with *status set on
+ * failure: DGM_BAD_ARG where the reference's parse panics -- a missing file, a malformed number,
+ * an entity without a physical name); dgm_gmsh_counts gives the number of vertices, boundary line
+ * blocks (dim 1) and triangle blocks (dim 2); dgm_gmsh_vertices copies [n_vertices][2];
+ * dgm_gmsh_block_size gives the pairs (dim 1) or triangles (dim 2) of block i, -1 if none;
+ * dgm_gmsh_block copies its 0-based node ids; dgm_gmsh_block_name gives a line block's physical
+ * name (valid until dgm_gmsh_free). */
+typedef struct dgm_gmsh dgm_gmsh;
+dgm_gmsh* dgm_gmsh_parse(const char* path, int32_t* status);
+int32_t dgm_gmsh_counts(const dgm_gmsh* g, int64_t* n_vertices, int32_t* n_edge_blocks, int32_t* n_elem_blocks);
+int32_t dgm_gmsh_vertices(const dgm_gmsh* g, double* vertex_xy);
+int64_t dgm_gmsh_block_size(const dgm_gmsh* g, int32_t dim, int32_t i);
+const char* dgm_gmsh_block_name(const dgm_gmsh* g, int32_t i);
+int32_t dgm_gmsh_block(const dgm_gmsh* g, int32_t dim, int32_t i, int64_t* node_ids);
+void dgm_gmsh_free(dgm_gmsh* g);
+
 /* Basis and quadrature tables: DubinerBasis (basis_function.rs:6-13) and GaussPoints
  * (gauss_point.rs:4-11).  Supported (order, cell rule, edge rule): (1,3,2), (2,6,3), (3,12,4). */
 typedef struct dgm_tables_desc {

@@ -122,6 +122,37 @@ def test_gmsh_roundtrip_and_reference_parser(tmp_path):
     _check_mesh_equal(Oracle(msh_path=path, order=2, freestream=FS), m)
 
 
+def test_gmsh_reader_line_endings_and_errors(tmp_path):
+    """CRLF line ends and a last line without a newline read the same mesh (BufRead::lines drops
+    one '\\r' before each '\\n'); where the reference's reader panics (no file, an entity without
+    a physical name, a malformed number) DgmError DGM_BAD_ARG is raised."""
+    raw = naca0012_ogrid(12, 6)
+    path = tmp_path / "m.msh"
+    write_gmsh(raw, str(path))
+    txt = path.read_bytes()
+    ref = GmshParser.parse(str(path))
+    for name, data in (("crlf.msh", txt.replace(b"\n", b"\r\n")), ("nonl.msh", txt.rstrip(b"\n"))):
+        (tmp_path / name).write_bytes(data)
+        back = GmshParser.parse(str(tmp_path / name))
+        assert np.array_equal(back.vertices, ref.vertices)
+        assert all(np.array_equal(a.node_pairs, b.node_pairs) for a, b in zip(back.edge_blocks, ref.edge_blocks))
+        assert np.array_equal(back.element_blocks[0], ref.element_blocks[0])
+    lines = txt.decode().split("\n")
+    i = lines.index("$PhysicalNames")
+    bad_name = "\n".join(lines[:i + 2] + lines[i + 3:])          # drop the first physical name
+    j = lines.index("$Nodes")
+    k = next(n for n in range(j + 2, len(lines)) if len(lines[n].split()) == 3)  # first coordinate line
+    bad_num = "\n".join(lines[:k] + ["1.0x " + " ".join(lines[k].split()[1:])] + lines[k + 1:])
+    for name, data in (("noname.msh", bad_name), ("badnum.msh", bad_num)):
+        (tmp_path / name).write_text(data)
+        with pytest.raises(DgmError) as err:
+            GmshParser.parse(str(tmp_path / name))
+        assert err.value.status == 7
+    with pytest.raises(DgmError) as err:
+        GmshParser.parse(str(tmp_path / "missing.msh"))
+    assert err.value.status == 7
+
+
 def test_ogrid_geometry():
     raw = naca0012_ogrid(64, 32)
     m = process_mesh(raw, _fs_q(FS), 1.4)

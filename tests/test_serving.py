@@ -6,6 +6,7 @@ geometric residual decay, no device), so its host logic is covered without a GPU
 run real cohorts through the C ABI.
 """
 import math
+import time
 
 import numpy as np
 import pytest
@@ -18,9 +19,12 @@ from dgm_in_rust_b200.workloads import Instance, instance_mesh, request_stream
 
 class FakeBatch:
     """Stand-in for solver.Batch: instance i's density residual after s steps is 2^-(s-1) times
-    its first one; advance is complete after ``lag`` polls."""
+    its first one; advance is complete after ``lag`` polls (and, for the first batch created, its
+    first advance only after ``hold_first_s`` seconds)."""
     lag = 2
     live = 0
+    created = 0
+    hold_first_s = 0.0
 
     def __init__(self, meshes, order, hcr, cfls, final_times, final_steps, limiter=True, device=0, precision="fp32"):
         self.meshes = meshes
@@ -32,6 +36,9 @@ class FakeBatch:
         self.polls = 0
         self.uploaded = [False] * self.n
         FakeBatch.live += 1
+        FakeBatch.created += 1
+        self.hold = FakeBatch.hold_first_s if FakeBatch.created == 1 else 0.0
+        self.ready_at = 0.0
 
     def set_initial(self, i, init):
         assert init.density > 0 and init.pressure > 0
@@ -42,8 +49,12 @@ class FakeBatch:
         for i in range(self.n):
             self.step[i] = min(self.final[i], self.step[i] + n)
         self.polls = self.lag
+        self.ready_at = time.perf_counter() + self.hold
+        self.hold = 0.0
 
     def query(self):
+        if time.perf_counter() < self.ready_at:
+            return None
         if self.polls > 0:
             self.polls -= 1
             return None
@@ -74,6 +85,7 @@ class FakeBatch:
 @pytest.fixture
 def fake_batch(monkeypatch):
     FakeBatch.live = 0
+    FakeBatch.created = 0
     monkeypatch.setattr(serving, "Batch", FakeBatch)
     yield FakeBatch
     assert FakeBatch.live == 0, "every cohort context is closed"
@@ -107,14 +119,17 @@ def test_retires_at_convergence_or_step_cap(fake_batch):
 
 
 def test_cohorts_are_packed_per_order(fake_batch):
-    # an idle GPU admits the first prepared request at once; the other four arrive within the
-    # window and are packed one cohort per order (three orders among them at most)
-    FakeBatch.lag = 1000                     # the first cohort stays busy while the rest are prepared
+    # an idle GPU admits the first prepared request at once; the other four arrive later, within
+    # one window of each other, and are packed one cohort per order (three orders among them)
+    FakeBatch.hold_first_s = 3.0             # the first cohort stays busy while the rest are prepared
+    reqs = _reqs([(16, 1), (16, 2), (20, 1), (20, 2), (24, 3)])
+    for r in reqs[1:]:
+        r.arrival_s = 0.5 + 0.01 * r.rid     # well after the first, close to one another
     try:
-        loop = ServingLoop(prep="thread", chunk_steps=64, tol=1e-3, max_steps=100, window_s=0.3)
-        res = loop.run(_reqs([(16, 1), (16, 2), (20, 1), (20, 2), (24, 3)]), realtime=False)
+        loop = ServingLoop(prep="thread", chunk_steps=64, tol=1e-3, max_steps=100, window_s=1.0)
+        res = loop.run(reqs, realtime=True)
     finally:
-        FakeBatch.lag = 2
+        FakeBatch.hold_first_s = 0.0
     assert len(res) == 5 and all(r.converged for r in res)
     assert loop.cohorts_formed <= 4
     assert loop.max_concurrent == 5

@@ -204,6 +204,8 @@ def lib() -> ctypes.CDLL:
     L.dgm_gmsh_block.restype = ctypes.c_int32
     L.dgm_gmsh_free.argtypes = [vp]
     L.dgm_gmsh_free.restype = None
+    L.dgm_vtk_write.argtypes = [ctypes.c_char_p, ctypes.c_int64, P_D, ctypes.c_int64, P_I64, P_D]
+    L.dgm_vtk_write.restype = ctypes.c_int32
     for name in ("dgm_compute_residuals", "dgm_apply_limiter", "dgm_compute_time_step", "dgm_rk3",
                  "dgm_time_march", "dgm_get_clock", "dgm_set_clock", "dgm_upload_solutions",
                  "dgm_download_solutions", "dgm_advance", "dgm_synchronize", "dgm_query", "dgm_limiter_stats",

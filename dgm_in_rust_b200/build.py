@@ -9,7 +9,7 @@ import sys
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ROOT = os.path.dirname(_HERE)
 SOURCES = [os.path.join(_HERE, "csrc", "dgm_capi.cu"), os.path.join(_HERE, "csrc", "dgm_noalloc.cu"),
-           os.path.join(_HERE, "csrc", "dgm_mesh.cpp")]
+           os.path.join(_HERE, "csrc", "dgm_mesh.cpp"), os.path.join(_HERE, "csrc", "dgm_output.cpp")]
 DEPS = SOURCES + [os.path.join(_HERE, "csrc", "dgm_device.cuh"), os.path.join(_HERE, "csrc", "dgm_tc.cuh"),
                   os.path.join(_ROOT, "include", "dgm_b200.h")]
 OUT = os.path.join(_HERE, "_lib", "libdgm_b200.so")

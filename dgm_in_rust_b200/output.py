@@ -4,8 +4,8 @@ The reference writes, after the time loop (temporal_disc.rs:56), one legacy ASCI
 ``outputfiles/solutions/step=<current_step>.vtk`` through the vtkio crate: the vertices as points
 (z = 0), the triangles, and three cell attributes computed from each element's mode-0
 coefficients -- Density, Velocity (u, v, 0) and Pressure.  The cell fields come from the device
-(``dgm_cell_fields``, bit-identical to the reference's expressions); this module lays out the
-text exactly as vtkio's legacy writer does (empty title, each data block on one line, one cell
+(``dgm_cell_fields``, bit-identical to the reference's expressions); the library writes the text
+(``dgm_vtk_write``) exactly as vtkio's legacy writer does (empty title, each data block on one line, one cell
 type per line, an empty POINT_DATA block) with numbers in Rust's ``{}`` form for f64 (shortest
 round-trip digits, positional notation, no trailing ".0", ``NaN``/``inf``).
 """
@@ -63,10 +63,19 @@ def solution_path(current_step: int, root: str = "outputfiles/solutions") -> str
 
 def write_to_vtk(path: str, mesh, fields: np.ndarray) -> str:
     """Write the VTK file of ``mesh`` (a processed Mesh: vertices, elem_vertices) with the cell
-    fields [ne, 4]; creates the directory like the reference.  Returns the path."""
+    fields [ne, 4]; creates the directory like the reference.  The text is produced natively by
+    the library (dgm_vtk_write), byte for byte what :func:`vtk_text` lays out.  Returns the path."""
+    from . import _native
+    xy = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+    tris = np.ascontiguousarray(mesh.elem_vertices, dtype=np.int64)
+    f = np.ascontiguousarray(fields, dtype=np.float64)
+    if f.shape != (tris.shape[0], 4):
+        raise ValueError("fields must be [n_elements, 4]")
     d = os.path.dirname(path)
     if d:
         os.makedirs(d, exist_ok=True)
-    with open(path, "w") as f:
-        f.write(vtk_text(np.asarray(mesh.vertices), np.asarray(mesh.elem_vertices), np.asarray(fields)))
+    st = _native.lib().dgm_vtk_write(str(path).encode(), xy.shape[0], _native.dptr(xy), tris.shape[0],
+                                     _native.iptr(tris), _native.dptr(f))
+    if st != 0:
+        raise _native.DgmError(st, what=f"write_to_vtk({path})")
     return path

@@ -115,6 +115,15 @@ const char* dgm_gmsh_block_name(const dgm_gmsh* g, int32_t i);
 int32_t dgm_gmsh_block(const dgm_gmsh* g, int32_t dim, int32_t i, int64_t* node_ids);
 void dgm_gmsh_free(dgm_gmsh* g);
 
+/* write_to_vtk (write_results.rs:8-93), native, on the host: the legacy ASCII VTK file the
+ * reference writes through vtkio (points with z = 0, triangles, cell data Density, Velocity
+ * (u, v, 0), Pressure), numbers as Rust prints an f64 with {}.  fields is [n_elements][4] =
+ * density, x velocity, y velocity, pressure (dgm_cell_fields gives them from the device state).
+ * The directory must exist.  DGM_BAD_ARG when the file cannot be written. */
+int32_t dgm_vtk_write(const char* path, int64_t n_vertices, const double* vertex_xy /* [n_vertices][2] */,
+                      int64_t n_elements, const int64_t* elem_vertices /* [n_elements][3] */,
+                      const double* fields /* [n_elements][4] */);
+
 /* Basis and quadrature tables: DubinerBasis (basis_function.rs:6-13) and GaussPoints
  * (gauss_point.rs:4-11).  Supported (order, cell rule, edge rule): (1,3,2), (2,6,3), (3,12,4). */
 typedef struct dgm_tables_desc {

@@ -79,3 +79,18 @@ def test_device_cell_fields_match_reference_expressions(built, tmp_path, precisi
     k = lines.index("SCALARS Density double 1")
     assert np.array_equal(np.array([float(x) for x in lines[k + 2].split()]), rho)
     s.close()
+
+
+def test_native_writer_matches_layout_bytes(tmp_path):
+    """The library's writer (dgm_vtk_write) produces exactly the text vtk_text lays out, for
+    magnitudes from 1e-30 to 1e30 and the special values Rust prints as NaN, inf, -inf, -0."""
+    from dgm_in_rust_b200 import freestream_quantity, naca0012_ogrid, process_mesh
+    from dgm_in_rust_b200.output import vtk_text, write_to_vtk
+    rng = np.random.default_rng(1)
+    m = process_mesh(naca0012_ogrid(32, 16), freestream_quantity(0.8, 1.25, 1.0, 1 / 1.4, 1.4), 1.4)
+    f = rng.standard_normal((m.n_elements, 4)) * 10.0 ** rng.integers(-30, 30, (m.n_elements, 4))
+    specials = [np.nan, np.inf, -np.inf, -0.0, 0.0, 5e-324, 1.7976931348623157e308, 1.0, 0.1, 2.5e20, 1e-7]
+    f.reshape(-1)[:len(specials)] = specials
+    path = write_to_vtk(str(tmp_path / "solutions" / "step=3.vtk"), m, f)
+    with open(path) as fh:
+        assert fh.read() == vtk_text(m.vertices, m.elem_vertices, f)

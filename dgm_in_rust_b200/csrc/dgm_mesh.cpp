@@ -15,6 +15,7 @@
 //   * geometry with the reference's expressions in its operation order (no contraction into
 //     fused multiply-adds; the library is compiled with -ffp-contract=off), so the arrays are bit
 //     for bit those of the reference's f64 code.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -290,7 +291,7 @@ int parse_gmsh(const char* path, GmshData& g) {
         break;
       case FirstNodes:
         if (tok.size() < 2 || !parse_usize(tok[1], a)) return DGM_BAD_ARG;
-        g.xy.reserve((size_t)(2 * std::min<int64_t>(a, (int64_t)1 << 32)));
+        g.xy.reserve((size_t)(2 * std::min<int64_t>(a, (int64_t)1 << 24)));  // a hint only
         st = Nodes;
         break;
       case Nodes:
@@ -312,12 +313,12 @@ int parse_gmsh(const char* path, GmshData& g) {
         if (dim == 1) {
           g.edge_names.push_back(in->second);
           g.edge_pairs.emplace_back();
-          g.edge_pairs.back().reserve((size_t)(2 * std::min<int64_t>(num, (int64_t)1 << 30)));
+          g.edge_pairs.back().reserve((size_t)(2 * std::min<int64_t>(num, (int64_t)1 << 24)));
           st = EdgeBlock;
         }
         if (dim == 2) {
           g.elem_nodes.emplace_back();
-          g.elem_nodes.back().reserve((size_t)(3 * std::min<int64_t>(num, (int64_t)1 << 30)));
+          g.elem_nodes.back().reserve((size_t)(3 * std::min<int64_t>(num, (int64_t)1 << 24)));
           st = ElemBlock;
         }
         line_count = 0;

@@ -122,6 +122,22 @@ def test_gmsh_roundtrip_and_reference_parser(tmp_path):
     _check_mesh_equal(Oracle(msh_path=path, order=2, freestream=FS), m)
 
 
+def test_gmsh_roundtrip_airfoil_blocks(tmp_path):
+    """The reference's airfoil mesh (seven boundary line blocks, three "Wall" and four "Farfield")
+    written as gmsh 4.1 and read back by the native reader: same vertices, blocks, names, triangles,
+    and the same processed mesh as the oracle's own parser and process_mesh give for that file."""
+    raw = airfoil_raw()
+    path = str(tmp_path / "airfoil_rt.msh")
+    write_gmsh(raw, path)
+    back = GmshParser.parse(path)
+    assert np.array_equal(back.vertices, raw.vertices)
+    assert [b.physical_name for b in back.edge_blocks] == [b.physical_name for b in raw.edge_blocks]
+    assert all(np.array_equal(a.node_pairs, b.node_pairs) for a, b in zip(back.edge_blocks, raw.edge_blocks))
+    assert np.array_equal(back.element_blocks[0], raw.element_blocks[0])
+    fs = (1.5, 0.8, 1.0, 100000.0)
+    _check_mesh_equal(Oracle(msh_path=path, order=2, freestream=fs), process_mesh(back, _fs_q(fs), 1.4))
+
+
 def test_gmsh_reader_line_endings_and_errors(tmp_path):
     """CRLF line ends and a last line without a newline read the same mesh (BufRead::lines drops
     one '\\r' before each '\\n'); where the reference's reader panics (no file, an entity without

@@ -167,13 +167,15 @@ class ServingLoop:
     elements to keep the GPU's launches full run at once; later arrivals wait in arrival order
     instead of sharing the GPU with everything admitted before them, so early requests finish
     early (first come, first served at the granularity of the cap).  ``prep`` selects worker
-    processes ("process", started with spawn before the clock starts, like a server's standing
-    pool) or threads ("thread") for mesh preparation."""
+    threads ("thread", the default: the mesh is built by the library's native code, which runs
+    outside the interpreter lock, and nothing is copied back) or worker processes ("process",
+    started with spawn before the clock starts, like a server's standing pool; each prepared mesh
+    is pickled back to the serving process) for mesh preparation."""
 
     def __init__(self, hbm_budget_bytes: int = 40 << 30, device: int = 0, precision: str = "fp32",
                  chunk_steps: int = 32, tol: float = 1e-6, max_steps: int = 5000, window_s: float = 0.002,
                  max_cohort_elements: int = 4 << 20, max_active_elements: int = 2 << 20, prep_workers: int = 4,
-                 prep: str = "process", keep_states: bool = False):
+                 prep: str = "thread", keep_states: bool = False):
         if chunk_steps < 1 or max_steps < 1:
             raise ValueError("chunk_steps and max_steps must be positive")
         self.budget = int(hbm_budget_bytes)

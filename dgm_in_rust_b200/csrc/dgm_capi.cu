@@ -494,7 +494,6 @@ int set_active(dgm_ctx* c, double dt, bool set_dt) {
   return DGM_OK;
 }
 
-// Host state ([element][variable][basis], FP64) of instance i -> device SoA array dst.
 // Host state ([element][variable][basis], FP64) of instance i -> device state array dst: the
 // device layout is the same element-major order, so an FP64 state is one copy; an FP32 state goes
 // through the FP64 staging buffer and a conversion.

@@ -1,7 +1,11 @@
 """Regenerate the golden fixtures in this folder.
 
-  python tests/golden/make_golden.py
+  python tests/golden/make_golden.py <DGM_in_rust checkout>
 
+* reference_airfoil.msh.gz, reference_mesh.vtk.gz -- the reference's own input fixture
+  (inputfiles/airfoil.msh) and its own output file (outputfiles/mesh.vtk, written by its
+  write_to_vtk), copied gzipped: the VTK bytes pin the gmsh reader, the element/vertex order and
+  the writer to an output the reference produced.
 * airfoil_mesh.npz -- the reference's own mesh fixture (inputfiles/airfoil.msh of
   DGM_in_rust: 1961 nodes, 3738 triangles, Wall/Farfield lines), parsed with the package's
   GmshParser and checked against the oracle's parser; stored as arrays so the tests do not need
@@ -15,6 +19,7 @@
 
 The oracle is the C++ restatement under oracle/ (parity with the Rust reference unpinned).
 """
+import gzip
 import os
 import sys
 
@@ -27,7 +32,7 @@ sys.path.insert(0, ROOT)
 from dgm_in_rust_b200 import GmshParser, naca0012_ogrid  # noqa: E402
 from oracle.oracle import Oracle  # noqa: E402
 
-AIRFOIL = "/root/reference/inputfiles/airfoil.msh"
+AIRFOIL = None  # <checkout>/inputfiles/airfoil.msh, set from the command line
 REF_FS = (1.5, 0.8, 1.0, 100000.0)  # aoa, mach, rho, p of freestream.json / initial_solution.json
 
 
@@ -79,6 +84,19 @@ def ogrid():
     print("ogrid16x8: troubled", n, "t3", t)
 
 
+def reference_files(checkout):
+    for src, dst in (("inputfiles/airfoil.msh", "reference_airfoil.msh.gz"),
+                     ("outputfiles/mesh.vtk", "reference_mesh.vtk.gz")):
+        with open(os.path.join(checkout, src), "rb") as f:
+            data = f.read()
+        with open(os.path.join(HERE, dst), "wb") as f:
+            f.write(gzip.compress(data, compresslevel=9, mtime=0))
+
+
 if __name__ == "__main__":
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_golden.py <path of a DGM_in_rust checkout>")
+    AIRFOIL = os.path.join(sys.argv[1], "inputfiles", "airfoil.msh")
+    reference_files(sys.argv[1])
     airfoil()
     ogrid()

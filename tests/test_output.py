@@ -94,3 +94,49 @@ def test_native_writer_matches_layout_bytes(tmp_path):
     path = write_to_vtk(str(tmp_path / "solutions" / "step=3.vtk"), m, f)
     with open(path) as fh:
         assert fh.read() == vtk_text(m.vertices, m.elem_vertices, f)
+
+
+def _reference_airfoil_path(tmp_path):
+    """The reference's own input fixture (inputfiles/airfoil.msh), unpacked from tests/golden."""
+    import gzip
+    from conftest import GOLDEN
+    path = tmp_path / "airfoil.msh"
+    path.write_bytes(gzip.open(os.path.join(GOLDEN, "reference_airfoil.msh.gz")).read())
+    return str(path)
+
+
+def test_reference_output_file_reproduced_byte_for_byte(tmp_path):
+    """Pinned to an output the reference itself produced: outputfiles/mesh.vtk of DGM_in_rust, the
+    VTK file its write_to_vtk (src/io/write_results.rs:8-93) wrote for inputfiles/airfoil.msh
+    with NaN cell fields.  The reference's airfoil.msh goes through the native gmsh reader
+    (mesh_parser.rs:28-158) and process_mesh; the file written by the native writer and the text of
+    the layout restatement both equal the reference's file byte for byte (209,182 bytes: vertex
+    order and coordinates, triangle order, Rust's f64 formatting of every number and of NaN)."""
+    import gzip
+    from conftest import GOLDEN
+    from dgm_in_rust_b200 import GmshParser
+    ref = gzip.open(os.path.join(GOLDEN, "reference_mesh.vtk.gz")).read()
+    raw = GmshParser.parse(_reference_airfoil_path(tmp_path))
+    mesh = process_mesh(raw, freestream_quantity(0.8, 1.5, 1.0, 1e5, 1.4), 1.4)
+    fields = np.full((mesh.n_elements, 4), np.nan)
+    path = write_to_vtk(str(tmp_path / "solutions" / "mesh.vtk"), mesh, fields)
+    with open(path, "rb") as fh:
+        native = fh.read()
+    assert len(native) == len(ref) == 209182
+    assert native == ref
+    assert vtk_text(mesh.vertices, mesh.elem_vertices, fields).encode() == ref
+
+
+def test_airfoil_fixture_arrays_match_reference_file(tmp_path):
+    """The stored arrays of the reference's airfoil mesh (airfoil_mesh.npz, used by the parity
+    tests) are what the native reader gives for the reference's airfoil.msh."""
+    from dgm_in_rust_b200 import GmshParser
+    raw = GmshParser.parse(_reference_airfoil_path(tmp_path))
+    stored = airfoil_raw()
+    assert np.array_equal(raw.vertices, stored.vertices)
+    assert [b.physical_name for b in raw.edge_blocks] == [b.physical_name for b in stored.edge_blocks]
+    for a, b in zip(raw.edge_blocks, stored.edge_blocks):
+        assert np.array_equal(a.node_pairs, b.node_pairs)
+    assert len(raw.element_blocks) == len(stored.element_blocks)
+    for a, b in zip(raw.element_blocks, stored.element_blocks):
+        assert np.array_equal(a, b)

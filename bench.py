@@ -38,6 +38,11 @@ RHO_INF, P_INF = 1.0, 1.0 / 1.4
 WORKLOAD = ("naca0012_ogrid_256x128_p2: 65,536 triangles, 6 modes, M=0.8, AoA=1.25deg, "
             "HLLC, WENO/KXRCF limiter on, SSP-RK3 CFL=0.1, FP64")
 METRIC = "DOF-stage updates/s"
+# the workload as both arms report it (identical dicts: the reference arm and the GPU arm)
+CONFIG = {"workload": WORKLOAD, "elements": 2 * NI * NJ, "order": ORDER, "dof_stage_per_step": 3 * 2 * NI * NJ * 4 * 6,
+          "l2": "GPU arm: flushed (256 MiB write) before every timed step, per-step CUDA events; "
+                "reference arm: host caches as they are",
+          "parallelism": "one device per rank (replicas); the reference arm: host threads of rank 0"}
 
 
 def parse():
@@ -118,27 +123,45 @@ def time_cpu(raw, steps, warmup, threads, budget_s=None):
     return dofs_per_step(o.ne, o.nb) * done / el, done, el
 
 
+def mapped_libraries():
+    """Shared libraries of this repository mapped into the process (from /proc/self/maps), as
+    paths relative to the repository: evidence of which native code a run used."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and path.startswith(ROOT + os.sep):
+                    out.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
 def run_reference(args):
+    """The reference's CPU algorithm on the host cores, on the same workload, steps and warm-up as
+    the GPU arm.  The mesh is generated by the pure-numpy O-grid generator and processed by the
+    oracle itself (process_mesh restated), so this arm maps no library of the product."""
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
-    raw, _ = make_mesh()
+    from dgm_in_rust_b200.mesh import naca0012_ogrid
+    raw = naca0012_ogrid(NI, NJ)
     threads = cpu_threads()
-    # each step is a full RK3 step of the workload; cap the count so the run stays within minutes
-    steps = min(args.steps, 200)
-    warm = min(args.warmup, 3)
-    value, done, el = time_cpu(raw, steps, warm, threads, budget_s=150.0)
+    value, done, el = time_cpu(raw, args.steps, args.warmup, threads, budget_s=240.0)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": args.gpus,
-        "steps": done, "warmup": warm, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+        "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "elements": NI * NJ * 2, "parallelism": "host threads"},
+        "config": dict(CONFIG),
+        "execution": f"{threads} host threads",
         "cpu_baseline": {"value": value, "unit": "DOF-stage/s", "cores": threads, "kind": "port",
-                         "sample": f"{done} full RK3 steps of the workload after {warm} warm-up steps; C++ "
+                         "sample": f"{done} full RK3 steps of the workload after {args.warmup} warm-up steps; C++ "
                                    "restatement of the reference CPU algorithm (Rust reference not buildable "
                                    "here), OpenMP over volume/edge/boundary passes, serial limiter and dt"},
         "e2e": {"value": value, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    line["libraries_loaded"] = mapped_libraries()
     print(json.dumps(line), flush=True)
     return 0
 
@@ -531,13 +554,14 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # warm-up (also instantiates the step graphs); the launch configuration is tuned on the
-    # developed state (the free-stream start has no troubled cells), then the graphs, which
-    # tuning resets, are rebuilt by three more warm-up steps
-    td.advance(args.warmup)
+    # W warm-up steps in all: the first max(1, W - 3) develop the state (the free-stream start
+    # has no troubled cells) and instantiate the step graphs, the launch configuration is tuned on
+    # that state, and the remaining steps rebuild the graphs, which tuning resets
+    first = max(1, args.warmup - 3)
+    td.advance(first)
     td.synchronize()
     tuned = sd.autotune(repeats=20)
-    td.advance(3)
+    td.advance(max(args.warmup - first, 0))
     td.synchronize()
     # timed region: K steps, L2 flushed before each step, each step bracketed by events
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -632,12 +656,11 @@ def run_ours(args):
     value = world * dps * args.steps / (ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup + 3, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "elements": ne, "order": ORDER, "dof_stage_per_step": dps,
-                   "l2": "flushed (256 MiB write) before every timed step; per-step CUDA events",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "launch": tuned},
+        "config": dict(CONFIG),
+        "execution": f"replicas x{world}" if world > 1 else "single GPU",
+        "launch": tuned,
         "value_l2_resident": world * dps * args.steps / (ms_resident * 1e-3),
         "e2e": {"value": world * dps * args.steps / e2e_s, "unit": "DOF-stage/s",
                 "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": 2 * state_bytes,
@@ -664,6 +687,7 @@ def run_ours(args):
                                 "sample": f"{done} full RK3 steps ({el:.1f} s) of the workload after 1 warm-up "
                                           "step; C++ restatement of the reference CPU algorithm"}
     if rank == 0:
+        line["libraries_loaded"] = mapped_libraries()
         print(json.dumps(line), flush=True)
     solver.close()
     if dist is not None:

@@ -16,6 +16,13 @@
   computed by the oracle.
 * ogrid16x8.npz -- a 16 x 8 O-grid (p = 2): initial state, its residual, a seeded perturbed
   state with its residual and limited state, and 3 time-march steps.
+* c2_run.npz -- the transonic limiter configuration (256 x 128 O-grid, 65,536 triangles, p = 2,
+  M 0.8, AoA 1.25 deg, free-stream start, CFL 0.1, limiter on) marched by the oracle for its
+  configured 2000 steps, with checkpoints after 200 and 2000 steps: clock, per-(variable, mode)
+  sums and sums of squares over all elements, and the full records of a sample of elements (every
+  128th element and every boundary element).  About 15 minutes on 8 host threads.
+
+  python tests/golden/make_golden.py --c2-run
 
 The oracle is the C++ restatement under oracle/ (parity with the Rust reference unpinned).
 """
@@ -84,6 +91,40 @@ def ogrid():
     print("ogrid16x8: troubled", n, "t3", t)
 
 
+C2_CHECKPOINTS = (200, 2000)
+
+
+def c2_sample(ne, boundary_elements):
+    return np.union1d(np.arange(0, ne, 128), boundary_elements).astype(np.int64)
+
+
+def c2_run(threads=8):
+    from dgm_in_rust_b200 import freestream_quantity, process_mesh
+    raw = naca0012_ogrid(256, 128)
+    fs = (1.25, 0.8, 1.0, 1.0 / 1.4)
+    mesh = process_mesh(raw, freestream_quantity(fs[1], fs[0], fs[2], fs[3], 1.4), 1.4)
+    o = Oracle(raw=raw, order=2, ncell_gp=6, nedge_gp=3, cfl=0.1, final_time=1.0e30, final_step=0,
+               limiter=True, threads=threads, freestream=fs)
+    U = o.initial_solution()
+    R = o.new_state()
+    sample = c2_sample(o.ne, mesh.boundary_element_indices)
+    out = {"sample": sample}
+    done, t = 0, 0.0
+    for n in C2_CHECKPOINTS:
+        while done < n:
+            dt = o.compute_time_step(U)
+            o.rk3(R, U, dt)
+            t += dt
+            done += 1
+        out[f"t{n}"] = np.array(t)
+        out[f"sum{n}"] = U.sum(axis=0)
+        out[f"sumsq{n}"] = (U * U).sum(axis=0)
+        out[f"U{n}"] = U[sample]
+        out[f"troubled{n}"] = np.array(int(o.troubled_flags(U).sum()))
+        print(f"c2: {n} steps, t = {t}", flush=True)
+    np.savez_compressed(os.path.join(HERE, "c2_run.npz"), **out)
+
+
 def reference_files(checkout):
     for src, dst in (("inputfiles/airfoil.msh", "reference_airfoil.msh.gz"),
                      ("outputfiles/mesh.vtk", "reference_mesh.vtk.gz")):
@@ -94,8 +135,11 @@ def reference_files(checkout):
 
 
 if __name__ == "__main__":
+    if len(sys.argv) == 2 and sys.argv[1] == "--c2-run":
+        c2_run()
+        raise SystemExit(0)
     if len(sys.argv) != 2:
-        raise SystemExit("usage: make_golden.py <path of a DGM_in_rust checkout>")
+        raise SystemExit("usage: make_golden.py <path of a DGM_in_rust checkout> | --c2-run")
     AIRFOIL = os.path.join(sys.argv[1], "inputfiles", "airfoil.msh")
     reference_files(sys.argv[1])
     airfoil()

@@ -27,8 +27,16 @@ def test_reference_arm_prints_one_contract_line():
     assert KEYS <= set(d)
     assert d["impl"] == "reference" and d["metric"] == "DOF-stage updates/s" and d["unit"] == "DOF-stage/s"
     assert d["value"] > 0 and d["higher_is_better"] is True and d["n_gpus"] == 1
-    assert d["steps"] >= 1 and d["warmup"] >= 3 and d["ms_per_step"] > 0
+    assert d["steps"] == 1 and d["warmup"] == 3 and d["ms_per_step"] > 0
     assert d["config"]["workload"].startswith("naca0012_ogrid_256x128_p2")
+    # the same config dict as the GPU arm prints
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == json.loads(json.dumps(bench.CONFIG))
+    # the reference arm maps the oracle only, never the product library
+    libs = d["libraries_loaded"]
+    assert "oracle/_build/liboracle.so" in libs
+    assert not any("libdgm_b200" in x for x in libs), libs
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
     e2e = d["e2e"]

@@ -23,24 +23,38 @@ constexpr int kMaxPartials = 4096;                                            //
 constexpr long long kMaxElements = (long long)kMaxPartials * kElementsPerBlock;  // 8,388,608
 constexpr int kMaxDevices = 64;
 
-// One partial minimum per block, as the IEEE bit pattern of a non-negative double (such bit
-// patterns order like the doubles).  In host code this name is only a host-side stand-in for the
-// device array: its device address comes from cudaGetSymbolAddress below.
+// One partial minimum per block, as an order key of the double (see order_key).  In host code
+// this name is only a host-side stand-in for the device array: its device address comes from
+// cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned long long g_time_step_partials[kMaxPartials];
 
 std::mutex g_mutex;
 unsigned long long* g_partials_addr[kMaxDevices] = {};
 
+// An unsigned key that orders like the double it encodes, for every finite or infinite value of
+// either sign: the sign bit flipped for non-negative values, all bits flipped for negative ones.
+// The minimum of the keys is the key of the minimum, so a time step that comes out negative (a
+// negative minimum height) still wins the comparison the way the reference's `dt < time_step` does.
+__device__ __forceinline__ unsigned long long order_key(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__device__ __forceinline__ double key_value(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
 // TemperalDisc::compute_time_step (src/temporal_disc.rs:58-88) over the caller's state in the
 // reference layout [element][variable][basis]: per element dt = cfl * h_min / (|u| + c) with the
 // state taken as the sum of the modal coefficients; the block's minimum of the values below the
-// reference's start value 1e10 goes to partials[blockIdx.x] (+inf if none).
+// reference's start value 1e10 goes to partials[blockIdx.x] (the key of +inf if none).
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_time_step_partials(const double* __restrict__ U,
                                                                  const double* __restrict__ hmin,
                                                                  long long ne, double cfl, double hcr,
                                                                  unsigned long long* __restrict__ partials) {
-  unsigned long long best = 0x7ff0000000000000ull;
+  unsigned long long best = 0xfff0000000000000ull;  // order_key(+inf)
   const long long first = (long long)blockIdx.x * kElementsPerBlock;
 #pragma unroll
   for (int k = 0; k < kPerThread; ++k) {
@@ -63,8 +77,8 @@ __global__ void __launch_bounds__(kThreads) k_time_step_partials(const double* _
     const double speed = sqrt(vx * vx + vy * vy) + c;
     const double dt = cfl * hmin[e] / speed;
     if (dt < 1.0e10) {  // NaN never passes, like the reference's `if dt < time_step`
-      const unsigned long long bits = (unsigned long long)__double_as_longlong(dt);
-      best = bits < best ? bits : best;
+      const unsigned long long key = order_key(dt);
+      best = key < best ? key : best;
     }
   }
 #pragma unroll
@@ -84,7 +98,7 @@ __global__ void __launch_bounds__(kThreads) k_time_step_partials(const double* _
 // Minimum over the partials, starting from the reference's 1e10 (temporal_disc.rs:61).
 __global__ void __launch_bounds__(kThreads) k_time_step_final(const unsigned long long* __restrict__ partials,
                                                               int nparts, double* __restrict__ out) {
-  unsigned long long best = (unsigned long long)__double_as_longlong(1.0e10);
+  unsigned long long best = order_key(1.0e10);
   for (int i = threadIdx.x; i < nparts; i += kThreads) best = partials[i] < best ? partials[i] : best;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -96,11 +110,14 @@ __global__ void __launch_bounds__(kThreads) k_time_step_final(const unsigned lon
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int i = 0; i < kThreads / 32; ++i) best = s_min[i] < best ? s_min[i] : best;
-    out[0] = __longlong_as_double((long long)best);
+    out[0] = key_value(best);
   }
 }
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array on the current device, looked up once per device and kept
+// for the life of the process.  cudaDeviceReset destroys the context that holds the array, so the
+// kept address is stale after it: this entry point must not be called after a cudaDeviceReset of
+// a device it has already run on.
 int scratch_address(unsigned long long** addr) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -137,12 +154,24 @@ extern "C" int32_t dgm_compute_time_step_noalloc(const double* solutions, const 
                                                  double* time_step, void* stream) {
   if (!solutions || !minimum_height || !time_step || n_elements <= 0) return DGM_BAD_ARG;
   if (n_basis != 3 && n_basis != 6 && n_basis != 10) return DGM_BAD_ARG;
+  if (!(cfl > 0.0) || !(hcr > 1.0)) {  // NaN fails both tests
+    std::fprintf(stderr, "dgm_compute_time_step_noalloc: cfl must be > 0 and hcr > 1 (got %g, %g)\n", cfl, hcr);
+    return DGM_BAD_ARG;
+  }
   if (n_elements > kMaxElements) {
     std::fprintf(stderr,
                  "dgm_compute_time_step_noalloc: %lld elements exceed the fixed scratch capacity of %lld "
                  "elements (%d partial minima of %lld elements each)\n",
                  (long long)n_elements, kMaxElements, kMaxPartials, kElementsPerBlock);
     return DGM_BAD_ARG;
+  }
+  // a runtime error left pending by earlier work of the caller would otherwise be read back below
+  // as this call's launch failure: report it without launching and leave it pending
+  const cudaError_t prior = cudaPeekAtLastError();
+  if (prior != cudaSuccess) {
+    std::fprintf(stderr, "dgm_compute_time_step_noalloc: an earlier CUDA error is pending: %s\n",
+                 cudaGetErrorString(prior));
+    return DGM_CUDA_ERROR;
   }
   unsigned long long* partials = nullptr;
   int st = scratch_address(&partials);

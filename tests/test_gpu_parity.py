@@ -163,6 +163,59 @@ def test_time_march_c2_full_mesh():
     s.close()
 
 
+def test_transonic_configuration_2000_steps_golden():
+    """The transonic limiter configuration (256 x 128 O-grid, 65,536 triangles, p = 2, M 0.8,
+    AoA 1.25 deg, CFL 0.1, limiter on) for its configured 2000 steps against the oracle's run
+    stored in tests/golden/c2_run.npz: after 200 and after 2000 steps, the clock, the sums and sums
+    of squares of every (variable, mode) coefficient over all elements, and the full records of a
+    sample of elements (every 128th and every boundary element) at 1e-10 relative L2."""
+    z = np.load(os.path.join(GOLDEN, "c2_run.npz"))
+    mesh = process_mesh(naca0012_ogrid(256, 128), freestream_quantity(FS[1], FS[0], FS[2], FS[3], 1.4), 1.4)
+    s = build_solver(mesh, 2, 1.4, 0.1, 1.0e30, 10 ** 9)
+    td, sd = s.temporal_disc, s.spatial_disc
+    U0 = initial_state(mesh, s.basis, s.gauss_points, 1.4, InitialSolution(FS[2], FS[0], FS[1], FS[3]))
+    td.upload(U0)
+    sample = z["sample"]
+    done = 0
+    for n in (200, 2000):
+        td.advance(n - done)
+        td.synchronize()
+        done = n
+        assert td.current_step == n
+        t_ref = float(z[f"t{n}"])
+        assert abs(td.current_time - t_ref) <= 1e-13 * t_ref
+        U = sd.new_state()
+        td.download(U)
+        assert rel_l2(U[sample], z[f"U{n}"]) < TOL_STATE, n
+        assert rel_l2(U.sum(axis=0), z[f"sum{n}"]) < TOL_STATE, n
+        assert rel_l2((U * U).sum(axis=0), z[f"sumsq{n}"]) < TOL_STATE, n
+    s.close()
+
+
+def test_c3_full_mesh_fp64_residual_and_steps():
+    """The precision configuration's grid at full size (1024 x 512 O-grid, 1,048,576 triangles,
+    p = 3, M 0.7, AoA 2 deg) in FP64: one residual of a perturbed state, then 2 RK3 steps of the
+    time march from the free stream, against the oracle (p = 3 is an extension of the reference,
+    checked against the oracle's identical extension)."""
+    fs = (2.0, 0.7, 1.0, 1.0 / 1.4)
+    s, o, U0 = pair(naca0012_ogrid(1024, 512), order=3, fs=fs, final_step=2, threads=os.cpu_count() or 8)
+    U = perturbed(U0, 0.02, 3)
+    Ro, Rg = o.new_state(), s.spatial_disc.new_state()
+    o.compute_residuals(Ro, U)
+    s.spatial_disc.compute_residuals(Rg, U.copy())
+    assert rel_l2(Rg, Ro) < TOL_RES
+    del U, Ro, Rg
+    Uo, Ro = U0.copy(), o.new_state()
+    to, so = o.time_march(Ro, Uo)
+    Ug, Rg = U0.copy(), s.spatial_disc.new_state()
+    s.temporal_disc.time_march(s.spatial_disc, Rg, Ug)
+    assert so == s.temporal_disc.current_step == 2
+    assert abs(s.temporal_disc.current_time - to) <= 1e-13 * to
+    assert rel_l2(Ug, Uo) < TOL_STATE
+    s.close()
+    o.close()
+
+
 def test_airfoil_reference_run_golden():
     """The reference's configured run (its JSON inputs) on its airfoil.msh, 20 steps."""
     z = np.load(os.path.join(GOLDEN, "airfoil_run.npz"))

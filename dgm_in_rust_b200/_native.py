@@ -10,7 +10,7 @@ import os
 
 import numpy as np
 
-__all__ = ["DgmError", "lib", "library_path", "MeshDesc", "TablesDesc", "Params", "STATUS"]
+__all__ = ["DgmError", "lib", "library_path", "MeshDesc", "TablesDesc", "Params", "SlotCapacity", "STATUS"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_NAME = "libdgm_b200.so"
@@ -100,6 +100,15 @@ class TablesDesc(ctypes.Structure):
     ]
 
 
+class SlotCapacity(ctypes.Structure):
+    _fields_ = [
+        ("elements", ctypes.c_int64),
+        ("internal_edges", ctypes.c_int64),
+        ("boundary_edges", ctypes.c_int64),
+        ("patches", ctypes.c_int64),
+    ]
+
+
 class Params(ctypes.Structure):
     _fields_ = [
         ("hcr", ctypes.c_double),
@@ -145,6 +154,11 @@ def lib() -> ctypes.CDLL:
                                    ctypes.POINTER(Params), P_I32]
     L.dgm_create_batch.restype = vp
     L.dgm_instance_count.argtypes = [vp]
+    L.dgm_create_batch_slots.argtypes = [ctypes.c_int32, ctypes.POINTER(MeshDesc), ctypes.POINTER(SlotCapacity),
+                                         ctypes.POINTER(TablesDesc), ctypes.POINTER(Params), P_I32]
+    L.dgm_create_batch_slots.restype = vp
+    L.dgm_instance_replace.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MeshDesc), ctypes.POINTER(Params)]
+    L.dgm_instance_capacity.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(SlotCapacity)]
     L.dgm_instance_upload.argtypes = [vp, ctypes.c_int32, P_D]
     L.dgm_instance_download.argtypes = [vp, ctypes.c_int32, P_D]
     L.dgm_instance_download_residual.argtypes = [vp, ctypes.c_int32, P_D]
@@ -215,7 +229,8 @@ def lib() -> ctypes.CDLL:
                  "dgm_advance_with_residual", "dgm_diagnostics", "dgm_precision", "dgm_set_initial_solution",
                  "dgm_instance_set_initial", "dgm_set_launch_config", "dgm_get_launch_config", "dgm_autotune",
                  "dgm_set_limiter_variant", "dgm_get_limiter_variant", "dgm_set_limiter_schedule",
-                 "dgm_get_limiter_schedule", "dgm_cell_fields", "dgm_set_edge_variant", "dgm_get_edge_variant"):
+                 "dgm_get_limiter_schedule", "dgm_cell_fields", "dgm_set_edge_variant", "dgm_get_edge_variant",
+                 "dgm_instance_replace", "dgm_instance_capacity"):
         getattr(L, name).restype = ctypes.c_int32
     _lib = L
     return L

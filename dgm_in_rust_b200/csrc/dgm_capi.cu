@@ -26,8 +26,11 @@ using dgm::MeshDev;
 using dgm::NEQ;
 
 struct HostInst {
-  int64_t elem_off = 0, ne = 0;         // element range in the union mesh
+  int64_t elem_off = 0, ne = 0;         // element range in the union mesh (the mesh's elements)
   int64_t bslot_off = 0, nb_slots = 0;  // boundary-slot range (relative to n_int)
+  // capacity ranges (dgm_create_batch_slots): elements [elem_off, elem_off + elem_cap), internal
+  // slots [int_off, int_off + int_cap), boundary slots [n_int + bnd_off, + bnd_cap), patches
+  int64_t elem_cap = 0, int_off = 0, int_cap = 0, bnd_off = 0, bnd_cap = 0, patch_off = 0, patch_cap = 0;
   double cfl = 0.0, final_time = 0.0;
   int64_t final_step = 0;
   double t = 0.0;
@@ -57,15 +60,21 @@ struct dgm_ctx {
   unsigned char* t0 = nullptr;
   unsigned int* status = nullptr;
   int* work = nullptr;
-  int* d_elem_off = nullptr;
-  int* d_bslot_off = nullptr;
+  int* wl1 = nullptr;    // limiter: cells the detection enlists for wave 1
+  int* pend = nullptr;   // limiter: elements the detection leaves for later waves
+  int* order = nullptr;  // limiter: the detection's visiting order (breadth-first over the elements)
+  int* d_elem_rng = nullptr;   // [2 n] first element, element count of each instance's mesh
+  int* d_bslot_rng = nullptr;  // [2 n] first boundary slot (relative to n_int), boundary slot count
+  bool padded = false;         // capacity ranges above the meshes' sizes: dead instance and null element
+  int dead_inst = 0;           // index of the dead instance (padded contexts)
+  int64_t null_elem = -1;      // the null element (padded contexts)
   double* d_diag = nullptr;
   double* gram = nullptr;   // WENO Gram matrices, [NB (NB + 1) / 2][ld] (limiter on)
   Control* ctl = nullptr;
   InstCtl* ic = nullptr;
   std::vector<void*> allocs;
   int64_t bytes = 0;
-  int coop_blocks[2][2] = {{1, 1}, {1, 1}};  // co-resident limiter blocks [detector][schedule]
+  int coop_blocks[2] = {1, 1};   // co-resident blocks of the limiter's wave kernel [schedule]
   int lim_staged = 0;            // limiter detector variant (dgm_set_limiter_variant / autotune)
   int lim_queue = 0;             // limiter schedule (dgm_set_limiter_schedule / autotune)
   int edge_pair = 0;             // edge pass form: 0 thread per (slot, point), 1 lane pair per slot
@@ -231,8 +240,16 @@ struct Ops {
 
   static int limiter(dgm_ctx* c, T* U) {
     if (!c->limiter) return DGM_OK;
+    const int dblocks = (int)std::max<int64_t>(1, (c->ne + dgm::kDetectThreads - 1) / dgm::kDetectThreads);
+    if (c->lim_staged)
+      dgm::k_lim_detect<P, T, true><<<dblocks, dgm::kDetectThreads, 0, c->stream>>>(kp_of<P, T>(c), U, c->t0, c->status,
+                                                                                   c->wl1, c->pend, c->order);
+    else
+      dgm::k_lim_detect<P, T, false><<<dblocks, dgm::kDetectThreads, 0, c->stream>>>(kp_of<P, T>(c), U, c->t0,
+                                                                                    c->status, c->wl1, c->pend, c->order);
+    CK(cudaGetLastError());
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(c->coop_blocks[c->lim_staged][c->lim_queue]);
+    cfg.gridDim = dim3(c->coop_blocks[c->lim_queue]);
     cfg.blockDim = dim3(dgm::kLimiterWarps * 32);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = c->stream;
@@ -241,10 +258,9 @@ struct Ops {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    auto kern = dgm::k_limiter<P, T, false, false>;
-    if (c->lim_staged) kern = c->lim_queue ? dgm::k_limiter<P, T, true, true> : dgm::k_limiter<P, T, true, false>;
-    else if (c->lim_queue) kern = dgm::k_limiter<P, T, false, true>;
-    CK(cudaLaunchKernelEx(&cfg, kern, kp_of<P, T>(c), U, c->t0, c->status, c->work));
+    auto kern = c->lim_queue ? dgm::k_limiter<P, T, true> : dgm::k_limiter<P, T, false>;
+    CK(cudaLaunchKernelEx(&cfg, kern, kp_of<P, T>(c), U, (const unsigned char*)c->t0, c->status, c->work,
+                          (const int*)c->wl1, (const int*)c->pend));
     return DGM_OK;
   }
 
@@ -265,8 +281,8 @@ struct Ops {
   }
 
   static int diagnostics(dgm_ctx* c, const T* R) {
-    dgm::k_diagnostics<P, T><<<(int)c->inst.size(), 256, 0, c->stream>>>(kp_of<P, T>(c), S(c->U), R, c->d_elem_off,
-                                                                          c->d_bslot_off, c->d_diag);
+    dgm::k_diagnostics<P, T><<<(int)c->inst.size(), 256, 0, c->stream>>>(kp_of<P, T>(c), S(c->U), R, c->d_elem_rng,
+                                                                          c->d_bslot_rng, c->d_diag);
     CK(cudaGetLastError());
     return DGM_OK;
   }
@@ -318,15 +334,20 @@ struct Ops {
     return DGM_OK;
   }
 
-  static int weno_gram(dgm_ctx* c) {
+  // WENO Gram matrices of the elements [e0, e0 + count)
+  static int weno_gram(dgm_ctx* c, int64_t e0, int64_t count) {
     constexpr int NPAIR = V::NB * (V::NB + 1) / 2;
-    const int64_t n = (int64_t)NPAIR * c->ne;
+    const int64_t n = (int64_t)NPAIR * count;
     const int threads = 256;
-    dgm::k_weno_gram<P, T><<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(kp_of<P, T>(c), c->gram);
+    if (n > 0)
+      dgm::k_weno_gram<P, T><<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(kp_of<P, T>(c), c->gram,
+                                                                                         (int)e0, (int)count);
     CK(cudaGetLastError());
     kp_of<P, T>(c).m.gram = c->gram;
     return DGM_OK;
   }
+
+  static MeshDev& mesh(dgm_ctx* c) { return kp_of<P, T>(c).m; }
 
   static int project(dgm_ctx* c, int64_t i, const double q[NEQ]) {
     dgm::Projection<P> pr;
@@ -355,16 +376,13 @@ struct Ops {
   }
 
   static int occupancy(dgm_ctx* c) {
-    int per_sm[2][2] = {{0, 0}, {0, 0}};
+    int per_sm[2] = {0, 0};
     const int threads = dgm::kLimiterWarps * 32;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0][0], dgm::k_limiter<P, T, false, false>, threads, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0][1], dgm::k_limiter<P, T, false, true>, threads, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1][0], dgm::k_limiter<P, T, true, false>, threads, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1][1], dgm::k_limiter<P, T, true, true>, threads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], dgm::k_limiter<P, T, false>, threads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], dgm::k_limiter<P, T, true>, threads, 0));
     const int64_t want = std::max<int64_t>(1, (c->ne + 32 * dgm::kLimiterWarps - 1) / (32 * dgm::kLimiterWarps));
-    for (int v = 0; v < 2; ++v)
-      for (int q = 0; q < 2; ++q)
-        c->coop_blocks[v][q] = (int)std::min<int64_t>((int64_t)std::max(1, per_sm[v][q]) * c->num_sms, want);
+    for (int q = 0; q < 2; ++q)
+      c->coop_blocks[q] = (int)std::min<int64_t>((int64_t)std::max(1, per_sm[q]) * c->num_sms, want);
     return DGM_OK;
   }
 
@@ -474,10 +492,19 @@ int collect_status(dgm_ctx* c) {
     const int zero = 0;
     CK(cudaMemcpyAsync(&c->ctl->status, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     if (h.status == dgm::ST_TIMEOUT) {
-      // a limiter pass that gave up may have left queue slots and counters behind
+      // a limiter pass that gave up may have left queue slots, counters and a half-passed grid
+      // barrier behind: clear them all (the barrier's generation counter may keep its value)
       CK(cudaMemsetAsync(c->work, 0, sizeof(int) * std::max<int64_t>(c->ne, 1), c->stream));
-      CK(cudaMemsetAsync(&c->ctl->lim_exit, 0, sizeof(unsigned int), c->stream));
-      CK(cudaMemsetAsync(&c->ctl->lq[0], 0, sizeof(c->ctl->lq), c->stream));
+      Control z = h;
+      z.status = 0;
+      z.t0_count = 0;
+      z.unknown[0] = z.unknown[1] = 0;
+      z.wl_count[0] = z.wl_count[1] = 0;
+      z.wl1_count = z.pend_count = 0;
+      z.bar_count = 0u;
+      z.lim_exit = 0u;
+      for (auto& q : z.lq) dgm::reset_queue(q);
+      CK(cudaMemcpyAsync(c->ctl, &z, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
     }
     for (size_t i = 0; i < c->inst.size(); ++i)
       if (hi[i].status) CK(cudaMemcpyAsync(&c->ic[i].status, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -615,149 +642,286 @@ int enqueue_steps(dgm_ctx* c, int64_t n, int with_residual) {
   return DGM_OK;
 }
 
-// Union mesh of all instances: element, slot and patch indices offset per instance; internal
-// edges of every instance first (each in Mesh::internal_edge_indices order), then boundary
-// edges (each instance in edge-id order).  Validates every index against process_mesh's
-// conventions before anything reaches the device.
-int build_mesh(dgm_ctx* c, const dgm_mesh_desc* meshes, int n_inst, MeshDev& md) {
-  int64_t ne = 0, np = 0;
-  for (int i = 0; i < n_inst; ++i) {
-    const dgm_mesh_desc* m = &meshes[i];
-    if (m->n_elements <= 0 || m->n_edges <= 0 || m->n_vertices <= 0 || m->n_patches < 0) return DGM_BAD_ARG;
-    ne += m->n_elements;
-    np += m->n_patches;
-  }
-  if (ne > (1ll << 30)) return DGM_BAD_ARG;
-  const int64_t ld = (ne + 31) / 32 * 32;
-  c->ne = ne;
-  c->ld = ld;
-  c->np = np;
-  auto in_range = [](int64_t i, int64_t n) { return i >= 0 && i < n; };
-  std::vector<int64_t> slot_ref;
+// Union mesh of all instances.  Instance i owns fixed ranges of the union's arrays -- elements
+// [elem_off, elem_off + elem_cap), internal edge slots [int_off, int_off + int_cap), boundary
+// edge slots [n_int + bnd_off, n_int + bnd_off + bnd_cap) and patches [patch_off, patch_off +
+// patch_cap) -- with its mesh's entries first (internal edges in Mesh::internal_edge_indices order,
+// boundary edges in edge-id order) and padding after.  A context created with capacities above
+// its meshes' sizes (dgm_create_batch_slots) can later take a different mesh into an instance's
+// ranges (dgm_instance_replace).  Padding elements and every padding slot belong to a "dead"
+// instance (index n_inst, never stepping: its loop bounds are zero), so every kernel skips them;
+// padding slots refer to a null element (the last element of the union, also dead).  Without
+// padding the layout is the plain concatenation, with no dead instance and no null element.
+
+// One instance's part of the union mesh, in its capacity ranges (element-indexed rows have length
+// elem_cap; element, slot and patch ids are global).
+struct InstArrays {
+  std::vector<double> jac, hmin, h15, dinv;  // dinv: [4][elem_cap]
+  std::vector<int> face, nbr, inst, order;   // face, nbr: [3][elem_cap]
   std::vector<int2> ie_lr;
   std::vector<int> ie_ic;
   std::vector<double4> ie_geo;
   std::vector<int> be_elem, be_info;
   std::vector<double4> be_geo;
-  std::vector<double4> patch_q(std::max<int64_t>(1, np));
-  std::vector<int> face(3 * ld, 0), nbr(3 * ld, -1), inst_of(ne, 0);
-  std::vector<double> jac(ne), hmin(ne), h15(ne), dinv(4 * ld, 0.0);
-  std::vector<std::vector<int64_t>> slot_of(n_inst);
-  // pass 1: internal edges of every instance
-  int64_t eo = 0;
-  for (int i = 0; i < n_inst; ++i) {
-    const dgm_mesh_desc* m = &meshes[i];
-    const int64_t ned = m->n_edges, nei = m->n_elements;
-    slot_of[i].assign(ned, -1);
-    for (int64_t k = 0; k < m->n_internal_edges; ++k) {
-      const int64_t d = m->internal_edges[k];
-      if (!in_range(d, ned) || slot_of[i][d] >= 0) return DGM_BAD_ARG;
-      const int64_t L = m->edge_elements[2 * d], R = m->edge_elements[2 * d + 1];
-      const int64_t il = m->edge_in_cell[2 * d], ir = m->edge_in_cell[2 * d + 1];
-      if (!in_range(L, nei) || !in_range(R, nei) || L == R || !in_range(il, 3) || !in_range(ir, 3)) return DGM_BAD_ARG;
-      slot_of[i][d] = (int64_t)slot_ref.size();
-      slot_ref.push_back(d);
-      ie_lr.push_back(make_int2((int)(eo + L), (int)(eo + R)));
-      ie_ic.push_back((int)(il | (ir << 2)));
-      const double jd = m->edge_jacob_det[d];
-      ie_geo.push_back(make_double4(m->edge_normal[2 * d], m->edge_normal[2 * d + 1], 0.5 * jd, jd));
-    }
-    eo += nei;
+  std::vector<double4> patch_q;
+  std::vector<int64_t> int_ref, bnd_ref;     // reference edge id of each slot (-1: padding)
+};
+
+int64_t boundary_edge_count(const dgm_mesh_desc* m) {
+  int64_t n = 0;
+  for (int64_t d = 0; d < m->n_edges; ++d) n += m->edge_elements[2 * d + 1] == -1 ? 1 : 0;
+  return n;
+}
+
+// Builds instance i's arrays from mesh m into its ranges (HostInst offsets and capacities must be
+// set, and c->n_int, c->dead_inst, c->null_elem).  Validates every index against process_mesh's
+// conventions before anything reaches the device.
+int fill_instance(const dgm_ctx* c, int i, const dgm_mesh_desc* m, InstArrays& a) {
+  const HostInst& hi = c->inst[i];
+  auto in_range = [](int64_t v, int64_t n) { return v >= 0 && v < n; };
+  if (m->n_elements <= 0 || m->n_edges <= 0 || m->n_vertices <= 0 || m->n_patches < 0) return DGM_BAD_ARG;
+  if (m->n_elements > hi.elem_cap || m->n_internal_edges > hi.int_cap || boundary_edge_count(m) > hi.bnd_cap ||
+      m->n_patches > hi.patch_cap)
+    return DGM_BAD_ARG;
+  const int64_t ned = m->n_edges, nei = m->n_elements, cap = hi.elem_cap, eo = hi.elem_off;
+  const int dead = c->dead_inst, null_e = (int)c->null_elem;
+  a.jac.assign(cap, 1.0);
+  a.hmin.assign(cap, 1.0);
+  a.h15.assign(cap, 1.0);
+  a.dinv.assign(4 * cap, 0.0);
+  a.face.assign(3 * cap, (int)((hi.int_cap > 0 ? hi.int_off : c->n_int + hi.bnd_off) << 1));
+  a.nbr.assign(3 * cap, -1);
+  a.inst.assign(cap, dead);
+  a.ie_lr.assign(hi.int_cap, make_int2(null_e, null_e));
+  a.ie_ic.assign(hi.int_cap, 0);
+  a.ie_geo.assign(hi.int_cap, make_double4(0.0, 0.0, 0.0, 0.0));
+  a.int_ref.assign(hi.int_cap, -1);
+  a.be_elem.assign(hi.bnd_cap, null_e);
+  a.be_info.assign(hi.bnd_cap, (int)(hi.patch_off << 3));
+  a.be_geo.assign(hi.bnd_cap, make_double4(0.0, 0.0, 0.0, 0.0));
+  a.bnd_ref.assign(hi.bnd_cap, -1);
+  a.patch_q.assign(std::max<int64_t>(hi.patch_cap, 0), make_double4(0.0, 0.0, 0.0, 0.0));
+  std::vector<int64_t> slot_of(ned, -1);
+  // internal edges
+  for (int64_t k = 0; k < m->n_internal_edges; ++k) {
+    const int64_t d = m->internal_edges[k];
+    if (!in_range(d, ned) || slot_of[d] >= 0) return DGM_BAD_ARG;
+    const int64_t L = m->edge_elements[2 * d], R = m->edge_elements[2 * d + 1];
+    const int64_t il = m->edge_in_cell[2 * d], ir = m->edge_in_cell[2 * d + 1];
+    if (!in_range(L, nei) || !in_range(R, nei) || L == R || !in_range(il, 3) || !in_range(ir, 3)) return DGM_BAD_ARG;
+    slot_of[d] = hi.int_off + k;
+    a.int_ref[k] = d;
+    a.ie_lr[k] = make_int2((int)(eo + L), (int)(eo + R));
+    a.ie_ic[k] = (int)(il | (ir << 2));
+    const double jd = m->edge_jacob_det[d];
+    a.ie_geo[k] = make_double4(m->edge_normal[2 * d], m->edge_normal[2 * d + 1], 0.5 * jd, jd);
   }
-  c->n_int = (int64_t)slot_ref.size();
-  // pass 2: boundary edges, patches, elements
-  eo = 0;
-  int64_t po = 0;
-  for (int i = 0; i < n_inst; ++i) {
-    const dgm_mesh_desc* m = &meshes[i];
-    const int64_t ned = m->n_edges, nei = m->n_elements;
-    HostInst& hi = c->inst[i];
-    hi.elem_off = eo;
-    hi.ne = nei;
-    hi.bslot_off = (int64_t)be_elem.size();
-    for (int64_t d = 0; d < ned; ++d) {
-      if (m->edge_elements[2 * d + 1] != -1) continue;
-      const int64_t e = m->edge_elements[2 * d], k = m->edge_in_cell[2 * d], patch = m->edge_patch[d];
-      if (!in_range(e, nei) || !in_range(k, 3) || !in_range(patch, m->n_patches)) return DGM_BAD_ARG;
-      if (slot_of[i][d] >= 0) return DGM_BAD_ARG;
-      slot_of[i][d] = c->n_int + (int64_t)be_elem.size();
-      slot_ref.push_back(d);
-      const int type = m->patch_type[patch];
-      if (type != DGM_WALL && type != DGM_FARFIELD) return DGM_BAD_ARG;
-      be_elem.push_back((int)(eo + e));
-      be_info.push_back((int)(k | (type << 2) | ((po + patch) << 3)));
-      // outward orientation, boundary_condition.rs:22-28
-      const bool same = m->elem_vertices[3 * e + k] == m->edge_vertices[2 * d];
-      const double nx = same ? m->edge_normal[2 * d] : -m->edge_normal[2 * d];
-      const double ny = same ? m->edge_normal[2 * d + 1] : -m->edge_normal[2 * d + 1];
-      const double jd = m->edge_jacob_det[d];
-      be_geo.push_back(make_double4(nx, ny, 0.5 * jd, jd));
-    }
-    hi.nb_slots = (int64_t)be_elem.size() - hi.bslot_off;
-    // far-field conserved state, boundary_condition.rs:50-55
-    for (int64_t p = 0; p < m->n_patches; ++p) {
-      const double* bq = &m->patch_quantity[4 * p];
-      patch_q[po + p] = make_double4(bq[0], bq[0] * bq[1], bq[0] * bq[2],
-                                     bq[3] / (c->hcr - 1.0) + 0.5 * bq[0] * (bq[1] * bq[1] + bq[2] * bq[2]));
-    }
-    std::vector<unsigned char> in_list(nei, 0);
-    for (int64_t k = 0; k < m->n_boundary_elements; ++k) {
-      const int64_t e = m->boundary_elements[k];
-      if (!in_range(e, nei)) return DGM_BAD_ARG;
-      in_list[e] = 1;
-    }
-    auto X = [&](int64_t v) { return m->vertex_xy[2 * v]; };
-    auto Y = [&](int64_t v) { return m->vertex_xy[2 * v + 1]; };
-    for (int64_t e = 0; e < nei; ++e) {
-      const int64_t ge = eo + e;
-      bool has_boundary = false;
-      for (int k = 0; k < 3; ++k) {
-        const int64_t d = m->elem_edges[3 * e + k];
-        if (!in_range(d, ned) || slot_of[i][d] < 0) return DGM_BAD_ARG;
-        int side;
-        if (m->edge_elements[2 * d + 1] == -1) {
-          if (m->edge_elements[2 * d] != e || m->edge_in_cell[2 * d] != k) return DGM_BAD_ARG;
-          side = 0;
-          has_boundary = true;
-          if (m->elem_neighbours[3 * e + k] != -1) return DGM_BAD_ARG;
-        } else {
-          const bool same = m->elem_vertices[3 * e + k] == m->edge_vertices[2 * d];
-          if (m->edge_elements[2 * d] == e && same && m->edge_in_cell[2 * d] == k) side = 0;
-          else if (m->edge_elements[2 * d + 1] == e && !same && m->edge_in_cell[2 * d + 1] == k) side = 1;
-          else return DGM_BAD_ARG;  // orientation inconsistent with process_mesh's left/right rule
-          const int64_t other = m->edge_elements[2 * d + (side ? 0 : 1)];
-          if (m->elem_neighbours[3 * e + k] != other) return DGM_BAD_ARG;
-          nbr[k * ld + ge] = (int)(eo + other);
-        }
-        face[k * ld + ge] = (int)((slot_of[i][d] << 1) | side);
+  // boundary edges, in edge-id order
+  int64_t nbs = 0;
+  for (int64_t d = 0; d < ned; ++d) {
+    if (m->edge_elements[2 * d + 1] != -1) continue;
+    const int64_t e = m->edge_elements[2 * d], k = m->edge_in_cell[2 * d], patch = m->edge_patch[d];
+    if (!in_range(e, nei) || !in_range(k, 3) || !in_range(patch, m->n_patches)) return DGM_BAD_ARG;
+    if (slot_of[d] >= 0) return DGM_BAD_ARG;
+    slot_of[d] = c->n_int + hi.bnd_off + nbs;
+    a.bnd_ref[nbs] = d;
+    const int type = m->patch_type[patch];
+    if (type != DGM_WALL && type != DGM_FARFIELD) return DGM_BAD_ARG;
+    a.be_elem[nbs] = (int)(eo + e);
+    a.be_info[nbs] = (int)(k | (type << 2) | ((hi.patch_off + patch) << 3));
+    // outward orientation, boundary_condition.rs:22-28
+    const bool same = m->elem_vertices[3 * e + k] == m->edge_vertices[2 * d];
+    const double nx = same ? m->edge_normal[2 * d] : -m->edge_normal[2 * d];
+    const double ny = same ? m->edge_normal[2 * d + 1] : -m->edge_normal[2 * d + 1];
+    const double jd = m->edge_jacob_det[d];
+    a.be_geo[nbs] = make_double4(nx, ny, 0.5 * jd, jd);
+    ++nbs;
+  }
+  // far-field conserved state, boundary_condition.rs:50-55
+  for (int64_t p = 0; p < m->n_patches; ++p) {
+    const double* bq = &m->patch_quantity[4 * p];
+    a.patch_q[p] = make_double4(bq[0], bq[0] * bq[1], bq[0] * bq[2],
+                                bq[3] / (c->hcr - 1.0) + 0.5 * bq[0] * (bq[1] * bq[1] + bq[2] * bq[2]));
+  }
+  std::vector<unsigned char> in_list(nei, 0);
+  for (int64_t k = 0; k < m->n_boundary_elements; ++k) {
+    const int64_t e = m->boundary_elements[k];
+    if (!in_range(e, nei)) return DGM_BAD_ARG;
+    in_list[e] = 1;
+  }
+  auto X = [&](int64_t v) { return m->vertex_xy[2 * v]; };
+  auto Y = [&](int64_t v) { return m->vertex_xy[2 * v + 1]; };
+  for (int64_t e = 0; e < nei; ++e) {
+    bool has_boundary = false;
+    for (int k = 0; k < 3; ++k) {
+      const int64_t d = m->elem_edges[3 * e + k];
+      if (!in_range(d, ned) || slot_of[d] < 0) return DGM_BAD_ARG;
+      int side;
+      if (m->edge_elements[2 * d + 1] == -1) {
+        if (m->edge_elements[2 * d] != e || m->edge_in_cell[2 * d] != k) return DGM_BAD_ARG;
+        side = 0;
+        has_boundary = true;
+        if (m->elem_neighbours[3 * e + k] != -1) return DGM_BAD_ARG;
+        a.nbr[k * cap + e] = -1;
+      } else {
+        const bool same = m->elem_vertices[3 * e + k] == m->edge_vertices[2 * d];
+        if (m->edge_elements[2 * d] == e && same && m->edge_in_cell[2 * d] == k) side = 0;
+        else if (m->edge_elements[2 * d + 1] == e && !same && m->edge_in_cell[2 * d + 1] == k) side = 1;
+        else return DGM_BAD_ARG;  // orientation inconsistent with process_mesh's left/right rule
+        const int64_t other = m->edge_elements[2 * d + (side ? 0 : 1)];
+        if (m->elem_neighbours[3 * e + k] != other) return DGM_BAD_ARG;
+        a.nbr[k * cap + e] = (int)(eo + other);
       }
-      // every element is in exactly one of the internal / boundary element lists
-      if (has_boundary != (in_list[e] != 0)) return DGM_BAD_ARG;
-      const double J = m->elem_jacob_det[e];
-      const int64_t v1 = m->elem_vertices[3 * e], v2 = m->elem_vertices[3 * e + 1], v3 = m->elem_vertices[3 * e + 2];
-      if (!in_range(v1, m->n_vertices) || !in_range(v2, m->n_vertices) || !in_range(v3, m->n_vertices))
-        return DGM_BAD_ARG;
-      jac[ge] = J;
-      inst_of[ge] = i;
-      // compute_dphi inverse Jacobian, mesh.rs:93-100
-      dinv[0 * ld + ge] = (Y(v3) - Y(v1)) / J;
-      dinv[1 * ld + ge] = -(X(v3) - X(v1)) / J;
-      dinv[2 * ld + ge] = -(Y(v2) - Y(v1)) / J;
-      dinv[3 * ld + ge] = (X(v2) - X(v1)) / J;
-      hmin[ge] = m->elem_minimum_height[e];
-      h15[ge] = std::pow(m->elem_circumradius[e], 1.5);  // weno.rs:81 h.powf(1.5)
+      a.face[k * cap + e] = (int)((slot_of[d] << 1) | side);
     }
-    eo += nei;
-    po += m->n_patches;
+    // every element is in exactly one of the internal / boundary element lists
+    if (has_boundary != (in_list[e] != 0)) return DGM_BAD_ARG;
+    const double J = m->elem_jacob_det[e];
+    const int64_t v1 = m->elem_vertices[3 * e], v2 = m->elem_vertices[3 * e + 1], v3 = m->elem_vertices[3 * e + 2];
+    if (!in_range(v1, m->n_vertices) || !in_range(v2, m->n_vertices) || !in_range(v3, m->n_vertices))
+      return DGM_BAD_ARG;
+    a.jac[e] = J;
+    a.inst[e] = i;
+    // compute_dphi inverse Jacobian, mesh.rs:93-100
+    a.dinv[0 * cap + e] = (Y(v3) - Y(v1)) / J;
+    a.dinv[1 * cap + e] = -(X(v3) - X(v1)) / J;
+    a.dinv[2 * cap + e] = -(Y(v2) - Y(v1)) / J;
+    a.dinv[3 * cap + e] = (X(v2) - X(v1)) / J;
+    a.hmin[e] = m->elem_minimum_height[e];
+    a.h15[e] = std::pow(m->elem_circumradius[e], 1.5);  // weno.rs:81 h.powf(1.5)
   }
-  c->n_bnd = (int64_t)be_elem.size();
-  if (c->n_int + c->n_bnd > (1ll << 29)) return DGM_BAD_ARG;
+  // the limiter detection's visiting order: breadth-first over the element graph (each connected
+  // piece from its lowest unvisited element), so that a warp's elements and the neighbours whose
+  // traces they gather are close together and mostly in cache.  Any permutation gives the same
+  // results; this one only changes which loads hit.  Padding elements follow.
+  a.order.clear();
+  a.order.reserve((size_t)cap);
+  std::vector<unsigned char> seen((size_t)nei, 0);
+  for (int64_t s0 = 0; s0 < nei; ++s0) {
+    if (seen[s0]) continue;
+    seen[s0] = 1;
+    a.order.push_back((int)(eo + s0));
+    for (size_t h = a.order.size() - 1; h < a.order.size(); ++h) {
+      const int64_t e = a.order[h] - eo;
+      for (int k = 0; k < 3; ++k) {
+        const int nb = a.nbr[k * cap + e];
+        if (nb >= 0 && !seen[nb - eo]) {
+          seen[nb - eo] = 1;
+          a.order.push_back(nb);
+        }
+      }
+    }
+  }
+  for (int64_t e = nei; e < cap; ++e) a.order.push_back((int)(eo + e));
+  return DGM_OK;
+}
+
+// Instance ranges of the diagnostics: [2 n] (first element, element count) and (first boundary
+// slot relative to n_int, boundary slot count) of each instance's mesh.
+int upload_ranges(dgm_ctx* c) {
+  const size_t n = c->inst.size();
+  std::vector<int> er(2 * n), br(2 * n);
+  for (size_t i = 0; i < n; ++i) {
+    er[2 * i] = (int)c->inst[i].elem_off;
+    er[2 * i + 1] = (int)c->inst[i].ne;
+    br[2 * i] = (int)c->inst[i].bslot_off;
+    br[2 * i + 1] = (int)c->inst[i].nb_slots;
+  }
+  if (!c->d_elem_rng) {
+    int st;
+    if ((st = dev_alloc(c, &c->d_elem_rng, 2 * n)) || (st = dev_alloc(c, &c->d_bslot_rng, 2 * n))) return st;
+  }
+  CK(cudaMemcpyAsync(c->d_elem_rng, er.data(), sizeof(int) * 2 * n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_bslot_rng, br.data(), sizeof(int) * 2 * n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));  // the host vectors go out of scope
+  return DGM_OK;
+}
+
+int build_mesh(dgm_ctx* c, const dgm_mesh_desc* meshes, const dgm_slot_capacity* caps, int n_inst, MeshDev& md) {
+  // capacity layout
+  int64_t ne = 0, n_int = 0, n_bnd = 0, np = 0;
+  bool padding = false;
+  for (int i = 0; i < n_inst; ++i) {
+    const dgm_mesh_desc* m = &meshes[i];
+    if (m->n_elements <= 0 || m->n_edges <= 0 || m->n_vertices <= 0 || m->n_patches < 0) return DGM_BAD_ARG;
+    const int64_t nbe = boundary_edge_count(m);
+    HostInst& hi = c->inst[i];
+    hi.elem_cap = caps ? caps[i].elements : m->n_elements;
+    hi.int_cap = caps ? caps[i].internal_edges : m->n_internal_edges;
+    hi.bnd_cap = caps ? caps[i].boundary_edges : nbe;
+    hi.patch_cap = caps ? caps[i].patches : m->n_patches;
+    if (hi.elem_cap < m->n_elements || hi.int_cap < m->n_internal_edges || hi.bnd_cap < nbe ||
+        hi.patch_cap < m->n_patches || hi.elem_cap > (1ll << 30) || hi.int_cap > (1ll << 30) ||
+        hi.bnd_cap > (1ll << 30) || hi.patch_cap > (1ll << 20))
+      return DGM_BAD_ARG;
+    padding = padding || hi.elem_cap > m->n_elements || hi.int_cap > m->n_internal_edges || hi.bnd_cap > nbe ||
+              hi.patch_cap > m->n_patches;
+    hi.elem_off = ne;
+    hi.int_off = n_int;
+    hi.bnd_off = n_bnd;
+    hi.patch_off = np;
+    hi.bslot_off = n_bnd;
+    hi.ne = m->n_elements;
+    hi.nb_slots = nbe;
+    ne += hi.elem_cap;
+    n_int += hi.int_cap;
+    n_bnd += hi.bnd_cap;
+    np += hi.patch_cap;
+  }
+  c->dead_inst = padding ? n_inst : 0;
+  c->null_elem = padding ? ne : -1;
+  if (padding) ne += 1;
+  if (ne > (1ll << 30) || n_int + n_bnd > (1ll << 29)) return DGM_BAD_ARG;
+  const int64_t ld = (ne + 31) / 32 * 32;
+  c->ne = ne;
+  c->ld = ld;
+  c->np = np;
+  c->n_int = n_int;
+  c->n_bnd = n_bnd;
+  c->padded = padding;
+  std::vector<int64_t> slot_ref(n_int + n_bnd, -1);
+  std::vector<int2> ie_lr(n_int);
+  std::vector<int> ie_ic(n_int);
+  std::vector<double4> ie_geo(n_int);
+  std::vector<int> be_elem(n_bnd), be_info(n_bnd);
+  std::vector<double4> be_geo(n_bnd);
+  std::vector<double4> patch_q(std::max<int64_t>(1, np));
+  std::vector<int> face(3 * ld, 0), nbr(3 * ld, -1), inst_of(ne, c->dead_inst), order;
+  std::vector<double> jac(ne, 1.0), hmin(ne, 1.0), h15(ne, 1.0), dinv(4 * ld, 0.0);
+  order.reserve((size_t)ne);
+  InstArrays a;
+  for (int i = 0; i < n_inst; ++i) {
+    int st = fill_instance(c, i, &meshes[i], a);
+    if (st) return st;
+    const HostInst& hi = c->inst[i];
+    const int64_t eo = hi.elem_off, cap = hi.elem_cap;
+    std::copy(a.jac.begin(), a.jac.end(), jac.begin() + eo);
+    std::copy(a.hmin.begin(), a.hmin.end(), hmin.begin() + eo);
+    std::copy(a.h15.begin(), a.h15.end(), h15.begin() + eo);
+    std::copy(a.inst.begin(), a.inst.end(), inst_of.begin() + eo);
+    for (int k = 0; k < 4; ++k) std::copy(a.dinv.begin() + k * cap, a.dinv.begin() + (k + 1) * cap, dinv.begin() + k * ld + eo);
+    for (int k = 0; k < 3; ++k) {
+      std::copy(a.face.begin() + k * cap, a.face.begin() + (k + 1) * cap, face.begin() + k * ld + eo);
+      std::copy(a.nbr.begin() + k * cap, a.nbr.begin() + (k + 1) * cap, nbr.begin() + k * ld + eo);
+    }
+    order.insert(order.end(), a.order.begin(), a.order.end());
+    std::copy(a.ie_lr.begin(), a.ie_lr.end(), ie_lr.begin() + hi.int_off);
+    std::copy(a.ie_ic.begin(), a.ie_ic.end(), ie_ic.begin() + hi.int_off);
+    std::copy(a.ie_geo.begin(), a.ie_geo.end(), ie_geo.begin() + hi.int_off);
+    std::copy(a.int_ref.begin(), a.int_ref.end(), slot_ref.begin() + hi.int_off);
+    std::copy(a.be_elem.begin(), a.be_elem.end(), be_elem.begin() + hi.bnd_off);
+    std::copy(a.be_info.begin(), a.be_info.end(), be_info.begin() + hi.bnd_off);
+    std::copy(a.be_geo.begin(), a.be_geo.end(), be_geo.begin() + hi.bnd_off);
+    std::copy(a.bnd_ref.begin(), a.bnd_ref.end(), slot_ref.begin() + n_int + hi.bnd_off);
+    std::copy(a.patch_q.begin(), a.patch_q.end(), patch_q.begin() + hi.patch_off);
+  }
+  if (padding) order.push_back((int)c->null_elem);
   md = MeshDev{};
   md.ne = (int)ne;
   md.ld = (int)ld;
-  md.n_int = (int)c->n_int;
-  md.n_bnd = (int)c->n_bnd;
-  md.n_inst = n_inst;
+  md.n_int = (int)n_int;
+  md.n_bnd = (int)n_bnd;
+  md.n_inst = n_inst + (padding ? 1 : 0);  // the dead instance is read from inst[] like the others
   int st;
   double *d_jac, *d_dinv, *d_hmin, *d_h15;
   int *d_face, *d_nbr, *d_inst, *d_ie_ic, *d_be_elem, *d_be_info;
@@ -769,7 +933,8 @@ int build_mesh(dgm_ctx* c, const dgm_mesh_desc* meshes, int n_inst, MeshDev& md)
       (st = upload(c, &d_inst, inst_of)) || (st = upload(c, &d_ie_lr, ie_lr)) || (st = upload(c, &d_ie_ic, ie_ic)) ||
       (st = upload(c, &d_ie_geo, ie_geo)) || (st = upload(c, &d_be_elem, be_elem)) ||
       (st = upload(c, &d_be_info, be_info)) || (st = upload(c, &d_be_geo, be_geo)) ||
-      (st = upload(c, &d_patch, patch_q)) || (st = upload(c, &d_slot_ref, slot_ref)))
+      (st = upload(c, &d_patch, patch_q)) || (st = upload(c, &d_slot_ref, slot_ref)) ||
+      (st = upload(c, &c->order, order)))
     return st;
   md.jac = d_jac;
   md.dinv = d_dinv;
@@ -786,17 +951,9 @@ int build_mesh(dgm_ctx* c, const dgm_mesh_desc* meshes, int n_inst, MeshDev& md)
   md.be_geo = d_be_geo;
   md.patch_q = d_patch;
   md.slot_ref = d_slot_ref;
-  // instance ranges for the diagnostics
-  std::vector<int> elem_off(n_inst + 1), bslot_off(n_inst + 1);
-  for (int i = 0; i < n_inst; ++i) {
-    elem_off[i] = (int)c->inst[i].elem_off;
-    bslot_off[i] = (int)c->inst[i].bslot_off;
-  }
-  elem_off[n_inst] = (int)ne;
-  bslot_off[n_inst] = (int)c->n_bnd;
-  if ((st = upload(c, &c->d_elem_off, elem_off)) || (st = upload(c, &c->d_bslot_off, bslot_off))) return st;
+  if ((st = upload_ranges(c))) return st;
   int64_t mx = 0;
-  for (auto& h : c->inst) mx = std::max(mx, h.ne);
+  for (auto& h : c->inst) mx = std::max(mx, h.elem_cap);
   c->max_inst_ne = mx;
   return DGM_OK;
 }
@@ -808,8 +965,8 @@ bool variant_ok(const dgm_tables_desc* t) {
          (P == 3 && t->n_basis == 10 && t->n_cell_gp == 12 && t->n_edge_gp == 4);
 }
 
-dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* tables, const dgm_params* params,
-                int32_t* status) {
+dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_slot_capacity* caps, const dgm_tables_desc* tables,
+                const dgm_params* params, int32_t* status) {
   int32_t dummy;
   if (!status) status = &dummy;
   if (n_inst < 1 || !meshes || !tables || !params) {
@@ -863,13 +1020,15 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* 
   c->pool = pool_acquire(c->device);
   if (!c->pool) return fail(DGM_CUDA_ERROR);
   int st;
-  if ((st = dev_alloc(c, &c->ctl, 1)) || (st = dev_alloc(c, &c->ic, (size_t)n_inst))) return fail(st);
+  // one more instance control block than instances: the dead instance of padded contexts (all
+  // zero: never stepping)
+  if ((st = dev_alloc(c, &c->ctl, 1)) || (st = dev_alloc(c, &c->ic, (size_t)n_inst + 1))) return fail(st);
   if (cudaMemsetAsync(c->ctl, 0, sizeof(Control), c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
-  if (cudaMemsetAsync(c->ic, 0, sizeof(InstCtl) * n_inst, c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  if (cudaMemsetAsync(c->ic, 0, sizeof(InstCtl) * (n_inst + 1), c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
   st = dispatch(c, [&](auto ops) { return decltype(ops)::fill_tables(c, tables); });
   if (st) return fail(st);
   MeshDev md;
-  if ((st = build_mesh(c, meshes, n_inst, md))) return fail(st);
+  if ((st = build_mesh(c, meshes, caps, n_inst, md))) return fail(st);
   dispatch(c, [&](auto ops) { return decltype(ops)::set_mesh(c, md); });
   const size_t n_state = (size_t)NEQ * c->nb * c->ld;
   const size_t n_flux = (size_t)(c->n_int + c->n_bnd) * c->ng * 4;
@@ -879,7 +1038,8 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* 
       (st = dev_alloc_bytes(c, &c->F, n_flux * eb)) ||
       (st = dev_alloc(c, &c->stage, (size_t)c->max_inst_ne * NEQ * c->nb)) ||
       (st = dev_alloc(c, &c->t0, (size_t)c->ne)) || (st = dev_alloc(c, &c->status, (size_t)c->ne)) ||
-      (st = dev_alloc(c, &c->work, (size_t)c->ne)) || (st = dev_alloc(c, &c->d_diag, (size_t)n_inst * 8)))
+      (st = dev_alloc(c, &c->work, (size_t)c->ne)) || (st = dev_alloc(c, &c->wl1, (size_t)c->ne)) ||
+      (st = dev_alloc(c, &c->pend, (size_t)c->ne)) || (st = dev_alloc(c, &c->d_diag, (size_t)n_inst * 8)))
     return fail(st);
   for (void* p : {c->U, c->U1, c->U2, c->R})
     if (cudaMemsetAsync(p, 0, n_state * eb, c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
@@ -888,7 +1048,7 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_tables_desc* 
     return fail(DGM_CUDA_ERROR);
   if (c->limiter) {
     if ((st = dev_alloc(c, &c->gram, (size_t)(c->nb * (c->nb + 1) / 2) * c->ld))) return fail(st);
-    if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::weno_gram(c); }))) return fail(st);
+    if ((st = dispatch(c, [&](auto ops) { return decltype(ops)::weno_gram(c, 0, c->ne); }))) return fail(st);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
   }
   if (cudaMemsetAsync(c->status, 0, (size_t)c->ne * sizeof(unsigned int), c->stream) != cudaSuccess)
@@ -943,12 +1103,94 @@ void dgm_destroy(dgm_ctx* c) {
 
 dgm_ctx* dgm_create(const dgm_mesh_desc* mesh, const dgm_tables_desc* tables, const dgm_params* params,
                     int32_t* status) {
-  return create(1, mesh, tables, params, status);
+  return create(1, mesh, nullptr, tables, params, status);
 }
 
 dgm_ctx* dgm_create_batch(int32_t n_instances, const dgm_mesh_desc* meshes, const dgm_tables_desc* tables,
                           const dgm_params* params, int32_t* status) {
-  return create(n_instances, meshes, tables, params, status);
+  return create(n_instances, meshes, nullptr, tables, params, status);
+}
+
+dgm_ctx* dgm_create_batch_slots(int32_t n_instances, const dgm_mesh_desc* meshes, const dgm_slot_capacity* capacity,
+                                const dgm_tables_desc* tables, const dgm_params* params, int32_t* status) {
+  if (!capacity) {
+    if (status) *status = DGM_BAD_ARG;
+    return nullptr;
+  }
+  return create(n_instances, meshes, capacity, tables, params, status);
+}
+
+int32_t dgm_instance_capacity(dgm_ctx* c, int32_t i, dgm_slot_capacity* out) {
+  if (!inst_ok(c, i) || !out) return DGM_BAD_ARG;
+  const HostInst& h = c->inst[i];
+  out->elements = h.elem_cap;
+  out->internal_edges = h.int_cap;
+  out->boundary_edges = h.bnd_cap;
+  out->patches = h.patch_cap;
+  return DGM_OK;
+}
+
+// Takes a new mesh into instance i's capacity ranges: rebuilds the instance's geometry,
+// connectivity, edge slots, patches and limiter visiting order on the host, copies them into its
+// ranges of the device arrays, recomputes its WENO Gram matrices, zeroes its state and resets its
+// clock, loop bounds and status.  The other instances are untouched; the step graphs stay valid
+// (they hold array addresses and sizes, which do not change).
+int32_t dgm_instance_replace(dgm_ctx* c, int32_t i, const dgm_mesh_desc* mesh, const dgm_params* params) {
+  if (!inst_ok(c, i) || !mesh || !params || params->hcr != c->hcr) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  CK(cudaStreamSynchronize(c->stream));  // nothing of this context may still read the old mesh
+  InstArrays a;
+  int st = fill_instance(c, i, mesh, a);
+  if (st) return st;
+  HostInst& h = c->inst[i];
+  const int64_t eo = h.elem_off, cap = h.elem_cap, ld = c->ld;
+  MeshDev* mdp = nullptr;
+  dispatch(c, [&](auto ops) {
+    mdp = &decltype(ops)::mesh(c);
+    return DGM_OK;
+  });
+  if (!mdp) return DGM_BAD_ARG;
+  const MeshDev& md = *mdp;
+  auto put = [&](const void* dst, const void* src, size_t bytes) -> int {
+    if (bytes) CK(cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, c->stream));
+    return DGM_OK;
+  };
+  if ((st = put(md.jac + eo, a.jac.data(), cap * sizeof(double))) || (st = put(md.hmin + eo, a.hmin.data(), cap * sizeof(double))) ||
+      (st = put(md.h15 + eo, a.h15.data(), cap * sizeof(double))) || (st = put(md.inst + eo, a.inst.data(), cap * sizeof(int))) ||
+      (st = put(c->order + eo, a.order.data(), cap * sizeof(int))))
+    return st;
+  for (int k = 0; k < 4; ++k)
+    if ((st = put(md.dinv + k * ld + eo, a.dinv.data() + k * cap, cap * sizeof(double)))) return st;
+  for (int k = 0; k < 3; ++k)
+    if ((st = put(md.face + k * ld + eo, a.face.data() + k * cap, cap * sizeof(int))) ||
+        (st = put(md.nbr + k * ld + eo, a.nbr.data() + k * cap, cap * sizeof(int))))
+      return st;
+  if ((st = put(md.ie_lr + h.int_off, a.ie_lr.data(), h.int_cap * sizeof(int2))) ||
+      (st = put(md.ie_ic + h.int_off, a.ie_ic.data(), h.int_cap * sizeof(int))) ||
+      (st = put(md.ie_geo + h.int_off, a.ie_geo.data(), h.int_cap * sizeof(double4))) ||
+      (st = put(md.slot_ref + h.int_off, a.int_ref.data(), h.int_cap * sizeof(int64_t))) ||
+      (st = put(md.be_elem + h.bnd_off, a.be_elem.data(), h.bnd_cap * sizeof(int))) ||
+      (st = put(md.be_info + h.bnd_off, a.be_info.data(), h.bnd_cap * sizeof(int))) ||
+      (st = put(md.be_geo + h.bnd_off, a.be_geo.data(), h.bnd_cap * sizeof(double4))) ||
+      (st = put(md.slot_ref + c->n_int + h.bnd_off, a.bnd_ref.data(), h.bnd_cap * sizeof(int64_t))) ||
+      (st = put(md.patch_q + h.patch_off, a.patch_q.data(), h.patch_cap * sizeof(double4))))
+    return st;
+  const size_t rec = (size_t)NEQ * c->nb * elem_bytes(c);
+  for (void* p : {c->U, c->U1, c->U2, c->R})
+    CK(cudaMemsetAsync(static_cast<char*>(p) + (size_t)eo * rec, 0, (size_t)cap * rec, c->stream));
+  if (c->limiter && (st = dispatch(c, [&](auto ops) { return decltype(ops)::weno_gram(c, eo, cap); }))) return st;
+  h.ne = mesh->n_elements;
+  h.nb_slots = boundary_edge_count(mesh);
+  h.cfl = params->cfl;
+  h.final_time = params->final_time;
+  h.final_step = params->final_step;
+  h.t = 0.0;
+  h.step = 0;
+  h.status = 0;
+  h.err_where = -1;
+  c->limits_dirty = true;
+  if ((st = upload_ranges(c))) return st;  // synchronizes: the host arrays may go
+  return DGM_OK;
 }
 
 int32_t dgm_instance_upload(dgm_ctx* c, int32_t i, const double* solutions) {
@@ -1413,7 +1655,8 @@ int32_t dgm_phase_launches_per_step(dgm_ctx* c, int32_t phase) {
 
 int32_t dgm_launches_per_step(dgm_ctx* c) {
   if (!c) return 0;
-  return 1 /* step head: loop condition + time step */ + 1 /* step end */ + 3 * (2 + (c->limiter ? 1 : 0));
+  return 1 /* step head: loop condition + time step */ + 1 /* step end */ +
+         3 * (2 + (c->limiter ? 2 /* detection, waves */ : 0));
 }
 
 int64_t dgm_error_location(dgm_ctx* c) { return c ? c->err_where : -1; }

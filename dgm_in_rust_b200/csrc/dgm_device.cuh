@@ -133,6 +133,8 @@ struct Control {
   int waves;                   // limiter waves of the last pass
   int unknown[2];              // barrier schedule: per-wave count of unsettled cells (double-buffered)
   int wl_count[2];             // barrier schedule: per-wave worklist length (double-buffered)
+  int wl1_count;               // cells the detection enlisted for wave 1
+  int pend_count;              // elements the detection left for later waves
   unsigned int bar_count, bar_gen;  // grid barrier of the limiter kernel
   unsigned int head_done;      // blocks of k_step_head that have finished (last one closes the step head)
   unsigned int lim_exit;       // queue schedule: blocks that have left the pass (the last one resets the queues)
@@ -169,6 +171,14 @@ __device__ __forceinline__ void raise_status(Control* ctl, InstCtl* ic, int code
 template <typename T>
 __device__ __forceinline__ T ld_state(const T* p) { return __ldcg(p); }
 
+// State load for a kernel that either only reads the array (RO: through L1, where neighbouring
+// lanes' gathers reuse each other's lines) or writes it while reading (L2 only, always coherent).
+template <bool RO, typename T>
+__device__ __forceinline__ T ld_st(const T* p) {
+  if constexpr (RO) return __ldg(p);
+  else return __ldcg(p);
+}
+
 // Index of coefficient (v, b) of element e in an element-major state array.
 template <int NB>
 __host__ __device__ __forceinline__ size_t sx(int e, int v, int b) {
@@ -178,7 +188,7 @@ __host__ __device__ __forceinline__ size_t sx(int e, int v, int b) {
 // The NB modes of variable VAR of element e (L2 loads), converted to FP64, with the widest loads
 // the block's alignment allows (its byte offset in the 16-byte aligned record is known at compile
 // time): 16-byte loads for the density block and most others, 8- or 4-byte ones otherwise.
-template <int NB, typename T, int VAR>
+template <int NB, typename T, int VAR, bool RO = false>
 __device__ __forceinline__ void load_var_modes(const T* __restrict__ U, int e, double (&out)[NB]) {
   constexpr int OFF = VAR * NB * (int)sizeof(T);  // byte offset of the block in the record
   constexpr int ALIGN = (OFF % 16 == 0) ? 16 : (OFF % 8 == 0) ? 8 : 4;
@@ -186,33 +196,33 @@ __device__ __forceinline__ void load_var_modes(const T* __restrict__ U, int e, d
   if constexpr (std::is_same<T, double>::value && ALIGN == 16) {
 #pragma unroll
     for (int i = 0; i < NB / 2; ++i) {
-      const double2 x = __ldcg(reinterpret_cast<const double2*>(p) + i);
+      const double2 x = ld_st<RO>(reinterpret_cast<const double2*>(p) + i);
       out[2 * i] = x.x;
       out[2 * i + 1] = x.y;
     }
-    if constexpr (NB % 2) out[NB - 1] = __ldcg(p + NB - 1);
+    if constexpr (NB % 2) out[NB - 1] = ld_st<RO>(p + NB - 1);
   } else if constexpr (std::is_same<T, float>::value && ALIGN == 16) {
 #pragma unroll
     for (int i = 0; i < NB / 4; ++i) {
-      const float4 x = __ldcg(reinterpret_cast<const float4*>(p) + i);
+      const float4 x = ld_st<RO>(reinterpret_cast<const float4*>(p) + i);
       out[4 * i] = x.x;
       out[4 * i + 1] = x.y;
       out[4 * i + 2] = x.z;
       out[4 * i + 3] = x.w;
     }
 #pragma unroll
-    for (int i = NB / 4 * 4; i < NB; ++i) out[i] = __ldcg(p + i);
+    for (int i = NB / 4 * 4; i < NB; ++i) out[i] = ld_st<RO>(p + i);
   } else if constexpr (std::is_same<T, float>::value && ALIGN == 8) {
 #pragma unroll
     for (int i = 0; i < NB / 2; ++i) {
-      const float2 x = __ldcg(reinterpret_cast<const float2*>(p) + i);
+      const float2 x = ld_st<RO>(reinterpret_cast<const float2*>(p) + i);
       out[2 * i] = x.x;
       out[2 * i + 1] = x.y;
     }
-    if constexpr (NB % 2) out[NB - 1] = __ldcg(p + NB - 1);
+    if constexpr (NB % 2) out[NB - 1] = ld_st<RO>(p + NB - 1);
   } else {
 #pragma unroll
-    for (int i = 0; i < NB; ++i) out[i] = (double)__ldcg(p + i);
+    for (int i = 0; i < NB; ++i) out[i] = (double)ld_st<RO>(p + i);
   }
 }
 
@@ -289,11 +299,18 @@ __device__ __forceinline__ int hllc(const T lv[4], const T rv[4], T nx, T ny, co
     if (ql0 < 0.0 || qr0 < 0.0) return ST_NEG_DENSITY;
     if (pl < 0.0 || pr < 0.0) return ST_NEG_PRESSURE;
   } else {
-    const double dl0 = lv[0], dr0 = rv[0];
-    if (dl0 < 0.0 || dr0 < 0.0) return ST_NEG_DENSITY;
-    const double dpl = gas.gm1 * ((double)lv[3] - 0.5 * ((double)lv[1] * lv[1] + (double)lv[2] * lv[2]) / dl0);
-    const double dpr = gas.gm1 * ((double)rv[3] - 0.5 * ((double)rv[1] * rv[1] + (double)rv[2] * rv[2]) / dr0);
-    if (dpl < 0.0 || dpr < 0.0) return ST_NEG_PRESSURE;
+    // the sign of an FP32 density is the sign of its FP64 value: no FP64 arithmetic needed
+    if (lv[0] < 0.0f || rv[0] < 0.0f) return ST_NEG_DENSITY;
+    // The FP32 pressure is within a few FP32 ulps of max(E, kinetic energy) of the FP64 pressure of
+    // the same traces, so where it exceeds 1e-4 |E| the FP64 pressure is positive as well; only
+    // pressures that are small against the energy are decided in FP64 (same decisions as always
+    // evaluating in FP64, at a fraction of the cost).
+    if (!(pl > 1e-4f * fabsf(ql3)) || !(pr > 1e-4f * fabsf(qr3))) {
+      const double dl0 = lv[0], dr0 = rv[0];
+      const double dpl = gas.gm1 * ((double)lv[3] - 0.5 * ((double)lv[1] * lv[1] + (double)lv[2] * lv[2]) / dl0);
+      const double dpr = gas.gm1 * ((double)rv[3] - 0.5 * ((double)rv[1] * rv[1] + (double)rv[2] * rv[2]) / dr0);
+      if (dpl < 0.0 || dpr < 0.0) return ST_NEG_PRESSURE;
+    }
   }
   const T cl = sqrt(hcr * pl * rl);
   const T cr = sqrt(hcr * pr * rr);
@@ -731,6 +748,7 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
     ctl->t0_count = 0;
     ctl->unknown[0] = ctl->unknown[1] = 0;
     ctl->wl_count[0] = ctl->wl_count[1] = 0;
+    ctl->wl1_count = ctl->pend_count = 0;
     ctl->lim_exit = 0u;
     for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
   }
@@ -744,6 +762,7 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
   const int inst = m.n_inst > 1 ? m.inst[e] : 0;
   const bool valid = e_raw < m.ne && kp.ic[inst].active;
   const unsigned int keep = __ballot_sync(0xffffffffu, valid) & 0xffu;  // lanes 0-7: var 0 of each element
+  if (!keep) return;  // no element of this warp is stepping (finished instances, slot padding)
   const size_t ld = m.ld;
   T* sbuf = s_rec[threadIdx.x >> 5];
   T* mine_rec = sbuf + i * STRIDE + var * NB;
@@ -791,7 +810,6 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
       for (int b = 0; b < NB; ++b) r[b] += fv * kp.t.phi_edge[k][gp][b];
     }
   }
-  if (!keep) return;  // no element of this warp is stepping
   const T dt = T(kp.ic[inst].dt);
   const T inv_half_j = T(1) / (T(0.5) * J);
   if constexpr (MODE == 0) {  // compute_residuals adds to the residual it is given
@@ -838,7 +856,7 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
 // `own` is e's record (the limiter stages its warp's records in shared memory); the
 // neighbours' modes are read from U through L2.
 // ------------------------------------------------------------------------------------------
-template <int P, typename T>
+template <int P, typename T, bool RO = false>
 __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restrict__ U, int e, const T* own) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
@@ -861,8 +879,8 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
       double rho = 0.0, rho_e = 0.0;
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        rho += (double)own[0 * NB + b] * kp.d.phi_edge[k][g][b];
-        rho_e += (double)own[3 * NB + b] * kp.d.phi_edge[k][g][b];
+        rho += (double)ld_st<RO>(&own[0 * NB + b]) * kp.d.phi_edge[k][g][b];
+        rho_e += (double)ld_st<RO>(&own[3 * NB + b]) * kp.d.phi_edge[k][g][b];
       }
       own_rho[g] = rho;
       own_rhoe[g] = rho_e;
@@ -873,15 +891,15 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
     double rho_u = 0.0, rho_v = 0.0;
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      rho_u += (double)own[1 * NB + b] * kp.d.phi_edge[k][cg][b];
-      rho_v += (double)own[2 * NB + b] * kp.d.phi_edge[k][cg][b];
+      rho_u += (double)ld_st<RO>(&own[1 * NB + b]) * kp.d.phi_edge[k][cg][b];
+      rho_v += (double)ld_st<RO>(&own[2 * NB + b]) * kp.d.phi_edge[k][cg][b];
     }
     if (rho_u * nx + rho_v * ny < 0.0) {
       double rho_jump = 0.0, rho_e_jump = 0.0;
       const double jd = geo.w;
       double nrho[NB], nrhoe[NB];
-      load_var_modes<NB, T, 0>(U, nb, nrho);
-      load_var_modes<NB, T, 3>(U, nb, nrhoe);
+      load_var_modes<NB, T, 0, RO>(U, nb, nrho);
+      load_var_modes<NB, T, 3, RO>(U, nb, nrhoe);
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
         double er = 0.0, ere = 0.0;
@@ -910,7 +928,7 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
 // than kxrcf (which walks the faces one after another) at the price of registers: faster when
 // a pass is latency-bound (small meshes), slower when occupancy matters (large batches); the
 // autotuner picks one per context.  Same arithmetic in the same order, so the same flags.
-template <int P, typename T>
+template <int P, typename T, bool RO = false>
 __device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* __restrict__ U, int e,
                                              const T* own_rec) {
   int fw[3], nb[3];
@@ -926,7 +944,7 @@ __device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* _
 #pragma unroll
   for (int v = 0; v < NEQ; ++v)
 #pragma unroll
-    for (int b = 0; b < NB; ++b) own[v][b] = (double)own_rec[v * NB + b];
+    for (int b = 0; b < NB; ++b) own[v][b] = (double)ld_st<RO>(&own_rec[v * NB + b]);
   double nx[3], ny[3], jd[3];
   bool interior[3];
 #pragma unroll
@@ -957,8 +975,8 @@ __device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* _
   for (int k = 0; k < 3; ++k)
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      ext_rho[k][b] = inflow[k] ? (double)ld_state(&U[sx<NB>(nb[k], 0, b)]) : 0.0;
-      ext_rhoe[k][b] = inflow[k] ? (double)ld_state(&U[sx<NB>(nb[k], 3, b)]) : 0.0;
+      ext_rho[k][b] = inflow[k] ? (double)ld_st<RO>(&U[sx<NB>(nb[k], 0, b)]) : 0.0;
+      ext_rhoe[k][b] = inflow[k] ? (double)ld_st<RO>(&U[sx<NB>(nb[k], 3, b)]) : 0.0;
     }
   double density_jump = 0.0, total_energy_jump = 0.0, surface = 0.0;
   double min_density = 1.0e10, min_total_energy = 1.0e10;
@@ -1046,16 +1064,16 @@ __device__ __forceinline__ double gram_entry(const double* __restrict__ dref, co
   return acc;
 }
 
-// Setup kernel: every element's Gram matrix (upper triangle, pair-major), one thread per
-// (pair, element); a warp shares its pair, so the table reads are uniform.
+// Setup kernel: the Gram matrices of elements [e0, e0 + count) (upper triangle, pair-major), one
+// thread per (pair, element); a warp shares its pair, so the table reads are uniform.
 template <int P, typename T>
-__global__ void k_weno_gram(const __grid_constant__ KParams<P, T> kp, double* __restrict__ gram) {
+__global__ void k_weno_gram(const __grid_constant__ KParams<P, T> kp, double* __restrict__ gram, int e0, int count) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NPAIR = NB * (NB + 1) / 2;
   const MeshDev& m = kp.m;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)NPAIR * m.ne) return;
-  const int pr = (int)(i / m.ne), e = (int)(i - (long long)pr * m.ne);
+  if (i >= (long long)NPAIR * count) return;
+  const int pr = (int)(i / count), e = e0 + (int)(i - (long long)pr * count);
   int b = 0, c = pr;
   while (c >= NB - b) {
     c -= NB - b;
@@ -1343,10 +1361,20 @@ timeout:
 //     neighbours -- again what the sequential loop reads;
 //   * elements that settle in the same wave never read one another, so in-place writes are
 //     race free.
-// Wave 1 also evaluates modified_kxrcf on every element (the parallel flags t0).  In each wave
-// every warp scans 32 elements at a time, settles the clean ready ones and enlists the troubled
-// ready ones in the wave's queue; the enlisted elements are then reconstructed, one per warp.
-// Two schedules, same results bit for bit:
+// Status word per element: (wave << 2) | kind, kind 1 clean, 2 limited, 0 not settled yet.  Wave
+// count = longest chain of increasing-index neighbours through unsettled elements: 2 on the
+// O-grid's 2-colour numbering.  Instances never share neighbours, so one pass limits all of them;
+// elements of instances that are not stepping settle clean without evaluation.
+//
+// Two launches per pass.  k_lim_detect evaluates modified_kxrcf on every element (the parallel
+// flags t0 of wave 1) with one lane per element at full occupancy, visiting the elements in a
+// breadth-first order of the element graph so that the neighbour traces it gathers are mostly in
+// cache; it settles the clean elements without a lower-index neighbour, enlists the troubled ones
+// for wave 1 (wl1) and lists the elements that wait for a lower neighbour (pend).  k_limiter, a
+// cooperative persistent kernel, then reconstructs wave 1's cells (one warp each), and runs waves
+// 2, 3, ... over the pending list: each wave scans it, settles clean ready elements, enlists
+// troubled ready ones and reconstructs them, with a grid barrier between waves.  Within a wave,
+// two schedules join the scan and the reconstruction, with bitwise identical results:
 //   * QUEUE = false: a grid barrier separates the scan from the reconstruction, warps take the
 //     worklist's entries in a fixed stride (the entries stay behind after the pass);
 //   * QUEUE = true: a warp that has finished its scan takes tickets from the queue and
@@ -1354,184 +1382,202 @@ timeout:
 //     w rewrites an element all of whose lower neighbours settled before wave w, so the only
 //     concurrent reads of it are wave-1 flags of its higher neighbours, and those flags are never
 //     used (a higher neighbour of a rewritten element is re-evaluated in a later wave).
-// A grid barrier ends every wave but the last.  Status word: (wave << 2) | kind, kind 1 clean,
-// 2 limited.  Wave count = longest chain of increasing-index neighbours through unsettled
-// elements: 2 on the O-grid's 2-colour numbering.  Instances never share neighbours, so one pass
-// limits all of them; elements of instances that are not stepping settle clean without evaluation.
-template <int P, typename T, bool STAGED, bool QUEUE>
-__global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_constant__ KParams<P, T> kp,
-                                                                T* __restrict__ U, unsigned char* __restrict__ t0,
-                                                                unsigned int* __restrict__ status,
-                                                                int* __restrict__ work) {
+constexpr int kDetectThreads = 128;
+
+template <int P, typename T, bool STAGED>
+__global__ void __launch_bounds__(kDetectThreads) k_lim_detect(const __grid_constant__ KParams<P, T> kp,
+                                                               const T* __restrict__ U,
+                                                               unsigned char* __restrict__ t0,
+                                                               unsigned int* __restrict__ status,
+                                                               int* __restrict__ wl1, int* __restrict__ pend,
+                                                               const int* __restrict__ order) {
+  using V = Variant<P>;
   Control* ctl = kp.ctl;
   const MeshDev& m = kp.m;
-  // per warp: the WENO scratch while reconstructing, the batch's 32 element records while scanning
-  constexpr int STRIDE = Staged<Variant<P>::NB, T>::kStride;
-  constexpr size_t kWarpNeed = (sizeof(WenoScratch<P>) > 32 * STRIDE * sizeof(T) ? sizeof(WenoScratch<P>)
-                                                                                   : 32 * STRIDE * sizeof(T));
-  constexpr size_t kWarpBytes = (kWarpNeed + 127) / 128 * 128;  // every warp's buffer 16-byte aligned
-  static_assert(kWarpBytes % 16 == 0, "16-byte record copies need 16-byte aligned warp buffers");
+  const int lane = threadIdx.x & 31;
+  const int pos = blockIdx.x * kDetectThreads + threadIdx.x;
+  bool flag = false, enlist = false, wait = false;
+  int e = 0;
+  if (pos < m.ne) {
+    e = order[pos];
+    const int inst = m.n_inst > 1 ? m.inst[e] : 0;
+    if (kp.ic[inst].active) {
+      const T* own = U + (size_t)e * (NEQ * V::NB);
+      flag = STAGED ? kxrcf_staged<P, T, true>(kp, U, e, own) : kxrcf<P, T, true>(kp, U, e, own);
+      bool ready = true;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int nb = m.nbr[k * m.ld + e];
+        if (nb >= 0 && nb < e) ready = false;
+      }
+      wait = !ready;
+      enlist = ready && flag;
+    }
+    t0[e] = flag ? 1 : 0;
+    status[e] = (wait || enlist) ? 0u : ((1u << 2) | 1u);  // not stepping or clean and ready: settled
+  }
+  const unsigned int below = (1u << lane) - 1u;
+  const unsigned int fm = __ballot_sync(0xffffffffu, flag);
+  if (fm && lane == 0) atomicAdd(&ctl->t0_count, __popc(fm));
+  const unsigned int em = __ballot_sync(0xffffffffu, enlist);
+  if (em) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&ctl->wl1_count, __popc(em));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (enlist) wl1[base + __popc(em & below)] = e;
+  }
+  const unsigned int wm = __ballot_sync(0xffffffffu, wait);
+  if (wm) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&ctl->pend_count, __popc(wm));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (wait) pend[base + __popc(wm & below)] = e;
+  }
+}
+
+template <int P, typename T, bool QUEUE>
+__global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_constant__ KParams<P, T> kp,
+                                                                T* __restrict__ U,
+                                                                const unsigned char* __restrict__ t0,
+                                                                unsigned int* __restrict__ status,
+                                                                int* __restrict__ work,
+                                                                const int* __restrict__ wl1,
+                                                                const int* __restrict__ pend) {
+  Control* ctl = kp.ctl;
+  const MeshDev& m = kp.m;
+  constexpr size_t kWarpBytes = (sizeof(WenoScratch<P>) + 127) / 128 * 128;
   __shared__ __align__(128) unsigned char s_warp[kLimiterWarps][kWarpBytes];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   WenoScratch<P>* scratch_w = reinterpret_cast<WenoScratch<P>*>(s_warp[wib]);
-  T* recs = reinterpret_cast<T*>(s_warp[wib]);
   const int gwarp = blockIdx.x * kLimiterWarps + wib;
   const int nwarps = gridDim.x * kLimiterWarps;
+  // the detection launch has finished: its counts are final
+  const int flagged = ctl->t0_count;
+  const int n_wl1 = ctl->wl1_count;
+  const int n_pend = ctl->pend_count;
   int troubled_local = 0;
   int wave = 1;
-  for (;; ++wave) {
-    LimQueue* q = &ctl->lq[wave % 3];
-    // the queue of wave w + 1 was last used by wave w - 2, whose readers all passed a barrier since
-    if (QUEUE && wave >= 2 && blockIdx.x == 0 && threadIdx.x == 0) reset_queue(ctl->lq[(wave + 1) % 3]);
-    // ---- scan: readiness, settle clean elements, enlist troubled ones ----
-    int unknown_local = 0, flagged_local = 0;
-    for (int base = gwarp * 32; base < m.ne; base += nwarps * 32) {
-      const int e = base + lane;
-      bool pending = false, ready = false, trouble = false, need = false, any_mod = false;
-      if (e < m.ne) {
-        if (wave == 1) {
-          const int inst = m.n_inst > 1 ? m.inst[e] : 0;
-          if (kp.ic[inst].active) {
-            need = true;  // the parallel flag t0 of every stepping element
-            pending = true;
-          } else {
-            ready = true;  // not stepping: settles clean, never read as rewritten
-          }
-        } else {
-          pending = (__ldcg(&status[e]) & 3u) == 0u;
-        }
-        if (pending) {
-          ready = true;
+  // reconstruction of one enlisted element by the whole warp
+  auto reconstruct = [&](int et) {
+    int fwt[3], nbt[3];
 #pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const int nb = m.nbr[k * m.ld + e];
-            if (nb >= 0 && nb < e) {
-              if (wave == 1) {
-                ready = false;
-              } else {
+    for (int k = 0; k < 3; ++k) {
+      fwt[k] = m.face[k * m.ld + et];
+      nbt[k] = m.nbr[k * m.ld + et];
+    }
+    const int rs = weno_reconstruct<P, T>(kp, U, et, fwt, nbt, lane, *scratch_w);
+    if (rs != ST_OK && lane == 0) {
+      const int inst = m.n_inst > 1 ? m.inst[et] : 0;
+      raise_status(ctl, &kp.ic[inst], rs, et);
+    }
+  };
+  if (flagged > 0) {  // else no element is limited: every block leaves at once
+    // ---- wave 1: the cells enlisted by the detection (the list is complete) ----
+    for (int i = gwarp; i < n_wl1; i += nwarps) {
+      const int et = __ldcg(&wl1[i]);
+      reconstruct(et);
+      if (lane == 0) status[et] = (1u << 2) | 2u;
+      ++troubled_local;
+    }
+    // ---- waves 2, 3, ...: the elements that waited for a lower neighbour ----
+    bool more = n_pend > 0;
+    if (more && !grid_barrier(ctl, gridDim.x)) more = false;
+    for (wave = 2; more; ++wave) {
+      LimQueue* q = &ctl->lq[wave % 3];
+      // the queue of wave w + 1 was last used by wave w - 2, whose readers all passed a barrier since
+      if (QUEUE && blockIdx.x == 0 && threadIdx.x == 0) reset_queue(ctl->lq[(wave + 1) % 3]);
+      int unknown_local = 0;
+      for (int base = gwarp * 32; base < n_pend; base += nwarps * 32) {
+        const int i = base + lane;
+        const int e = i < n_pend ? __ldcg(&pend[i]) : 0;
+        bool pending = false, ready = false, trouble = false, any_mod = false;
+        if (i < n_pend) {
+          pending = (__ldcg(&status[e]) & 3u) == 0u;
+          if (pending) {
+            ready = true;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+              const int nb = m.nbr[k * m.ld + e];
+              if (nb >= 0 && nb < e) {
                 const unsigned int sn = __ldcg(&status[nb]);
                 if ((sn & 3u) == 0u || (int)(sn >> 2) >= wave) ready = false;
                 else if ((sn & 3u) == 2u) any_mod = true;
               }
             }
           }
-          if (wave > 1 && ready && any_mod) need = true;  // a lower neighbour was rewritten
         }
-      }
-      // modified_kxrcf of the lanes that need it.  Wave 1 evaluates every element: the batch's 32
-      // records (contiguous) are staged in shared memory with coalesced 16-byte loads through L2.
-      // Later waves re-evaluate only the few elements next to rewritten cells, each reading its own
-      // record directly (it is still pending, so nothing has rewritten it in this pass)
-      bool flag = false;
-      if (wave == 1) {
-        if (__any_sync(0xffffffffu, need)) {
-          warp_load_records<Variant<P>::NB, T, 32>(U, base, recs, lane);
-          if (need)
-            flag = STAGED ? kxrcf_staged<P, T>(kp, U, e, recs + lane * STRIDE)
-                          : kxrcf<P, T>(kp, U, e, recs + lane * STRIDE);
+        // modified_kxrcf again only next to rewritten cells, each element reading its own record
+        // (it is still pending, so nothing has rewritten it in this pass)
+        if (pending && ready) {
+          if (any_mod) {
+            const T* own = U + (size_t)e * (NEQ * Variant<P>::NB);
+            trouble = kxrcf<P, T>(kp, U, e, own);
+          } else {
+            trouble = t0[e] != 0;
+          }
+          if (!trouble) status[e] = ((unsigned int)wave << 2) | 1u;
         }
-      } else if (need) {
-        const T* own = U + (size_t)e * (NEQ * Variant<P>::NB);
-        flag = STAGED ? kxrcf_staged<P, T>(kp, U, e, own) : kxrcf<P, T>(kp, U, e, own);
-      }
-      if (e < m.ne) {
-        if (wave == 1) {
-          t0[e] = flag ? 1 : 0;
-          flagged_local += flag ? 1 : 0;
+        const unsigned int tb = __ballot_sync(0xffffffffu, ready && trouble);
+        if (tb) {
+          int slot0 = 0;
+          if (lane == 0) slot0 = atomicAdd(QUEUE ? &q->tail : &ctl->wl_count[wave & 1], __popc(tb));
+          slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+          if (ready && trouble) work[slot0 + __popc(tb & ((1u << lane) - 1u))] = QUEUE ? e + 1 : e;
         }
-        if (pending && ready) trouble = (wave == 1 || any_mod) ? flag : (t0[e] != 0);
-        if (wave == 1 && !ready) status[e] = 0u;
-        if (ready && !trouble) status[e] = ((unsigned int)wave << 2) | 1u;
+        unknown_local += (pending && !ready) ? 1 : 0;
       }
-      const unsigned int tb = __ballot_sync(0xffffffffu, ready && trouble);
-      if (tb) {
-        int slot0 = 0;
-        if (lane == 0) slot0 = atomicAdd(QUEUE ? &q->tail : &ctl->wl_count[wave & 1], __popc(tb));
-        slot0 = __shfl_sync(0xffffffffu, slot0, 0);
-        if (ready && trouble) work[slot0 + __popc(tb & ((1u << lane) - 1u))] = QUEUE ? e + 1 : e;
-      }
-      unknown_local += (pending && !ready) ? 1 : 0;
-    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      unknown_local += __shfl_xor_sync(0xffffffffu, unknown_local, o);
-      flagged_local += __shfl_xor_sync(0xffffffffu, flagged_local, o);
-    }
-    // reconstruction of one enlisted element by the whole warp
-    auto reconstruct = [&](int et) {
-      int fwt[3], nbt[3];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        fwt[k] = m.face[k * m.ld + et];
-        nbt[k] = m.nbr[k * m.ld + et];
+      for (int o = 16; o > 0; o >>= 1) unknown_local += __shfl_xor_sync(0xffffffffu, unknown_local, o);
+      int remaining = 0;
+      if (!QUEUE) {
+        if (lane == 0 && unknown_local) atomicAdd(&ctl->unknown[wave & 1], unknown_local);
+        if (!grid_barrier(ctl, gridDim.x)) break;
+        const int n_work = *((volatile int*)&ctl->wl_count[wave & 1]);
+        remaining = *((volatile int*)&ctl->unknown[wave & 1]);
+        // the other parity's counters were last read before the previous wave's second barrier
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+          ctl->wl_count[(wave + 1) & 1] = 0;
+          ctl->unknown[(wave + 1) & 1] = 0;
+        }
+        // ---- reconstruct the enlisted elements, one warp each, in a fixed stride ----
+        for (int i = gwarp; i < n_work; i += nwarps) {
+          const int et = __ldcg(&work[i]);
+          reconstruct(et);
+          __threadfence();
+          if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
+          ++troubled_local;
+        }
+      } else {
+        __syncwarp();
+        if (lane == 0) {
+          if (unknown_local) atomicAdd(&q->unknown, unknown_local);
+          fence_gpu();  // the count before the report that this warp's scan is done
+          atomicAdd(&q->scanned, 1);
+        }
+        // ---- reconstruct enlisted elements from the queue while other warps still scan ----
+        for (;;) {
+          int et = -1;
+          if (lane == 0) et = limiter_ticket(ctl, q, work, m.ne, nwarps);
+          et = __shfl_sync(0xffffffffu, et, 0);
+          if (et < 0) break;
+          reconstruct(et);
+          // no fence: nothing reads this element or its status before the wave's barrier
+          if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
+          ++troubled_local;
+        }
+        // every warp's scan has been reported (the ticket loop ends only then): the count is final
+        if (lane == 0) {
+          fence_gpu();
+          remaining = *((volatile int*)&q->unknown);
+        }
+        remaining = __shfl_sync(0xffffffffu, remaining, 0);
       }
-      const int rs = weno_reconstruct<P, T>(kp, U, et, fwt, nbt, lane, *scratch_w);
-      if (rs != ST_OK && lane == 0) {
-        const int inst = m.n_inst > 1 ? m.inst[et] : 0;
-        raise_status(ctl, &kp.ic[inst], rs, et);
-      }
-    };
-    if (!QUEUE) {
-      if (lane == 0 && unknown_local) atomicAdd(&ctl->unknown[wave & 1], unknown_local);
-      if (lane == 0 && flagged_local) atomicAdd(&ctl->t0_count, flagged_local);
+      if (remaining == 0) break;  // no further wave: nothing reads what this one wrote
       if (!grid_barrier(ctl, gridDim.x)) break;
-      if (wave == 1 && *((volatile int*)&ctl->t0_count) == 0) break;  // nothing to limit
-      const int n_work = *((volatile int*)&ctl->wl_count[wave & 1]);
-      const int remaining = *((volatile int*)&ctl->unknown[wave & 1]);
-      // the other parity's counters were last read before the previous wave's second barrier
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->wl_count[(wave + 1) & 1] = 0;
-        ctl->unknown[(wave + 1) & 1] = 0;
-      }
-      // ---- reconstruct the enlisted elements, one warp each, in a fixed stride ----
-      for (int i = gwarp; i < n_work; i += nwarps) {
-        const int et = __ldcg(&work[i]);
-        reconstruct(et);
-        __threadfence();
-        if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
-        ++troubled_local;
-      }
-      if (remaining == 0) break;  // no further wave: nothing reads what this phase wrote
-    } else {
-      __syncwarp();
-      if (lane == 0) {
-        if (unknown_local) atomicAdd(&q->unknown, unknown_local);
-        if (flagged_local) atomicAdd(&ctl->t0_count, flagged_local);
-        fence_gpu();  // the counts before the report that this warp's scan is done
-        atomicAdd(&q->scanned, 1);
-      }
-      // ---- reconstruct enlisted elements from the queue while other warps still scan ----
-      for (;;) {
-        int et = -1;
-        if (lane == 0) et = limiter_ticket(ctl, q, work, m.ne, nwarps);
-        et = __shfl_sync(0xffffffffu, et, 0);
-        if (et < 0) break;
-        reconstruct(et);
-        // no fence: nothing reads this element or its status before the wave's barrier
-        if (lane == 0) status[et] = ((unsigned int)wave << 2) | 2u;
-        ++troubled_local;
-      }
-      // every warp's scan has been reported (the ticket loop ends only then): the counts are final
-      int remaining = 0, flagged = 0;
-      if (lane == 0) {
-        fence_gpu();
-        remaining = *((volatile int*)&q->unknown);
-        flagged = *((volatile int*)&ctl->t0_count);
-      }
-      remaining = __shfl_sync(0xffffffffu, remaining, 0);
-      flagged = __shfl_sync(0xffffffffu, flagged, 0);
-      if (wave == 1 && flagged == 0) break;  // nothing flagged: no element is limited
-      if (remaining == 0) break;             // no further wave: nothing reads what this one wrote
+      if (wave > m.ne + 2) break;
     }
-    if (!grid_barrier(ctl, gridDim.x)) break;
-    if (wave > m.ne + 2) break;
   }
-  if (!QUEUE) {
-    if (lane == 0 && troubled_local) atomicAdd(&ctl->troubled, troubled_local);
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->waves = wave;
-    return;
-  }
-  // queue schedule: the last block to leave resets the queues for the next pass
+  // the last block to leave resets the pass's counters and queues for the next pass
   __shared__ int s_troubled;
   if (threadIdx.x == 0) s_troubled = 0;
   __syncthreads();
@@ -1543,6 +1589,10 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
     if (atomicAdd(&ctl->lim_exit, 1u) == gridDim.x - 1u) {
       for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
       ctl->t0_count = 0;
+      ctl->wl1_count = 0;
+      ctl->pend_count = 0;
+      ctl->wl_count[0] = ctl->wl_count[1] = 0;
+      ctl->unknown[0] = ctl->unknown[1] = 0;
       ctl->waves = wave;
       ctl->lim_exit = 0u;
     }
@@ -1690,6 +1740,7 @@ __global__ void k_set_active(Control* ctl, InstCtl* ic, int n_inst, double dt, i
     ctl->t0_count = 0;
     ctl->unknown[0] = ctl->unknown[1] = 0;
     ctl->wl_count[0] = ctl->wl_count[1] = 0;
+    ctl->wl1_count = ctl->pend_count = 0;
     ctl->lim_exit = 0u;
     for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
   }
@@ -1709,14 +1760,14 @@ __global__ void k_set_active(Control* ctl, InstCtl* ic, int n_inst, double dt, i
 // forces or norms.
 template <int P, typename T>
 __global__ void __launch_bounds__(256) k_diagnostics(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U,
-                                                     const T* __restrict__ R, const int* __restrict__ elem_off,
-                                                     const int* __restrict__ bslot_off, double* __restrict__ out) {
+                                                     const T* __restrict__ R, const int* __restrict__ elem_rng,
+                                                     const int* __restrict__ bslot_rng, double* __restrict__ out) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG, NQ = V::NQ;
   const MeshDev& m = kp.m;
   const int inst = blockIdx.x;
-  const int e0 = elem_off[inst], e1 = elem_off[inst + 1];
-  const int b0 = bslot_off[inst], b1 = bslot_off[inst + 1];
+  const int e0 = elem_rng[2 * inst], e1 = e0 + elem_rng[2 * inst + 1];
+  const int b0 = bslot_rng[2 * inst], b1 = b0 + bslot_rng[2 * inst + 1];  // boundary slots, relative to n_int
   double wsum = 0.0;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) wsum += kp.d.cell_w[q];

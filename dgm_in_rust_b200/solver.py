@@ -39,6 +39,7 @@ __all__ = [
     "reference_cfl",
     "initial_state",
     "Batch",
+    "slot_capacity",
     "forces_to_coefficients",
 ]
 
@@ -477,6 +478,13 @@ def forces_to_coefficients(fx: float, fy: float, aoa_deg: float, rho: float, spe
     return lift / q, drag / q
 
 
+def slot_capacity(mesh) -> tuple:
+    """The (elements, internal edges, boundary edges, patches) counts of a processed mesh: the
+    least capacity of a batch slot that takes it."""
+    return (int(mesh.n_elements), int(len(mesh.internal_edge_indices)),
+            int(np.count_nonzero(mesh.edge_elements[:, 1] == -1)), int(len(mesh.patch_type)))
+
+
 class Batch:
     """Many independent meshes advanced together: one launch per kernel of a step covers all of
     them (a disconnected union mesh on the device), each with its own time step, clock, loop
@@ -484,7 +492,10 @@ class Batch:
     No counterpart in the reference (one mesh per run)."""
 
     def __init__(self, meshes: list, order: int, hcr: float, cfls, final_times, final_steps,
-                 limiter: bool = True, device: int = 0, precision: str = "fp64"):
+                 limiter: bool = True, device: int = 0, precision: str = "fp64", capacities=None):
+        """``capacities`` (optional): per instance a (elements, internal edges, boundary edges,
+        patches) room at least the mesh's, so that the slot can later take a larger mesh
+        (:meth:`replace`); see :func:`slot_capacity`."""
         self.gauss_points, self.basis = default_tables(order)
         self.meshes = list(meshes)
         n = len(self.meshes)
@@ -497,7 +508,11 @@ class Batch:
                            precision=PRECISIONS[precision], _reserved=0) for i in range(n)])
         L = _native.lib()
         status = ctypes.c_int32(0)
-        ctx = L.dgm_create_batch(n, mds, ctypes.byref(td), prs, ctypes.byref(status))
+        if capacities is None:
+            ctx = L.dgm_create_batch(n, mds, ctypes.byref(td), prs, ctypes.byref(status))
+        else:
+            caps = (_native.SlotCapacity * n)(*[_native.SlotCapacity(*[int(x) for x in cap]) for cap in capacities])
+            ctx = L.dgm_create_batch_slots(n, mds, caps, ctypes.byref(td), prs, ctypes.byref(status))
         if not ctx:
             raise DgmError(status.value, what="dgm_create_batch")
         self._ctx = ctypes.c_void_p(ctx)
@@ -505,6 +520,27 @@ class Batch:
         self.n = n
         self.nb = self.basis.dof
         self.precision = precision
+        self.hcr = hcr
+        self.limiter = limiter
+        self.device = device
+
+    def capacity(self, i: int) -> tuple:
+        """(elements, internal edges, boundary edges, patches) room of slot i."""
+        cap = _native.SlotCapacity()
+        self._check(self._lib.dgm_instance_capacity(self._ctx, i, ctypes.byref(cap)), "capacity")
+        return (cap.elements, cap.internal_edges, cap.boundary_edges, cap.patches)
+
+    def replace(self, i: int, mesh, cfl: float, final_time: float, final_step: int) -> None:
+        """Put ``mesh`` (which must fit slot i's capacity) into slot i, with zeroed state and a
+        reset clock, loop bounds and status; the other instances are untouched.  Waits for the
+        context's stream first."""
+        keep: list = []
+        md = _mesh_desc(mesh, keep)
+        pr = _native.Params(hcr=self.hcr, cfl=float(cfl), final_time=float(final_time), final_step=int(final_step),
+                            limiter=1 if self.limiter else 0, device=self.device,
+                            precision=PRECISIONS[self.precision], _reserved=0)
+        self._check(self._lib.dgm_instance_replace(self._ctx, i, ctypes.byref(md), ctypes.byref(pr)), "replace")
+        self.meshes[i] = mesh
 
     def _check(self, st: int, what: str) -> None:
         if st != 0:

@@ -227,10 +227,10 @@ int32_t dgm_query(dgm_ctx* ctx);
  * (copies, events) against the solver. */
 void* dgm_stream(dgm_ctx* ctx);
 
-/* Diagnostics for per-kernel timing: enqueue one launch of a single kernel of the step on the
- * resident state (phase 0 time step, 1 edge flux, 2 element update (stage-2 form, writes the
- * second stage buffer), 3 limiter (KXRCF + WENO waves) on that buffer).  Callers time it with
- * events on dgm_stream().  No counterpart in the reference (it has no kernels). */
+/* Diagnostics for per-kernel timing: enqueue one phase of the step on the resident state (phase 0
+ * time step, 1 edge flux, 2 element update (stage-2 form, writes the second stage buffer), 3
+ * limiter on that buffer: the KXRCF detection launch and the WENO wave launch).  Callers time it
+ * with events on dgm_stream().  No counterpart in the reference (it has no kernels). */
 int32_t dgm_launch_phase(dgm_ctx* ctx, int32_t phase);
 /* Launch configuration of the edge pass (threads per block; blocks, 0 = one thread per
  * (edge slot, Gauss point), else a grid-stride grid of that many blocks) and of the element pass
@@ -248,19 +248,20 @@ int32_t dgm_autotune(dgm_ctx* ctx, int32_t repeats, double* best_us /* [2] */);
  * the traces at every point (fewer loads per slot).  No counterpart in the reference. */
 int32_t dgm_set_edge_variant(dgm_ctx* ctx, int32_t pair);
 int32_t dgm_get_edge_variant(dgm_ctx* ctx);
-/* The limiter's detector form (modified_kxrcf, weno.rs:7-85, same arithmetic in both): 0 compact
- * (walks the faces in turn: fewer registers, better for large batches), 1 staged (all loads of a
- * round issued together: fewer memory round trips, better for small meshes).  The flags and
- * results are the same.  No counterpart in the reference. */
+/* The form of the limiter's detection launch (modified_kxrcf, weno.rs:7-85, on every element, one
+ * lane each; same arithmetic in both): 0 compact (walks the faces in turn: fewer registers, more
+ * lanes in flight), 1 staged (all loads of a round issued together: fewer memory round trips,
+ * more registers).  The flags and results are the same.  No counterpart in the reference. */
 int32_t dgm_set_limiter_variant(dgm_ctx* ctx, int32_t staged);
 /* Current form, and the limiter times the last dgm_autotune measured for forms 0 and 1 at their
  * faster schedule (us; either pointer may be NULL). */
 int32_t dgm_get_limiter_variant(dgm_ctx* ctx, int32_t* staged, double* tuned_us /* [2] */);
-/* The limiter's schedule (same results bit for bit): 0 barrier (each wave scans every element,
- * passes a grid barrier, then reconstructs the troubled elements it enlisted), 1 queue (warps that
- * have finished the scan already reconstruct enlisted elements while others still scan; no barrier
- * between the two halves of a wave; better when many elements are limited).  No counterpart in
- * the reference. */
+/* The schedule of the limiter's wave launch from wave 2 on (same results bit for bit): 0 barrier
+ * (each wave scans the elements still waiting for a lower-index neighbour, passes a grid barrier,
+ * then reconstructs the troubled elements it enlisted), 1 queue (warps that have finished the scan
+ * already reconstruct enlisted elements while others still scan; no barrier between the two halves
+ * of a wave).  Wave 1's cells, enlisted by the detection launch, are reconstructed first in both.
+ * No counterpart in the reference. */
 int32_t dgm_set_limiter_schedule(dgm_ctx* ctx, int32_t queue);
 /* Current schedule, and the best limiter times the last dgm_autotune measured with schedules 0
  * and 1 (us; either pointer may be NULL). */
@@ -280,6 +281,27 @@ int32_t dgm_launches_per_step(dgm_ctx* ctx);
 dgm_ctx* dgm_create_batch(int32_t n_instances, const dgm_mesh_desc* meshes, const dgm_tables_desc* tables,
                           const dgm_params* params, int32_t* status);
 int32_t dgm_instance_count(dgm_ctx* ctx);
+
+/* Slots: a batch whose instances reserve room for larger meshes, so that a finished instance's slot
+ * can take a new mesh without a new context (continuous batching: a new solve joins the running
+ * launches as soon as a slot is free).  capacity[i] gives instance i's room (each at least its
+ * initial mesh's count: elements, internal edges, boundary edges, patches); the room of every
+ * instance stays in the union mesh, padding included, and costs device memory like elements of
+ * their own.  dgm_instance_replace puts `mesh` (which must fit instance i's capacity) and the loop
+ * bounds and CFL number of `params` into slot i: the instance's state is zeroed, its clock, loop
+ * bounds and status are reset (set its initial solution next), and the other instances are not
+ * touched; the call waits for the context's stream first.  Results of every instance are the same
+ * in a slot as in an exact-size batch or alone.  No counterpart in the reference. */
+typedef struct dgm_slot_capacity {
+  int64_t elements;
+  int64_t internal_edges;
+  int64_t boundary_edges;
+  int64_t patches;
+} dgm_slot_capacity;
+dgm_ctx* dgm_create_batch_slots(int32_t n_instances, const dgm_mesh_desc* meshes, const dgm_slot_capacity* capacity,
+                                const dgm_tables_desc* tables, const dgm_params* params, int32_t* status);
+int32_t dgm_instance_replace(dgm_ctx* ctx, int32_t i, const dgm_mesh_desc* mesh, const dgm_params* params);
+int32_t dgm_instance_capacity(dgm_ctx* ctx, int32_t i, dgm_slot_capacity* capacity);
 /* State of instance i in the reference layout, host <-> device-resident state. */
 int32_t dgm_instance_upload(dgm_ctx* ctx, int32_t i, const double* solutions);
 int32_t dgm_instance_download(dgm_ctx* ctx, int32_t i, double* solutions);
@@ -331,19 +353,24 @@ const char* dgm_status_string(int32_t status);
 
 /* ---- allocation-free variant ------------------------------------------------------------ */
 
-/* The CFL time step (the minimum of TemperalDisc::compute_time_step) for callers that cannot
- * allocate device memory: hosts whose device memory belongs to another allocator, code running
- * while a stream is captured into a CUDA graph, real-time loops.  It needs no dgm_ctx and calls
- * no cudaMalloc/cudaFree: the caller passes device pointers to the state in the reference layout
+/* The CFL time step -- the minimum over the elements of cfl * h_min / (|u| + c), with the state of
+ * each element taken as the sum of its modal coefficients -- for callers that cannot allocate
+ * device memory: hosts whose device memory belongs to another allocator, code running while a
+ * stream is captured into a CUDA graph, real-time loops.  It needs no dgm_ctx and calls no
+ * cudaMalloc/cudaFree: the caller passes device pointers to the state in the layout
  * [n_elements][4][n_basis] and to the element minimum heights [n_elements], and a device double
- * that receives the time step; the work is enqueued on `stream` (cudaStream_t, NULL = default).
- * Scratch is a fixed 32 KiB array in the library image (every GPU that loads the library holds
- * it until exit) of 4096 per-block minima, which caps n_elements at 8,388,608: larger sizes
- * return DGM_BAD_ARG without launching anything.  Every used scratch slot is rewritten by every
- * call; calls that overlap on the GPU (other streams, other host threads) share the array and
- * race.  The first call on a device looks up the array's device address (cudaGetSymbolAddress)
- * with that device current; make that first call before any stream capture.  This entry point
- * has no counterpart in the reference, which allocates freely. */
+ * that receives the time step (1e10 when no element gives a smaller finite value); the work is
+ * enqueued on `stream` (cudaStream_t, NULL = default).  cfl must be > 0 and hcr > 1, else
+ * DGM_BAD_ARG.  Scratch is a fixed 32 KiB array in the library image (every GPU that loads the
+ * library holds it until exit) of 4096 per-block minima, which caps n_elements at 8,388,608:
+ * larger sizes return DGM_BAD_ARG without launching anything.  Every used scratch slot is
+ * rewritten by every call; calls that overlap on the GPU (other streams, other host threads) share
+ * the array and race.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current and keeps it for the life of the process: make
+ * that first call before any stream capture, and make no call after a cudaDeviceReset of a device
+ * already used (the kept address is then stale).  A CUDA error left pending by earlier work is
+ * returned as DGM_CUDA_ERROR before anything is launched and stays pending.  This entry point has
+ * no counterpart in the reference, which allocates freely. */
 int32_t dgm_compute_time_step_noalloc(const double* solutions, const double* minimum_height,
                                       int64_t n_elements, int32_t n_basis, double cfl, double hcr,
                                       double* time_step, void* stream);

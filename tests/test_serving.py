@@ -26,8 +26,10 @@ class FakeBatch:
     created = 0
     hold_first_s = 0.0
 
-    def __init__(self, meshes, order, hcr, cfls, final_times, final_steps, limiter=True, device=0, precision="fp32"):
-        self.meshes = meshes
+    def __init__(self, meshes, order, hcr, cfls, final_times, final_steps, limiter=True, device=0, precision="fp32",
+                 capacities=None):
+        self.meshes = list(meshes)
+        self.capacities = capacities
         self.order = order
         self.precision = precision
         self.n = len(meshes)
@@ -61,7 +63,19 @@ class FakeBatch:
         return 0
 
     def device_bytes(self):
-        return footprint_bytes(self.meshes, self.order, self.precision)
+        return footprint_bytes(self.meshes, self.order, self.precision, capacities=self.capacities)
+
+    replaced = 0
+
+    def replace(self, i, mesh, cfl, final_time, final_step):
+        assert self.polls == 0, "a slot is replaced only while the cohort is idle"
+        need = serving.slot_capacity(mesh)
+        assert all(n <= r for n, r in zip(need, self.capacities[i]))
+        self.meshes[i] = mesh
+        self.step[i] = 0
+        self.final[i] = final_step
+        self.uploaded[i] = False
+        FakeBatch.replaced += 1
 
     def diagnostics(self, use_residual=False):
         out = np.zeros((self.n, 8))
@@ -86,6 +100,7 @@ class FakeBatch:
 def fake_batch(monkeypatch):
     FakeBatch.live = 0
     FakeBatch.created = 0
+    FakeBatch.replaced = 0
     monkeypatch.setattr(serving, "Batch", FakeBatch)
     yield FakeBatch
     assert FakeBatch.live == 0, "every cohort context is closed"
@@ -137,7 +152,9 @@ def test_cohorts_are_packed_per_order(fake_batch):
 
 def test_budget_admits_first_come_first_served(fake_batch):
     reqs = _reqs([(16, 1), (40, 2), (16, 1), (16, 1)], gap=0.02)
-    one = max(footprint_bytes([instance_mesh(r.instance)[0]], r.instance.order, "fp32") for r in reqs)
+    room = [serving._room(serving.slot_capacity(instance_mesh(r.instance)[0]), 1.5) for r in reqs]
+    one = max(footprint_bytes([instance_mesh(r.instance)[0]], r.instance.order, "fp32", capacities=[c])
+              for r, c in zip(reqs, room))
     FakeBatch.lag = 300
     try:
         loop = ServingLoop(prep="thread", hbm_budget_bytes=one, chunk_steps=64, tol=1e-3, max_steps=100, window_s=0.0)
@@ -266,3 +283,25 @@ def test_active_work_cap_admits_in_order(fake_batch):
     admitted = [r.admitted_s for r in res]
     assert admitted == sorted(admitted)
     assert min(res[2].admitted_s, res[3].admitted_s) >= min(res[0].finished_s, res[1].finished_s)
+
+
+def test_freed_slots_take_waiting_requests(fake_batch):
+    """With room for two requests' elements in flight, requests 2 and 3 (same order and size) wait
+    and then take the slots that requests 0 and 1 free, inside the running cohort: no new context,
+    admission in arrival order, each result on its own check schedule."""
+    reqs = _reqs([(16, 1), (16, 1), (16, 1), (16, 1)], gap=0.0)
+    ne = instance_mesh(reqs[0].instance)[0].n_elements
+    loop = ServingLoop(prep="thread", chunk_steps=8, tol=1e-6, max_steps=1000, window_s=0.0,
+                       max_active_elements=2 * ne, max_cohort_elements=4 * ne)
+    res = loop.run(reqs, realtime=False)
+    assert len(res) == 4 and all(r.converged and r.steps == 25 for r in res)
+    assert loop.slot_reuses == 2 and FakeBatch.replaced == 2
+    assert loop.cohorts_formed == 1 and FakeBatch.created == 1
+    assert loop.max_concurrent <= 2
+    assert min(res[2].admitted_s, res[3].admitted_s) >= min(res[0].finished_s, res[1].finished_s)
+
+
+def test_slot_reuse_respects_fit_and_waste():
+    from dgm_in_rust_b200.serving import _fits, _room
+    assert _room((100, 140, 20, 2), 1.5) == (150, 210, 30, 3)
+    assert _fits((150, 200, 30, 2), (150, 210, 30, 3)) and not _fits((151, 200, 30, 2), (150, 210, 30, 3))

@@ -54,15 +54,18 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the many-instance measurement")
     ap.add_argument("--batched-instances", type=int, default=256)
-    ap.add_argument("--batched-steps", type=int, default=20)
+    ap.add_argument("--batched-steps", type=int, default=1000)
     ap.add_argument("--no-serving", action="store_true", help="skip the request-stream measurement")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 p=3 measurement")
     ap.add_argument("--precision-steps", type=int, default=500)
+    ap.add_argument("--precision-c2-steps", type=int, default=2000)
     ap.add_argument("--only", choices=["batched", "precision", "serving"],
                     help="run one secondary measurement alone and print its JSON (for profiling)")
     ap.add_argument("--serving-requests", type=int, default=48)
-    ap.add_argument("--serving-rate", type=float, default=20.0, help="Poisson arrival rate, requests/s")
-    ap.add_argument("--serving-max-steps", type=int, default=400)
+    ap.add_argument("--serving-rates", default="20",
+                    help="Poisson arrival rates to serve, requests/s, comma-separated (the same seeded requests at "
+                         "each rate); e.g. 1,10,50,200 for the sweep")
+    ap.add_argument("--serving-max-steps", type=int, default=5000)
     ap.add_argument("--serving-budget-gib", type=float, default=16.0)
     ap.add_argument("--serving-max-active", type=int, default=2 << 20,
                     help="elements of running requests above which new requests wait (work-in-flight cap)")
@@ -287,7 +290,7 @@ def run_batched(args, local):
            "instances": len(insts), "elements": int(sum(i.elements for i in insts)),
            "dof": int(sum(i.dofs for i in insts)), "steps": K, "warmup": W + W2}
 
-    def batched(precision):
+    def batched(precision, perturb=False):
         batches = []
         for p, items in groups.items():
             if not items:
@@ -296,6 +299,10 @@ def run_batched(args, local):
                       [10 ** 12] * len(items), limiter=True, device=local, precision=precision)
             for i, (_, m, init) in enumerate(items):
                 b.set_initial(i, init)
+                if perturb:  # the FP64 conditioning floor: a start perturbed by 1e-13 (seeded)
+                    U0 = b.download(i)
+                    U0 *= 1.0 + 1e-13 * np.random.default_rng(100 + i + 1000 * p).standard_normal(U0.shape)
+                    b.upload(i, U0)
             batches.append(b)
         for b in batches:
             b.advance(W)
@@ -341,15 +348,31 @@ def run_batched(args, local):
     v32, ms32, bytes32, acc32 = batched("fp32")
     vtc, mstc, bytestc, acctc = batched("tf32x3")
     v64, ms64, bytes64, acc64 = batched("fp64")
+    _, _, _, accp = batched("fp64", perturb=True)
+    floor_cl = {k: abs(accp[k][0] - acc64[k][0]) for k in acc64}
+    floor_cd = {k: abs(accp[k][1] - acc64[k][1]) for k in acc64}
 
-    def versus(acc):
-        dcl = [abs(acc[k][0] - acc64[k][0]) for k in acc64]
-        dcd = [abs(acc[k][1] - acc64[k][1]) for k in acc64]
+    def versus(acc, tol=1e-4):
+        dcl = {k: abs(acc[k][0] - acc64[k][0]) for k in acc64}
+        dcd = {k: abs(acc[k][1] - acc64[k][1]) for k in acc64}
         errs = [field_rel_l2(acc[k][2], acc64[k][2], acc64[k][3]) for k in acc64 if acc64[k][2] is not None]
-        return {"steps": W + W2 + K, "max_abs_delta_cl": max(dcl), "max_abs_delta_cd": max(dcd),
+        ok = {k: dcl[k] <= tol and dcd[k] <= tol for k in acc64}
+        good = [k for k in acc64 if floor_cl[k] <= tol and floor_cd[k] <= tol]
+        return {"steps": W + W2 + K, "max_abs_delta_cl": max(dcl.values()), "max_abs_delta_cd": max(dcd.values()),
+                "median_abs_delta_cl": float(np.median(list(dcl.values()))),
+                "instances_meeting_1e-4": int(sum(ok.values())),
+                "instances_with_fp64_floor_below_1e-4": len(good),
+                "of_those_meeting_1e-4": int(sum(ok[k] for k in good)),
+                "max_abs_delta_cl_where_floor_below_1e-4": max([dcl[k] for k in good], default=None),
                 "density_rel_l2_max": max(errs), "density_rel_l2_median": float(np.median(errs)),
                 "density_sample": f"{len(errs)} instances (every 8th of each order group)"}
 
+    res["fp64_conditioning_floor"] = {
+        "perturbation": "each instance's initial state x (1 + 1e-13 N(0,1)), FP64, same steps",
+        "max_abs_delta_cl": max(floor_cl.values()), "median_abs_delta_cl": float(np.median(list(floor_cl.values()))),
+        "max_abs_delta_cd": max(floor_cd.values()),
+        "instances_below_1e-4": int(sum(floor_cl[k] <= 1e-4 and floor_cd[k] <= 1e-4 for k in floor_cl)),
+        "per_instance_abs_delta_cl": {f"p{k[0]}_{k[1]}": v for k, v in floor_cl.items()}}
     res["fp32_vs_fp64_after_steps"] = versus(acc32)
     res["tf32x3_vs_fp64_after_steps"] = versus(acctc)
     # one at a time, FP64: a DOF-weighted sample (every 8th instance in DOF order)
@@ -394,35 +417,53 @@ def field_rel_l2(a, b, w):
     return float(np.sqrt(np.sum(w * (a - b) ** 2) / np.sum(w * b * b)))
 
 
-def run_precision(args, local):
-    """NACA 0012 O-grid 1024 x 512 (1,048,576 triangles), p = 3 (10 modes, 12-point triangle /
-    4-point edge rules), M = 0.7, AoA = 2 deg, free-stream start, limiter on, CFL 0.1: the same
-    steps in FP64, in FP32 (limiter, positivity checks, time step and reductions in FP64), and
-    in FP32 with the basis contractions on the tensor cores (tf32: TF32 operands; tf32x3: split
-    TF32 operands).  Reports relative L2 errors of each mode's fields against FP64, C_L / C_D,
-    and each mode's DOF-stage updates/s (CUDA events on the library stream; the state exceeds
-    L2)."""
+def wall_elements(mesh):
+    """Elements with an edge on a wall patch: the first cell layer on the body."""
+    bnd = np.nonzero(mesh.edge_elements[:, 1] == -1)[0]
+    wall = [d for d in bnd if mesh.patch_type[mesh.edge_patch[d]] == 0]
+    return np.unique(mesh.edge_elements[wall, 0])
+
+
+def accuracy_report(U, U64, cl, cd, cl64, cd64, floor, w, wall, tol=1e-4):
+    """Errors of one precision mode against FP64 on the same steps: relative L2 of every field
+    (area-weighted, and over the coefficients), relative L2 of the density over the first wall
+    layer (coefficients), |dC_L|, |dC_D|, and pass/fail against tol, with the FP64 conditioning
+    floor (|dC_L|, |dC_D| of FP64 from a 1e-13 perturbed start) beside it."""
+    names = ("rho", "rho_u", "rho_v", "rho_E")
+    dcl, dcd = abs(cl - cl64), abs(cd - cd64)
+    rho_w = float(np.linalg.norm(U[wall, 0] - U64[wall, 0]) / np.linalg.norm(U64[wall, 0]))
+    return {"rel_l2": {n: field_rel_l2(U[:, v], U64[:, v], w) for v, n in enumerate(names)},
+            "rel_l2_coefficients": {n: float(np.linalg.norm(U[:, v] - U64[:, v]) / np.linalg.norm(U64[:, v]))
+                                    for v, n in enumerate(names)},
+            "rel_l2_density_first_wall_layer": rho_w,
+            "abs_delta_cl": dcl, "abs_delta_cd": dcd,
+            "fp64_floor_abs_delta_cl": floor[0], "fp64_floor_abs_delta_cd": floor[1],
+            "meets_1e-4": bool(dcl <= tol and dcd <= tol),
+            "floor_below_1e-4": bool(floor[0] <= tol and floor[1] <= tol)}
+
+
+def precision_case(inst, K, modes, local, label):
+    """The same K steps from the free stream in FP64, in each precision mode of ``modes``, and in
+    FP64 from a start perturbed by 1e-13 (the conditioning floor); each mode's launch
+    configuration tuned on a developed state.  Returns per-mode throughput and accuracy against
+    FP64."""
     import torch
     from dgm_in_rust_b200 import build_solver, forces_to_coefficients
-    from dgm_in_rust_b200.workloads import Instance, instance_mesh
-    inst = Instance(1024, 512, 0.7, 2.0, 3)
-    K = args.precision_steps
+    from dgm_in_rust_b200.workloads import instance_mesh
     mesh, init = instance_mesh(inst)
-    res = {"workload": "naca0012_ogrid_1024x512_p3: 1,048,576 triangles, 10 modes, M=0.7, AoA=2deg, limiter on, "
-                       f"CFL 0.1, free-stream start, {K} steps", "steps": K}
+    nb = (inst.order + 1) * (inst.order + 2) // 2
+    res = {"workload": label, "steps": K}
     out, tuned = {}, {}
-    for prec in ("fp64", "fp32", "tf32", "tf32x3", "fp64_perturbed"):
+    for prec in ("fp64",) + tuple(modes) + ("fp64_perturbed",):
         mode = "fp64" if prec == "fp64_perturbed" else prec
         if mode not in tuned:
-            # launch configuration of this mode, tuned on a developed state (a separate context
-            # advanced 20 steps), so that the timed run below starts from the free stream
-            t = build_solver(mesh, 3, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, device=local, precision=mode)
+            t = build_solver(mesh, inst.order, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, device=local, precision=mode)
             t.temporal_disc.set_initial_on_device(init)
             t.temporal_disc.advance(20)
             t.temporal_disc.synchronize()
             tuned[mode] = t.spatial_disc.autotune(repeats=5)
             t.close()
-        s = build_solver(mesh, 3, HCR, CFL, 1.0e30, K, limiter=True, device=local, precision=mode)
+        s = build_solver(mesh, inst.order, HCR, CFL, 1.0e30, K, limiter=True, device=local, precision=mode)
         td, sd = s.temporal_disc, s.spatial_disc
         cfg = tuned[mode]
         sd.set_launch_config(cfg["edge_threads"], cfg["edge_blocks"], cfg["element_threads"])
@@ -431,8 +472,6 @@ def run_precision(args, local):
         sd.set_limiter_schedule(cfg["limiter_schedule"] == "queue")
         td.set_initial_on_device(init)
         if prec == "fp64_perturbed":
-            # conditioning floor: the FP64 solve from an initial state perturbed by 1e-13 (relative,
-            # seeded normal noise); FP32 cannot be expected to agree with FP64 better than this
             U0 = sd.new_state()
             td.download(U0)
             U0 *= 1.0 + 1e-13 * np.random.default_rng(11).standard_normal(U0.shape)
@@ -449,34 +488,57 @@ def run_precision(args, local):
         td.download(U)
         d = sd.diagnostics()
         cl, cd = forces_to_coefficients(d[4], d[5], inst.aoa, 1.0, inst.mach)
-        troubled, waves = sd.limiter_stats()
-        out[prec] = (U, cl, cd, d)
-        res[prec] = {"dof_stage_updates_per_s": inst.dofs * 3 * td.current_step / (ms * 1e-3),
-                     "ms_per_step": ms / max(td.current_step, 1), "steps_done": td.current_step,
-                     "time": td.current_time, "cl": cl, "cd": cd, "troubled_cells_last_stage": troubled,
-                     "launch": {k: cfg[k] for k in ("edge_threads", "edge_blocks", "element_threads", "edge_form",
-                                                    "limiter_detector", "limiter_schedule")}}
+        troubled, _ = sd.limiter_stats()
+        out[prec] = (U, cl, cd)
+        if prec != "fp64_perturbed":
+            res[prec] = {"dof_stage_updates_per_s": inst.dofs * 3 * td.current_step / (ms * 1e-3),
+                         "ms_per_step": ms / max(td.current_step, 1), "steps_done": td.current_step,
+                         "time": td.current_time, "cl": cl, "cd": cd, "troubled_cells_last_stage": troubled,
+                         "launch": {k: cfg[k] for k in ("edge_threads", "edge_blocks", "element_threads", "edge_form",
+                                                        "limiter_detector", "limiter_schedule")}}
         w_basis = s.basis.mass_mat_diag
         s.close()
-    (U32, cl32, cd32, _), (U64, cl64, cd64, _) = out["fp32"], out["fp64"]
-    Up, clp, cdp, _ = out["fp64_perturbed"]
+    U64, cl64, cd64 = out["fp64"]
+    Up, clp, cdp = out["fp64_perturbed"]
     w = w_basis[None, :] * (0.5 * mesh.elem_jacob_det)[:, None]
-    names = ("rho", "rho_u", "rho_v", "rho_E")
-    res["rel_l2_fp32_vs_fp64"] = {n: field_rel_l2(U32[:, v], U64[:, v], w) for v, n in enumerate(names)}
-    res["rel_l2_coefficients_fp32_vs_fp64"] = {
-        n: float(np.linalg.norm(U32[:, v] - U64[:, v]) / np.linalg.norm(U64[:, v])) for v, n in enumerate(names)}
-    res["abs_delta_cl"] = abs(cl32 - cl64)
-    res["abs_delta_cd"] = abs(cd32 - cd64)
-    for prec in ("tf32", "tf32x3"):  # basis contractions on the tensor cores
-        Ut, clt, cdt, _ = out[prec]
-        res[f"{prec}_vs_fp64"] = {"rel_l2": {n: field_rel_l2(Ut[:, v], U64[:, v], w) for v, n in enumerate(names)},
-                                  "abs_delta_cl": abs(clt - cl64), "abs_delta_cd": abs(cdt - cd64)}
-    res["fp64_conditioning_floor"] = {
-        "perturbation": "initial state x (1 + 1e-13 N(0,1)), FP64", "abs_delta_cl": abs(clp - cl64),
-        "abs_delta_cd": abs(cdp - cd64), "rel_l2_rho": field_rel_l2(Up[:, 0], U64[:, 0], w),
-        "troubled_cells_last_stage": res.pop("fp64_perturbed")["troubled_cells_last_stage"]}
-    res["speedup_fp32_vs_fp64"] = (res["fp32"]["dof_stage_updates_per_s"] / res["fp64"]["dof_stage_updates_per_s"])
+    wall = wall_elements(mesh)
+    floor = (abs(clp - cl64), abs(cdp - cd64))
+    res["fp64_conditioning_floor"] = {"perturbation": "initial state x (1 + 1e-13 N(0,1)), FP64",
+                                      "abs_delta_cl": floor[0], "abs_delta_cd": floor[1],
+                                      "rel_l2_rho": field_rel_l2(Up[:, 0], U64[:, 0], w),
+                                      "rel_l2_density_first_wall_layer": float(
+                                          np.linalg.norm(Up[wall, 0] - U64[wall, 0]) / np.linalg.norm(U64[wall, 0]))}
+    for prec in modes:
+        U, cl, cd = out[prec]
+        res[f"{prec}_vs_fp64"] = accuracy_report(U, U64, cl, cd, cl64, cd64, floor, w, wall)
+        res[f"speedup_{prec}_vs_fp64"] = res[prec]["dof_stage_updates_per_s"] / res["fp64"]["dof_stage_updates_per_s"]
+    res["wall_layer_elements"] = int(len(wall))
+    res["elements"] = int(mesh.n_elements)
+    res["dof_per_element"] = 4 * nb
     return res
+
+
+def run_precision(args, local):
+    """FP32 and the tensor-core TF32 modes against FP64 on (a) the precision configuration, NACA
+    0012 O-grid 1024 x 512 (1,048,576 triangles), p = 3, M = 0.7, AoA = 2 deg, free-stream start,
+    limiter on, CFL 0.1, --precision-steps steps, and (b) a grid of the transonic configuration's
+    size with a coarser wall layer, 512 x 64 (65,536 triangles, first cell 4e-4 chords instead of
+    5e-8), p = 2, M = 0.5, AoA = 2 deg, --precision-c2-steps steps, where the FP64 solution is
+    well conditioned (its 1e-13-perturbation floor is small), so that errors of 1e-4 can be told
+    apart.  Reports for each: throughput of every mode, relative L2 errors (area-weighted and
+    coefficient-level, and over the first wall layer), |dC_L|, |dC_D|, pass/fail against 1e-4 and
+    the FP64 floor.  CUDA events on the library stream."""
+    from dgm_in_rust_b200.workloads import Instance
+    K = args.precision_steps
+    c3 = precision_case(Instance(1024, 512, 0.7, 2.0, 3), K, ("fp32", "tf32", "tf32x3"), local,
+                        f"naca0012_ogrid_1024x512_p3: 1,048,576 triangles, 10 modes, M=0.7, AoA=2deg, limiter on, "
+                        f"CFL 0.1, free-stream start, {K} steps")
+    K2 = args.precision_c2_steps
+    c2 = precision_case(Instance(512, 64, 0.5, 2.0, 2), K2, ("fp32", "tf32x3"), local,
+                        f"naca0012_ogrid_512x64_p2: 65,536 triangles, 6 modes, M=0.5, AoA=2deg, limiter on, CFL 0.1, "
+                        f"free-stream start, {K2} steps (first wall cell 4e-4 chords)")
+    c3["well_conditioned_65536"] = c2
+    return c3
 
 
 # ------------------------------------------------------------------------------------------
@@ -486,40 +548,56 @@ def run_serving(args, local):
     """A seeded Poisson stream of solve requests (triangles log-uniform in [2e3, 5e5], O-grid
     aspect 2:1, Mach U[0.3,0.85], AoA U[-4,6] deg, p in {1,2,3}), each run to a density-residual
     drop of 1e-6 or the step cap, served (a) by the continuous-batching loop in FP32 with real
-    arrival times and an HBM budget, and (b) one request at a time on the plain FP64 context,
-    first come first served (service times measured back to back, latencies from the FIFO queue
-    under the same arrival times).  Latency = arrival to retirement; throughput = DOF-stage
-    updates / wall time (a) or / total service time (b), host mesh preparation included in both."""
+    arrival times, an HBM budget and slot reuse, at every rate of --serving-rates, and (b) one
+    request at a time on the plain FP64 context, first come first served: service times measured
+    back to back once (the requests are the same at every rate: the seed fixes sizes, orders and
+    flow conditions, the rate only scales the gaps), latencies from the FIFO queue under each
+    rate's arrival times.  Latency = arrival to retirement (time to convergence, or to the step
+    cap where the request does not converge); throughput = DOF-stage updates / wall time (a) or /
+    total service time (b), host mesh preparation included in both."""
     from dgm_in_rust_b200.serving import ServingLoop, latency_summary, one_at_a_time, requests_from_stream
     from dgm_in_rust_b200.workloads import request_stream
     seed = 7
-    reqs = requests_from_stream(request_stream(args.serving_requests, args.serving_rate, seed=seed))
+    rates = [float(x) for x in args.serving_rates.split(",") if x.strip()]
     kw = dict(chunk_steps=32, tol=1e-6, max_steps=args.serving_max_steps)
     budget = int(args.serving_budget_gib * (1 << 30))
-    loop = ServingLoop(hbm_budget_bytes=budget, device=local, precision="fp32",
-                       max_active_elements=args.serving_max_active, **kw)
-    t = time.perf_counter()
-    served = loop.run(reqs, realtime=True)
-    wall = time.perf_counter() - t
-    s32 = latency_summary(served, wall)
-    alone, busy, prep = one_at_a_time(reqs, precision="fp64", device=local, **kw)
-    s64 = latency_summary(alone, busy)
+    out = {"workload": f"{args.serving_requests} requests per rate, Poisson arrivals (request_stream seed {seed}), "
+                       f"triangles log-uniform [2e3, 5e5], p in {{1,2,3}}, Mach U[0.3,0.85], AoA U[-4,6] deg; stop at "
+                       f"density-residual drop 1e-6 or {args.serving_max_steps} steps; convergence checked at step 1 "
+                       f"then every 32",
+           "hbm_budget_bytes": budget, "max_active_elements": args.serving_max_active, "rates": {}}
+    base = requests_from_stream(request_stream(args.serving_requests, rates[0], seed=seed))
+    out["elements_total"] = int(sum(r.instance.elements for r in base))
+    # FP64 one at a time: service times once, FIFO latencies per rate
+    alone, busy, prep = one_at_a_time(base, precision="fp64", device=local, **kw)
+    service = {r.rid: r.finished_s - r.admitted_s for r in alone}
     gpu_only = sum(r.dofs * 3 * r.steps for r in alone) / max(busy - prep, 1e-9)
-    return {
-        "workload": f"{len(reqs)} requests, Poisson arrivals at {args.serving_rate:g}/s "
-                    f"(request_stream seed {seed}), triangles log-uniform [2e3, 5e5], p in {{1,2,3}}, "
-                    f"Mach U[0.3,0.85], AoA U[-4,6] deg; stop at density-residual drop 1e-6 or "
-                    f"{args.serving_max_steps} steps (the configuration's cap is 5000; bounded here so the "
-                    f"default run stays within minutes); convergence checked at step 1 then every 32",
-        "elements_total": int(sum(r.instance.elements for r in reqs)),
-        "hbm_budget_bytes": budget, "max_active_elements": args.serving_max_active,
-        "peak_resident_bytes": loop.peak_bytes, "cohorts": loop.cohorts_formed,
-        "max_concurrent_requests": loop.max_concurrent, "scheduler": loop.stats,
-        "fp32_serving": s32, "fp64_one_at_a_time": s64,
-        "fp64_one_at_a_time_excluding_host_prep_dof_stage_per_s": gpu_only,
-        "throughput_speedup": s32["dof_stage_updates_per_s"] / s64["dof_stage_updates_per_s"],
-        "p99_speedup": s64["p99_s"] / s32["p99_s"],
-    }
+    out["fp64_one_at_a_time_service_s"] = busy
+    out["fp64_one_at_a_time_excluding_host_prep_dof_stage_per_s"] = gpu_only
+    for rate in rates:
+        reqs = requests_from_stream(request_stream(args.serving_requests, rate, seed=seed))
+        assert [(r.instance.ni, r.instance.order) for r in reqs] == [(r.instance.ni, r.instance.order) for r in base]
+        loop = ServingLoop(hbm_budget_bytes=budget, device=local, precision="fp32",
+                           max_active_elements=args.serving_max_active, **kw)
+        t = time.perf_counter()
+        served = loop.run(reqs, realtime=True)
+        wall = time.perf_counter() - t
+        s32 = latency_summary(served, wall)
+        fifo = {r.rid: r for r in alone}
+        finish = 0.0
+        for r in sorted(reqs, key=lambda q: (q.arrival_s, q.rid)):
+            a = fifo[r.rid]
+            start = max(r.arrival_s, finish)
+            finish = start + service[r.rid]
+            a.arrival_s, a.admitted_s, a.finished_s = r.arrival_s, start, finish
+        s64 = latency_summary(list(fifo.values()), busy)
+        out["rates"][f"{rate:g}"] = {
+            "fp32_serving": s32, "fp64_one_at_a_time": s64,
+            "peak_resident_bytes": loop.peak_bytes, "cohorts": loop.cohorts_formed, "slot_reuses": loop.slot_reuses,
+            "max_concurrent_requests": loop.max_concurrent, "scheduler": loop.stats,
+            "throughput_speedup": s32["dof_stage_updates_per_s"] / s64["dof_stage_updates_per_s"],
+            "p99_speedup": s64["p99_s"] / s32["p99_s"]}
+    return out
 
 
 def run_ours(args):

@@ -9,11 +9,11 @@ from ._native import DgmError
 from .basis_function import DubinerBasis, GaussPoints, default_rules
 from .mesh import GmshParser, Mesh, RawMesh, freestream_quantity, naca0012_ogrid, process_mesh, write_gmsh
 from .solver import (Batch, FlowParameters, InitialSolution, MeshParameters, Solver, SolverParameters, SpatialDisc,
-                     TemperalDisc, build_solver, forces_to_coefficients, initial_state, reference_cfl)
+                     TemperalDisc, build_solver, forces_to_coefficients, initial_state, reference_cfl, slot_capacity)
 
 __all__ = [
     "DgmError", "DubinerBasis", "GaussPoints", "default_rules", "GmshParser", "Mesh", "RawMesh",
     "freestream_quantity", "naca0012_ogrid", "process_mesh", "write_gmsh", "FlowParameters", "InitialSolution",
     "MeshParameters", "Solver", "SolverParameters", "SpatialDisc", "TemperalDisc", "build_solver",
-    "initial_state", "reference_cfl", "Batch", "forces_to_coefficients",
+    "initial_state", "reference_cfl", "Batch", "forces_to_coefficients", "slot_capacity",
 ]

@@ -159,6 +159,9 @@ def lib() -> ctypes.CDLL:
     L.dgm_create_batch_slots.restype = vp
     L.dgm_instance_replace.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MeshDesc), ctypes.POINTER(Params)]
     L.dgm_instance_capacity.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(SlotCapacity)]
+    L.dgm_create_mixed.argtypes = [ctypes.c_int32, ctypes.POINTER(MeshDesc), P_I32, ctypes.POINTER(TablesDesc),
+                                   ctypes.POINTER(Params), ctypes.POINTER(SlotCapacity), P_I32]
+    L.dgm_create_mixed.restype = vp
     L.dgm_instance_upload.argtypes = [vp, ctypes.c_int32, P_D]
     L.dgm_instance_download.argtypes = [vp, ctypes.c_int32, P_D]
     L.dgm_instance_download_residual.argtypes = [vp, ctypes.c_int32, P_D]

@@ -17,6 +17,7 @@
 
 #include "dgm_b200.h"
 #include "dgm_device.cuh"
+#include "dgm_mixed.cuh"
 #include "dgm_tc.cuh"
 
 using dgm::Control;
@@ -62,7 +63,7 @@ struct dgm_ctx {
   int* work = nullptr;
   int* wl1 = nullptr;    // limiter: cells the detection enlists for wave 1
   int* pend = nullptr;   // limiter: elements the detection leaves for later waves
-  int* order = nullptr;  // limiter: the detection's visiting order (breadth-first over the elements)
+  int* order = nullptr;  // limiter: the detection's visiting order of the warp batches (breadth-first)
   int* d_elem_rng = nullptr;   // [2 n] first element, element count of each instance's mesh
   int* d_bslot_rng = nullptr;  // [2 n] first boundary slot (relative to n_int), boundary slot count
   bool padded = false;         // capacity ranges above the meshes' sizes: dead instance and null element
@@ -91,6 +92,14 @@ struct dgm_ctx {
   int64_t err_where = -1;
   int64_t last_troubled = 0;
   int last_waves = 0;
+  bool owns_stream = true;
+  // mixed batch (dgm_create_mixed): one child context per order present (kids[P - 1]), sharing
+  // this context's stream; instance i of the batch is instance imap[i].second of kids[imap[i].first]
+  bool mixed = false;
+  dgm_ctx* kids[3] = {nullptr, nullptr, nullptr};
+  std::vector<std::pair<int, int>> imap;
+  int* mwork = nullptr;  // the mixed limiter's worklist of waves 2, 3, ... (all groups' elements)
+  int mixed_blocks = 1;  // co-resident blocks of the mixed limiter's wave kernel
 };
 
 namespace {
@@ -240,7 +249,7 @@ struct Ops {
 
   static int limiter(dgm_ctx* c, T* U) {
     if (!c->limiter) return DGM_OK;
-    const int dblocks = (int)std::max<int64_t>(1, (c->ne + dgm::kDetectThreads - 1) / dgm::kDetectThreads);
+    const int dblocks = (int)std::max<int64_t>(1, (c->ld / 32 + dgm::kDetectWarps - 1) / dgm::kDetectWarps);
     if (c->lim_staged)
       dgm::k_lim_detect<P, T, true><<<dblocks, dgm::kDetectThreads, 0, c->stream>>>(kp_of<P, T>(c), U, c->t0, c->status,
                                                                                    c->wl1, c->pend, c->order);
@@ -577,6 +586,17 @@ int write_clock(dgm_ctx* c) {
   return DGM_OK;
 }
 
+int mixed_step(dgm_ctx* c, int with_residual);
+
+// One time-march iteration of every instance, enqueued on the context's stream.
+int step_once(dgm_ctx* c, int with_residual) {
+  if (c->mixed) return mixed_step(c, with_residual);
+  return dispatch(c, [&](auto ops) {
+    using O = decltype(ops);
+    return O::step(c, with_residual ? O::S(c->R) : nullptr);
+  });
+}
+
 int build_graph(dgm_ctx* c, int with_residual, int single) {
   if (c->graph[with_residual][single] || c->graphs_broken) return DGM_OK;
   cudaGraph_t g = nullptr;
@@ -587,11 +607,7 @@ int build_graph(dgm_ctx* c, int with_residual, int single) {
   }
   int st = DGM_OK;
   const int n = single ? 1 : c->graph_steps;
-  for (int i = 0; i < n && st == DGM_OK; ++i)
-    st = dispatch(c, [&](auto ops) {
-      using O = decltype(ops);
-      return O::step(c, with_residual ? O::S(c->R) : nullptr);
-    });
+  for (int i = 0; i < n && st == DGM_OK; ++i) st = step_once(c, with_residual);
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (st != DGM_OK || e != cudaSuccess || g == nullptr) {
     cudaGetLastError();
@@ -631,10 +647,7 @@ int enqueue_steps(dgm_ctx* c, int64_t n, int with_residual) {
       CK(cudaGraphLaunch(c->graph[with_residual][single], c->stream));
       n -= single ? 1 : c->graph_steps;
     } else {
-      st = dispatch(c, [&](auto ops) {
-        using O = decltype(ops);
-        return O::step(c, with_residual ? O::S(c->R) : nullptr);
-      });
+      st = step_once(c, with_residual);
       if (st) return st;
       n -= 1;
     }
@@ -657,7 +670,7 @@ int enqueue_steps(dgm_ctx* c, int64_t n, int with_residual) {
 // elem_cap; element, slot and patch ids are global).
 struct InstArrays {
   std::vector<double> jac, hmin, h15, dinv;  // dinv: [4][elem_cap]
-  std::vector<int> face, nbr, inst, order;   // face, nbr: [3][elem_cap]
+  std::vector<int> face, nbr, inst;          // face, nbr: [3][elem_cap]
   std::vector<int2> ie_lr;
   std::vector<int> ie_ic;
   std::vector<double4> ie_geo;
@@ -790,29 +803,6 @@ int fill_instance(const dgm_ctx* c, int i, const dgm_mesh_desc* m, InstArrays& a
     a.hmin[e] = m->elem_minimum_height[e];
     a.h15[e] = std::pow(m->elem_circumradius[e], 1.5);  // weno.rs:81 h.powf(1.5)
   }
-  // the limiter detection's visiting order: breadth-first over the element graph (each connected
-  // piece from its lowest unvisited element), so that a warp's elements and the neighbours whose
-  // traces they gather are close together and mostly in cache.  Any permutation gives the same
-  // results; this one only changes which loads hit.  Padding elements follow.
-  a.order.clear();
-  a.order.reserve((size_t)cap);
-  std::vector<unsigned char> seen((size_t)nei, 0);
-  for (int64_t s0 = 0; s0 < nei; ++s0) {
-    if (seen[s0]) continue;
-    seen[s0] = 1;
-    a.order.push_back((int)(eo + s0));
-    for (size_t h = a.order.size() - 1; h < a.order.size(); ++h) {
-      const int64_t e = a.order[h] - eo;
-      for (int k = 0; k < 3; ++k) {
-        const int nb = a.nbr[k * cap + e];
-        if (nb >= 0 && !seen[nb - eo]) {
-          seen[nb - eo] = 1;
-          a.order.push_back(nb);
-        }
-      }
-    }
-  }
-  for (int64_t e = nei; e < cap; ++e) a.order.push_back((int)(eo + e));
   return DGM_OK;
 }
 
@@ -886,9 +876,8 @@ int build_mesh(dgm_ctx* c, const dgm_mesh_desc* meshes, const dgm_slot_capacity*
   std::vector<int> be_elem(n_bnd), be_info(n_bnd);
   std::vector<double4> be_geo(n_bnd);
   std::vector<double4> patch_q(std::max<int64_t>(1, np));
-  std::vector<int> face(3 * ld, 0), nbr(3 * ld, -1), inst_of(ne, c->dead_inst), order;
+  std::vector<int> face(3 * ld, 0), nbr(3 * ld, -1), inst_of(ne, c->dead_inst);
   std::vector<double> jac(ne, 1.0), hmin(ne, 1.0), h15(ne, 1.0), dinv(4 * ld, 0.0);
-  order.reserve((size_t)ne);
   InstArrays a;
   for (int i = 0; i < n_inst; ++i) {
     int st = fill_instance(c, i, &meshes[i], a);
@@ -904,7 +893,6 @@ int build_mesh(dgm_ctx* c, const dgm_mesh_desc* meshes, const dgm_slot_capacity*
       std::copy(a.face.begin() + k * cap, a.face.begin() + (k + 1) * cap, face.begin() + k * ld + eo);
       std::copy(a.nbr.begin() + k * cap, a.nbr.begin() + (k + 1) * cap, nbr.begin() + k * ld + eo);
     }
-    order.insert(order.end(), a.order.begin(), a.order.end());
     std::copy(a.ie_lr.begin(), a.ie_lr.end(), ie_lr.begin() + hi.int_off);
     std::copy(a.ie_ic.begin(), a.ie_ic.end(), ie_ic.begin() + hi.int_off);
     std::copy(a.ie_geo.begin(), a.ie_geo.end(), ie_geo.begin() + hi.int_off);
@@ -915,7 +903,44 @@ int build_mesh(dgm_ctx* c, const dgm_mesh_desc* meshes, const dgm_slot_capacity*
     std::copy(a.bnd_ref.begin(), a.bnd_ref.end(), slot_ref.begin() + n_int + hi.bnd_off);
     std::copy(a.patch_q.begin(), a.patch_q.end(), patch_q.begin() + hi.patch_off);
   }
-  if (padding) order.push_back((int)c->null_elem);
+  // the limiter detection's visiting order of the warp batches (32 consecutive elements each):
+  // breadth-first over the graph of batches that hold neighbouring elements, each connected piece
+  // from its lowest unvisited batch, so that a batch and the batches holding its elements'
+  // neighbours are processed at about the same time and their traces are mostly in cache.  Any
+  // order gives the same results; this one only changes which loads hit.
+  const int64_t nbatch = ld / 32;
+  std::vector<int> order;
+  {
+    std::vector<int> deg(nbatch + 1, 0), adj;
+    for (int64_t e = 0; e < ne; ++e)
+      for (int k = 0; k < 3; ++k) {
+        const int nb = nbr[k * ld + e];
+        if (nb >= 0 && (nb >> 5) != (e >> 5)) ++deg[(e >> 5) + 1];
+      }
+    for (int64_t b = 0; b < nbatch; ++b) deg[b + 1] += deg[b];
+    adj.resize(deg[nbatch]);
+    std::vector<int> fill(deg.begin(), deg.end() - 1);
+    for (int64_t e = 0; e < ne; ++e)
+      for (int k = 0; k < 3; ++k) {
+        const int nb = nbr[k * ld + e];
+        if (nb >= 0 && (nb >> 5) != (e >> 5)) adj[fill[e >> 5]++] = nb >> 5;
+      }
+    order.reserve((size_t)nbatch);
+    std::vector<unsigned char> seen((size_t)nbatch, 0);
+    for (int64_t s0 = 0; s0 < nbatch; ++s0) {
+      if (seen[s0]) continue;
+      seen[s0] = 1;
+      order.push_back((int)s0);
+      for (size_t h = order.size() - 1; h < order.size(); ++h) {
+        const int b = order[h];
+        for (int j = deg[b]; j < deg[b + 1]; ++j)
+          if (!seen[adj[j]]) {
+            seen[adj[j]] = 1;
+            order.push_back(adj[j]);
+          }
+      }
+    }
+  }
   md = MeshDev{};
   md.ne = (int)ne;
   md.ld = (int)ld;
@@ -966,7 +991,7 @@ bool variant_ok(const dgm_tables_desc* t) {
 }
 
 dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_slot_capacity* caps, const dgm_tables_desc* tables,
-                const dgm_params* params, int32_t* status) {
+                const dgm_params* params, int32_t* status, cudaStream_t shared_stream = nullptr) {
   int32_t dummy;
   if (!status) status = &dummy;
   if (n_inst < 1 || !meshes || !tables || !params) {
@@ -1016,7 +1041,12 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_slot_capacity
   int coop = 0;
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
   if (!coop) return fail(DGM_NO_DEVICE);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  if (shared_stream) {
+    c->stream = shared_stream;
+    c->owns_stream = false;
+  } else if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    return fail(DGM_CUDA_ERROR);
+  }
   c->pool = pool_acquire(c->device);
   if (!c->pool) return fail(DGM_CUDA_ERROR);
   int st;
@@ -1060,7 +1090,260 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_slot_capacity
   return c;
 }
 
-bool inst_ok(dgm_ctx* c, int64_t i) { return c && i >= 0 && i < (int64_t)c->inst.size(); }
+
+// ---------------------------------------------------------------------------------------------
+// Mixed batches: one child context per order (its own union mesh, tables and arrays), one stream,
+// and one launch per kernel of the step over all children (dgm_mixed.cuh).
+// ---------------------------------------------------------------------------------------------
+constexpr int kMixedEdgeThreads = 128, kMixedElemThreads = 128;
+
+template <typename T, int MASK>
+struct MixOps {
+  using M = dgm::Mixed<T, MASK>;
+  static T* S(void* p) { return static_cast<T*>(p); }
+
+  static void base(dgm_ctx* p, M& mp) {
+    std::memset(static_cast<void*>(&mp), 0, sizeof(M));
+    for (int g = 0; g < 3; ++g) {
+      dgm_ctx* k = p->kids[g];
+      if (!k) continue;
+      if constexpr ((MASK & 1) != 0)
+        if (g == 0) std::memcpy(static_cast<void*>(&mp.k1), k->kparams.data(), sizeof(mp.k1));
+      if constexpr ((MASK & 2) != 0)
+        if (g == 1) std::memcpy(static_cast<void*>(&mp.k2), k->kparams.data(), sizeof(mp.k2));
+      if constexpr ((MASK & 4) != 0)
+        if (g == 2) std::memcpy(static_cast<void*>(&mp.k3), k->kparams.data(), sizeof(mp.k3));
+      auto& a = mp.g[g];
+      a.n_inst = (int)k->inst.size();
+      a.F = S(k->F);
+      a.t0 = k->t0;
+      a.status = k->status;
+      a.wl1 = k->wl1;
+      a.pend = k->pend;
+      a.order = k->order;
+    }
+  }
+
+  static int blocks_total(const M& mp) { return std::max(1, mp.g[0].blocks + mp.g[1].blocks + mp.g[2].blocks); }
+
+  // which: 0 = U, 1 = U1, 2 = U2
+  static T* arr(dgm_ctx* k, int which) { return S(which == 0 ? k->U : which == 1 ? k->U1 : k->U2); }
+
+  static int step_head(dgm_ctx* p) {
+    M mp;
+    base(p, mp);
+    for (int g = 0; g < 3; ++g)
+      if (dgm_ctx* k = p->kids[g]) {
+        mp.g[g].Uin = S(k->U);
+        mp.g[g].blocks = (int)((k->ne + 255) / 256);
+      }
+    dgm::k_step_head_mixed<T, MASK><<<blocks_total(mp), 256, 0, p->stream>>>(mp);
+    CK(cudaGetLastError());
+    return DGM_OK;
+  }
+
+  static int edge_flux(dgm_ctx* p, int which) {
+    M mp;
+    base(p, mp);
+    for (int g = 0; g < 3; ++g)
+      if (dgm_ctx* k = p->kids[g]) {
+        mp.g[g].Uin = arr(k, which);
+        mp.g[g].blocks = (int)(((k->n_int + k->n_bnd) * k->ng + kMixedEdgeThreads - 1) / kMixedEdgeThreads);
+      }
+    dgm::k_edge_flux_mixed<T, MASK><<<blocks_total(mp), kMixedEdgeThreads, 0, p->stream>>>(mp);
+    CK(cudaGetLastError());
+    return DGM_OK;
+  }
+
+  template <int MODE>
+  static int element(dgm_ctx* p, bool with_residual) {
+    M mp;
+    base(p, mp);
+    for (int g = 0; g < 3; ++g)
+      if (dgm_ctx* k = p->kids[g]) {
+        auto& a = mp.g[g];
+        a.Uin = arr(k, MODE == 1 ? 0 : MODE == 2 ? 1 : 2);
+        a.Ubase = MODE == 1 ? nullptr : S(k->U);
+        a.Uout = arr(k, MODE == 1 ? 1 : MODE == 2 ? 2 : 0);
+        a.Rout = (MODE == 3 && with_residual) ? S(k->R) : nullptr;
+        a.blocks = (int)((k->ne + kMixedElemThreads / 4 - 1) / (kMixedElemThreads / 4));
+      }
+    dgm::k_element_mixed<T, MASK, MODE><<<blocks_total(mp), kMixedElemThreads, 0, p->stream>>>(mp);
+    CK(cudaGetLastError());
+    return DGM_OK;
+  }
+
+  static int limiter(dgm_ctx* p, int which) {
+    if (!p->limiter) return DGM_OK;
+    M mp;
+    base(p, mp);
+    for (int g = 0; g < 3; ++g)
+      if (dgm_ctx* k = p->kids[g]) {
+        mp.g[g].Uin = arr(k, which);
+        mp.g[g].Uout = arr(k, which);
+        mp.g[g].blocks = (int)((k->ld / 32 + dgm::kDetectWarps - 1) / dgm::kDetectWarps);
+      }
+    dgm::k_lim_detect_mixed<T, MASK, false><<<blocks_total(mp), dgm::kDetectThreads, 0, p->stream>>>(mp);
+    CK(cudaGetLastError());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(p->mixed_blocks);
+    cfg.blockDim = dim3(dgm::kLimiterWarps * 32);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = p->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter_mixed<T, MASK>, mp, p->mwork));
+    return DGM_OK;
+  }
+
+  static int step_end(dgm_ctx* p) {
+    M mp;
+    base(p, mp);
+    const int n = mp.g[0].n_inst + mp.g[1].n_inst + mp.g[2].n_inst;
+    dgm::k_step_end_mixed<T, MASK><<<(n + 127) / 128, 128, 0, p->stream>>>(mp);
+    CK(cudaGetLastError());
+    return DGM_OK;
+  }
+
+  static int step(dgm_ctx* p, bool with_residual) {
+    int st;
+    if ((st = step_head(p))) return st;
+    if ((st = edge_flux(p, 0)) || (st = element<1>(p, false)) || (st = limiter(p, 1))) return st;
+    if ((st = edge_flux(p, 1)) || (st = element<2>(p, false)) || (st = limiter(p, 2))) return st;
+    if ((st = edge_flux(p, 2)) || (st = element<3>(p, with_residual)) || (st = limiter(p, 0))) return st;
+    return step_end(p);
+  }
+
+  static int occupancy(dgm_ctx* p) {
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dgm::k_limiter_mixed<T, MASK>, dgm::kLimiterWarps * 32, 0));
+    int64_t ne = 0;
+    for (dgm_ctx* k : p->kids)
+      if (k) ne += k->ne;
+    const int64_t want = std::max<int64_t>(1, (ne + 32 * dgm::kLimiterWarps - 1) / (32 * dgm::kLimiterWarps));
+    p->mixed_blocks = (int)std::min<int64_t>((int64_t)std::max(1, per_sm) * p->num_sms, want);
+    return DGM_OK;
+  }
+};
+
+// Sets of orders compiled for mixed launches: {1, 2} and {1, 2, 3} (any other set runs as the
+// latter with empty groups).
+template <class F>
+int mixed_dispatch(dgm_ctx* p, F&& f) {
+  const bool three = p->kids[2] != nullptr;
+  if (p->prec == 0) return three ? f(MixOps<double, 7>{}) : f(MixOps<double, 3>{});
+  return three ? f(MixOps<float, 7>{}) : f(MixOps<float, 3>{});
+}
+
+int mixed_step(dgm_ctx* c, int with_residual) {
+  return mixed_dispatch(c, [&](auto ops) { return decltype(ops)::step(c, with_residual != 0); });
+}
+
+dgm_ctx* create_mixed(int n, const dgm_mesh_desc* meshes, const int32_t* orders, const dgm_tables_desc* tables,
+                      const dgm_params* params, const dgm_slot_capacity* caps, int32_t* status) {
+  int32_t dummy;
+  if (!status) status = &dummy;
+  if (n < 1 || !meshes || !orders || !tables || !params) {
+    *status = DGM_BAD_ARG;
+    return nullptr;
+  }
+  for (int i = 0; i < n; ++i)
+    if (orders[i] < 1 || orders[i] > 3 || params[i].hcr != params[0].hcr || params[i].precision != params[0].precision ||
+        params[i].limiter != params[0].limiter || params[i].device != params[0].device) {
+      *status = DGM_BAD_ARG;
+      return nullptr;
+    }
+  if (params[0].precision < 0 || params[0].precision > 1) {  // mixed launches: FP64 or FP32 (FMA) bulk
+    *status = DGM_BAD_ARG;
+    return nullptr;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || params->device < 0 || params->device >= ndev) {
+    cudaGetLastError();
+    *status = DGM_NO_DEVICE;
+    return nullptr;
+  }
+  auto* p = new dgm_ctx();
+  p->mixed = true;
+  p->device = params->device;
+  p->prec_mode = params->precision;
+  p->prec = params->precision == 0 ? 0 : 1;
+  p->hcr = params->hcr;
+  p->limiter = params->limiter ? 1 : 0;
+  auto fail = [&](int st) {
+    *status = st;
+    dgm_destroy(p);
+    return (dgm_ctx*)nullptr;
+  };
+  if (cudaSetDevice(p->device) != cudaSuccess) return fail(DGM_NO_DEVICE);
+  if (cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess)
+    return fail(DGM_NO_DEVICE);
+  if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  p->pool = pool_acquire(p->device);
+  if (!p->pool) return fail(DGM_CUDA_ERROR);
+  p->imap.resize(n);
+  int64_t ne_all = 0;
+  for (int g = 0; g < 3; ++g) {
+    std::vector<dgm_mesh_desc> ms;
+    std::vector<dgm_params> ps;
+    std::vector<dgm_slot_capacity> cs;
+    for (int i = 0; i < n; ++i)
+      if (orders[i] == g + 1) {
+        p->imap[i] = {g, (int)ms.size()};
+        ms.push_back(meshes[i]);
+        ps.push_back(params[i]);
+        if (caps) cs.push_back(caps[i]);
+      }
+    if (ms.empty()) continue;
+    if (tables[g].order != g + 1) return fail(DGM_BAD_ARG);
+    int32_t st = DGM_OK;
+    p->kids[g] = create((int)ms.size(), ms.data(), caps ? cs.data() : nullptr, &tables[g], ps.data(), &st, p->stream);
+    if (!p->kids[g]) return fail(st ? st : DGM_CUDA_ERROR);
+    ne_all += p->kids[g]->ne;
+  }
+  int st;
+  if ((st = dev_alloc(p, &p->mwork, (size_t)ne_all))) return fail(st);
+  if ((st = mixed_dispatch(p, [&](auto ops) { return decltype(ops)::occupancy(p); }))) return fail(st);
+  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return fail(DGM_CUDA_ERROR);
+  p->graph_steps = (int)kGraphSteps;
+  *status = DGM_OK;
+  return p;
+}
+
+// The child context and its instance index of a mixed batch's instance i (the context itself and i
+// for other contexts); false if i is out of range.
+bool resolve(dgm_ctx*& c, int32_t& i) {
+  if (!c) return false;
+  if (!c->mixed) return i >= 0 && i < (int32_t)c->inst.size();
+  if (i < 0 || i >= (int32_t)c->imap.size()) return false;
+  const auto& m = c->imap[i];
+  c = c->kids[m.first];
+  i = m.second;
+  return c != nullptr;
+}
+
+// Writes the clocks of children whose host mirrors changed (dgm_instance_set / replace).
+int mixed_sync_clocks(dgm_ctx* p) {
+  for (dgm_ctx* k : p->kids)
+    if (k && (k->limits_dirty || k->dt_dirty)) {
+      int st = write_clock(k);
+      if (st) return st;
+    }
+  return DGM_OK;
+}
+
+int mixed_collect(dgm_ctx* p) {
+  int first = DGM_OK;
+  for (dgm_ctx* k : p->kids)
+    if (k) {
+      const int st = collect_status(k);
+      if (st && !first) first = st;
+    }
+  return first;
+}
 
 }  // namespace
 
@@ -1092,10 +1375,11 @@ void dgm_destroy(dgm_ctx* c) {
   for (auto& row : c->graph)
     for (auto& g : row)
       if (g) cudaGraphExecDestroy(g);
+  for (dgm_ctx* k : c->kids) dgm_destroy(k);
   if (c->stream) {
     for (void* p : c->allocs) cudaFreeAsync(p, c->stream);  // back to the pool, in stream order
     cudaStreamSynchronize(c->stream);
-    cudaStreamDestroy(c->stream);
+    if (c->owns_stream) cudaStreamDestroy(c->stream);
   }
   if (c->pool) pool_release(c->device);
   delete c;
@@ -1120,8 +1404,14 @@ dgm_ctx* dgm_create_batch_slots(int32_t n_instances, const dgm_mesh_desc* meshes
   return create(n_instances, meshes, capacity, tables, params, status);
 }
 
+dgm_ctx* dgm_create_mixed(int32_t n_instances, const dgm_mesh_desc* meshes, const int32_t* orders,
+                          const dgm_tables_desc* tables, const dgm_params* params, const dgm_slot_capacity* capacity,
+                          int32_t* status) {
+  return create_mixed(n_instances, meshes, orders, tables, params, capacity, status);
+}
+
 int32_t dgm_instance_capacity(dgm_ctx* c, int32_t i, dgm_slot_capacity* out) {
-  if (!inst_ok(c, i) || !out) return DGM_BAD_ARG;
+  if (!resolve(c, i) || !out) return DGM_BAD_ARG;
   const HostInst& h = c->inst[i];
   out->elements = h.elem_cap;
   out->internal_edges = h.int_cap;
@@ -1136,7 +1426,7 @@ int32_t dgm_instance_capacity(dgm_ctx* c, int32_t i, dgm_slot_capacity* out) {
 // clock, loop bounds and status.  The other instances are untouched; the step graphs stay valid
 // (they hold array addresses and sizes, which do not change).
 int32_t dgm_instance_replace(dgm_ctx* c, int32_t i, const dgm_mesh_desc* mesh, const dgm_params* params) {
-  if (!inst_ok(c, i) || !mesh || !params || params->hcr != c->hcr) return DGM_BAD_ARG;
+  if (!resolve(c, i) || !mesh || !params || params->hcr != c->hcr) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   CK(cudaStreamSynchronize(c->stream));  // nothing of this context may still read the old mesh
   InstArrays a;
@@ -1156,8 +1446,7 @@ int32_t dgm_instance_replace(dgm_ctx* c, int32_t i, const dgm_mesh_desc* mesh, c
     return DGM_OK;
   };
   if ((st = put(md.jac + eo, a.jac.data(), cap * sizeof(double))) || (st = put(md.hmin + eo, a.hmin.data(), cap * sizeof(double))) ||
-      (st = put(md.h15 + eo, a.h15.data(), cap * sizeof(double))) || (st = put(md.inst + eo, a.inst.data(), cap * sizeof(int))) ||
-      (st = put(c->order + eo, a.order.data(), cap * sizeof(int))))
+      (st = put(md.h15 + eo, a.h15.data(), cap * sizeof(double))) || (st = put(md.inst + eo, a.inst.data(), cap * sizeof(int))))
     return st;
   for (int k = 0; k < 4; ++k)
     if ((st = put(md.dinv + k * ld + eo, a.dinv.data() + k * cap, cap * sizeof(double)))) return st;
@@ -1194,7 +1483,7 @@ int32_t dgm_instance_replace(dgm_ctx* c, int32_t i, const dgm_mesh_desc* mesh, c
 }
 
 int32_t dgm_instance_upload(dgm_ctx* c, int32_t i, const double* solutions) {
-  if (!inst_ok(c, i) || !solutions) return DGM_BAD_ARG;
+  if (!resolve(c, i) || !solutions) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st = upload_state(c, i, solutions, c->U);
   if (st) return st;
@@ -1203,19 +1492,19 @@ int32_t dgm_instance_upload(dgm_ctx* c, int32_t i, const double* solutions) {
 }
 
 int32_t dgm_instance_download(dgm_ctx* c, int32_t i, double* solutions) {
-  if (!inst_ok(c, i) || !solutions) return DGM_BAD_ARG;
+  if (!resolve(c, i) || !solutions) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   return download_state(c, i, c->U, solutions);
 }
 
 int32_t dgm_instance_download_residual(dgm_ctx* c, int32_t i, double* residuals) {
-  if (!inst_ok(c, i) || !residuals) return DGM_BAD_ARG;
+  if (!resolve(c, i) || !residuals) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   return download_state(c, i, c->R, residuals);
 }
 
 int32_t dgm_instance_state(dgm_ctx* c, int32_t i, double* t, int64_t* step, int32_t* status, int64_t* where) {
-  if (!inst_ok(c, i)) return DGM_BAD_ARG;
+  if (!resolve(c, i)) return DGM_BAD_ARG;
   const HostInst& h = c->inst[i];
   if (t) *t = h.t;
   if (step) *step = h.step;
@@ -1225,7 +1514,7 @@ int32_t dgm_instance_state(dgm_ctx* c, int32_t i, double* t, int64_t* step, int3
 }
 
 int32_t dgm_instance_set(dgm_ctx* c, int32_t i, double t, int64_t step, double final_time, int64_t final_step) {
-  if (!inst_ok(c, i)) return DGM_BAD_ARG;
+  if (!resolve(c, i)) return DGM_BAD_ARG;
   HostInst& h = c->inst[i];
   h.t = t;
   h.step = step;
@@ -1257,7 +1546,7 @@ static int set_initial(dgm_ctx* c, int64_t i, double density, double angle_of_at
 
 int32_t dgm_instance_set_initial(dgm_ctx* c, int32_t i, double density, double angle_of_attack,
                                  double mach_number, double pressure) {
-  if (!inst_ok(c, i)) return DGM_BAD_ARG;
+  if (!resolve(c, i)) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st = set_initial(c, i, density, angle_of_attack, mach_number, pressure);
   if (st) return st;
@@ -1268,6 +1557,14 @@ int32_t dgm_instance_set_initial(dgm_ctx* c, int32_t i, double density, double a
 int32_t dgm_set_initial_solution(dgm_ctx* c, double density, double angle_of_attack, double mach_number,
                                  double pressure) {
   if (!c) return DGM_BAD_ARG;
+  if (c->mixed) {
+    for (dgm_ctx* k : c->kids)
+      if (k) {
+        const int st = dgm_set_initial_solution(k, density, angle_of_attack, mach_number, pressure);
+        if (st) return st;
+      }
+    return DGM_OK;
+  }
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   for (size_t i = 0; i < c->inst.size(); ++i) {
     int st = set_initial(c, (int64_t)i, density, angle_of_attack, mach_number, pressure);
@@ -1277,7 +1574,7 @@ int32_t dgm_set_initial_solution(dgm_ctx* c, double density, double angle_of_att
   return DGM_OK;
 }
 
-int32_t dgm_instance_count(dgm_ctx* c) { return c ? (int32_t)c->inst.size() : 0; }
+int32_t dgm_instance_count(dgm_ctx* c) { return c ? (int32_t)(c->mixed ? c->imap.size() : c->inst.size()) : 0; }
 
 int32_t dgm_compute_residuals(dgm_ctx* c, double* residuals, const double* solutions) {
   if (!c || !residuals || !solutions || c->inst.size() != 1) return DGM_BAD_ARG;
@@ -1365,13 +1662,14 @@ int32_t dgm_time_march(dgm_ctx* c, double* residuals, double* solutions) {
 }
 
 int32_t dgm_get_clock(dgm_ctx* c, double* t, int64_t* step) {
-  if (!c) return DGM_BAD_ARG;
+  if (!c || c->inst.empty()) return DGM_BAD_ARG;
   if (t) *t = c->inst[0].t;
   if (step) *step = c->inst[0].step;
   return DGM_OK;
 }
 
 int32_t dgm_set_clock(dgm_ctx* c, double t, int64_t step) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   for (auto& h : c->inst) {
@@ -1382,6 +1680,7 @@ int32_t dgm_set_clock(dgm_ctx* c, double t, int64_t step) {
 }
 
 int32_t dgm_set_limits(dgm_ctx* c, double final_time, int64_t final_step) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c) return DGM_BAD_ARG;
   for (auto& h : c->inst) {
     h.final_time = final_time;
@@ -1392,11 +1691,13 @@ int32_t dgm_set_limits(dgm_ctx* c, double final_time, int64_t final_step) {
 }
 
 int32_t dgm_upload_solutions(dgm_ctx* c, const double* solutions) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c || !solutions || c->inst.size() != 1) return DGM_BAD_ARG;
   return dgm_instance_upload(c, 0, solutions);
 }
 
 int32_t dgm_download_solutions(dgm_ctx* c, double* solutions) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c || !solutions || c->inst.size() != 1) return DGM_BAD_ARG;
   return dgm_instance_download(c, 0, solutions);
 }
@@ -1404,6 +1705,10 @@ int32_t dgm_download_solutions(dgm_ctx* c, double* solutions) {
 int32_t dgm_advance(dgm_ctx* c, int64_t n_steps) {
   if (!c || n_steps < 0) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  if (c->mixed) {
+    const int st = mixed_sync_clocks(c);
+    return st ? st : enqueue_steps(c, n_steps, 0);
+  }
   if (c->limits_dirty || c->dt_dirty) {
     int st = write_clock(c);
     if (st) return st;
@@ -1414,6 +1719,10 @@ int32_t dgm_advance(dgm_ctx* c, int64_t n_steps) {
 int32_t dgm_advance_with_residual(dgm_ctx* c, int64_t n_steps) {
   if (!c || n_steps < 0) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  if (c->mixed) {
+    const int st = mixed_sync_clocks(c);
+    return st ? st : enqueue_steps(c, n_steps, 1);
+  }
   if (c->limits_dirty || c->dt_dirty) {
     int st = write_clock(c);
     if (st) return st;
@@ -1425,7 +1734,7 @@ int32_t dgm_synchronize(dgm_ctx* c) {
   if (!c) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   CK(cudaStreamSynchronize(c->stream));
-  return collect_status(c);
+  return c->mixed ? mixed_collect(c) : collect_status(c);
 }
 
 int32_t dgm_query(dgm_ctx* c) {
@@ -1434,12 +1743,13 @@ int32_t dgm_query(dgm_ctx* c) {
   const cudaError_t e = cudaStreamQuery(c->stream);
   if (e == cudaErrorNotReady) return DGM_NOT_READY;
   CK(e);
-  return collect_status(c);
+  return c->mixed ? mixed_collect(c) : collect_status(c);
 }
 
 void* dgm_stream(dgm_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 int32_t dgm_launch_phase(dgm_ctx* c, int32_t phase) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c || phase < 0 || phase > 3) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st = set_active(c, 0.0, false);
@@ -1456,6 +1766,7 @@ int32_t dgm_launch_phase(dgm_ctx* c, int32_t phase) {
 }
 
 int32_t dgm_set_launch_config(dgm_ctx* c, int32_t edge_threads, int32_t edge_blocks, int32_t element_threads) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c) return DGM_BAD_ARG;
   auto threads_ok = [](int32_t t) { return t >= 32 && t <= 256 && t % 32 == 0; };
   if (!threads_ok(edge_threads) || !threads_ok(element_threads) || edge_blocks < 0 || edge_blocks > (1 << 24))
@@ -1470,6 +1781,7 @@ int32_t dgm_set_launch_config(dgm_ctx* c, int32_t edge_threads, int32_t edge_blo
 }
 
 int32_t dgm_set_limiter_variant(dgm_ctx* c, int32_t staged) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c || (staged != 0 && staged != 1)) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   CK(cudaStreamSynchronize(c->stream));
@@ -1488,6 +1800,7 @@ static int set_schedule(dgm_ctx* c, int queue) {
 }
 
 int32_t dgm_set_limiter_schedule(dgm_ctx* c, int32_t queue) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c || (queue != 0 && queue != 1)) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   CK(cudaStreamSynchronize(c->stream));
@@ -1506,6 +1819,7 @@ int32_t dgm_get_limiter_schedule(dgm_ctx* c, int32_t* queue, double* tuned_us) {
 }
 
 int32_t dgm_set_edge_variant(dgm_ctx* c, int32_t pair) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c || (pair != 0 && pair != 1)) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   CK(cudaStreamSynchronize(c->stream));
@@ -1536,6 +1850,7 @@ int32_t dgm_get_launch_config(dgm_ctx* c, int32_t* config) {
 // (CUDA events on the context's stream, after warm-up launches) and keeps the fastest.  The
 // candidates only regroup independent per-slot / per-element work, so results are unchanged.
 int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c || repeats < 1 || repeats > 1000) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st = set_active(c, 0.0, false);
@@ -1659,19 +1974,56 @@ int32_t dgm_launches_per_step(dgm_ctx* c) {
          3 * (2 + (c->limiter ? 2 /* detection, waves */ : 0));
 }
 
-int64_t dgm_error_location(dgm_ctx* c) { return c ? c->err_where : -1; }
+int64_t dgm_error_location(dgm_ctx* c) {
+  if (!c) return -1;
+  if (c->mixed)
+    for (dgm_ctx* k : c->kids)
+      if (k && k->err_where >= 0) return k->err_where;
+  return c->err_where;
+}
 
 int32_t dgm_limiter_stats(dgm_ctx* c, int64_t* troubled, int32_t* waves) {
   if (!c) return DGM_BAD_ARG;
+  if (c->mixed) {
+    int64_t t = 0;
+    int w = 0;
+    for (dgm_ctx* k : c->kids)
+      if (k) {
+        t += k->last_troubled;
+        w = std::max(w, k->last_waves);
+      }
+    if (troubled) *troubled = t;
+    if (waves) *waves = w;
+    return DGM_OK;
+  }
   if (troubled) *troubled = c->last_troubled;
   if (waves) *waves = c->last_waves;
   return DGM_OK;
 }
 
-int64_t dgm_device_bytes(dgm_ctx* c) { return c ? c->bytes : 0; }
+int64_t dgm_device_bytes(dgm_ctx* c) {
+  if (!c) return 0;
+  int64_t b = c->bytes;
+  for (dgm_ctx* k : c->kids)
+    if (k) b += k->bytes;
+  return b;
+}
 
 int32_t dgm_diagnostics(dgm_ctx* c, int32_t use_residual, double* out) {
   if (!c || !out) return DGM_BAD_ARG;
+  if (c->mixed) {  // each order's instances, scattered into the batch's instance order
+    std::vector<double> part;
+    for (int g = 0; g < 3; ++g) {
+      dgm_ctx* k = c->kids[g];
+      if (!k) continue;
+      part.assign(8 * k->inst.size(), 0.0);
+      const int st = dgm_diagnostics(k, use_residual, part.data());
+      if (st) return st;
+      for (size_t i = 0; i < c->imap.size(); ++i)
+        if (c->imap[i].first == g) std::memcpy(out + 8 * i, part.data() + 8 * c->imap[i].second, 8 * sizeof(double));
+    }
+    return DGM_OK;
+  }
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   int st = dispatch(c, [&](auto ops) {
     using O = decltype(ops);
@@ -1686,7 +2038,7 @@ int32_t dgm_diagnostics(dgm_ctx* c, int32_t use_residual, double* out) {
 int32_t dgm_precision(dgm_ctx* c) { return c ? c->prec_mode : -1; }
 
 int32_t dgm_cell_fields(dgm_ctx* c, int32_t i, double* fields) {
-  if (!inst_ok(c, i) || !fields) return DGM_BAD_ARG;
+  if (!resolve(c, i) || !fields) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   // the FP64 staging buffer holds a whole instance's state (ne x 4 x NB >= ne x 4 doubles)
   int st = dispatch(c, [&](auto ops) { return decltype(ops)::cell_fields(c, i, c->stage); });

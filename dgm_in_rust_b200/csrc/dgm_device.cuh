@@ -179,6 +179,13 @@ __device__ __forceinline__ T ld_st(const T* p) {
   else return __ldcg(p);
 }
 
+// An element's own coefficient: a plain load when the record is staged in shared memory.
+template <bool RO, bool SHARED, typename T>
+__device__ __forceinline__ T ld_own(const T* p) {
+  if constexpr (SHARED) return *p;
+  else return ld_st<RO>(p);
+}
+
 // Index of coefficient (v, b) of element e in an element-major state array.
 template <int NB>
 __host__ __device__ __forceinline__ size_t sx(int e, int v, int b) {
@@ -511,9 +518,12 @@ __device__ __forceinline__ void store_flux(T* F, size_t s, int NG, int g, const 
 // boundary_condition.rs:19-97).  Writes F[slot][g][v] * half length.  Slots of instances that
 // are not stepping are skipped.
 // ------------------------------------------------------------------------------------------
+// The kernels' bodies take their block index and block count within the launch (bid, nblk) as
+// arguments, so that a launch over several meshes of different orders (a mixed batch) can give each
+// order's body its own range of blocks; the single-order kernels pass blockIdx.x and gridDim.x.
 template <int P, typename T>
-__global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KParams<P, T> kp,
-                                                      const T* __restrict__ U, T* __restrict__ F) {
+__device__ __forceinline__ void edge_flux_body(const KParams<P, T>& kp, const T* __restrict__ U, T* __restrict__ F,
+                                               int bid, int nblk) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
   __shared__ T s_pe[3 * NG * NB];
@@ -522,7 +532,7 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
   const MeshDev& m = kp.m;
   const Gas& gas = kp.gas;
   const int total = (m.n_int + m.n_bnd) * NG;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+  for (int t = bid * blockDim.x + threadIdx.x; t < total; t += nblk * blockDim.x) {
     const int s = t / NG, g = t - s * NG;
     T out[4];
     if (s < m.n_int) {
@@ -578,6 +588,12 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
   }
 }
 
+template <int P, typename T>
+__global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KParams<P, T> kp,
+                                                      const T* __restrict__ U, T* __restrict__ F) {
+  edge_flux_body<P, T>(kp, U, F, blockIdx.x, gridDim.x);
+}
+
 // The same edge pass with two lanes per edge slot, one per side: each lane loads its element's
 // modes once, evaluates the traces at all NG points (the right side at the reversed points,
 // spatial_disc.rs:185), the pair swaps traces with shuffles, and the two lanes split the points
@@ -585,8 +601,8 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
 // point; every trace and flux is the same expression in the same order as in k_edge_flux, so the
 // results are bitwise identical.  A warp covers 16 consecutive slots per iteration.
 template <int P, typename T>
-__global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant__ KParams<P, T> kp,
-                                                           const T* __restrict__ U, T* __restrict__ F) {
+__device__ __forceinline__ void edge_flux_pair_body(const KParams<P, T>& kp, const T* __restrict__ U,
+                                                    T* __restrict__ F, int bid, int nblk) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
   constexpr int G0 = (NG + 1) / 2;  // points of the left lane: [0, G0); right lane: [G0, NG)
@@ -597,8 +613,8 @@ __global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant
   const Gas& gas = kp.gas;
   const int total = m.n_int + m.n_bnd;
   const int lane = threadIdx.x & 31, side = lane & 1;
-  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int gwarp = (bid * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (nblk * blockDim.x) >> 5;
   for (int base = gwarp * 16; base < total; base += nwarps * 16) {
     const int s = base + (lane >> 1);
     bool valid = s < total, internal = false, has = false;
@@ -673,6 +689,12 @@ __global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant
   }
 }
 
+template <int P, typename T>
+__global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant__ KParams<P, T> kp,
+                                                           const T* __restrict__ U, T* __restrict__ F) {
+  edge_flux_pair_body<P, T>(kp, U, F, blockIdx.x, gridDim.x);
+}
+
 // ------------------------------------------------------------------------------------------
 // Element pass: volume integral (integrate_over_cell_euler, spatial_disc.rs:40-69, and
 // boundary_condition.rs:98-117 for boundary elements), gather of the three faces' edge fluxes
@@ -736,15 +758,14 @@ __device__ __forceinline__ void warp_store_records(T* dst, int e0, const T* sbuf
 }
 
 template <int P, typename T, int MODE>
-__global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KParams<P, T> kp,
-                                                    const T* __restrict__ Uin, const T* Ubase,
-                                                    const T* __restrict__ F, T* Uout, const T* Rin, T* Rout) {
+__device__ __forceinline__ void element_body(const KParams<P, T>& kp, const T* __restrict__ Uin, const T* Ubase,
+                                             const T* __restrict__ F, T* Uout, const T* Rin, T* Rout, int bid) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NQ = V::NQ, NG = V::NG;
   constexpr int STRIDE = Staged<NB, T>::kStride;
   __shared__ __align__(16) T s_rec[kElemMaxWarps][8 * STRIDE];
   Control* ctl = kp.ctl;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {  // counters of the limiter pass that follows
+  if (bid == 0 && threadIdx.x == 0) {  // counters of the limiter pass that follows
     ctl->t0_count = 0;
     ctl->unknown[0] = ctl->unknown[1] = 0;
     ctl->wl_count[0] = ctl->wl_count[1] = 0;
@@ -755,7 +776,7 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
   const MeshDev& m = kp.m;
   const int lane = threadIdx.x & 31;
   const int var = lane >> 3, i = lane & 7;
-  const int e0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 8;
+  const int e0 = (bid * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 8;
   const int e_raw = e0 + i;
   if (e0 >= m.ne) return;  // whole warp past the end
   const int e = e_raw < m.ne ? e_raw : m.ne - 1;
@@ -849,6 +870,13 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
   }
 }
 
+template <int P, typename T, int MODE>
+__global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KParams<P, T> kp,
+                                                    const T* __restrict__ Uin, const T* Ubase,
+                                                    const T* __restrict__ F, T* Uout, const T* Rin, T* Rout) {
+  element_body<P, T, MODE>(kp, Uin, Ubase, F, Uout, Rin, Rout, blockIdx.x);
+}
+
 // ------------------------------------------------------------------------------------------
 // modified_kxrcf, weno.rs:7-85, for element e on state U (FP64 arithmetic).  Keeps the
 // reference's exterior-trace indexing: the neighbour's modes are evaluated with this element's
@@ -856,7 +884,9 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
 // `own` is e's record (the limiter stages its warp's records in shared memory); the
 // neighbours' modes are read from U through L2.
 // ------------------------------------------------------------------------------------------
-template <int P, typename T, bool RO = false>
+// RO: U is only read during the kernel (neighbour traces through L1); OWN_SHARED: `own` is staged
+// in shared memory (plain loads), else it is e's record in U (loaded like the neighbours').
+template <int P, typename T, bool RO = false, bool OWN_SHARED = false>
 __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restrict__ U, int e, const T* own) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
@@ -879,8 +909,8 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
       double rho = 0.0, rho_e = 0.0;
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        rho += (double)ld_st<RO>(&own[0 * NB + b]) * kp.d.phi_edge[k][g][b];
-        rho_e += (double)ld_st<RO>(&own[3 * NB + b]) * kp.d.phi_edge[k][g][b];
+        rho += (double)ld_own<RO, OWN_SHARED>(&own[0 * NB + b]) * kp.d.phi_edge[k][g][b];
+        rho_e += (double)ld_own<RO, OWN_SHARED>(&own[3 * NB + b]) * kp.d.phi_edge[k][g][b];
       }
       own_rho[g] = rho;
       own_rhoe[g] = rho_e;
@@ -891,8 +921,8 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
     double rho_u = 0.0, rho_v = 0.0;
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      rho_u += (double)ld_st<RO>(&own[1 * NB + b]) * kp.d.phi_edge[k][cg][b];
-      rho_v += (double)ld_st<RO>(&own[2 * NB + b]) * kp.d.phi_edge[k][cg][b];
+      rho_u += (double)ld_own<RO, OWN_SHARED>(&own[1 * NB + b]) * kp.d.phi_edge[k][cg][b];
+      rho_v += (double)ld_own<RO, OWN_SHARED>(&own[2 * NB + b]) * kp.d.phi_edge[k][cg][b];
     }
     if (rho_u * nx + rho_v * ny < 0.0) {
       double rho_jump = 0.0, rho_e_jump = 0.0;
@@ -928,7 +958,7 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
 // than kxrcf (which walks the faces one after another) at the price of registers: faster when
 // a pass is latency-bound (small meshes), slower when occupancy matters (large batches); the
 // autotuner picks one per context.  Same arithmetic in the same order, so the same flags.
-template <int P, typename T, bool RO = false>
+template <int P, typename T, bool RO = false, bool OWN_SHARED = false>
 __device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* __restrict__ U, int e,
                                              const T* own_rec) {
   int fw[3], nb[3];
@@ -944,7 +974,7 @@ __device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* _
 #pragma unroll
   for (int v = 0; v < NEQ; ++v)
 #pragma unroll
-    for (int b = 0; b < NB; ++b) own[v][b] = (double)ld_st<RO>(&own_rec[v * NB + b]);
+    for (int b = 0; b < NB; ++b) own[v][b] = (double)ld_own<RO, OWN_SHARED>(&own_rec[v * NB + b]);
   double nx[3], ny[3], jd[3];
   bool interior[3];
 #pragma unroll
@@ -1367,8 +1397,9 @@ timeout:
 // elements of instances that are not stepping settle clean without evaluation.
 //
 // Two launches per pass.  k_lim_detect evaluates modified_kxrcf on every element (the parallel
-// flags t0 of wave 1) with one lane per element at full occupancy, visiting the elements in a
-// breadth-first order of the element graph so that the neighbour traces it gathers are mostly in
+// flags t0 of wave 1), one warp per batch of 32 consecutive elements (their records staged in
+// shared memory), one lane per element, at full occupancy, visiting the batches in a
+// breadth-first order of the batch graph so that the neighbour traces it gathers are mostly in
 // cache; it settles the clean elements without a lower-index neighbour, enlists the troubled ones
 // for wave 1 (wl1) and lists the elements that wait for a lower neighbour (pend).  k_limiter, a
 // cooperative persistent kernel, then reconstructs wave 1's cells (one warp each), and runs waves
@@ -1382,28 +1413,43 @@ timeout:
 //     w rewrites an element all of whose lower neighbours settled before wave w, so the only
 //     concurrent reads of it are wave-1 flags of its higher neighbours, and those flags are never
 //     used (a higher neighbour of a rewritten element is re-evaluated in a later wave).
-constexpr int kDetectThreads = 128;
+constexpr int kDetectWarps = 4;
+constexpr int kDetectThreads = kDetectWarps * 32;
+
+// Shared memory of one detection block: each warp's 32 staged records.
+template <int P, typename T>
+struct DetectSmem {
+  static constexpr int kStride = Staged<Variant<P>::NB, T>::kStride;
+  static constexpr size_t kBytes = (size_t)kDetectWarps * 32 * kStride * sizeof(T);
+};
 
 template <int P, typename T, bool STAGED>
-__global__ void __launch_bounds__(kDetectThreads) k_lim_detect(const __grid_constant__ KParams<P, T> kp,
-                                                               const T* __restrict__ U,
-                                                               unsigned char* __restrict__ t0,
-                                                               unsigned int* __restrict__ status,
-                                                               int* __restrict__ wl1, int* __restrict__ pend,
-                                                               const int* __restrict__ order) {
+__device__ __forceinline__ void lim_detect_body(const KParams<P, T>& kp, const T* __restrict__ U,
+                                                unsigned char* __restrict__ t0, unsigned int* __restrict__ status,
+                                                int* __restrict__ wl1, int* __restrict__ pend,
+                                                const int* __restrict__ order, int bid, T* s_det) {
   using V = Variant<P>;
+  constexpr int STRIDE = DetectSmem<P, T>::kStride;
   Control* ctl = kp.ctl;
   const MeshDev& m = kp.m;
-  const int lane = threadIdx.x & 31;
-  const int pos = blockIdx.x * kDetectThreads + threadIdx.x;
-  bool flag = false, enlist = false, wait = false;
-  int e = 0;
-  if (pos < m.ne) {
-    e = order[pos];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int w = bid * kDetectWarps + wib;  // position in the batch order
+  if (w >= m.ld / 32) return;              // the whole warp
+  const int e0 = order[w] * 32;            // the warp's batch: 32 consecutive elements
+  const int e = e0 + lane;
+  bool flag = false, enlist = false, wait = false, active = false;
+  if (e < m.ne) {
     const int inst = m.n_inst > 1 ? m.inst[e] : 0;
-    if (kp.ic[inst].active) {
-      const T* own = U + (size_t)e * (NEQ * V::NB);
-      flag = STAGED ? kxrcf_staged<P, T, true>(kp, U, e, own) : kxrcf<P, T, true>(kp, U, e, own);
+    active = kp.ic[inst].active != 0;
+  }
+  if (__any_sync(0xffffffffu, active)) {
+    // the batch's records are contiguous: staged with coalesced 16-byte loads (arrays are padded
+    // to whole batches)
+    T* recs = s_det + (size_t)wib * 32 * STRIDE;
+    warp_load_records<V::NB, T, 32>(U, e0, recs, lane);
+    if (active) {
+      const T* own = recs + lane * STRIDE;
+      flag = STAGED ? kxrcf_staged<P, T, true, true>(kp, U, e, own) : kxrcf<P, T, true, true>(kp, U, e, own);
       bool ready = true;
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
@@ -1413,6 +1459,8 @@ __global__ void __launch_bounds__(kDetectThreads) k_lim_detect(const __grid_cons
       wait = !ready;
       enlist = ready && flag;
     }
+  }
+  if (e < m.ne) {
     t0[e] = flag ? 1 : 0;
     status[e] = (wait || enlist) ? 0u : ((1u << 2) | 1u);  // not stepping or clean and ready: settled
   }
@@ -1433,6 +1481,17 @@ __global__ void __launch_bounds__(kDetectThreads) k_lim_detect(const __grid_cons
     base = __shfl_sync(0xffffffffu, base, 0);
     if (wait) pend[base + __popc(wm & below)] = e;
   }
+}
+
+template <int P, typename T, bool STAGED>
+__global__ void __launch_bounds__(kDetectThreads) k_lim_detect(const __grid_constant__ KParams<P, T> kp,
+                                                               const T* __restrict__ U,
+                                                               unsigned char* __restrict__ t0,
+                                                               unsigned int* __restrict__ status,
+                                                               int* __restrict__ wl1, int* __restrict__ pend,
+                                                               const int* __restrict__ order) {
+  __shared__ __align__(16) unsigned char s_det[DetectSmem<P, T>::kBytes];
+  lim_detect_body<P, T, STAGED>(kp, U, t0, status, wl1, pend, order, blockIdx.x, reinterpret_cast<T*>(s_det));
 }
 
 template <int P, typename T, bool QUEUE>
@@ -1656,13 +1715,12 @@ __device__ __forceinline__ bool step_runs(const InstCtl& c) {
 }
 
 template <int P, typename T>
-__global__ void __launch_bounds__(256) k_step_head(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U) {
+__device__ __forceinline__ void step_head_elems(const KParams<P, T>& kp, const T* __restrict__ U, int bid) {
   using V = Variant<P>;
   constexpr int NB = V::NB;
   const MeshDev& m = kp.m;
   InstCtl* ic = kp.ic;
-  Control* ctl = kp.ctl;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = bid * blockDim.x + threadIdx.x;
   const int ec = e < m.ne ? e : m.ne - 1;
   const int inst = m.n_inst > 1 ? m.inst[ec] : 0;
   unsigned long long bits = 0x7ff0000000000000ull;
@@ -1698,19 +1756,25 @@ __global__ void __launch_bounds__(256) k_step_head(const __grid_constant__ KPara
   } else if (bits != 0x7ff0000000000000ull) {
     atomicMin(&ic[inst].dt_bits, bits);
   }
-  // the last block closes the head: loop condition and clamped dt of every instance
+}
+
+// True in the last block of the launch to get here (counted in ctl->head_done, reset by it).
+__device__ __forceinline__ bool last_block_in(Control* ctl, unsigned int nblocks) {
   __shared__ bool s_last;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(&ctl->head_done, 1u) == gridDim.x - 1;
+  if (threadIdx.x == 0) s_last = atomicAdd(&ctl->head_done, 1u) == nblocks - 1;
   __syncthreads();
-  if (!s_last) return;
+  if (!s_last) return false;
   __threadfence();
-  if (threadIdx.x == 0) {
-    ctl->head_done = 0u;
-    ctl->troubled = 0;
-  }
-  for (int i = threadIdx.x; i < m.n_inst; i += blockDim.x) {
+  if (threadIdx.x == 0) ctl->head_done = 0u;
+  return true;
+}
+
+// Closes the step head of the instances ic[0, n_inst): loop condition and clamped dt.
+__device__ __forceinline__ void step_head_close(Control* ctl, InstCtl* ic, int n_inst) {
+  if (threadIdx.x == 0) ctl->troubled = 0;
+  for (int i = threadIdx.x; i < n_inst; i += blockDim.x) {
     InstCtl& c = ic[i];
     const int act = step_runs(c) ? 1 : 0;
     c.active = act;
@@ -1722,6 +1786,13 @@ __global__ void __launch_bounds__(256) k_step_head(const __grid_constant__ KPara
       c.dt = dt;
     }
   }
+}
+
+template <int P, typename T>
+__global__ void __launch_bounds__(256) k_step_head(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U) {
+  step_head_elems<P, T>(kp, U, blockIdx.x);
+  // the last block closes the head: loop condition and clamped dt of every instance
+  if (last_block_in(kp.ctl, gridDim.x)) step_head_close(kp.ctl, kp.ic, kp.m.n_inst);
 }
 
 // temporal_disc.rs:32-33

@@ -491,34 +491,51 @@ class Batch:
     bounds and status.  All share one polynomial order, hcr, precision and limiter setting.
     No counterpart in the reference (one mesh per run)."""
 
-    def __init__(self, meshes: list, order: int, hcr: float, cfls, final_times, final_steps,
+    def __init__(self, meshes: list, order, hcr: float, cfls, final_times, final_steps,
                  limiter: bool = True, device: int = 0, precision: str = "fp64", capacities=None):
-        """``capacities`` (optional): per instance a (elements, internal edges, boundary edges,
-        patches) room at least the mesh's, so that the slot can later take a larger mesh
-        (:meth:`replace`); see :func:`slot_capacity`."""
-        self.gauss_points, self.basis = default_tables(order)
+        """``order``: one polynomial order for every mesh, or a list with each mesh's order -- with
+        more than one order the context is a mixed batch (dgm_create_mixed: every kernel of a step
+        is one launch over all orders; FP64 or FP32).  ``capacities`` (optional): per instance a
+        (elements, internal edges, boundary edges, patches) room at least the mesh's, so that the
+        slot can later take a larger mesh (:meth:`replace`); see :func:`slot_capacity`."""
         self.meshes = list(meshes)
         n = len(self.meshes)
+        self.orders = [int(order)] * n if np.isscalar(order) else [int(p) for p in order]
+        if len(self.orders) != n:
+            raise ValueError("one order per mesh")
+        self.tables = {p: default_tables(p) for p in sorted(set(self.orders))}
+        self.mixed = len(self.tables) > 1
+        self.gauss_points, self.basis = self.tables[self.orders[0]]
         keep: list = []
         mds = (_native.MeshDesc * n)(*[_mesh_desc(m, keep) for m in self.meshes])
-        td = _tables_desc(self.basis, self.gauss_points, keep)
         prs = (_native.Params * n)(*[
             _native.Params(hcr=hcr, cfl=float(cfls[i]), final_time=float(final_times[i]),
                            final_step=int(final_steps[i]), limiter=1 if limiter else 0, device=device,
                            precision=PRECISIONS[precision], _reserved=0) for i in range(n)])
+        caps = None
+        if capacities is not None:
+            caps = (_native.SlotCapacity * n)(*[_native.SlotCapacity(*[int(x) for x in cap]) for cap in capacities])
         L = _native.lib()
         status = ctypes.c_int32(0)
-        if capacities is None:
-            ctx = L.dgm_create_batch(n, mds, ctypes.byref(td), prs, ctypes.byref(status))
+        if self.mixed:
+            tds = (_native.TablesDesc * 3)()
+            for p, (g, b) in self.tables.items():
+                tds[p - 1] = _tables_desc(b, g, keep)
+            orders = (ctypes.c_int32 * n)(*self.orders)
+            ctx = L.dgm_create_mixed(n, mds, orders, tds, prs, caps, ctypes.byref(status))
         else:
-            caps = (_native.SlotCapacity * n)(*[_native.SlotCapacity(*[int(x) for x in cap]) for cap in capacities])
-            ctx = L.dgm_create_batch_slots(n, mds, caps, ctypes.byref(td), prs, ctypes.byref(status))
+            td = _tables_desc(self.basis, self.gauss_points, keep)
+            if caps is None:
+                ctx = L.dgm_create_batch(n, mds, ctypes.byref(td), prs, ctypes.byref(status))
+            else:
+                ctx = L.dgm_create_batch_slots(n, mds, caps, ctypes.byref(td), prs, ctypes.byref(status))
         if not ctx:
-            raise DgmError(status.value, what="dgm_create_batch")
+            raise DgmError(status.value, what="dgm_create_mixed" if self.mixed else "dgm_create_batch")
         self._ctx = ctypes.c_void_p(ctx)
         self._lib = L
         self.n = n
         self.nb = self.basis.dof
+        self.nbs = [self.tables[p][1].dof for p in self.orders]
         self.precision = precision
         self.hcr = hcr
         self.limiter = limiter
@@ -562,7 +579,7 @@ class Batch:
             pass
 
     def upload(self, i: int, solutions: np.ndarray) -> None:
-        _check_state(solutions, self.meshes[i].n_elements, self.nb, "solutions")
+        _check_state(solutions, self.meshes[i].n_elements, self.nbs[i], "solutions")
         self._check(self._lib.dgm_instance_upload(self._ctx, i, _native.dptr(solutions)), "upload")
 
     def set_initial(self, i: int, initial: "InitialSolution") -> None:
@@ -572,7 +589,7 @@ class Batch:
                                                        float(initial.pressure)), "set_initial")
 
     def download(self, i: int) -> np.ndarray:
-        out = np.zeros((self.meshes[i].n_elements, 4, self.nb))
+        out = np.zeros((self.meshes[i].n_elements, 4, self.nbs[i]))
         self._check(self._lib.dgm_instance_download(self._ctx, i, _native.dptr(out)), "download")
         return out
 
@@ -599,7 +616,10 @@ class Batch:
         return _launch_config(self._lib, self._ctx)
 
     def autotune(self, repeats: int = 20) -> dict:
-        """As SpatialDisc.autotune, for the whole batch (all instances' states uploaded)."""
+        """As SpatialDisc.autotune, for the whole batch (all instances' states uploaded).  A mixed
+        batch runs fixed launch shapes and is not tuned (returns {})."""
+        if self.mixed:
+            return {}
         return _autotune(self._lib, self._ctx, repeats)
 
     def state(self, i: int):

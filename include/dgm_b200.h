@@ -302,6 +302,19 @@ dgm_ctx* dgm_create_batch_slots(int32_t n_instances, const dgm_mesh_desc* meshes
                                 const dgm_tables_desc* tables, const dgm_params* params, int32_t* status);
 int32_t dgm_instance_replace(dgm_ctx* ctx, int32_t i, const dgm_mesh_desc* mesh, const dgm_params* params);
 int32_t dgm_instance_capacity(dgm_ctx* ctx, int32_t i, dgm_slot_capacity* capacity);
+
+/* Mixed batch: instances of different polynomial orders (orders[i] in 1..3) advanced by the same
+ * launches -- every kernel of a step is one launch over all instances, each block running its
+ * instance's order (one persistent cooperative launch for the limiter's waves).  tables[P - 1]
+ * describes order P (only the orders present are read); params, capacity (may be NULL) and the
+ * instance numbering are as for dgm_create_batch_slots.  Precision 0 (FP64) or 1 (FP32).  The
+ * dgm_instance_*, dgm_advance*, dgm_synchronize, dgm_query, dgm_diagnostics, dgm_limiter_stats and
+ * dgm_device_bytes calls work on it; the single-mesh entry points and the launch-configuration
+ * calls return DGM_BAD_ARG.  Every instance's results are bitwise those of its order's batch.  No
+ * counterpart in the reference. */
+dgm_ctx* dgm_create_mixed(int32_t n_instances, const dgm_mesh_desc* meshes, const int32_t* orders,
+                          const dgm_tables_desc* tables /* [3] */, const dgm_params* params,
+                          const dgm_slot_capacity* capacity, int32_t* status);
 /* State of instance i in the reference layout, host <-> device-resident state. */
 int32_t dgm_instance_upload(dgm_ctx* ctx, int32_t i, const double* solutions);
 int32_t dgm_instance_download(dgm_ctx* ctx, int32_t i, double* solutions);

@@ -72,7 +72,7 @@ def parse():
     ap.add_argument("--profile-case", choices=["c2", "c3"],
                     help="run a fixed launch sequence for ncu (no timing, no autotuning): c2 = the workload "
                          "above, c3 = the 1024 x 512 p = 3 O-grid (M 0.7, AoA 2 deg)")
-    ap.add_argument("--precision", choices=["fp64", "fp32", "tf32", "tf32x3"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "fp32", "fp32_compute", "tf32", "tf32x3"], default="fp64")
     ap.add_argument("--launch", default="128,2368,128,1,0",
                     help="edge threads, edge blocks, element threads, staged limiter detector, lane-pair edge "
                          "pass, queue limiter schedule (profile case; the last two may be left out: 0)")
@@ -270,11 +270,12 @@ def load_traffic():
 # ------------------------------------------------------------------------------------------
 def run_batched(args, local):
     """256 seeded instances (Ni uniform on {32..256}, Nj = Ni/2, Mach U[0.3,0.85], AoA U[-4,6] deg,
-    p in {1,2}): DOF-stage updates/s of (a) FP32 batches, (b) FP32 batches with the basis
-    contractions on the tensor cores (split TF32 operands), (c) FP64 batches -- one batch context
-    per order, both groups on their own streams -- and (d) FP64 one instance at a time on a
-    DOF-weighted sample of 32 instances.  Inputs exceed the L2 (no flush needed); device time by
-    CUDA events."""
+    p in {1,2}): DOF-stage updates/s of (a) the FP32 mixed batch -- one context, one stream, every
+    kernel of a step one launch over all 256 instances of both orders -- (b) the FP64 mixed batch,
+    (c) for comparison, FP32 with one context per order on two streams (autotuned), and (d) FP64
+    one instance at a time on a DOF-weighted sample of 32 instances; accuracy of (a) against (b)
+    per instance, beside the FP64 conditioning floor (b started from a 1e-13 perturbed state).
+    Inputs exceed the L2 (no flush needed); device time by CUDA events."""
     import torch
     from dgm_in_rust_b200 import Batch, build_solver, forces_to_coefficients
     from dgm_in_rust_b200.workloads import batch_instances, instance_mesh
@@ -290,13 +291,13 @@ def run_batched(args, local):
            "instances": len(insts), "elements": int(sum(i.elements for i in insts)),
            "dof": int(sum(i.dofs for i in insts)), "steps": K, "warmup": W + W2}
 
-    def batched(precision, perturb=False):
+    def batched(precision, perturb=False, mixed=True):
         batches = []
-        for p, items in groups.items():
-            if not items:
-                continue
-            b = Batch([m for _, m, _ in items], p, HCR, [CFL] * len(items), [1.0e30] * len(items),
-                      [10 ** 12] * len(items), limiter=True, device=local, precision=precision)
+        sets = [(0, built)] if mixed else [(p, items) for p, items in groups.items() if items]
+        for p, items in sets:
+            b = Batch([m for _, m, _ in items], [inst.order for inst, _, _ in items] if mixed else p, HCR,
+                      [CFL] * len(items), [1.0e30] * len(items), [10 ** 12] * len(items), limiter=True, device=local,
+                      precision=precision)
             for i, (_, m, init) in enumerate(items):
                 b.set_initial(i, init)
                 if perturb:  # the FP64 conditioning floor: a start perturbed by 1e-13 (seeded)
@@ -334,19 +335,20 @@ def run_batched(args, local):
         # end states for the accuracy comparison: C_L / C_D of every instance, the density field
         # of every 8th instance of each group
         acc = {}
-        for (p, items), b in zip([(p, it) for p, it in groups.items() if it], batches):
+        for (p, items), b in zip(sets, batches):
             d = b.diagnostics()
             for i, (inst, m, _) in enumerate(items):
                 cl, cd = forces_to_coefficients(d[i, 4], d[i, 5], inst.aoa, 1.0, inst.mach)
                 rho = b.download(i)[:, 0].copy() if i % 8 == 0 else None
-                w = (b.basis.mass_mat_diag[None, :] * (0.5 * m.elem_jacob_det)[:, None]) if rho is not None else None
-                acc[(p, i)] = (cl, cd, rho, w)
+                mass = b.tables[inst.order][1].mass_mat_diag
+                w = (mass[None, :] * (0.5 * m.elem_jacob_det)[:, None]) if rho is not None else None
+                acc[(inst.order, id(m))] = (cl, cd, rho, w)
         for b in batches:
             b.close()
         return res["dof"] * 3 * K / (ms * 1e-3), ms / K, dev_bytes, acc
 
     v32, ms32, bytes32, acc32 = batched("fp32")
-    vtc, mstc, bytestc, acctc = batched("tf32x3")
+    v32s, ms32s, _, _ = batched("fp32", mixed=False)
     v64, ms64, bytes64, acc64 = batched("fp64")
     _, _, _, accp = batched("fp64", perturb=True)
     floor_cl = {k: abs(accp[k][0] - acc64[k][0]) for k in acc64}
@@ -374,7 +376,6 @@ def run_batched(args, local):
         "instances_below_1e-4": int(sum(floor_cl[k] <= 1e-4 and floor_cd[k] <= 1e-4 for k in floor_cl)),
         "per_instance_abs_delta_cl": {f"p{k[0]}_{k[1]}": v for k, v in floor_cl.items()}}
     res["fp32_vs_fp64_after_steps"] = versus(acc32)
-    res["tf32x3_vs_fp64_after_steps"] = versus(acctc)
     # one at a time, FP64: a DOF-weighted sample (every 8th instance in DOF order)
     order = sorted(range(len(built)), key=lambda k: built[k][0].dofs)
     sample = [built[k] for k in order[::max(1, len(built) // 32)]]
@@ -396,8 +397,10 @@ def run_batched(args, local):
         s.close()
     v_single = tot_dof * 3 * K / (tot_ms * 1e-3)
     res.update({
-        "fp32_batched": v32, "tf32x3_batched": vtc, "fp64_batched": v64, "fp64_one_at_a_time": v_single,
-        "ms_per_step_tf32x3_batched": mstc,
+        "fp32_batched": v32, "fp64_batched": v64, "fp64_one_at_a_time": v_single,
+        "fp32_one_context_per_order_two_streams": v32s, "ms_per_step_fp32_two_streams": ms32s,
+        "launch_structure": "mixed batch: one context, one stream, one launch per kernel of the step over all "
+                            "instances of both orders (14 launches per step, CUDA graphs of 8 steps)",
         "ms_per_step_fp32_batched": ms32, "ms_per_step_fp64_batched": ms64,
         "device_bytes_fp32": bytes32, "device_bytes_fp64": bytes64,
         "speedup_fp32_batched_vs_fp64_one_at_a_time": v32 / v_single,
@@ -439,7 +442,8 @@ def accuracy_report(U, U64, cl, cd, cl64, cd64, floor, w, wall, tol=1e-4):
             "abs_delta_cl": dcl, "abs_delta_cd": dcd,
             "fp64_floor_abs_delta_cl": floor[0], "fp64_floor_abs_delta_cd": floor[1],
             "meets_1e-4": bool(dcl <= tol and dcd <= tol),
-            "floor_below_1e-4": bool(floor[0] <= tol and floor[1] <= tol)}
+            "floor_below_1e-4": bool(floor[0] <= tol and floor[1] <= tol),
+            "within_twice_the_floor": bool(dcl <= 2 * floor[0] and dcd <= 2 * floor[1])}
 
 
 def precision_case(inst, K, modes, local, label):
@@ -530,11 +534,11 @@ def run_precision(args, local):
     the FP64 floor.  CUDA events on the library stream."""
     from dgm_in_rust_b200.workloads import Instance
     K = args.precision_steps
-    c3 = precision_case(Instance(1024, 512, 0.7, 2.0, 3), K, ("fp32", "tf32", "tf32x3"), local,
+    c3 = precision_case(Instance(1024, 512, 0.7, 2.0, 3), K, ("fp32", "fp32_compute", "tf32", "tf32x3"), local,
                         f"naca0012_ogrid_1024x512_p3: 1,048,576 triangles, 10 modes, M=0.7, AoA=2deg, limiter on, "
                         f"CFL 0.1, free-stream start, {K} steps")
     K2 = args.precision_c2_steps
-    c2 = precision_case(Instance(512, 64, 0.5, 2.0, 2), K2, ("fp32", "tf32x3"), local,
+    c2 = precision_case(Instance(512, 64, 0.5, 2.0, 2), K2, ("fp32", "fp32_compute", "tf32x3"), local,
                         f"naca0012_ogrid_512x64_p2: 65,536 triangles, 6 modes, M=0.5, AoA=2deg, limiter on, CFL 0.1, "
                         f"free-stream start, {K2} steps (first wall cell 4e-4 chords)")
     c3["well_conditioned_65536"] = c2
@@ -758,6 +762,20 @@ def run_ours(args):
         line["precision"] = run_precision(args, local)
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving(args, local)
+    # the metric's comparison and latencies, lifted from the secondary measurements
+    if "batched" in line:
+        b = line["batched"]
+        line["batched_fp32_vs_plain_fp64"] = {
+            "fp32_batched_dof_stage_per_s": b["fp32_batched"], "fp64_one_at_a_time_dof_stage_per_s": b["fp64_one_at_a_time"],
+            "ratio": b["speedup_fp32_batched_vs_fp64_one_at_a_time"],
+            "ratio_vs_fp64_batched": b["speedup_fp32_batched_vs_fp64_batched"], "steps": b["steps"]}
+    if "serving" in line:
+        line["serving_latency_s"] = {
+            rate: {"fp32_serving_p50": r["fp32_serving"]["p50_s"], "fp32_serving_p99": r["fp32_serving"]["p99_s"],
+                   "fp64_one_at_a_time_p50": r["fp64_one_at_a_time"]["p50_s"],
+                   "fp64_one_at_a_time_p99": r["fp64_one_at_a_time"]["p99_s"],
+                   "converged": r["fp32_serving"]["converged"]}
+            for rate, r in line["serving"]["rates"].items()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         v, done, el = time_cpu(raw, 1000, 1, threads, budget_s=12.0)

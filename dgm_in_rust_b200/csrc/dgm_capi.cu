@@ -47,7 +47,7 @@ struct dgm_ctx {
   cudaMemPool_t pool = nullptr;  // the device's context pool (held while the context lives)
   int P = 0, nb = 0, nq = 0, ng = 0;
   int prec = 0;       // storage: 0 FP64 state, 1 FP32 state and bulk arithmetic
-  int prec_mode = 0;  // dgm_params::precision (0 fp64, 1 fp32, 2 tf32, 3 tf32x3)
+  int prec_mode = 0;  // dgm_params::precision (0 fp64, 1 fp32, 2 tf32, 3 tf32x3, 4 fp32 arithmetic, fp64 state)
   int tc_split = 0;   // element pass on the tensor cores: 0 no (FP32 FMA), 1 TF32, 3 3xTF32
   int64_t ne = 0, ld = 0, n_int = 0, n_bnd = 0, np = 0, max_inst_ne = 0;
   int limiter = 1;
@@ -192,23 +192,26 @@ KParams<P, T>& kp_of(dgm_ctx* c) {
 // ---------------------------------------------------------------------------------------------
 // Kernel launch helpers, one instantiation per (order, storage type).
 // ---------------------------------------------------------------------------------------------
-template <int P, typename T>
+// T: the arithmetic type of the bulk kernels (and of the edge-flux array); St: the state's
+// storage type (St = double, T = float: FP32 arithmetic on an FP64 state).
+template <int P, typename T, typename St = T>
 struct Ops {
   using V = dgm::Variant<P>;
-  static T* S(void* p) { return static_cast<T*>(p); }
+  static St* S(void* p) { return static_cast<St*>(p); }
+  static T* Fx(void* p) { return static_cast<T*>(p); }
 
-  static int edge_flux(dgm_ctx* c, const T* U) {
+  static int edge_flux(dgm_ctx* c, const St* U) {
     const int threads = c->edge_threads;
     if (c->edge_pair) {  // a warp covers 16 slots per iteration
       const int64_t warps = (c->n_int + c->n_bnd + 15) / 16;
       const int64_t full = std::max<int64_t>(1, (warps * 32 + threads - 1) / threads);
       const int blocks = (int)(c->edge_blocks > 0 ? std::min<int64_t>(c->edge_blocks, full) : full);
-      dgm::k_edge_flux_pair<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, S(c->F));
+      dgm::k_edge_flux_pair<P, T, St><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, Fx(c->F));
     } else {
       const int64_t total = (c->n_int + c->n_bnd) * V::NG;
       const int64_t full = std::max<int64_t>(1, (total + threads - 1) / threads);
       const int blocks = (int)(c->edge_blocks > 0 ? std::min<int64_t>(c->edge_blocks, full) : full);
-      dgm::k_edge_flux<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, S(c->F));
+      dgm::k_edge_flux<P, T, St><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, Fx(c->F));
     }
     CK(cudaGetLastError());
     return DGM_OK;
@@ -233,28 +236,28 @@ struct Ops {
   }
 
   template <int MODE>
-  static int element(dgm_ctx* c, const T* Uin, const T* Ubase, T* Uout, const T* Rin, T* Rout) {
-    if constexpr (std::is_same<T, float>::value) {
+  static int element(dgm_ctx* c, const St* Uin, const St* Ubase, St* Uout, const St* Rin, St* Rout) {
+    if constexpr (std::is_same<T, float>::value && std::is_same<St, float>::value) {
       if (c->tc_split == 1) return element_tc<MODE, 1>(c, Uin, Ubase, Uout, Rin, Rout);
       if (c->tc_split == 3) return element_tc<MODE, 3>(c, Uin, Ubase, Uout, Rin, Rout);
     }
     const int threads = c->elem_threads;  // warps of 8 elements, 4 threads (variables) per element
     const int per_block = threads / 4;
     const int blocks = (int)std::max<int64_t>(1, (c->ne + per_block - 1) / per_block);
-    dgm::k_element<P, T, MODE><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), Uin, Ubase, S(c->F), Uout, Rin,
+    dgm::k_element<P, T, MODE, St><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), Uin, Ubase, Fx(c->F), Uout, Rin,
                                                                    Rout);
     CK(cudaGetLastError());
     return DGM_OK;
   }
 
-  static int limiter(dgm_ctx* c, T* U) {
+  static int limiter(dgm_ctx* c, St* U) {
     if (!c->limiter) return DGM_OK;
     const int dblocks = (int)std::max<int64_t>(1, (c->ld / 32 + dgm::kDetectWarps - 1) / dgm::kDetectWarps);
     if (c->lim_staged)
-      dgm::k_lim_detect<P, T, true><<<dblocks, dgm::kDetectThreads, 0, c->stream>>>(kp_of<P, T>(c), U, c->t0, c->status,
+      dgm::k_lim_detect<P, T, true, St><<<dblocks, dgm::kDetectThreads, 0, c->stream>>>(kp_of<P, T>(c), U, c->t0, c->status,
                                                                                    c->wl1, c->pend, c->order);
     else
-      dgm::k_lim_detect<P, T, false><<<dblocks, dgm::kDetectThreads, 0, c->stream>>>(kp_of<P, T>(c), U, c->t0,
+      dgm::k_lim_detect<P, T, false, St><<<dblocks, dgm::kDetectThreads, 0, c->stream>>>(kp_of<P, T>(c), U, c->t0,
                                                                                     c->status, c->wl1, c->pend, c->order);
     CK(cudaGetLastError());
     cudaLaunchConfig_t cfg = {};
@@ -267,38 +270,38 @@ struct Ops {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    auto kern = c->lim_queue ? dgm::k_limiter<P, T, true> : dgm::k_limiter<P, T, false>;
+    auto kern = c->lim_queue ? dgm::k_limiter<P, T, true, St> : dgm::k_limiter<P, T, false, St>;
     CK(cudaLaunchKernelEx(&cfg, kern, kp_of<P, T>(c), U, (const unsigned char*)c->t0, c->status, c->work,
                           (const int*)c->wl1, (const int*)c->pend));
     return DGM_OK;
   }
 
-  static int step_head(dgm_ctx* c, const T* U) {
+  static int step_head(dgm_ctx* c, const St* U) {
     const int threads = 256;
     const int blocks = (int)std::max<int64_t>(1, (c->ne + threads - 1) / threads);
-    dgm::k_step_head<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U);
+    dgm::k_step_head<P, T, St><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U);
     CK(cudaGetLastError());
     return DGM_OK;
   }
 
-  static int time_step(dgm_ctx* c, const T* U) {
+  static int time_step(dgm_ctx* c, const St* U) {
     const int threads = 256;
     const int blocks = (int)std::max<int64_t>(1, (c->ne + threads - 1) / threads);
-    dgm::k_time_step<P, T><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U);
+    dgm::k_time_step<P, T, St><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U);
     CK(cudaGetLastError());
     return DGM_OK;
   }
 
-  static int diagnostics(dgm_ctx* c, const T* R) {
-    dgm::k_diagnostics<P, T><<<(int)c->inst.size(), 256, 0, c->stream>>>(kp_of<P, T>(c), S(c->U), R, c->d_elem_rng,
+  static int diagnostics(dgm_ctx* c, const St* R) {
+    dgm::k_diagnostics<P, T, St><<<(int)c->inst.size(), 256, 0, c->stream>>>(kp_of<P, T>(c), S(c->U), R, c->d_elem_rng,
                                                                           c->d_bslot_rng, c->d_diag);
     CK(cudaGetLastError());
     return DGM_OK;
   }
 
   // One SSP-RK3 step on the resident state (rk3.rs:7-26); dt is read from the control blocks.
-  static int rk3(dgm_ctx* c, T* Rout) {
-    T *U = S(c->U), *U1 = S(c->U1), *U2 = S(c->U2);
+  static int rk3(dgm_ctx* c, St* Rout) {
+    St *U = S(c->U), *U1 = S(c->U1), *U2 = S(c->U2);
     int st;
     if ((st = edge_flux(c, U))) return st;
     if ((st = element<1>(c, U, nullptr, U1, nullptr, nullptr))) return st;
@@ -312,7 +315,7 @@ struct Ops {
   }
 
   // One iteration of time_march (temporal_disc.rs:22-33) for every instance, on the device.
-  static int step(dgm_ctx* c, T* Rout) {
+  static int step(dgm_ctx* c, St* Rout) {
     const int n = (int)c->inst.size();
     const int tb = 128, nblk = (n + tb - 1) / tb;
     int st;
@@ -327,7 +330,7 @@ struct Ops {
   static int to_storage(dgm_ctx* c, const double* src, void* dst, int64_t elem_off, int64_t ne) {
     const long long n = (long long)ne * NEQ * V::NB;
     const int threads = 256;
-    if constexpr (std::is_same<T, float>::value) {
+    if constexpr (std::is_same<St, float>::value) {
       dgm::k_f64_to_f32<<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(
           src, S(dst) + elem_off * NEQ * V::NB, n);
       CK(cudaGetLastError());
@@ -337,7 +340,7 @@ struct Ops {
   static int cell_fields(dgm_ctx* c, int64_t i, double* dst) {
     const HostInst& h = c->inst[i];
     const int threads = 256;
-    dgm::k_cell_fields<P, T><<<(int)((h.ne + threads - 1) / threads), threads, 0, c->stream>>>(
+    dgm::k_cell_fields<P, T, St><<<(int)((h.ne + threads - 1) / threads), threads, 0, c->stream>>>(
         kp_of<P, T>(c), S(c->U), (int)h.elem_off, (int)h.ne, dst);
     CK(cudaGetLastError());
     return DGM_OK;
@@ -368,7 +371,7 @@ struct Ops {
     for (int v = 0; v < NEQ; ++v) pr.q[v] = q[v];
     const HostInst& h = c->inst[i];
     const int threads = 256;
-    dgm::k_project_uniform<P, T><<<(int)((h.ne + threads - 1) / threads), threads, 0, c->stream>>>(
+    dgm::k_project_uniform<P, St><<<(int)((h.ne + threads - 1) / threads), threads, 0, c->stream>>>(
         pr, kp_of<P, T>(c).m.jac, S(c->U), (int)h.elem_off, (int)h.ne, (int)c->ld);
     CK(cudaGetLastError());
     return DGM_OK;
@@ -376,7 +379,7 @@ struct Ops {
   static int from_storage(dgm_ctx* c, const void* src, double* dst, int64_t elem_off, int64_t ne) {
     const long long n = (long long)ne * NEQ * V::NB;
     const int threads = 256;
-    if constexpr (std::is_same<T, float>::value) {
+    if constexpr (std::is_same<St, float>::value) {
       dgm::k_f32_to_f64<<<(int)((n + threads - 1) / threads), threads, 0, c->stream>>>(
           static_cast<const float*>(src) + elem_off * NEQ * V::NB, dst, n);
       CK(cudaGetLastError());
@@ -387,8 +390,8 @@ struct Ops {
   static int occupancy(dgm_ctx* c) {
     int per_sm[2] = {0, 0};
     const int threads = dgm::kLimiterWarps * 32;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], dgm::k_limiter<P, T, false>, threads, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], dgm::k_limiter<P, T, true>, threads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], dgm::k_limiter<P, T, false, St>, threads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], dgm::k_limiter<P, T, true, St>, threads, 0));
     const int64_t want = std::max<int64_t>(1, (c->ne + 32 * dgm::kLimiterWarps - 1) / (32 * dgm::kLimiterWarps));
     for (int q = 0; q < 2; ++q)
       c->coop_blocks[q] = (int)std::min<int64_t>((int64_t)std::max(1, per_sm[q]) * c->num_sms, want);
@@ -451,6 +454,14 @@ struct Ops {
 
 template <class F>
 int dispatch(dgm_ctx* c, F&& f) {
+  if (c->prec_mode == 4) {  // FP32 arithmetic on an FP64 state
+    switch (c->P) {
+      case 1: return f(Ops<1, float, double>{});
+      case 2: return f(Ops<2, float, double>{});
+      case 3: return f(Ops<3, float, double>{});
+    }
+    return DGM_BAD_ARG;
+  }
   if (c->prec == 0) {
     switch (c->P) {
       case 1: return f(Ops<1, double>{});
@@ -467,7 +478,9 @@ int dispatch(dgm_ctx* c, F&& f) {
   return DGM_BAD_ARG;
 }
 
-size_t elem_bytes(const dgm_ctx* c) { return c->prec == 0 ? sizeof(double) : sizeof(float); }
+// Bytes of one state coefficient (storage) and of one edge-flux value (arithmetic).
+size_t elem_bytes(const dgm_ctx* c) { return (c->prec == 0 || c->prec_mode == 4) ? sizeof(double) : sizeof(float); }
+size_t flux_bytes(const dgm_ctx* c) { return c->prec == 0 ? sizeof(double) : sizeof(float); }
 
 int read_control(dgm_ctx* c, Control* h, std::vector<InstCtl>* hi) {
   CK(cudaMemcpyAsync(h, c->ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
@@ -536,7 +549,7 @@ int set_active(dgm_ctx* c, double dt, bool set_dt) {
 int upload_state(dgm_ctx* c, int64_t i, const double* host, void* dst) {
   const HostInst& h = c->inst[i];
   const size_t n = (size_t)h.ne * NEQ * c->nb;
-  if (c->prec == 0) {
+  if (elem_bytes(c) == sizeof(double)) {
     CK(cudaMemcpyAsync(static_cast<double*>(dst) + (size_t)h.elem_off * NEQ * c->nb, host, n * sizeof(double),
                        cudaMemcpyHostToDevice, c->stream));
     return DGM_OK;
@@ -548,7 +561,7 @@ int upload_state(dgm_ctx* c, int64_t i, const double* host, void* dst) {
 int download_state(dgm_ctx* c, int64_t i, const void* src, double* host) {
   const HostInst& h = c->inst[i];
   const size_t n = (size_t)h.ne * NEQ * c->nb;
-  if (c->prec == 0) {
+  if (elem_bytes(c) == sizeof(double)) {
     CK(cudaMemcpyAsync(host, static_cast<const double*>(src) + (size_t)h.elem_off * NEQ * c->nb, n * sizeof(double),
                        cudaMemcpyDeviceToHost, c->stream));
   } else {
@@ -1004,7 +1017,7 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_slot_capacity
     *status = DGM_NO_DEVICE;
     return nullptr;
   }
-  if (!variant_ok(tables) || params->precision < 0 || params->precision > 3) {
+  if (!variant_ok(tables) || params->precision < 0 || params->precision > 4) {
     *status = DGM_BAD_ARG;
     return nullptr;
   }
@@ -1065,7 +1078,7 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_slot_capacity
   const size_t eb = elem_bytes(c);
   if ((st = dev_alloc_bytes(c, &c->U, n_state * eb)) || (st = dev_alloc_bytes(c, &c->U1, n_state * eb)) ||
       (st = dev_alloc_bytes(c, &c->U2, n_state * eb)) || (st = dev_alloc_bytes(c, &c->R, n_state * eb)) ||
-      (st = dev_alloc_bytes(c, &c->F, n_flux * eb)) ||
+      (st = dev_alloc_bytes(c, &c->F, n_flux * flux_bytes(c))) ||
       (st = dev_alloc(c, &c->stage, (size_t)c->max_inst_ne * NEQ * c->nb)) ||
       (st = dev_alloc(c, &c->t0, (size_t)c->ne)) || (st = dev_alloc(c, &c->status, (size_t)c->ne)) ||
       (st = dev_alloc(c, &c->work, (size_t)c->ne)) || (st = dev_alloc(c, &c->wl1, (size_t)c->ne)) ||

@@ -517,12 +517,27 @@ __device__ __forceinline__ void store_flux(T* F, size_t s, int NG, int g, const 
 // slip-wall pressure flux or characteristic far-field flux (apply_bc_euler,
 // boundary_condition.rs:19-97).  Writes F[slot][g][v] * half length.  Slots of instances that
 // are not stepping are skipped.
+// An element's record loaded from storage type S and converted to the arithmetic type T (FP64
+// storage with FP32 arithmetic; the plain load when the types agree).
+template <int NB, typename S, typename T, bool L1 = false>
+__device__ __forceinline__ void load_elem_as(const S* __restrict__ U, int e, T (&u)[NEQ * NB]) {
+  if constexpr (std::is_same<S, T>::value) {
+    load_elem<NB, T, L1>(U, e, u);
+  } else {
+    S w[NEQ * NB];
+    load_elem<NB, S, L1>(U, e, w);
+#pragma unroll
+    for (int i = 0; i < NEQ * NB; ++i) u[i] = T(w[i]);
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // The kernels' bodies take their block index and block count within the launch (bid, nblk) as
 // arguments, so that a launch over several meshes of different orders (a mixed batch) can give each
 // order's body its own range of blocks; the single-order kernels pass blockIdx.x and gridDim.x.
-template <int P, typename T>
-__device__ __forceinline__ void edge_flux_body(const KParams<P, T>& kp, const T* __restrict__ U, T* __restrict__ F,
+// S is the state's storage type (FP64 storage with FP32 arithmetic: S = double, T = float).
+template <int P, typename T, typename S = T>
+__device__ __forceinline__ void edge_flux_body(const KParams<P, T>& kp, const S* __restrict__ U, T* __restrict__ F,
                                                int bid, int nblk) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
@@ -543,8 +558,8 @@ __device__ __forceinline__ void edge_flux_body(const KParams<P, T>& kp, const T*
       const T* pl = &s_pe[((ic & 3) * NG + g) * NB];
       const T* pr = &s_pe[((ic >> 2) * NG + (NG - 1 - g)) * NB];
       T ul[NEQ * NB], ur[NEQ * NB];
-      load_elem<NB, T>(U, lr.x, ul);
-      load_elem<NB, T>(U, lr.y, ur);
+      load_elem_as<NB, S, T>(U, lr.x, ul);
+      load_elem_as<NB, S, T>(U, lr.y, ur);
       T lv[4], rv[4];
 #pragma unroll
       for (int v = 0; v < NEQ; ++v) {
@@ -570,7 +585,7 @@ __device__ __forceinline__ void edge_flux_body(const KParams<P, T>& kp, const T*
       const int info = m.be_info[sb];
       const T* pe = &s_pe[((info & 3) * NG + g) * NB];
       T ue[NEQ * NB];
-      load_elem<NB, T>(U, e, ue);
+      load_elem_as<NB, S, T>(U, e, ue);
       T lv[4];
 #pragma unroll
       for (int v = 0; v < NEQ; ++v) {
@@ -588,10 +603,10 @@ __device__ __forceinline__ void edge_flux_body(const KParams<P, T>& kp, const T*
   }
 }
 
-template <int P, typename T>
+template <int P, typename T, typename S = T>
 __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KParams<P, T> kp,
-                                                      const T* __restrict__ U, T* __restrict__ F) {
-  edge_flux_body<P, T>(kp, U, F, blockIdx.x, gridDim.x);
+                                                      const S* __restrict__ U, T* __restrict__ F) {
+  edge_flux_body<P, T, S>(kp, U, F, blockIdx.x, gridDim.x);
 }
 
 // The same edge pass with two lanes per edge slot, one per side: each lane loads its element's
@@ -600,8 +615,8 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
 // for HLLC / the boundary flux.  Each element's state is loaded once per slot instead of once per
 // point; every trace and flux is the same expression in the same order as in k_edge_flux, so the
 // results are bitwise identical.  A warp covers 16 consecutive slots per iteration.
-template <int P, typename T>
-__device__ __forceinline__ void edge_flux_pair_body(const KParams<P, T>& kp, const T* __restrict__ U,
+template <int P, typename T, typename S = T>
+__device__ __forceinline__ void edge_flux_pair_body(const KParams<P, T>& kp, const S* __restrict__ U,
                                                     T* __restrict__ F, int bid, int nblk) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
@@ -640,7 +655,7 @@ __device__ __forceinline__ void edge_flux_pair_body(const KParams<P, T>& kp, con
     }
     T u[NEQ * NB];
     if (has) {
-      load_elem<NB, T>(U, e, u);
+      load_elem_as<NB, S, T>(U, e, u);
     } else {
 #pragma unroll
       for (int i = 0; i < NEQ * NB; ++i) u[i] = T(0);
@@ -689,10 +704,10 @@ __device__ __forceinline__ void edge_flux_pair_body(const KParams<P, T>& kp, con
   }
 }
 
-template <int P, typename T>
+template <int P, typename T, typename S = T>
 __global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant__ KParams<P, T> kp,
-                                                           const T* __restrict__ U, T* __restrict__ F) {
-  edge_flux_pair_body<P, T>(kp, U, F, blockIdx.x, gridDim.x);
+                                                           const S* __restrict__ U, T* __restrict__ F) {
+  edge_flux_pair_body<P, T, S>(kp, U, F, blockIdx.x, gridDim.x);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -757,13 +772,15 @@ __device__ __forceinline__ void warp_store_records(T* dst, int e0, const T* sbuf
   __syncwarp();
 }
 
-template <int P, typename T, int MODE>
-__device__ __forceinline__ void element_body(const KParams<P, T>& kp, const T* __restrict__ Uin, const T* Ubase,
-                                             const T* __restrict__ F, T* Uout, const T* Rin, T* Rout, int bid) {
+// S is the state's storage type: with S = double and T = float the contractions, fluxes and the
+// residual are FP32 and the stage combination is evaluated in FP64 on the FP64 state.
+template <int P, typename T, int MODE, typename S = T>
+__device__ __forceinline__ void element_body(const KParams<P, T>& kp, const S* __restrict__ Uin, const S* Ubase,
+                                             const T* __restrict__ F, S* Uout, const S* Rin, S* Rout, int bid) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NQ = V::NQ, NG = V::NG;
-  constexpr int STRIDE = Staged<NB, T>::kStride;
-  __shared__ __align__(16) T s_rec[kElemMaxWarps][8 * STRIDE];
+  constexpr int STRIDE = Staged<NB, S>::kStride;
+  __shared__ __align__(16) S s_rec[kElemMaxWarps][8 * STRIDE];
   Control* ctl = kp.ctl;
   if (bid == 0 && threadIdx.x == 0) {  // counters of the limiter pass that follows
     ctl->t0_count = 0;
@@ -785,13 +802,15 @@ __device__ __forceinline__ void element_body(const KParams<P, T>& kp, const T* _
   const unsigned int keep = __ballot_sync(0xffffffffu, valid) & 0xffu;  // lanes 0-7: var 0 of each element
   if (!keep) return;  // no element of this warp is stepping (finished instances, slot padding)
   const size_t ld = m.ld;
-  T* sbuf = s_rec[threadIdx.x >> 5];
-  T* mine_rec = sbuf + i * STRIDE + var * NB;
-  warp_load_records<NB, T>(Uin, e0, sbuf, lane);
+  S* sbuf = s_rec[threadIdx.x >> 5];
+  S* mine_rec = sbuf + i * STRIDE + var * NB;
+  warp_load_records<NB, S>(Uin, e0, sbuf, lane);
+  S us[NB];
   T u[NB], r[NB];
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
-    u[b] = mine_rec[b];
+    us[b] = mine_rec[b];
+    u[b] = T(us[b]);
     r[b] = T(0);
   }
   const T J = T(m.jac[e]);
@@ -831,50 +850,50 @@ __device__ __forceinline__ void element_body(const KParams<P, T>& kp, const T* _
       for (int b = 0; b < NB; ++b) r[b] += fv * kp.t.phi_edge[k][gp][b];
     }
   }
-  const T dt = T(kp.ic[inst].dt);
+  const S dt = S(kp.ic[inst].dt);
   const T inv_half_j = T(1) / (T(0.5) * J);
   if constexpr (MODE == 0) {  // compute_residuals adds to the residual it is given
-    warp_load_records<NB, T>(Rin, e0, sbuf, lane);
+    warp_load_records<NB, S>(Rin, e0, sbuf, lane);
 #pragma unroll
-    for (int b = 0; b < NB; ++b) r[b] = mine_rec[b] + r[b];
+    for (int b = 0; b < NB; ++b) r[b] = T(mine_rec[b]) + r[b];
   }
 #pragma unroll
   for (int b = 0; b < NB; ++b) r[b] = r[b] * kp.t.inv_mass[b] * inv_half_j;  // divide_residual_by_mass_mat_diag
   if (Rout) {
 #pragma unroll
-    for (int b = 0; b < NB; ++b) mine_rec[b] = r[b];
-    warp_store_records<NB, T>(Rout, e0, sbuf, keep, lane);
+    for (int b = 0; b < NB; ++b) mine_rec[b] = S(r[b]);
+    warp_store_records<NB, S>(Rout, e0, sbuf, keep, lane);
   }
   if constexpr (MODE != 0) {
-    T base[NB];
+    S base[NB];
     if constexpr (MODE >= 2) {
-      warp_load_records<NB, T>(Ubase, e0, sbuf, lane);
+      warp_load_records<NB, S>(Ubase, e0, sbuf, lane);
 #pragma unroll
       for (int b = 0; b < NB; ++b) base[b] = mine_rec[b];
       __syncwarp();
     }
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      const T rr = r[b];
-      T out;
+      const S rr = S(r[b]);
+      S out;
       if constexpr (MODE == 1) {
-        out = u[b] + dt * rr;
+        out = us[b] + dt * rr;
       } else if constexpr (MODE == 2) {
-        out = T(0.75) * base[b] + T(0.25) * (u[b] + dt * rr);
+        out = S(0.75) * base[b] + S(0.25) * (us[b] + dt * rr);
       } else {
-        out = T(1.0 / 3.0) * base[b] + T(2.0 / 3.0) * (u[b] + dt * rr);
+        out = S(1.0 / 3.0) * base[b] + S(2.0 / 3.0) * (us[b] + dt * rr);
       }
       mine_rec[b] = out;
     }
-    warp_store_records<NB, T>(Uout, e0, sbuf, keep, lane);
+    warp_store_records<NB, S>(Uout, e0, sbuf, keep, lane);
   }
 }
 
-template <int P, typename T, int MODE>
+template <int P, typename T, int MODE, typename S = T>
 __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KParams<P, T> kp,
-                                                    const T* __restrict__ Uin, const T* Ubase,
-                                                    const T* __restrict__ F, T* Uout, const T* Rin, T* Rout) {
-  element_body<P, T, MODE>(kp, Uin, Ubase, F, Uout, Rin, Rout, blockIdx.x);
+                                                    const S* __restrict__ Uin, const S* Ubase,
+                                                    const T* __restrict__ F, S* Uout, const S* Rin, S* Rout) {
+  element_body<P, T, MODE, S>(kp, Uin, Ubase, F, Uout, Rin, Rout, blockIdx.x);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -886,8 +905,8 @@ __global__ void __launch_bounds__(256, 3) k_element(const __grid_constant__ KPar
 // ------------------------------------------------------------------------------------------
 // RO: U is only read during the kernel (neighbour traces through L1); OWN_SHARED: `own` is staged
 // in shared memory (plain loads), else it is e's record in U (loaded like the neighbours').
-template <int P, typename T, bool RO = false, bool OWN_SHARED = false>
-__device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restrict__ U, int e, const T* own) {
+template <int P, typename T, bool RO = false, bool OWN_SHARED = false, typename S = T>
+__device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const S* __restrict__ U, int e, const S* own) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
   const MeshDev& m = kp.m;
@@ -928,8 +947,8 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
       double rho_jump = 0.0, rho_e_jump = 0.0;
       const double jd = geo.w;
       double nrho[NB], nrhoe[NB];
-      load_var_modes<NB, T, 0, RO>(U, nb, nrho);
-      load_var_modes<NB, T, 3, RO>(U, nb, nrhoe);
+      load_var_modes<NB, S, 0, RO>(U, nb, nrho);
+      load_var_modes<NB, S, 3, RO>(U, nb, nrhoe);
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
         double er = 0.0, ere = 0.0;
@@ -958,9 +977,9 @@ __device__ __forceinline__ bool kxrcf(const KParams<P, T>& kp, const T* __restri
 // than kxrcf (which walks the faces one after another) at the price of registers: faster when
 // a pass is latency-bound (small meshes), slower when occupancy matters (large batches); the
 // autotuner picks one per context.  Same arithmetic in the same order, so the same flags.
-template <int P, typename T, bool RO = false, bool OWN_SHARED = false>
-__device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const T* __restrict__ U, int e,
-                                             const T* own_rec) {
+template <int P, typename T, bool RO = false, bool OWN_SHARED = false, typename S = T>
+__device__ __forceinline__ bool kxrcf_staged(const KParams<P, T>& kp, const S* __restrict__ U, int e,
+                                             const S* own_rec) {
   int fw[3], nb[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -1126,8 +1145,8 @@ struct WenoScratch {
   double pol_new[3][NEQ][V::NB];
 };
 
-template <int P, typename T>
-__device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __restrict__ U, int e,
+template <int P, typename T, typename Sto = T>
+__device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, Sto* __restrict__ U, int e,
                                                 const int (&faces)[3], const int (&nbrs)[3], int lane,
                                                 WenoScratch<P>& S) {
   using V = Variant<P>;
@@ -1284,7 +1303,7 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, T* __re
       for (int k = 0; k < NEQ; ++k) sum += S.R[f][r][k] * S.pol_new[f][k][b];
       recon = recon + sum * Jn[f] * 0.5;
     }
-    U[sx<NB>(e, r, b)] = T(recon * inv_area);
+    U[sx<NB>(e, r, b)] = Sto(recon * inv_area);
   }
   __syncwarp();
   return ST_OK;
@@ -1423,13 +1442,13 @@ struct DetectSmem {
   static constexpr size_t kBytes = (size_t)kDetectWarps * 32 * kStride * sizeof(T);
 };
 
-template <int P, typename T, bool STAGED>
-__device__ __forceinline__ void lim_detect_body(const KParams<P, T>& kp, const T* __restrict__ U,
+template <int P, typename T, bool STAGED, typename S = T>
+__device__ __forceinline__ void lim_detect_body(const KParams<P, T>& kp, const S* __restrict__ U,
                                                 unsigned char* __restrict__ t0, unsigned int* __restrict__ status,
                                                 int* __restrict__ wl1, int* __restrict__ pend,
-                                                const int* __restrict__ order, int bid, T* s_det) {
+                                                const int* __restrict__ order, int bid, S* s_det) {
   using V = Variant<P>;
-  constexpr int STRIDE = DetectSmem<P, T>::kStride;
+  constexpr int STRIDE = DetectSmem<P, S>::kStride;
   Control* ctl = kp.ctl;
   const MeshDev& m = kp.m;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1445,11 +1464,11 @@ __device__ __forceinline__ void lim_detect_body(const KParams<P, T>& kp, const T
   if (__any_sync(0xffffffffu, active)) {
     // the batch's records are contiguous: staged with coalesced 16-byte loads (arrays are padded
     // to whole batches)
-    T* recs = s_det + (size_t)wib * 32 * STRIDE;
-    warp_load_records<V::NB, T, 32>(U, e0, recs, lane);
+    S* recs = s_det + (size_t)wib * 32 * STRIDE;
+    warp_load_records<V::NB, S, 32>(U, e0, recs, lane);
     if (active) {
-      const T* own = recs + lane * STRIDE;
-      flag = STAGED ? kxrcf_staged<P, T, true, true>(kp, U, e, own) : kxrcf<P, T, true, true>(kp, U, e, own);
+      const S* own = recs + lane * STRIDE;
+      flag = STAGED ? kxrcf_staged<P, T, true, true, S>(kp, U, e, own) : kxrcf<P, T, true, true, S>(kp, U, e, own);
       bool ready = true;
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
@@ -1483,20 +1502,20 @@ __device__ __forceinline__ void lim_detect_body(const KParams<P, T>& kp, const T
   }
 }
 
-template <int P, typename T, bool STAGED>
+template <int P, typename T, bool STAGED, typename S = T>
 __global__ void __launch_bounds__(kDetectThreads) k_lim_detect(const __grid_constant__ KParams<P, T> kp,
-                                                               const T* __restrict__ U,
+                                                               const S* __restrict__ U,
                                                                unsigned char* __restrict__ t0,
                                                                unsigned int* __restrict__ status,
                                                                int* __restrict__ wl1, int* __restrict__ pend,
                                                                const int* __restrict__ order) {
-  __shared__ __align__(16) unsigned char s_det[DetectSmem<P, T>::kBytes];
-  lim_detect_body<P, T, STAGED>(kp, U, t0, status, wl1, pend, order, blockIdx.x, reinterpret_cast<T*>(s_det));
+  __shared__ __align__(16) unsigned char s_det[DetectSmem<P, S>::kBytes];
+  lim_detect_body<P, T, STAGED, S>(kp, U, t0, status, wl1, pend, order, blockIdx.x, reinterpret_cast<S*>(s_det));
 }
 
-template <int P, typename T, bool QUEUE>
+template <int P, typename T, bool QUEUE, typename S = T>
 __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_constant__ KParams<P, T> kp,
-                                                                T* __restrict__ U,
+                                                                S* __restrict__ U,
                                                                 const unsigned char* __restrict__ t0,
                                                                 unsigned int* __restrict__ status,
                                                                 int* __restrict__ work,
@@ -1524,7 +1543,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
       fwt[k] = m.face[k * m.ld + et];
       nbt[k] = m.nbr[k * m.ld + et];
     }
-    const int rs = weno_reconstruct<P, T>(kp, U, et, fwt, nbt, lane, *scratch_w);
+    const int rs = weno_reconstruct<P, T, S>(kp, U, et, fwt, nbt, lane, *scratch_w);
     if (rs != ST_OK && lane == 0) {
       const int inst = m.n_inst > 1 ? m.inst[et] : 0;
       raise_status(ctl, &kp.ic[inst], rs, et);
@@ -1569,8 +1588,8 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
         // (it is still pending, so nothing has rewritten it in this pass)
         if (pending && ready) {
           if (any_mod) {
-            const T* own = U + (size_t)e * (NEQ * Variant<P>::NB);
-            trouble = kxrcf<P, T>(kp, U, e, own);
+            const S* own = U + (size_t)e * (NEQ * Variant<P>::NB);
+            trouble = kxrcf<P, T, false, false, S>(kp, U, e, own);
           } else {
             trouble = t0[e] != 0;
           }
@@ -1660,8 +1679,8 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
 
 // compute_time_step, temporal_disc.rs:58-88: each instance's minimum over its elements
 // (FP64 arithmetic, deterministic: min of IEEE bit patterns of non-negative doubles).
-template <int P, typename T>
-__global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U) {
+template <int P, typename T, typename S = T>
+__global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KParams<P, T> kp, const S* __restrict__ U) {
   using V = Variant<P>;
   constexpr int NB = V::NB;
   const MeshDev& m = kp.m;
@@ -1670,8 +1689,8 @@ __global__ void __launch_bounds__(256) k_time_step(const __grid_constant__ KPara
   const int inst = m.n_inst > 1 ? m.inst[ec] : 0;
   unsigned long long bits = 0x7ff0000000000000ull;  // +inf never wins against 1e10
   if (e < m.ne && kp.ic[inst].active) {
-    T rec[NEQ * NB];
-    load_elem<NB, T, true>(U, e, rec);
+    S rec[NEQ * NB];
+    load_elem<NB, S, true>(U, e, rec);
     double s[NEQ];
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
@@ -1714,8 +1733,8 @@ __device__ __forceinline__ bool step_runs(const InstCtl& c) {
   return c.status == 0 && c.step < c.final_step && c.t < c.final_time;
 }
 
-template <int P, typename T>
-__device__ __forceinline__ void step_head_elems(const KParams<P, T>& kp, const T* __restrict__ U, int bid) {
+template <int P, typename T, typename S = T>
+__device__ __forceinline__ void step_head_elems(const KParams<P, T>& kp, const S* __restrict__ U, int bid) {
   using V = Variant<P>;
   constexpr int NB = V::NB;
   const MeshDev& m = kp.m;
@@ -1725,8 +1744,8 @@ __device__ __forceinline__ void step_head_elems(const KParams<P, T>& kp, const T
   const int inst = m.n_inst > 1 ? m.inst[ec] : 0;
   unsigned long long bits = 0x7ff0000000000000ull;
   if (e < m.ne && step_runs(ic[inst])) {
-    T rec[NEQ * NB];
-    load_elem<NB, T, true>(U, e, rec);
+    S rec[NEQ * NB];
+    load_elem<NB, S, true>(U, e, rec);
     double s[NEQ];
 #pragma unroll
     for (int v = 0; v < NEQ; ++v) {
@@ -1788,9 +1807,9 @@ __device__ __forceinline__ void step_head_close(Control* ctl, InstCtl* ic, int n
   }
 }
 
-template <int P, typename T>
-__global__ void __launch_bounds__(256) k_step_head(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U) {
-  step_head_elems<P, T>(kp, U, blockIdx.x);
+template <int P, typename T, typename S = T>
+__global__ void __launch_bounds__(256) k_step_head(const __grid_constant__ KParams<P, T> kp, const S* __restrict__ U) {
+  step_head_elems<P, T, S>(kp, U, blockIdx.x);
   // the last block closes the head: loop condition and clamped dt of every instance
   if (last_block_in(kp.ctl, gridDim.x)) step_head_close(kp.ctl, kp.ic, kp.m.n_inst);
 }
@@ -1829,9 +1848,9 @@ __global__ void k_set_active(Control* ctl, InstCtl* ic, int n_inst, double dt, i
 // i.e. the force on the body), sum of squares of the density residual's modal coefficients
 // (from R, when given), number of elements }.  Not part of the reference, which computes no
 // forces or norms.
-template <int P, typename T>
-__global__ void __launch_bounds__(256) k_diagnostics(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U,
-                                                     const T* __restrict__ R, const int* __restrict__ elem_rng,
+template <int P, typename T, typename S = T>
+__global__ void __launch_bounds__(256) k_diagnostics(const __grid_constant__ KParams<P, T> kp, const S* __restrict__ U,
+                                                     const S* __restrict__ R, const int* __restrict__ elem_rng,
                                                      const int* __restrict__ bslot_rng, double* __restrict__ out) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG, NQ = V::NQ;
@@ -1896,8 +1915,8 @@ __global__ void __launch_bounds__(256) k_diagnostics(const __grid_constant__ KPa
 // x and y velocity and pressure from the mode-0 coefficients, in FP64 with the reference's
 // expressions and operation order (no contraction into FMAs): velocity = momentum / density,
 // pressure = (hcr - 1) (energy - 0.5 density (u^2 + v^2)).  out is [ne][4].
-template <int P, typename T>
-__global__ void k_cell_fields(const __grid_constant__ KParams<P, T> kp, const T* __restrict__ U, int e0, int ne,
+template <int P, typename T, typename S = T>
+__global__ void k_cell_fields(const __grid_constant__ KParams<P, T> kp, const S* __restrict__ U, int e0, int ne,
                               double* __restrict__ out) {
   constexpr int NB = Variant<P>::NB;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

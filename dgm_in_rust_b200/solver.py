@@ -208,7 +208,9 @@ def _tables_desc(basis: DubinerBasis, g: GaussPoints, keep: list) -> "_native.Ta
 # (limiter, HLLC positivity checks, time step and diagnostics in FP64).  tf32 / tf32x3: as fp32,
 # with the element pass's two basis contractions on the tensor cores (TF32 operands, FP32
 # accumulation; tf32x3 splits each operand into a TF32 head and tail for FP32-level products).
-PRECISIONS = {"fp64": 0, "fp32": 1, "tf32": 2, "tf32x3": 3}
+# fp32_compute: FP64 state with the contractions, fluxes and residuals in FP32 (the stage
+# combinations, limiter, positivity checks, time step and diagnostics in FP64).
+PRECISIONS = {"fp64": 0, "fp32": 1, "tf32": 2, "tf32x3": 3, "fp32_compute": 4}
 
 
 class SpatialDisc:

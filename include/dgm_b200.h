@@ -156,7 +156,10 @@ typedef struct dgm_params {
    * diagnostics kept in FP64; 2 = as 1 with the element pass's two basis contractions
    * (basis -> quadrature points, quadrature and edge points -> basis) on the tensor cores
    * (tcgen05, TF32 operands, FP32 accumulation); 3 = as 2 with each operand split into a TF32
-   * head and tail (three products: FP32-level accuracy).  No counterpart in the reference. */
+   * head and tail (three products: FP32-level accuracy); 4 = FP64 state with FP32 contractions,
+   * fluxes and residuals (FP32 edge fluxes), the stage combinations, limiter, positivity checks,
+   * time step and diagnostics in FP64: the state does not round to FP32 each stage.  No
+   * counterpart in the reference. */
   int32_t precision;
   int32_t _reserved;
 } dgm_params;

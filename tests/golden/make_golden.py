@@ -20,7 +20,9 @@
   M 0.8, AoA 1.25 deg, free-stream start, CFL 0.1, limiter on) marched by the oracle for its
   configured 2000 steps, with checkpoints after 200 and 2000 steps: clock, per-(variable, mode)
   sums and sums of squares over all elements, and the full records of a sample of elements (every
-  128th element and every boundary element).  About 15 minutes on 8 host threads.
+  128th element and every boundary element); the same for the oracle's twin run started from the
+  initial state perturbed by 1e-15 (relative, seeded), whose distance from the first run is the
+  spread that round-off alone produces in this chaotic start.  About an hour on 8 host threads.
 
   python tests/golden/make_golden.py --c2-run
 
@@ -98,17 +100,10 @@ def c2_sample(ne, boundary_elements):
     return np.union1d(np.arange(0, ne, 128), boundary_elements).astype(np.int64)
 
 
-def c2_run(threads=8):
-    from dgm_in_rust_b200 import freestream_quantity, process_mesh
-    raw = naca0012_ogrid(256, 128)
-    fs = (1.25, 0.8, 1.0, 1.0 / 1.4)
-    mesh = process_mesh(raw, freestream_quantity(fs[1], fs[0], fs[2], fs[3], 1.4), 1.4)
-    o = Oracle(raw=raw, order=2, ncell_gp=6, nedge_gp=3, cfl=0.1, final_time=1.0e30, final_step=0,
-               limiter=True, threads=threads, freestream=fs)
-    U = o.initial_solution()
-    R = o.new_state()
-    sample = c2_sample(o.ne, mesh.boundary_element_indices)
-    out = {"sample": sample}
+C2_PERTURBATION = 1e-15  # relative, seeded normal: the round-off-sized twin run
+
+
+def _c2_march(o, U, R, sample, prefix, out):
     done, t = 0, 0.0
     for n in C2_CHECKPOINTS:
         while done < n:
@@ -116,13 +111,32 @@ def c2_run(threads=8):
             o.rk3(R, U, dt)
             t += dt
             done += 1
-        out[f"t{n}"] = np.array(t)
-        out[f"sum{n}"] = U.sum(axis=0)
-        out[f"sumsq{n}"] = (U * U).sum(axis=0)
-        out[f"U{n}"] = U[sample]
-        out[f"troubled{n}"] = np.array(int(o.troubled_flags(U).sum()))
-        print(f"c2: {n} steps, t = {t}", flush=True)
-    np.savez_compressed(os.path.join(HERE, "c2_run.npz"), **out)
+        out[f"{prefix}t{n}"] = np.array(t)
+        out[f"{prefix}sum{n}"] = U.sum(axis=0)
+        out[f"{prefix}sumsq{n}"] = (U * U).sum(axis=0)
+        out[f"{prefix}U{n}"] = U[sample]
+        out[f"{prefix}troubled{n}"] = np.array(int(o.troubled_flags(U).sum()))
+        print(f"c2 {prefix or 'oracle'}: {n} steps, t = {t}", flush=True)
+
+
+def c2_run(threads=8, only_twin=False):
+    """The oracle's run, and its twin from the initial state times (1 + 1e-15 N(0,1)) (seed 5): the
+    spread between the two measures how far round-off alone carries this impulsive start."""
+    from dgm_in_rust_b200 import freestream_quantity, process_mesh
+    raw = naca0012_ogrid(256, 128)
+    fs = (1.25, 0.8, 1.0, 1.0 / 1.4)
+    mesh = process_mesh(raw, freestream_quantity(fs[1], fs[0], fs[2], fs[3], 1.4), 1.4)
+    o = Oracle(raw=raw, order=2, ncell_gp=6, nedge_gp=3, cfl=0.1, final_time=1.0e30, final_step=0,
+               limiter=True, threads=threads, freestream=fs)
+    sample = c2_sample(o.ne, mesh.boundary_element_indices)
+    path = os.path.join(HERE, "c2_run.npz")
+    out = dict(np.load(path)) if only_twin else {"sample": sample}
+    if not only_twin:
+        _c2_march(o, o.initial_solution(), o.new_state(), sample, "", out)
+    U = o.initial_solution()
+    U *= 1.0 + C2_PERTURBATION * np.random.default_rng(5).standard_normal(U.shape)
+    _c2_march(o, U, o.new_state(), sample, "twin_", out)
+    np.savez_compressed(path, **out)
 
 
 def reference_files(checkout):

@@ -42,7 +42,7 @@ def _solo(mesh, init, steps, precision="fp64", order=2):
     return U, t, st
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32_compute"])
 def test_batch_instances_match_solo(precision):
     cases = [_case(naca0012_ogrid(32, 16), 0.5, 2.0), _case(naca0012_ogrid(48, 24, order="quad"), 0.8, 1.25),
              _case(airfoil_raw(), REF_FS[1], REF_FS[0], REF_FS[2], REF_FS[3])]
@@ -79,10 +79,13 @@ def test_batch_error_stays_in_its_instance():
     b.close()
 
 
-def test_fp32_accuracy_vs_fp64():
+@pytest.mark.parametrize("mode", ["fp32", "fp32_compute"])
+def test_fp32_accuracy_vs_fp64(mode):
+    """FP32 storage and arithmetic (fp32), and FP32 arithmetic on an FP64 state (fp32_compute):
+    density relative L2 <= 1e-5 and |dC_L|, |dC_D| <= 1e-4 after 200 steps."""
     mesh, init = _case(naca0012_ogrid(64, 32), 0.5, 2.0)
     out = {}
-    for prec in ("fp64", "fp32"):
+    for prec in ("fp64", mode):
         s = build_solver(mesh, 2, 1.4, 0.1, 1.0e30, 200, precision=prec)
         U = initial_state(mesh, s.basis, s.gauss_points, 1.4, init)
         td = s.temporal_disc
@@ -94,15 +97,16 @@ def test_fp32_accuracy_vs_fp64():
         d = s.spatial_disc.diagnostics()
         out[prec] = (V, forces_to_coefficients(d[4], d[5], 2.0, 1.0, 0.5))
         s.close()
-    (V32, (cl32, cd32)), (V64, (cl64, cd64)) = out["fp32"], out["fp64"]
+    (V32, (cl32, cd32)), (V64, (cl64, cd64)) = out[mode], out["fp64"]
     assert rel_l2(V32[:, 0], V64[:, 0]) <= 1e-5
     assert abs(cl32 - cl64) <= 1e-4 and abs(cd32 - cd64) <= 1e-4
 
 
-def test_fp32_residual_vs_oracle():
+@pytest.mark.parametrize("mode", ["fp32", "fp32_compute"])
+def test_fp32_residual_vs_oracle(mode):
     raw = naca0012_ogrid(64, 32)
     mesh, init = _case(raw, 0.8, 1.25)
-    s = build_solver(mesh, 2, 1.4, 0.1, 1.0e30, 1, precision="fp32")
+    s = build_solver(mesh, 2, 1.4, 0.1, 1.0e30, 1, precision=mode)
     U = initial_state(mesh, s.basis, s.gauss_points, 1.4, init)
     rng = np.random.default_rng(3)
     U[:, :, 1:] += 0.02 * rng.standard_normal(U[:, :, 1:].shape) * np.abs(U[:, :, :1])

@@ -166,9 +166,17 @@ def test_time_march_c2_full_mesh():
 def test_transonic_configuration_2000_steps_golden():
     """The transonic limiter configuration (256 x 128 O-grid, 65,536 triangles, p = 2, M 0.8,
     AoA 1.25 deg, CFL 0.1, limiter on) for its configured 2000 steps against the oracle's run
-    stored in tests/golden/c2_run.npz: after 200 and after 2000 steps, the clock, the sums and sums
-    of squares of every (variable, mode) coefficient over all elements, and the full records of a
-    sample of elements (every 128th and every boundary element) at 1e-10 relative L2."""
+    stored in tests/golden/c2_run.npz.
+
+    Round-off differences grow about twofold per step in this impulsive start: run in lockstep,
+    GPU and oracle differ by 1e-16 (relative L2) up to step 10, 1e-13 at step 19, 2.5e-10 at step
+    25 and 2e-6 at step 37, so past about 24 steps no two FP64 implementations with different
+    summation orders agree to 1e-10 -- nor does the reference with itself, whose rayon reductions
+    change their order from run to run.  test_time_march_c2_full_mesh holds the 1e-10 bar for 24
+    steps.  Here the stored twin run (the oracle started from the initial state perturbed by 1e-15)
+    measures the spread round-off alone produces; after 200 and 2000 steps the GPU run must be no
+    further from the oracle than three times the twin is: clock, per-(variable, mode) sums and sums
+    of squares over all elements, and the full records of the sampled elements."""
     z = np.load(os.path.join(GOLDEN, "c2_run.npz"))
     mesh = process_mesh(naca0012_ogrid(256, 128), freestream_quantity(FS[1], FS[0], FS[2], FS[3], 1.4), 1.4)
     s = build_solver(mesh, 2, 1.4, 0.1, 1.0e30, 10 ** 9)
@@ -182,13 +190,13 @@ def test_transonic_configuration_2000_steps_golden():
         td.synchronize()
         done = n
         assert td.current_step == n
-        t_ref = float(z[f"t{n}"])
-        assert abs(td.current_time - t_ref) <= 1e-13 * t_ref
+        t_ref, t_twin = float(z[f"t{n}"]), float(z[f"twin_t{n}"])
+        assert abs(td.current_time - t_ref) <= 3.0 * abs(t_twin - t_ref) + 1e-13 * t_ref, n
         U = sd.new_state()
         td.download(U)
-        assert rel_l2(U[sample], z[f"U{n}"]) < TOL_STATE, n
-        assert rel_l2(U.sum(axis=0), z[f"sum{n}"]) < TOL_STATE, n
-        assert rel_l2((U * U).sum(axis=0), z[f"sumsq{n}"]) < TOL_STATE, n
+        for key, gpu in ((f"U{n}", U[sample]), (f"sum{n}", U.sum(axis=0)), (f"sumsq{n}", (U * U).sum(axis=0))):
+            spread = rel_l2(z[f"twin_{key}"], z[key])
+            assert rel_l2(gpu, z[key]) <= 3.0 * spread + TOL_STATE, (key, rel_l2(gpu, z[key]), spread)
     s.close()
 
 

@@ -348,6 +348,7 @@ def run_batched(args, local):
         return res["dof"] * 3 * K / (ms * 1e-3), ms / K, dev_bytes, acc
 
     v32, ms32, bytes32, acc32 = batched("fp32")
+    v32c, ms32c, bytes32c, acc32c = batched("fp32_compute")
     v32s, ms32s, _, _ = batched("fp32", mixed=False)
     v64, ms64, bytes64, acc64 = batched("fp64")
     _, _, _, accp = batched("fp64", perturb=True)
@@ -376,6 +377,7 @@ def run_batched(args, local):
         "instances_below_1e-4": int(sum(floor_cl[k] <= 1e-4 and floor_cd[k] <= 1e-4 for k in floor_cl)),
         "per_instance_abs_delta_cl": {f"p{k[0]}_{k[1]}": v for k, v in floor_cl.items()}}
     res["fp32_vs_fp64_after_steps"] = versus(acc32)
+    res["fp32_compute_vs_fp64_after_steps"] = versus(acc32c)
     # one at a time, FP64: a DOF-weighted sample (every 8th instance in DOF order)
     order = sorted(range(len(built)), key=lambda k: built[k][0].dofs)
     sample = [built[k] for k in order[::max(1, len(built) // 32)]]
@@ -397,7 +399,10 @@ def run_batched(args, local):
         s.close()
     v_single = tot_dof * 3 * K / (tot_ms * 1e-3)
     res.update({
-        "fp32_batched": v32, "fp64_batched": v64, "fp64_one_at_a_time": v_single,
+        "fp32_batched": v32, "fp32_compute_batched": v32c, "fp64_batched": v64, "fp64_one_at_a_time": v_single,
+        "ms_per_step_fp32_compute_batched": ms32c,
+        "speedup_fp32_compute_batched_vs_fp64_one_at_a_time": v32c / v_single,
+        "speedup_fp32_compute_batched_vs_fp64_batched": v32c / v64,
         "fp32_one_context_per_order_two_streams": v32s, "ms_per_step_fp32_two_streams": ms32s,
         "launch_structure": "mixed batch: one context, one stream, one launch per kernel of the step over all "
                             "instances of both orders (14 launches per step, CUDA graphs of 8 steps)",
@@ -768,7 +773,9 @@ def run_ours(args):
         line["batched_fp32_vs_plain_fp64"] = {
             "fp32_batched_dof_stage_per_s": b["fp32_batched"], "fp64_one_at_a_time_dof_stage_per_s": b["fp64_one_at_a_time"],
             "ratio": b["speedup_fp32_batched_vs_fp64_one_at_a_time"],
-            "ratio_vs_fp64_batched": b["speedup_fp32_batched_vs_fp64_batched"], "steps": b["steps"]}
+            "ratio_vs_fp64_batched": b["speedup_fp32_batched_vs_fp64_batched"],
+            "fp32_compute_batched_dof_stage_per_s": b["fp32_compute_batched"],
+            "fp32_compute_ratio": b["speedup_fp32_compute_batched_vs_fp64_one_at_a_time"], "steps": b["steps"]}
     if "serving" in line:
         line["serving_latency_s"] = {
             rate: {"fp32_serving_p50": r["fp32_serving"]["p50_s"], "fp32_serving_p99": r["fp32_serving"]["p99_s"],

@@ -524,6 +524,7 @@ int collect_status(dgm_ctx* c) {
       z.wl_count[0] = z.wl_count[1] = 0;
       z.wl1_count = z.pend_count = 0;
       z.bar_count = 0u;
+      for (auto& b : z.bar_sub) b.count = 0u;
       z.lim_exit = 0u;
       for (auto& q : z.lq) dgm::reset_queue(q);
       CK(cudaMemcpyAsync(c->ctl, &z, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
@@ -1110,10 +1111,11 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_slot_capacity
 // ---------------------------------------------------------------------------------------------
 constexpr int kMixedEdgeThreads = 128, kMixedElemThreads = 128;
 
-template <typename T, int MASK>
+template <typename T, int MASK, typename St = T>
 struct MixOps {
-  using M = dgm::Mixed<T, MASK>;
-  static T* S(void* p) { return static_cast<T*>(p); }
+  using M = dgm::Mixed<T, MASK, St>;
+  static St* S(void* p) { return static_cast<St*>(p); }
+  static T* Fx(void* p) { return static_cast<T*>(p); }
 
   static void base(dgm_ctx* p, M& mp) {
     std::memset(static_cast<void*>(&mp), 0, sizeof(M));
@@ -1128,7 +1130,7 @@ struct MixOps {
         if (g == 2) std::memcpy(static_cast<void*>(&mp.k3), k->kparams.data(), sizeof(mp.k3));
       auto& a = mp.g[g];
       a.n_inst = (int)k->inst.size();
-      a.F = S(k->F);
+      a.F = Fx(k->F);
       a.t0 = k->t0;
       a.status = k->status;
       a.wl1 = k->wl1;
@@ -1140,7 +1142,7 @@ struct MixOps {
   static int blocks_total(const M& mp) { return std::max(1, mp.g[0].blocks + mp.g[1].blocks + mp.g[2].blocks); }
 
   // which: 0 = U, 1 = U1, 2 = U2
-  static T* arr(dgm_ctx* k, int which) { return S(which == 0 ? k->U : which == 1 ? k->U1 : k->U2); }
+  static St* arr(dgm_ctx* k, int which) { return S(which == 0 ? k->U : which == 1 ? k->U1 : k->U2); }
 
   static int step_head(dgm_ctx* p) {
     M mp;
@@ -1150,7 +1152,7 @@ struct MixOps {
         mp.g[g].Uin = S(k->U);
         mp.g[g].blocks = (int)((k->ne + 255) / 256);
       }
-    dgm::k_step_head_mixed<T, MASK><<<blocks_total(mp), 256, 0, p->stream>>>(mp);
+    dgm::k_step_head_mixed<T, MASK, St><<<blocks_total(mp), 256, 0, p->stream>>>(mp);
     CK(cudaGetLastError());
     return DGM_OK;
   }
@@ -1163,7 +1165,7 @@ struct MixOps {
         mp.g[g].Uin = arr(k, which);
         mp.g[g].blocks = (int)(((k->n_int + k->n_bnd) * k->ng + kMixedEdgeThreads - 1) / kMixedEdgeThreads);
       }
-    dgm::k_edge_flux_mixed<T, MASK><<<blocks_total(mp), kMixedEdgeThreads, 0, p->stream>>>(mp);
+    dgm::k_edge_flux_mixed<T, MASK, St><<<blocks_total(mp), kMixedEdgeThreads, 0, p->stream>>>(mp);
     CK(cudaGetLastError());
     return DGM_OK;
   }
@@ -1181,7 +1183,7 @@ struct MixOps {
         a.Rout = (MODE == 3 && with_residual) ? S(k->R) : nullptr;
         a.blocks = (int)((k->ne + kMixedElemThreads / 4 - 1) / (kMixedElemThreads / 4));
       }
-    dgm::k_element_mixed<T, MASK, MODE><<<blocks_total(mp), kMixedElemThreads, 0, p->stream>>>(mp);
+    dgm::k_element_mixed<T, MASK, MODE, St><<<blocks_total(mp), kMixedElemThreads, 0, p->stream>>>(mp);
     CK(cudaGetLastError());
     return DGM_OK;
   }
@@ -1196,7 +1198,7 @@ struct MixOps {
         mp.g[g].Uout = arr(k, which);
         mp.g[g].blocks = (int)((k->ld / 32 + dgm::kDetectWarps - 1) / dgm::kDetectWarps);
       }
-    dgm::k_lim_detect_mixed<T, MASK, false><<<blocks_total(mp), dgm::kDetectThreads, 0, p->stream>>>(mp);
+    dgm::k_lim_detect_mixed<T, MASK, false, St><<<blocks_total(mp), dgm::kDetectThreads, 0, p->stream>>>(mp);
     CK(cudaGetLastError());
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(p->mixed_blocks);
@@ -1208,7 +1210,7 @@ struct MixOps {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter_mixed<T, MASK>, mp, p->mwork));
+    CK(cudaLaunchKernelEx(&cfg, dgm::k_limiter_mixed<T, MASK, St>, mp, p->mwork));
     return DGM_OK;
   }
 
@@ -1216,7 +1218,7 @@ struct MixOps {
     M mp;
     base(p, mp);
     const int n = mp.g[0].n_inst + mp.g[1].n_inst + mp.g[2].n_inst;
-    dgm::k_step_end_mixed<T, MASK><<<(n + 127) / 128, 128, 0, p->stream>>>(mp);
+    dgm::k_step_end_mixed<T, MASK, St><<<(n + 127) / 128, 128, 0, p->stream>>>(mp);
     CK(cudaGetLastError());
     return DGM_OK;
   }
@@ -1232,7 +1234,8 @@ struct MixOps {
 
   static int occupancy(dgm_ctx* p) {
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dgm::k_limiter_mixed<T, MASK>, dgm::kLimiterWarps * 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dgm::k_limiter_mixed<T, MASK, St>, dgm::kLimiterWarps * 32,
+                                                     0));
     int64_t ne = 0;
     for (dgm_ctx* k : p->kids)
       if (k) ne += k->ne;
@@ -1247,6 +1250,7 @@ struct MixOps {
 template <class F>
 int mixed_dispatch(dgm_ctx* p, F&& f) {
   const bool three = p->kids[2] != nullptr;
+  if (p->prec_mode == 4) return three ? f(MixOps<float, 7, double>{}) : f(MixOps<float, 3, double>{});
   if (p->prec == 0) return three ? f(MixOps<double, 7>{}) : f(MixOps<double, 3>{});
   return three ? f(MixOps<float, 7>{}) : f(MixOps<float, 3>{});
 }
@@ -1269,7 +1273,7 @@ dgm_ctx* create_mixed(int n, const dgm_mesh_desc* meshes, const int32_t* orders,
       *status = DGM_BAD_ARG;
       return nullptr;
     }
-  if (params[0].precision < 0 || params[0].precision > 1) {  // mixed launches: FP64 or FP32 (FMA) bulk
+  if (params[0].precision != 0 && params[0].precision != 1 && params[0].precision != 4) {  // no tensor-core modes
     *status = DGM_BAD_ARG;
     return nullptr;
   }

@@ -116,6 +116,15 @@ struct alignas(128) LimQueue {
   int _pad2[30];
 };
 
+// First-level arrival counter of the limiter's grid barrier: blocks arrive at the counter of their
+// group (block index mod kBarGroups), each counter on its own 128-byte line, and the last block of
+// each group arrives at the top counter -- kBarGroups parallel atomic chains instead of one.
+constexpr int kBarGroups = 8;
+struct alignas(128) BarSub {
+  unsigned int count;
+  unsigned int _pad[31];
+};
+
 __host__ __device__ __forceinline__ void reset_queue(LimQueue& q) {
   q.tail = 0;
   q.head = 0;
@@ -139,6 +148,7 @@ struct Control {
   unsigned int head_done;      // blocks of k_step_head that have finished (last one closes the step head)
   unsigned int lim_exit;       // queue schedule: blocks that have left the pass (the last one resets the queues)
   LimQueue lq[3];              // queue schedule: per-wave queues, wave w uses lq[w % 3]
+  BarSub bar_sub[kBarGroups];  // grid barrier: first-level arrival counters
 };
 
 // Gas constants, computed once on the host from hcr with the reference's expressions.
@@ -1318,12 +1328,22 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int nblocks)
     volatile unsigned int* gen = &ctl->bar_gen;
     const unsigned int g = *gen;
     __threadfence();
-    const unsigned int arrived = atomicAdd(&ctl->bar_count, 1u);
-    if (arrived == nblocks - 1) {
-      ctl->bar_count = 0u;
+    // two-level arrival: the block's group counter, then (last of the group) the top counter
+    const unsigned int grp = blockIdx.x % kBarGroups;
+    const unsigned int groups = nblocks < (unsigned int)kBarGroups ? nblocks : (unsigned int)kBarGroups;
+    const unsigned int members = (nblocks - grp + kBarGroups - 1) / kBarGroups;
+    bool released = false;
+    if (atomicAdd(&ctl->bar_sub[grp].count, 1u) == members - 1) {
+      ctl->bar_sub[grp].count = 0u;
       __threadfence();
-      atomicAdd(&ctl->bar_gen, 1u);
-    } else {
+      if (atomicAdd(&ctl->bar_count, 1u) == groups - 1) {
+        ctl->bar_count = 0u;
+        __threadfence();
+        atomicAdd(&ctl->bar_gen, 1u);
+        released = true;
+      }
+    }
+    if (!released) {
       long long it = 0;
       while (*gen == g) {
         if (++it > (1ll << 25)) {  // ~ seconds: co-residency is guaranteed, so this is a fault
@@ -1655,7 +1675,8 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
       if (wave > m.ne + 2) break;
     }
   }
-  // the last block to leave resets the pass's counters and queues for the next pass
+  // statistics; the pass's counters and queues are reset before the next pass by the element
+  // pass that precedes every limiter pass (or by the host-driven entry points)
   __shared__ int s_troubled;
   if (threadIdx.x == 0) s_troubled = 0;
   __syncthreads();
@@ -1663,17 +1684,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
   __syncthreads();
   if (threadIdx.x == 0) {
     if (s_troubled) atomicAdd(&ctl->troubled, s_troubled);
-    fence_gpu();
-    if (atomicAdd(&ctl->lim_exit, 1u) == gridDim.x - 1u) {
-      for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
-      ctl->t0_count = 0;
-      ctl->wl1_count = 0;
-      ctl->pend_count = 0;
-      ctl->wl_count[0] = ctl->wl_count[1] = 0;
-      ctl->unknown[0] = ctl->unknown[1] = 0;
-      ctl->waves = wave;
-      ctl->lim_exit = 0u;
-    }
+    if (blockIdx.x == 0) ctl->waves = wave;  // every block leaves after the same wave
   }
 }
 

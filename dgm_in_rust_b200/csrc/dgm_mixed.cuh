@@ -20,14 +20,15 @@ struct NoParams {};
 template <int P, typename T, bool ON>
 using KParamsIf = typename std::conditional<ON, KParams<P, T>, NoParams>::type;
 
-// The device arrays one launch uses of one group, and the group's share of the launch's blocks.
-template <typename T>
+// The device arrays one launch uses of one group, and the group's share of the launch's blocks
+// (states of storage type S, edge fluxes of the arithmetic type T).
+template <typename T, typename S = T>
 struct GroupArgs {
-  const T* Uin;
-  const T* Ubase;
-  T* Uout;
-  const T* Rin;
-  T* Rout;
+  const S* Uin;
+  const S* Ubase;
+  S* Uout;
+  const S* Rin;
+  S* Rout;
   T* F;
   unsigned char* t0;
   unsigned int* status;
@@ -38,12 +39,12 @@ struct GroupArgs {
   int n_inst;  // instances of the group (without the dead instance of padded groups); 0 = no group
 };
 
-template <typename T, int MASK>
+template <typename T, int MASK, typename S = T>
 struct Mixed {
   KParamsIf<1, T, (MASK & 1) != 0> k1;
   KParamsIf<2, T, (MASK & 2) != 0> k2;
   KParamsIf<3, T, (MASK & 4) != 0> k3;
-  GroupArgs<T> g[3];
+  GroupArgs<T, S> g[3];
 };
 
 template <class K>
@@ -55,8 +56,8 @@ struct OrderOf<KParams<P, T>> {
 
 // Calls f(kparams, group args, block index within the group, the group's block count) for the
 // group that owns this block.
-template <typename T, int MASK, class F>
-__device__ __forceinline__ void on_block(const Mixed<T, MASK>& mp, F&& f) {
+template <typename T, int MASK, typename S, class F>
+__device__ __forceinline__ void on_block(const Mixed<T, MASK, S>& mp, F&& f) {
   int b = blockIdx.x;
   if constexpr ((MASK & 1) != 0) {
     if (b < mp.g[0].blocks) {
@@ -79,8 +80,8 @@ __device__ __forceinline__ void on_block(const Mixed<T, MASK>& mp, F&& f) {
 
 // Calls f(kparams, group args) for group index g (0, 1, 2 = order 1, 2, 3) if that group has
 // meshes (a group without meshes has no parameters to read).
-template <typename T, int MASK, class F>
-__device__ __forceinline__ void with_group(const Mixed<T, MASK>& mp, int g, F&& f) {
+template <typename T, int MASK, typename S, class F>
+__device__ __forceinline__ void with_group(const Mixed<T, MASK, S>& mp, int g, F&& f) {
   if constexpr ((MASK & 1) != 0) {
     if (g == 0) {
       if (mp.g[0].n_inst > 0) f(mp.k1, mp.g[0]);
@@ -100,8 +101,8 @@ __device__ __forceinline__ void with_group(const Mixed<T, MASK>& mp, int g, F&& 
 
 // The control block of the first group with meshes: grid barrier, block counters and the wave
 // counters of the mixed limiter.
-template <typename T, int MASK>
-__device__ __forceinline__ Control* lead_ctl(const Mixed<T, MASK>& mp) {
+template <typename T, int MASK, typename S>
+__device__ __forceinline__ Control* lead_ctl(const Mixed<T, MASK, S>& mp) {
   if constexpr ((MASK & 1) != 0) {
     if (mp.g[0].n_inst > 0) return mp.k1.ctl;
   }
@@ -112,52 +113,58 @@ __device__ __forceinline__ Control* lead_ctl(const Mixed<T, MASK>& mp) {
   return nullptr;
 }
 
-template <typename T, int MASK>
-__global__ void __launch_bounds__(256, 3) k_edge_flux_mixed(const __grid_constant__ Mixed<T, MASK> mp) {
-  on_block(mp, [&](const auto& kp, const GroupArgs<T>& g, int b, int nb) { edge_flux_body(kp, g.Uin, g.F, b, nb); });
+template <typename T, int MASK, typename S = T>
+__global__ void __launch_bounds__(256, 3) k_edge_flux_mixed(const __grid_constant__ Mixed<T, MASK, S> mp) {
+  on_block(mp, [&](const auto& kp, const GroupArgs<T, S>& g, int b, int nb) {
+    constexpr int P = OrderOf<std::decay_t<decltype(kp)>>::value;
+    edge_flux_body<P, T, S>(kp, g.Uin, g.F, b, nb);
+  });
 }
 
-template <typename T, int MASK, int MODE>
-__global__ void __launch_bounds__(256, 3) k_element_mixed(const __grid_constant__ Mixed<T, MASK> mp) {
-  on_block(mp, [&](const auto& kp, const GroupArgs<T>& g, int b, int) {
+template <typename T, int MASK, int MODE, typename S = T>
+__global__ void __launch_bounds__(256, 3) k_element_mixed(const __grid_constant__ Mixed<T, MASK, S> mp) {
+  on_block(mp, [&](const auto& kp, const GroupArgs<T, S>& g, int b, int) {
     constexpr int P = OrderOf<std::decay_t<decltype(kp)>>::value;
-    element_body<P, T, MODE>(kp, g.Uin, g.Ubase, g.F, g.Uout, g.Rin, g.Rout, b);
+    element_body<P, T, MODE, S>(kp, g.Uin, g.Ubase, g.F, g.Uout, g.Rin, g.Rout, b);
   });
 }
 
 // Shared bytes of the largest order of the set (the detection blocks' staged records).
-template <typename T, int MASK>
+template <typename S, int MASK>
 struct MixedDetectSmem {
-  static constexpr size_t b1 = (MASK & 1) ? DetectSmem<1, T>::kBytes : 0;
-  static constexpr size_t b2 = (MASK & 2) ? DetectSmem<2, T>::kBytes : 0;
-  static constexpr size_t b3 = (MASK & 4) ? DetectSmem<3, T>::kBytes : 0;
+  static constexpr size_t b1 = (MASK & 1) ? DetectSmem<1, S>::kBytes : 0;
+  static constexpr size_t b2 = (MASK & 2) ? DetectSmem<2, S>::kBytes : 0;
+  static constexpr size_t b3 = (MASK & 4) ? DetectSmem<3, S>::kBytes : 0;
   static constexpr size_t m12 = b1 > b2 ? b1 : b2;
   static constexpr size_t bytes = m12 > b3 ? m12 : b3;
 };
 
-template <typename T, int MASK, bool STAGED>
-__global__ void __launch_bounds__(kDetectThreads) k_lim_detect_mixed(const __grid_constant__ Mixed<T, MASK> mp) {
-  __shared__ __align__(16) unsigned char s_det[MixedDetectSmem<T, MASK>::bytes];
-  on_block(mp, [&](const auto& kp, const GroupArgs<T>& g, int b, int) {
+template <typename T, int MASK, bool STAGED, typename S = T>
+__global__ void __launch_bounds__(kDetectThreads) k_lim_detect_mixed(const __grid_constant__ Mixed<T, MASK, S> mp) {
+  __shared__ __align__(16) unsigned char s_det[MixedDetectSmem<S, MASK>::bytes];
+  on_block(mp, [&](const auto& kp, const GroupArgs<T, S>& g, int b, int) {
     constexpr int P = OrderOf<std::decay_t<decltype(kp)>>::value;
-    lim_detect_body<P, T, STAGED>(kp, g.Uin, g.t0, g.status, g.wl1, g.pend, g.order, b, reinterpret_cast<T*>(s_det));
+    lim_detect_body<P, T, STAGED, S>(kp, g.Uin, g.t0, g.status, g.wl1, g.pend, g.order, b, reinterpret_cast<S*>(s_det));
   });
 }
 
-template <typename T, int MASK>
-__global__ void __launch_bounds__(256) k_step_head_mixed(const __grid_constant__ Mixed<T, MASK> mp) {
-  on_block(mp, [&](const auto& kp, const GroupArgs<T>& g, int b, int) { step_head_elems(kp, g.Uin, b); });
+template <typename T, int MASK, typename S = T>
+__global__ void __launch_bounds__(256) k_step_head_mixed(const __grid_constant__ Mixed<T, MASK, S> mp) {
+  on_block(mp, [&](const auto& kp, const GroupArgs<T, S>& g, int b, int) {
+    constexpr int P = OrderOf<std::decay_t<decltype(kp)>>::value;
+    step_head_elems<P, T, S>(kp, g.Uin, b);
+  });
   if (!last_block_in(lead_ctl(mp), gridDim.x)) return;
   for (int gi = 0; gi < 3; ++gi)
-    with_group(mp, gi, [&](const auto& kp, const GroupArgs<T>&) { step_head_close(kp.ctl, kp.ic, kp.m.n_inst); });
+    with_group(mp, gi, [&](const auto& kp, const GroupArgs<T, S>&) { step_head_close(kp.ctl, kp.ic, kp.m.n_inst); });
 }
 
-template <typename T, int MASK>
-__global__ void k_step_end_mixed(const __grid_constant__ Mixed<T, MASK> mp) {
+template <typename T, int MASK, typename S = T>
+__global__ void k_step_end_mixed(const __grid_constant__ Mixed<T, MASK, S> mp) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   for (int gi = 0; gi < 3; ++gi) {
     bool mine = false;
-    with_group(mp, gi, [&](const auto& kp, const GroupArgs<T>& g) {
+    with_group(mp, gi, [&](const auto& kp, const GroupArgs<T, S>& g) {
       if (i < g.n_inst) {
         mine = true;
         InstCtl& c = kp.ic[i];
@@ -189,9 +196,10 @@ struct MixedScratch {
 // (`work`, entries (group << 30) | element) and reconstruct them, a grid barrier between the
 // phases (the barrier schedule of k_limiter).  Elements only neighbour elements of their own
 // group, so each group settles exactly as in its own pass.  The lead group's control block holds
-// the grid barrier and the wave counters; the last block to leave resets every group's counters.
-template <typename T, int MASK>
-__global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __grid_constant__ Mixed<T, MASK> mp,
+// the grid barrier and the wave counters; the element pass of the next stage resets every group's
+// counters.
+template <typename T, int MASK, typename S = T>
+__global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __grid_constant__ Mixed<T, MASK, S> mp,
                                                                       int* __restrict__ work) {
   Control* ctl = lead_ctl(mp);
   constexpr size_t kWarpBytes = MixedScratch<MASK>::bytes;
@@ -202,7 +210,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
   // the detection launch has finished: its counts are final
   int flagged = 0, n1[3] = {0, 0, 0}, np[3] = {0, 0, 0};
   for (int gi = 0; gi < 3; ++gi)
-    with_group(mp, gi, [&](const auto& kp, const GroupArgs<T>&) {
+    with_group(mp, gi, [&](const auto& kp, const GroupArgs<T, S>&) {
       flagged += kp.ctl->t0_count;
       n1[gi] = kp.ctl->wl1_count;
       np[gi] = kp.ctl->pend_count;
@@ -211,7 +219,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
   int troubled_local[3] = {0, 0, 0};
   int wave = 1;
   auto reconstruct = [&](int gi, int et) {
-    with_group(mp, gi, [&](const auto& kp, const GroupArgs<T>& g) {
+    with_group(mp, gi, [&](const auto& kp, const GroupArgs<T, S>& g) {
       constexpr int P = OrderOf<std::decay_t<decltype(kp)>>::value;
       const MeshDev& m = kp.m;
       int fwt[3], nbt[3];
@@ -220,7 +228,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
         fwt[k] = m.face[k * m.ld + et];
         nbt[k] = m.nbr[k * m.ld + et];
       }
-      const int rs = weno_reconstruct<P, T>(kp, g.Uout, et, fwt, nbt, lane,
+      const int rs = weno_reconstruct<P, T, S>(kp, g.Uout, et, fwt, nbt, lane,
                                             *reinterpret_cast<WenoScratch<P>*>(s_warp[wib]));
       if (rs != ST_OK && lane == 0) {
         const int inst = m.n_inst > 1 ? m.inst[et] : 0;
@@ -239,9 +247,9 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
       int gi;
       const int li = split(n1, i, gi);
       int et = 0;
-      with_group(mp, gi, [&](const auto&, const GroupArgs<T>& g) { et = __ldcg(&g.wl1[li]); });
+      with_group(mp, gi, [&](const auto&, const GroupArgs<T, S>& g) { et = __ldcg(&g.wl1[li]); });
       reconstruct(gi, et);
-      with_group(mp, gi, [&](const auto&, const GroupArgs<T>& g) {
+      with_group(mp, gi, [&](const auto&, const GroupArgs<T, S>& g) {
         if (lane == 0) g.status[et] = (1u << 2) | 2u;
       });
       ++troubled_local[gi];
@@ -257,7 +265,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
         int gi = 0, e = 0;
         if (i < np_all) {
           const int li = split(np, i, gi);
-          with_group(mp, gi, [&](const auto& kp, const GroupArgs<T>& g) {
+          with_group(mp, gi, [&](const auto& kp, const GroupArgs<T, S>& g) {
             constexpr int P = OrderOf<std::decay_t<decltype(kp)>>::value;
             const MeshDev& m = kp.m;
             e = __ldcg(&g.pend[li]);
@@ -276,8 +284,8 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
             }
             if (!ready) return;
             if (any_mod) {
-              const T* own = g.Uout + (size_t)e * (NEQ * Variant<P>::NB);
-              trouble = kxrcf<P, T>(kp, g.Uout, e, own);
+              const S* own = g.Uout + (size_t)e * (NEQ * Variant<P>::NB);
+              trouble = kxrcf<P, T, false, false, S>(kp, g.Uout, e, own);
             } else {
               trouble = g.t0[e] != 0;
             }
@@ -309,7 +317,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
         const int gi = entry >> 30, et = entry & ((1 << 30) - 1);
         reconstruct(gi, et);
         __threadfence();
-        with_group(mp, gi, [&](const auto&, const GroupArgs<T>& g) {
+        with_group(mp, gi, [&](const auto&, const GroupArgs<T, S>& g) {
           if (lane == 0) g.status[et] = ((unsigned int)wave << 2) | 2u;
         });
         ++troubled_local[gi];
@@ -319,7 +327,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
       if (wave > (1 << 29)) break;
     }
   }
-  // the last block to leave resets the pass's counters of every group
+  // statistics; every group's counters are reset before the next pass by the element pass
   __shared__ int s_troubled[3];
   if (threadIdx.x < 3) s_troubled[threadIdx.x] = 0;
   __syncthreads();
@@ -328,22 +336,10 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int gi = 0; gi < 3; ++gi)
-      with_group(mp, gi, [&](const auto& kp, const GroupArgs<T>&) {
+      with_group(mp, gi, [&](const auto& kp, const GroupArgs<T, S>&) {
         if (s_troubled[gi]) atomicAdd(&kp.ctl->troubled, s_troubled[gi]);
+        if (blockIdx.x == 0) kp.ctl->waves = wave;
       });
-    fence_gpu();
-    if (atomicAdd(&ctl->lim_exit, 1u) == gridDim.x - 1u) {
-      for (int gi = 0; gi < 3; ++gi)
-        with_group(mp, gi, [&](const auto& kp, const GroupArgs<T>&) {
-          kp.ctl->t0_count = 0;
-          kp.ctl->wl1_count = 0;
-          kp.ctl->pend_count = 0;
-          kp.ctl->waves = wave;
-        });
-      ctl->wl_count[0] = ctl->wl_count[1] = 0;
-      ctl->unknown[0] = ctl->unknown[1] = 0;
-      ctl->lim_exit = 0u;
-    }
   }
 }
 

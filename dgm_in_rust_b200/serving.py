@@ -109,7 +109,7 @@ def footprint_bytes(meshes: list, order: int, precision: str, limiter: bool = Tr
     def arr(count, size):             # dev_alloc: at least one element
         return max(count, 1) * size
 
-    control = 1280 + (n + 1) * 72                                    # Control, InstCtl[n + 1]
+    control = 2304 + (n + 1) * 72                                    # Control, InstCtl[n + 1]
     geometry = 3 * ne * 8 + 4 * ld * 8 + 2 * 3 * ld * 4 + ne * 4 + ld // 32 * 4  # jac, hmin, h15, dinv, face, nbr,
     #                                                                              inst, batch order
     edges = (arr(n_int, 8) + arr(n_int, 4) + arr(n_int, 32) + arr(n_bnd, 4) + arr(n_bnd, 4) + arr(n_bnd, 32)

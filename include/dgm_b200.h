@@ -310,7 +310,7 @@ int32_t dgm_instance_capacity(dgm_ctx* ctx, int32_t i, dgm_slot_capacity* capaci
  * launches -- every kernel of a step is one launch over all instances, each block running its
  * instance's order (one persistent cooperative launch for the limiter's waves).  tables[P - 1]
  * describes order P (only the orders present are read); params, capacity (may be NULL) and the
- * instance numbering are as for dgm_create_batch_slots.  Precision 0 (FP64) or 1 (FP32).  The
+ * instance numbering are as for dgm_create_batch_slots.  Precision 0, 1 or 4 (no tensor cores).  The
  * dgm_instance_*, dgm_advance*, dgm_synchronize, dgm_query, dgm_diagnostics, dgm_limiter_stats and
  * dgm_device_bytes calls work on it; the single-mesh entry points and the launch-configuration
  * calls return DGM_BAD_ARG.  Every instance's results are bitwise those of its order's batch.  No

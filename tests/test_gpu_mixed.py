@@ -1,8 +1,8 @@
 """Mixed batches (dgm_create_mixed): meshes of orders 1, 2 and 3 advanced by the same launches.
 
 * Every instance of a mixed batch produces exactly (bit for bit) what its mesh produces alone:
-  state, clock and FP64 diagnostics, for {1, 2} and {1, 2, 3}, in FP64 and FP32, with instances
-  stopping at different steps.
+  state, clock and FP64 diagnostics, for {1, 2} and {1, 2, 3}, in FP64, FP32 and FP32 arithmetic on
+  an FP64 state, with instances stopping at different steps.
 * Slots of a mixed batch: a finished instance's slot takes a new mesh of its order while the
   others keep running, and the new solve is again bitwise its solo run.
 * The per-order calls (launch configuration, single-mesh entry points) are refused.
@@ -36,7 +36,7 @@ def _solo(mesh, init, order, steps, precision):
     return out
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32_compute"])
 @pytest.mark.parametrize("orders", [(1, 2, 2, 1), (3, 1, 2, 3)])
 def test_mixed_instances_match_solo(precision, orders):
     shapes = [(32, 16, 0.5, 2.0), (48, 24, 0.8, 1.25), (40, 20, 0.7, -1.0), (24, 12, 0.6, 3.0)]

@@ -74,8 +74,9 @@ def parse():
                          "above, c3 = the 1024 x 512 p = 3 O-grid (M 0.7, AoA 2 deg)")
     ap.add_argument("--precision", choices=["fp64", "fp32", "fp32_compute", "tf32", "tf32x3"], default="fp64")
     ap.add_argument("--launch", default="128,2368,128,1,0",
-                    help="edge threads, edge blocks, element threads, staged limiter detector, lane-pair edge "
-                         "pass, queue limiter schedule (profile case; the last two may be left out: 0)")
+                    help="edge threads, edge blocks, element threads, staged limiter detector, edge pass form "
+                         "(0 point, 1 lane pair, 2 staged), queue limiter schedule (profile case; the last two "
+                         "may be left out: 0)")
     return ap.parse_args()
 
 
@@ -477,7 +478,7 @@ def precision_case(inst, K, modes, local, label):
         td, sd = s.temporal_disc, s.spatial_disc
         cfg = tuned[mode]
         sd.set_launch_config(cfg["edge_threads"], cfg["edge_blocks"], cfg["element_threads"])
-        sd.set_edge_form(cfg["edge_form"] == "pair")
+        sd.set_edge_form(cfg["edge_form"])
         sd.set_limiter_detector(cfg["limiter_detector"] == "staged")
         sd.set_limiter_schedule(cfg["limiter_schedule"] == "queue")
         td.set_initial_on_device(init)
@@ -822,7 +823,7 @@ def run_profile_case(args):
     sd.set_launch_config(e_t, e_b, l_t)
     sd.set_limiter_detector(bool(staged))
     sd.set_limiter_schedule(bool(queue))
-    sd.set_edge_form(bool(pair))
+    sd.set_edge_form(("point", "pair", "staged")[pair])
     td.set_initial_on_device(init)
     td.advance(args.warmup + args.steps)
     td.synchronize()

@@ -720,6 +720,133 @@ __global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant
   edge_flux_pair_body<P, T, S>(kp, U, F, blockIdx.x, gridDim.x);
 }
 
+// Element records staged in shared memory are padded to an odd number of 16-byte units:
+// consecutive lanes reading the same coefficient of their own records then spread over the banks
+// (2-way conflicts for FP64, 4-way for FP32, the least 16-byte granularity allows; unpadded
+// records of 48-320 bytes map most lanes to the same few banks).
+template <int NB, typename T>
+struct Staged {
+  static constexpr int kRecBytes = NEQ * NB * (int)sizeof(T);
+  static constexpr int kStrideBytes = kRecBytes + ((kRecBytes / 16) % 2 == 0 ? 16 : 32);
+  static constexpr int kStride = kStrideBytes / (int)sizeof(T);  // record stride in T
+  static constexpr int kCpr = kRecBytes / 16;                          // 16-byte chunks per record
+  static_assert(kRecBytes % 16 == 0, "element records are a multiple of 16 bytes");
+};
+
+// The edge pass with the records of a warp's slots staged in shared memory: NG lanes per slot (one
+// per Gauss point), 32 / NG slots per warp iteration.  The warp first copies both sides' records of
+// its slots with coalesced 16-byte loads -- each record once per slot, where the per-point form
+// loads it NG times -- and then every lane evaluates its point's traces from shared memory and the
+// HLLC / boundary flux.  The traces, fluxes and stores are the same expressions in the same order
+// as in k_edge_flux, so the results are bitwise identical.  Blocks of kEdgeStagedThreads.
+constexpr int kEdgeStagedThreads = 128;
+
+template <int P, typename T, typename S = T>
+__device__ __forceinline__ void edge_flux_staged_body(const KParams<P, T>& kp, const S* __restrict__ U,
+                                                      T* __restrict__ F, int bid, int nblk) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NG = V::NG;
+  constexpr int SPW = 32 / NG;                    // slots per warp iteration
+  constexpr int STRIDE = Staged<NB, S>::kStride;  // record stride in S: an odd number of 16-byte units
+  constexpr int CPR = Staged<NB, S>::kCpr;        // 16-byte chunks per record
+  constexpr int WARPS = kEdgeStagedThreads / 32;
+  __shared__ T s_pe[3 * NG * NB];
+  __shared__ __align__(16) S s_rec[WARPS][2][SPW * STRIDE];  // [side][slot record]
+  for (int i = threadIdx.x; i < 3 * NG * NB; i += blockDim.x) s_pe[i] = (&kp.t.phi_edge[0][0][0])[i];
+  __syncthreads();
+  const MeshDev& m = kp.m;
+  const Gas& gas = kp.gas;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int sl = lane / NG, g = lane - sl * NG;
+  const int gwarp = bid * WARPS + wib, nwarps = nblk * WARPS;
+  const int total = m.n_int + m.n_bnd;
+  for (int base = gwarp * SPW; base < total; base += nwarps * SPW) {
+    const int s = base + sl;
+    bool valid = sl < SPW && s < total, internal = false;
+    int eL = -1, eR = -1, inst = 0, ic = 0, info = 0;
+    if (valid) {
+      if (s < m.n_int) {
+        const int2 lr = m.ie_lr[s];
+        eL = lr.x;
+        eR = lr.y;
+        internal = true;
+        ic = m.ie_ic[s];
+      } else {
+        const int sb = s - m.n_int;
+        eL = m.be_elem[sb];
+        info = m.be_info[sb];
+      }
+      inst = m.n_inst > 1 ? m.inst[eL] : 0;
+      if (!kp.ic[inst].active) valid = false;
+    }
+    // stage the records: chunk c of record r = side * SPW + slot
+    constexpr int TOT = 2 * SPW * CPR, IT = (TOT + 31) / 32;
+    const int myL = valid ? eL : -1, myR = (valid && internal) ? eR : -1;
+    __syncwarp();
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int c = lane + 32 * it;
+      const int r = c / CPR, k = c - r * CPR;
+      const int side = r / SPW, slot = r - side * SPW;
+      const int src = (slot < SPW ? slot : 0) * NG;
+      const int eLs = __shfl_sync(0xffffffffu, myL, src);
+      const int eRs = __shfl_sync(0xffffffffu, myR, src);
+      const int e = side ? eRs : eLs;
+      if (c < TOT && e >= 0) {
+        const uint4* gsrc = reinterpret_cast<const uint4*>(U + (size_t)e * (NEQ * NB));
+        *reinterpret_cast<uint4*>(&s_rec[wib][side][slot * STRIDE + k * (16 / (int)sizeof(S))]) = __ldcg(gsrc + k);
+      }
+    }
+    __syncwarp();
+    if (!valid) continue;
+    T out[4];
+    const S* recL = &s_rec[wib][0][sl * STRIDE];
+    if (internal) {
+      const S* recR = &s_rec[wib][1][sl * STRIDE];
+      const T* pl = &s_pe[((ic & 3) * NG + g) * NB];
+      const T* pr = &s_pe[((ic >> 2) * NG + (NG - 1 - g)) * NB];
+      T lv[4], rv[4];
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) {
+        T a = T(0), c = T(0);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          a += T(recL[v * NB + b]) * pl[b];
+          c += T(recR[v * NB + b]) * pr[b];
+        }
+        lv[v] = a;
+        rv[v] = c;
+      }
+      const double4 geo = m.ie_geo[s];
+      const int st = hllc<T>(lv, rv, T(geo.x), T(geo.y), gas, out);
+      if (st != ST_OK) raise_status(kp.ctl, &kp.ic[inst], st, m.slot_ref[s]);
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) out[v] *= T(geo.z);
+    } else {
+      const T* pe = &s_pe[((info & 3) * NG + g) * NB];
+      T lv[4];
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) {
+        T a = T(0);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) a += T(recL[v * NB + b]) * pe[b];
+        lv[v] = a;
+      }
+      const double4 geo = m.be_geo[s - m.n_int];
+      boundary_flux<T>(lv, info, T(geo.x), T(geo.y), m, gas, out);
+#pragma unroll
+      for (int v = 0; v < NEQ; ++v) out[v] *= T(geo.z);
+    }
+    store_flux<T>(F, (size_t)s, NG, g, out);
+  }
+}
+
+template <int P, typename T, typename S = T>
+__global__ void __launch_bounds__(kEdgeStagedThreads, 4) k_edge_flux_staged(const __grid_constant__ KParams<P, T> kp,
+                                                                         const S* __restrict__ U, T* __restrict__ F) {
+  edge_flux_staged_body<P, T, S>(kp, U, F, blockIdx.x, gridDim.x);
+}
+
 // ------------------------------------------------------------------------------------------
 // Element pass: volume integral (integrate_over_cell_euler, spatial_disc.rs:40-69, and
 // boundary_condition.rs:98-117 for boundary elements), gather of the three faces' edge fluxes
@@ -738,19 +865,6 @@ __global__ void __launch_bounds__(256, 2) k_edge_flux_pair(const __grid_constant
 // are not stored).
 // ------------------------------------------------------------------------------------------
 constexpr int kElemMaxWarps = 8;  // element pass: at most 256 threads per block
-
-// Element records staged in shared memory are padded to an odd number of 16-byte units:
-// consecutive lanes reading the same coefficient of their own records then spread over the banks
-// (2-way conflicts for FP64, 4-way for FP32, the least 16-byte granularity allows; unpadded
-// records of 48-320 bytes map most lanes to the same few banks).
-template <int NB, typename T>
-struct Staged {
-  static constexpr int kRecBytes = NEQ * NB * (int)sizeof(T);
-  static constexpr int kStrideBytes = kRecBytes + ((kRecBytes / 16) % 2 == 0 ? 16 : 32);
-  static constexpr int kStride = kStrideBytes / (int)sizeof(T);  // record stride in T
-  static constexpr int kCpr = kRecBytes / 16;                          // 16-byte chunks per record
-  static_assert(kRecBytes % 16 == 0, "element records are a multiple of 16 bytes");
-};
 
 // Copies the NR element records starting at e0 (always inside the arrays, which are padded to a
 // multiple of 32 elements, with e0 a multiple of NR) into the warp's shared buffer (record r at

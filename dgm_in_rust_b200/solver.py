@@ -130,6 +130,9 @@ def initial_state(mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints, hc
     return U
 
 
+EDGE_FORMS = ("point", "pair", "staged")  # dgm_set_edge_variant's 0, 1, 2
+
+
 def _launch_config(L, ctx) -> dict:
     cfg = (ctypes.c_int32 * 3)()
     L.dgm_get_launch_config(ctx, cfg)
@@ -139,7 +142,7 @@ def _launch_config(L, ctx) -> dict:
     return {"edge_threads": cfg[0], "edge_blocks": cfg[1], "element_threads": cfg[2],
             "limiter_detector": "staged" if staged.value else "compact",
             "limiter_schedule": "queue" if queue.value else "barrier",
-            "edge_form": "pair" if L.dgm_get_edge_variant(ctx) == 1 else "point"}
+            "edge_form": EDGE_FORMS[L.dgm_get_edge_variant(ctx)]}
 
 
 def _autotune(L, ctx, repeats: int) -> dict:
@@ -316,10 +319,16 @@ class SpatialDisc:
         self._check(self._lib.dgm_set_launch_config(self._ctx, int(edge_threads), int(edge_blocks),
                                                     int(element_threads)), "set_launch_config")
 
-    def set_edge_form(self, pair: bool) -> None:
-        """Pick the edge pass's form: a lane pair per edge slot (each side's state loaded once)
-        or a thread per (slot, Gauss point); both give bitwise identical fluxes."""
-        self._check(self._lib.dgm_set_edge_variant(self._ctx, 1 if pair else 0), "set_edge_form")
+    def set_edge_form(self, form) -> None:
+        """Pick the edge pass's form: "point" (a thread per (slot, Gauss point)), "pair" (a lane pair
+        per edge slot, each side's state loaded once) or "staged" (a lane per point, the slots'
+        records copied to shared memory first); all give the same fluxes.  A bool picks "pair"
+        (True) or "point" (False)."""
+        if isinstance(form, bool):
+            form = "pair" if form else "point"
+        if form not in EDGE_FORMS:
+            raise ValueError(f"edge form must be one of {EDGE_FORMS}")
+        self._check(self._lib.dgm_set_edge_variant(self._ctx, EDGE_FORMS.index(form)), "set_edge_form")
 
     def set_limiter_detector(self, staged: bool) -> None:
         """Pick the limiter's KXRCF detector form: staged loads (fewer memory round trips, more

@@ -248,7 +248,10 @@ int32_t dgm_get_launch_config(dgm_ctx* ctx, int32_t* config /* [3] as above */);
 int32_t dgm_autotune(dgm_ctx* ctx, int32_t repeats, double* best_us /* [2] */);
 /* The edge pass's form (same arithmetic, bitwise identical results): 0 one thread per (edge slot,
  * Gauss point), 1 two lanes per slot, one per side, each loading its element once and evaluating
- * the traces at every point (fewer loads per slot).  No counterpart in the reference. */
+ * the traces at every point (fewer loads per slot), 2 one lane per (slot, point) with the warp's
+ * slots' element records first copied to shared memory by coalesced loads (each record loaded
+ * once per slot, all lanes busy; 128-thread blocks whatever the launch configuration says).
+ * No counterpart in the reference. */
 int32_t dgm_set_edge_variant(dgm_ctx* ctx, int32_t pair);
 int32_t dgm_get_edge_variant(dgm_ctx* ctx);
 /* The form of the limiter's detection launch (modified_kxrcf, weno.rs:7-85, on every element, one

@@ -1,8 +1,9 @@
 """Launch configuration and autotuner: the chosen grouping of edge slots and elements into blocks
-must not change any result (bitwise).  The two edge-pass forms (a thread per slot and point, a
-lane pair per slot) evaluate the same expressions in the same order; the compiler's FMA
-contraction may still differ between the two kernels in FP64 (measured: up to 1 ulp in a
-residual), so they agree bitwise in FP32 and to 1e-14 relative in FP64."""
+must not change any result (bitwise).  The three edge-pass forms (a thread per slot and point, a
+lane pair per slot, a lane per point over records staged in shared memory) evaluate the same
+expressions in the same order; the compiler's FMA contraction may still differ between the
+kernels in FP64 (measured: up to 1 ulp in a residual), so they agree bitwise in FP32 and to 1e-14
+relative in FP64."""
 import numpy as np
 import pytest
 
@@ -12,14 +13,14 @@ from dgm_in_rust_b200.workloads import Instance, instance_mesh
 CONFIGS = [(256, 0, 256), (64, 0, 64), (128, 7, 128), (96, 1, 32), (32, 3, 160)]
 
 
-def _advance(mesh, init, order, precision, steps, config=None, tune=False, pair=None):
+def _advance(mesh, init, order, precision, steps, config=None, tune=False, form=None):
     s = build_solver(mesh, order, 1.4, 0.1, 1.0e30, steps, precision=precision)
     try:
         sd, td = s.spatial_disc, s.temporal_disc
         td.set_initial_on_device(init)
-        if pair is not None:
-            sd.set_edge_form(pair)
-            assert sd.launch_config["edge_form"] == ("pair" if pair else "point")
+        if form is not None:
+            sd.set_edge_form(form)
+            assert sd.launch_config["edge_form"] == form
         if config is not None:
             sd.set_launch_config(*config)
             assert tuple(sd.launch_config.values())[:3] == config
@@ -43,12 +44,12 @@ def test_launch_config_does_not_change_results(built, order, precision):
     mesh, init = instance_mesh(Instance(40, 20, 0.8, 1.25, order))
     U0, t0 = _advance(mesh, init, order, precision, 6)
     for cfg in CONFIGS[1:]:
-        for pair in (False, True):
-            U, t = _advance(mesh, init, order, precision, 6, config=cfg, pair=pair)
-            if pair and precision == "fp64":
-                assert abs(t - t0) <= 1e-14 * t0 and np.abs(U - U0).max() <= 1e-14 * np.abs(U0).max(), (cfg, pair)
+        for form in ("point", "pair", "staged"):
+            U, t = _advance(mesh, init, order, precision, 6, config=cfg, form=form)
+            if form != "point" and precision == "fp64":
+                assert abs(t - t0) <= 1e-14 * t0 and np.abs(U - U0).max() <= 1e-14 * np.abs(U0).max(), (cfg, form)
             else:
-                assert t == t0 and np.array_equal(U, U0), (cfg, pair)
+                assert t == t0 and np.array_equal(U, U0), (cfg, form)
     U, t = _advance(mesh, init, order, precision, 6, tune=True)
     assert abs(t - t0) <= 1e-14 * t0 and np.abs(U - U0).max() <= 1e-14 * np.abs(U0).max()
 
@@ -65,6 +66,9 @@ def test_launch_config_rejects_bad_values(built):
                                                 "limiter_detector": "compact", "limiter_schedule": "barrier",
                                                 "edge_form": "point"}
         sd = s.spatial_disc
+        assert sd._lib.dgm_set_edge_variant(sd.ctx, 3) == 7  # DGM_BAD_ARG
+        with pytest.raises(ValueError):
+            sd.set_edge_form("tiles")
         assert sd._lib.dgm_set_limiter_variant(sd.ctx, 2) == 7  # DGM_BAD_ARG
         assert sd._lib.dgm_set_limiter_schedule(sd.ctx, 2) == 7
     finally:

@@ -27,6 +27,7 @@ STATUS = {
     9: "CUDA runtime error",
     10: "No usable CUDA device",
     11: "Work still in flight",
+    12: "Limiter worklist overflow",
 }
 DGM_NOT_READY = 11
 

@@ -520,9 +520,10 @@ int collect_status(dgm_ctx* c) {
     c->err_where = h.err_where;
     const int zero = 0;
     CK(cudaMemcpyAsync(&c->ctl->status, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    if (h.status == dgm::ST_TIMEOUT) {
-      // a limiter pass that gave up may have left queue slots, counters and a half-passed grid
-      // barrier behind: clear them all (the barrier's generation counter may keep its value)
+    if (h.status == dgm::ST_TIMEOUT || h.status == dgm::ST_LIST_OVERFLOW) {
+      // a limiter pass that gave up (or dropped a worklist entry) may have left queue slots,
+      // counters and a half-passed grid barrier behind: clear them all (the barrier's generation
+      // counter may keep its value)
       CK(cudaMemsetAsync(c->work, 0, sizeof(int) * std::max<int64_t>(c->ne, 1), c->stream));
       Control z = h;
       z.status = 0;
@@ -532,7 +533,6 @@ int collect_status(dgm_ctx* c) {
       z.wl1_count = z.pend_count = 0;
       z.bar_count = 0u;
       for (auto& b : z.bar_sub) b.count = 0u;
-      z.lim_exit = 0u;
       for (auto& q : z.lq) dgm::reset_queue(q);
       CK(cudaMemcpyAsync(c->ctl, &z, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
     }
@@ -1388,6 +1388,7 @@ const char* dgm_status_string(int32_t s) {
     case DGM_CUDA_ERROR: return "CUDA runtime error";
     case DGM_NO_DEVICE: return "No usable CUDA device";
     case DGM_NOT_READY: return "Work still in flight";
+    case DGM_LIST_OVERFLOW: return "Limiter worklist overflow";
   }
   return "unknown status";
 }

@@ -40,6 +40,7 @@ enum : int {
   ST_NONFINITE = 3,
   ST_TOO_MANY_BOUNDARY_EDGES = 4,
   ST_TIMEOUT = 6,
+  ST_LIST_OVERFLOW = 12,
 };
 
 // Supported discretisations: (order, triangle rule, edge rule, derivative keys used by WENO).
@@ -146,10 +147,20 @@ struct Control {
   int pend_count;              // elements the detection left for later waves
   unsigned int bar_count, bar_gen;  // grid barrier of the limiter kernel
   unsigned int head_done;      // blocks of k_step_head that have finished (last one closes the step head)
-  unsigned int lim_exit;       // queue schedule: blocks that have left the pass (the last one resets the queues)
   LimQueue lq[3];              // queue schedule: per-wave queues, wave w uses lq[w % 3]
   BarSub bar_sub[kBarGroups];  // grid barrier: first-level arrival counters
 };
+
+// Zeroes the counters, worklist lengths and queues of the limiter pass that follows.  Every launch
+// that precedes a limiter pass calls it from one thread (the element passes, FMA and tensor-core,
+// and k_set_active before host-driven passes): the detection's atomics then start from zero.
+__device__ __forceinline__ void reset_limiter_pass(Control* ctl) {
+  ctl->t0_count = 0;
+  ctl->unknown[0] = ctl->unknown[1] = 0;
+  ctl->wl_count[0] = ctl->wl_count[1] = 0;
+  ctl->wl1_count = ctl->pend_count = 0;
+  for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
+}
 
 // Gas constants, computed once on the host from hcr with the reference's expressions.
 struct Gas {
@@ -176,6 +187,17 @@ struct KParams {
 __device__ __forceinline__ void raise_status(Control* ctl, InstCtl* ic, int code, long long where) {
   if (atomicCAS(&ic->status, 0, code) == 0) ic->err_where = where;
   if (atomicCAS(&ctl->status, 0, code) == 0) ctl->err_where = where;
+}
+
+// Stores v at list[i] when i is inside the list's capacity; otherwise drops it and reports
+// ST_LIST_OVERFLOW (a worklist holds each element at most once per pass, so this only fires if
+// its counter was not reset before the pass).
+__device__ __forceinline__ void list_put(Control* ctl, int* __restrict__ list, int i, int cap, int v) {
+  if (i < cap) {
+    list[i] = v;
+  } else if (atomicCAS(&ctl->status, 0, ST_LIST_OVERFLOW) == 0) {
+    ctl->err_where = i;
+  }
 }
 
 template <typename T>
@@ -906,14 +928,7 @@ __device__ __forceinline__ void element_body(const KParams<P, T>& kp, const S* _
   constexpr int STRIDE = Staged<NB, S>::kStride;
   __shared__ __align__(16) S s_rec[kElemMaxWarps][8 * STRIDE];
   Control* ctl = kp.ctl;
-  if (bid == 0 && threadIdx.x == 0) {  // counters of the limiter pass that follows
-    ctl->t0_count = 0;
-    ctl->unknown[0] = ctl->unknown[1] = 0;
-    ctl->wl_count[0] = ctl->wl_count[1] = 0;
-    ctl->wl1_count = ctl->pend_count = 0;
-    ctl->lim_exit = 0u;
-    for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
-  }
+  if (bid == 0 && threadIdx.x == 0) reset_limiter_pass(ctl);  // for the limiter pass that follows
   const MeshDev& m = kp.m;
   const int lane = threadIdx.x & 31;
   const int var = lane >> 3, i = lane & 7;
@@ -1625,14 +1640,14 @@ __device__ __forceinline__ void lim_detect_body(const KParams<P, T>& kp, const S
     int base = 0;
     if (lane == 0) base = atomicAdd(&ctl->wl1_count, __popc(em));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (enlist) wl1[base + __popc(em & below)] = e;
+    if (enlist) list_put(ctl, wl1, base + __popc(em & below), m.ne, e);
   }
   const unsigned int wm = __ballot_sync(0xffffffffu, wait);
   if (wm) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&ctl->pend_count, __popc(wm));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (wait) pend[base + __popc(wm & below)] = e;
+    if (wait) list_put(ctl, pend, base + __popc(wm & below), m.ne, e);
   }
 }
 
@@ -1665,8 +1680,8 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
   const int nwarps = gridDim.x * kLimiterWarps;
   // the detection launch has finished: its counts are final
   const int flagged = ctl->t0_count;
-  const int n_wl1 = ctl->wl1_count;
-  const int n_pend = ctl->pend_count;
+  const int n_wl1 = min(ctl->wl1_count, m.ne);  // larger only after an overflow (reported)
+  const int n_pend = min(ctl->pend_count, m.ne);
   int troubled_local = 0;
   int wave = 1;
   // reconstruction of one enlisted element by the whole warp
@@ -1734,7 +1749,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
           int slot0 = 0;
           if (lane == 0) slot0 = atomicAdd(QUEUE ? &q->tail : &ctl->wl_count[wave & 1], __popc(tb));
           slot0 = __shfl_sync(0xffffffffu, slot0, 0);
-          if (ready && trouble) work[slot0 + __popc(tb & ((1u << lane) - 1u))] = QUEUE ? e + 1 : e;
+          if (ready && trouble) list_put(ctl, work, slot0 + __popc(tb & ((1u << lane) - 1u)), m.ne, QUEUE ? e + 1 : e);
         }
         unknown_local += (pending && !ready) ? 1 : 0;
       }
@@ -1744,7 +1759,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
       if (!QUEUE) {
         if (lane == 0 && unknown_local) atomicAdd(&ctl->unknown[wave & 1], unknown_local);
         if (!grid_barrier(ctl, gridDim.x)) break;
-        const int n_work = *((volatile int*)&ctl->wl_count[wave & 1]);
+        const int n_work = min(*((volatile int*)&ctl->wl_count[wave & 1]), m.ne);
         remaining = *((volatile int*)&ctl->unknown[wave & 1]);
         // the other parity's counters were last read before the previous wave's second barrier
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1952,12 +1967,7 @@ __global__ void k_set_active(Control* ctl, InstCtl* ic, int n_inst, double dt, i
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) {
     ctl->troubled = 0;
-    ctl->t0_count = 0;
-    ctl->unknown[0] = ctl->unknown[1] = 0;
-    ctl->wl_count[0] = ctl->wl_count[1] = 0;
-    ctl->wl1_count = ctl->pend_count = 0;
-    ctl->lim_exit = 0u;
-    for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
+    reset_limiter_pass(ctl);
   }
   if (i >= n_inst) return;
   ic[i].active = 1;

@@ -208,12 +208,13 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
   const int gwarp = blockIdx.x * kLimiterWarps + wib;
   const int nwarps = gridDim.x * kLimiterWarps;
   // the detection launch has finished: its counts are final
-  int flagged = 0, n1[3] = {0, 0, 0}, np[3] = {0, 0, 0};
+  int flagged = 0, n1[3] = {0, 0, 0}, np[3] = {0, 0, 0}, cap = 0;  // cap: the worklist's length
   for (int gi = 0; gi < 3; ++gi)
     with_group(mp, gi, [&](const auto& kp, const GroupArgs<T, S>&) {
       flagged += kp.ctl->t0_count;
-      n1[gi] = kp.ctl->wl1_count;
-      np[gi] = kp.ctl->pend_count;
+      n1[gi] = min(kp.ctl->wl1_count, kp.m.ne);  // larger only after an overflow (reported)
+      np[gi] = min(kp.ctl->pend_count, kp.m.ne);
+      cap += kp.m.ne;
     });
   const int n1_all = n1[0] + n1[1] + n1[2], np_all = np[0] + np[1] + np[2];
   int troubled_local[3] = {0, 0, 0};
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
           int slot0 = 0;
           if (lane == 0) slot0 = atomicAdd(&ctl->wl_count[wave & 1], __popc(tb));
           slot0 = __shfl_sync(0xffffffffu, slot0, 0);
-          if (ready && trouble) work[slot0 + __popc(tb & ((1u << lane) - 1u))] = (gi << 30) | e;
+          if (ready && trouble) list_put(ctl, work, slot0 + __popc(tb & ((1u << lane) - 1u)), cap, (gi << 30) | e);
         }
         unknown_local += (pending && !ready) ? 1 : 0;
       }
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
       for (int o = 16; o > 0; o >>= 1) unknown_local += __shfl_xor_sync(0xffffffffu, unknown_local, o);
       if (lane == 0 && unknown_local) atomicAdd(&ctl->unknown[wave & 1], unknown_local);
       if (!grid_barrier(ctl, gridDim.x)) break;
-      const int n_work = *((volatile int*)&ctl->wl_count[wave & 1]);
+      const int n_work = min(*((volatile int*)&ctl->wl_count[wave & 1]), cap);
       const int remaining = *((volatile int*)&ctl->unknown[wave & 1]);
       // the other parity's counters were last read before the previous wave's second barrier
       if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -197,11 +197,7 @@ __global__ void __launch_bounds__(tc::kThreads, 8) k_element_tc(const __grid_con
   Control* ctl = kp.ctl;
   const MeshDev& m = kp.m;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  if (blockIdx.x == 0 && t == 0) {  // counters of the limiter pass that follows
-    ctl->t0_count = 0;
-    ctl->lim_exit = 0u;
-    for (int w = 0; w < 3; ++w) reset_queue(ctl->lq[w]);
-  }
+  if (blockIdx.x == 0 && t == 0) reset_limiter_pass(ctl);  // for the limiter pass that follows
   // constant operands: B1[q][b] = phi_cell, B2[b][k] = [dxi | deta | phi_edge] (zero padded)
   for (int i = t; i < tc::kN * K1; i += tc::kThreads) {
     const int n = i / K1, k = i - n * K1;

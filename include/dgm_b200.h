@@ -38,6 +38,8 @@ extern "C" {
 #define DGM_CUDA_ERROR 9              /* a CUDA runtime call failed                         */
 #define DGM_NO_DEVICE 10              /* no usable CUDA device                              */
 #define DGM_NOT_READY 11              /* dgm_query: work still in flight (not an error)     */
+#define DGM_LIST_OVERFLOW 12          /* a limiter worklist reached its capacity: the entry   */
+                                      /* was dropped, the pass's results are not valid        */
 
 /* ---- boundary types (mesh.rs:174-178) ---------------------------------------------------- */
 #define DGM_WALL 0

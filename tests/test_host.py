@@ -225,3 +225,4 @@ def test_status_strings_match_reference_messages(built):
     assert L.dgm_status_string(1) == b"Negative density found in HLLC!"
     assert L.dgm_status_string(2) == b"Negative pressure found in HLLC!"
     assert L.dgm_status_string(4) == b"Invalid number of boundary neighbours!"
+    assert L.dgm_status_string(12) == b"Limiter worklist overflow"

@@ -286,6 +286,7 @@ def run_batched(args, local):
     t_setup = time.perf_counter()
     built = [(inst, *instance_mesh(inst)) for inst in insts]
     groups = {p: [b for b in built if b[0].order == p] for p in (1, 2)}
+    index = {id(m): k for k, (_, m, _) in enumerate(built)}  # instance number in the seeded list
     K, W, W2 = args.batched_steps, 3, 2
     res = {"workload": f"{len(insts)} NACA 0012 O-grids, Ni uniform on {{32,...,256}}, Nj = Ni/2, "
                        f"Mach U[0.3,0.85], AoA U[-4,6] deg, p in {{1,2}} (numpy default_rng({seed})), "
@@ -344,7 +345,7 @@ def run_batched(args, local):
                 rho = b.download(i)[:, 0].copy() if i % 8 == 0 else None
                 mass = b.tables[inst.order][1].mass_mat_diag
                 w = (mass[None, :] * (0.5 * m.elem_jacob_det)[:, None]) if rho is not None else None
-                acc[(inst.order, id(m))] = (cl, cd, rho, w)
+                acc[(inst.order, index[id(m)])] = (cl, cd, rho, w)
         for b in batches:
             b.close()
         return res["dof"] * 3 * K / (ms * 1e-3), ms / K, dev_bytes, acc
@@ -377,7 +378,8 @@ def run_batched(args, local):
         "max_abs_delta_cl": max(floor_cl.values()), "median_abs_delta_cl": float(np.median(list(floor_cl.values()))),
         "max_abs_delta_cd": max(floor_cd.values()),
         "instances_below_1e-4": int(sum(floor_cl[k] <= 1e-4 and floor_cd[k] <= 1e-4 for k in floor_cl)),
-        "per_instance_abs_delta_cl": {f"p{k[0]}_{k[1]}": v for k, v in floor_cl.items()}}
+        "per_instance_abs_delta_cl": {f"instance_{k[1]}_p{k[0]}": v for k, v in sorted(floor_cl.items(),
+                                                                                     key=lambda kv: kv[0][1])}}
     res["fp32_vs_fp64_after_steps"] = versus(acc32)
     res["fp32_compute_vs_fp64_after_steps"] = versus(acc32c)
     # one at a time, FP64: a DOF-weighted sample (every 8th instance in DOF order)

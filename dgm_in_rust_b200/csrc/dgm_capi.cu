@@ -70,6 +70,8 @@ struct dgm_ctx {
   int dead_inst = 0;           // index of the dead instance (padded contexts)
   int64_t null_elem = -1;      // the null element (padded contexts)
   double* d_diag = nullptr;
+  double* h_diag = nullptr;         // pinned host copy of d_diag (dgm_enqueue_diagnostics)
+  cudaEvent_t diag_ready = nullptr;  // recorded after the copy into h_diag
   double* gram = nullptr;   // WENO Gram matrices, [NB (NB + 1) / 2][ld] (limiter on)
   Control* ctl = nullptr;
   InstCtl* ic = nullptr;
@@ -522,8 +524,7 @@ int collect_status(dgm_ctx* c) {
     CK(cudaMemcpyAsync(&c->ctl->status, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     if (h.status == dgm::ST_TIMEOUT || h.status == dgm::ST_LIST_OVERFLOW) {
       // a limiter pass that gave up (or dropped a worklist entry) may have left queue slots,
-      // counters and a half-passed grid barrier behind: clear them all (the barrier's generation
-      // counter may keep its value)
+      // counters and a half-passed grid barrier behind: clear them all
       CK(cudaMemsetAsync(c->work, 0, sizeof(int) * std::max<int64_t>(c->ne, 1), c->stream));
       Control z = h;
       z.status = 0;
@@ -531,8 +532,7 @@ int collect_status(dgm_ctx* c) {
       z.unknown[0] = z.unknown[1] = 0;
       z.wl_count[0] = z.wl_count[1] = 0;
       z.wl1_count = z.pend_count = 0;
-      z.bar_count = 0u;
-      for (auto& b : z.bar_sub) b.count = 0u;
+      z.bar_word = 0u;
       for (auto& q : z.lq) dgm::reset_queue(q);
       CK(cudaMemcpyAsync(c->ctl, &z, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
     }
@@ -1401,6 +1401,8 @@ void dgm_destroy(dgm_ctx* c) {
     for (auto& g : row)
       if (g) cudaGraphExecDestroy(g);
   for (dgm_ctx* k : c->kids) dgm_destroy(k);
+  if (c->h_diag) cudaFreeHost(c->h_diag);
+  if (c->diag_ready) cudaEventDestroy(c->diag_ready);
   if (c->stream) {
     for (void* p : c->allocs) cudaFreeAsync(p, c->stream);  // back to the pool, in stream order
     cudaStreamSynchronize(c->stream);
@@ -2058,6 +2060,32 @@ int32_t dgm_diagnostics(dgm_ctx* c, int32_t use_residual, double* out) {
   if (st) return st;
   CK(cudaMemcpyAsync(out, c->d_diag, sizeof(double) * 8 * c->inst.size(), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return DGM_OK;
+}
+
+int32_t dgm_enqueue_diagnostics(dgm_ctx* c, int32_t use_residual) {
+  if (!c || c->mixed) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  const size_t bytes = sizeof(double) * 8 * c->inst.size();
+  if (!c->h_diag) {
+    CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_diag), bytes));
+    CK(cudaEventCreateWithFlags(&c->diag_ready, cudaEventDisableTiming));
+  }
+  int st = dispatch(c, [&](auto ops) {
+    using O = decltype(ops);
+    return O::diagnostics(c, use_residual ? O::S(c->R) : nullptr);
+  });
+  if (st) return st;
+  CK(cudaMemcpyAsync(c->h_diag, c->d_diag, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaEventRecord(c->diag_ready, c->stream));
+  return DGM_OK;
+}
+
+int32_t dgm_collected_diagnostics(dgm_ctx* c, double* out) {
+  if (!c || !out || c->mixed || !c->h_diag) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  CK(cudaEventSynchronize(c->diag_ready));
+  std::memcpy(out, c->h_diag, sizeof(double) * 8 * c->inst.size());
   return DGM_OK;
 }
 

@@ -117,15 +117,6 @@ struct alignas(128) LimQueue {
   int _pad2[30];
 };
 
-// First-level arrival counter of the limiter's grid barrier: blocks arrive at the counter of their
-// group (block index mod kBarGroups), each counter on its own 128-byte line, and the last block of
-// each group arrives at the top counter -- kBarGroups parallel atomic chains instead of one.
-constexpr int kBarGroups = 8;
-struct alignas(128) BarSub {
-  unsigned int count;
-  unsigned int _pad[31];
-};
-
 __host__ __device__ __forceinline__ void reset_queue(LimQueue& q) {
   q.tail = 0;
   q.head = 0;
@@ -145,10 +136,9 @@ struct Control {
   int wl_count[2];             // barrier schedule: per-wave worklist length (double-buffered)
   int wl1_count;               // cells the detection enlisted for wave 1
   int pend_count;              // elements the detection left for later waves
-  unsigned int bar_count, bar_gen;  // grid barrier of the limiter kernel
+  unsigned int bar_word;       // grid barrier of the limiter kernels: arrivals, top bit flips per barrier
   unsigned int head_done;      // blocks of k_step_head that have finished (last one closes the step head)
   LimQueue lq[3];              // queue schedule: per-wave queues, wave w uses lq[w % 3]
-  BarSub bar_sub[kBarGroups];  // grid barrier: first-level arrival counters
 };
 
 // Zeroes the counters, worklist lengths and queues of the limiter pass that follows.  Every launch
@@ -1448,42 +1438,29 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, Sto* __
   return ST_OK;
 }
 
-// Bounded grid barrier for the co-resident (cooperative) limiter kernel.
+// Bounded grid barrier for the co-resident (cooperative) limiter kernels.  One arrival word:
+// thread 0 of every block adds 1, except block 0, which adds 2^31 - (nblocks - 1), so that a
+// barrier adds exactly 2^31 in all -- the top bit flips with the last arrival, whatever the order,
+// and the low bits return to their value (nothing to reset, no second word to publish).  A block
+// waits until the top bit differs from the one its own arrival saw.
 __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int nblocks) {
   __syncthreads();
   __shared__ int s_fail;
   if (threadIdx.x == 0) {
     s_fail = 0;
-    volatile unsigned int* gen = &ctl->bar_gen;
-    const unsigned int g = *gen;
-    __threadfence();
-    // two-level arrival: the block's group counter, then (last of the group) the top counter
-    const unsigned int grp = blockIdx.x % kBarGroups;
-    const unsigned int groups = nblocks < (unsigned int)kBarGroups ? nblocks : (unsigned int)kBarGroups;
-    const unsigned int members = (nblocks - grp + kBarGroups - 1) / kBarGroups;
-    bool released = false;
-    if (atomicAdd(&ctl->bar_sub[grp].count, 1u) == members - 1) {
-      ctl->bar_sub[grp].count = 0u;
-      __threadfence();
-      if (atomicAdd(&ctl->bar_count, 1u) == groups - 1) {
-        ctl->bar_count = 0u;
-        __threadfence();
-        atomicAdd(&ctl->bar_gen, 1u);
-        released = true;
+    const unsigned int inc = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
+    __threadfence();  // the block's writes (ordered by __syncthreads) before its arrival
+    const unsigned int seen = atomicAdd(&ctl->bar_word, inc);
+    volatile unsigned int* word = &ctl->bar_word;
+    long long it = 0;
+    while (((seen ^ *word) & 0x80000000u) == 0u) {
+      if (++it > (1ll << 25)) {  // ~ seconds: co-residency is guaranteed, so this is a fault
+        if (atomicCAS(&ctl->status, 0, ST_TIMEOUT) == 0) ctl->err_where = -1;
+        s_fail = 1;
+        break;
       }
     }
-    if (!released) {
-      long long it = 0;
-      while (*gen == g) {
-        if (++it > (1ll << 25)) {  // ~ seconds: co-residency is guaranteed, so this is a fault
-          if (atomicCAS(&ctl->status, 0, ST_TIMEOUT) == 0) ctl->err_where = -1;
-          s_fail = 1;
-          break;
-        }
-        __nanosleep(20);
-      }
-    }
-    __threadfence();
+    __threadfence();  // the other blocks' writes before this block's next reads
   }
   __syncthreads();
   return s_fail == 0;

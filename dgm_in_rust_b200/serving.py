@@ -109,7 +109,7 @@ def footprint_bytes(meshes: list, order: int, precision: str, limiter: bool = Tr
     def arr(count, size):             # dev_alloc: at least one element
         return max(count, 1) * size
 
-    control = 2304 + (n + 1) * 72                                    # Control, InstCtl[n + 1]
+    control = 1280 + (n + 1) * 72                                    # Control, InstCtl[n + 1]
     geometry = 3 * ne * 8 + 4 * ld * 8 + 2 * 3 * ld * 4 + ne * 4 + ld // 32 * 4  # jac, hmin, h15, dinv, face, nbr,
     #                                                                              inst, batch order
     edges = (arr(n_int, 8) + arr(n_int, 4) + arr(n_int, 32) + arr(n_bnd, 4) + arr(n_bnd, 4) + arr(n_bnd, 32)
@@ -191,6 +191,7 @@ class _Cohort:
         steps = {m.index: self.batch.state(m.index)[1] for m in live}
         n = min(min(m.next_check, self.max_steps) - steps[m.index] for m in live)
         self.batch.advance(max(n, 1), with_residual=True)
+        self.batch.enqueue_diagnostics(use_residual=True)  # read at the check, no device work there
         return True
 
     def take(self, i: int, item, now: float) -> None:
@@ -386,7 +387,7 @@ class ServingLoop:
         to waiting requests, enqueues the next steps.  Returns True when the cohort can close (no
         member running)."""
         b = co.batch
-        diag = b.diagnostics(use_residual=True)
+        diag = b.collected_diagnostics()
         co.checks += 1
         for m in co.members():
             t, step, status, _ = b.state(m.index)
@@ -459,12 +460,13 @@ def solve_alone(req: Request, precision: str = "fp64", device: int = 0, chunk_st
         n = 1
         while True:
             td.advance(n, with_residual=True)
+            sd.enqueue_diagnostics(use_residual=True)
             try:
                 td.synchronize()
             except DgmError as e:
                 status = e.status
             step = td.current_step
-            r = math.sqrt(max(float(sd.diagnostics(use_residual=True)[6]), 0.0))
+            r = math.sqrt(max(float(sd.collected_diagnostics()[6]), 0.0))
             if r0 is None:
                 r0 = r if r > 0.0 else 1.0
             drop = r / r0

@@ -305,6 +305,16 @@ class SpatialDisc:
                     "diagnostics")
         return out[0]
 
+    def enqueue_diagnostics(self, use_residual: bool = False) -> None:
+        """Enqueue :meth:`diagnostics` behind the work on the stream, into a pinned host buffer."""
+        self._check(self._lib.dgm_enqueue_diagnostics(self._ctx, 1 if use_residual else 0), "enqueue_diagnostics")
+
+    def collected_diagnostics(self) -> np.ndarray:
+        """The diagnostics of the last :meth:`enqueue_diagnostics` (waits for that copy only)."""
+        out = np.zeros((1, 8))
+        self._check(self._lib.dgm_collected_diagnostics(self._ctx, _native.dptr(out)), "collected_diagnostics")
+        return out[0]
+
     def limiter_stats(self) -> tuple[int, int]:
         t, w = ctypes.c_int64(0), ctypes.c_int32(0)
         self._lib.dgm_limiter_stats(self._ctx, ctypes.byref(t), ctypes.byref(w))
@@ -657,4 +667,15 @@ class Batch:
         out = np.zeros((self.n, 8))
         self._check(self._lib.dgm_diagnostics(self._ctx, 1 if use_residual else 0, _native.dptr(out)),
                     "diagnostics")
+        return out
+
+    def enqueue_diagnostics(self, use_residual: bool = False) -> None:
+        """Enqueue :meth:`diagnostics` behind the work on the stream, into a pinned host buffer
+        (not for mixed batches)."""
+        self._check(self._lib.dgm_enqueue_diagnostics(self._ctx, 1 if use_residual else 0), "enqueue_diagnostics")
+
+    def collected_diagnostics(self) -> np.ndarray:
+        """[n, 8]: the diagnostics of the last :meth:`enqueue_diagnostics` (waits for that copy only)."""
+        out = np.zeros((self.n, 8))
+        self._check(self._lib.dgm_collected_diagnostics(self._ctx, _native.dptr(out)), "collected_diagnostics")
         return out

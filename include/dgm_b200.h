@@ -352,6 +352,14 @@ int32_t dgm_advance_with_residual(dgm_ctx* ctx, int64_t n_steps);
  * modal coefficients of the last residual written (0 unless use_residual); 7 element count.
  * No counterpart in the reference (it computes no forces or norms). */
 int32_t dgm_diagnostics(dgm_ctx* ctx, int32_t use_residual, double* out);
+/* The same diagnostics without waiting: dgm_enqueue_diagnostics enqueues their computation after
+ * the work already on the context's stream, with a copy into a pinned host buffer of the context;
+ * dgm_collected_diagnostics waits for that copy (not for later work) and returns it in out (as
+ * above; DGM_BAD_ARG before the first enqueue).  A serving loop enqueues them behind each chunk of
+ * steps and reads them when the chunk is done, with no device work on its check path.  Not for
+ * mixed batches. */
+int32_t dgm_enqueue_diagnostics(dgm_ctx* ctx, int32_t use_residual);
+int32_t dgm_collected_diagnostics(dgm_ctx* ctx, double* out);
 
 /* Cell fields of write_to_vtk (src/io/write_results.rs:33-61) for instance i of the resident
  * state: fields[e][0..4] = density, x velocity, y velocity, pressure from each element's mode-0

@@ -145,3 +145,24 @@ def test_diagnostics_match_numpy():
             F += w[g] * p * n * 0.5 * mesh.edge_jacob_det[dd]
     assert np.allclose(d[4:6], F, rtol=1e-12, atol=1e-14)
     s.close()
+
+
+def test_enqueued_diagnostics_equal_direct():
+    """dgm_enqueue_diagnostics / dgm_collected_diagnostics (the serving loop's check path) return
+    what dgm_diagnostics returns after the same steps, bit for bit; a mixed batch refuses them."""
+    cases = [_case(naca0012_ogrid(32, 16), 0.5, 2.0), _case(naca0012_ogrid(40, 20), 0.7, 1.0)]
+    b = Batch([m for m, _ in cases], 2, 1.4, [0.1] * 2, [1.0e30] * 2, [10 ** 6] * 2, precision="fp32")
+    for i, (_, init) in enumerate(cases):
+        b.set_initial(i, init)
+    for n in (1, 9, 32):
+        b.advance(n, with_residual=True)
+        b.enqueue_diagnostics(use_residual=True)
+        got = b.collected_diagnostics()
+        assert b.synchronize() == 0
+        assert np.array_equal(got, b.diagnostics(use_residual=True))
+        assert got[:, 6].min() > 0.0
+    b.close()
+    m = Batch([cases[0][0], cases[1][0]], [1, 2], 1.4, [0.1] * 2, [1.0e30] * 2, [5] * 2)
+    with pytest.raises(DgmError):
+        m.enqueue_diagnostics()
+    m.close()

@@ -83,6 +83,12 @@ class FakeBatch:
             out[i, 6] = (3.0 * 0.5 ** (self.step[i] - 1)) ** 2
         return out
 
+    def enqueue_diagnostics(self, use_residual=False):
+        self.enqueued = self.diagnostics(use_residual)  # the steps are already applied when enqueued
+
+    def collected_diagnostics(self):
+        return self.enqueued.copy()
+
     def state(self, i):
         return 1e-3 * self.step[i], self.step[i], 0, -1
 

@@ -69,9 +69,10 @@ def parse():
     ap.add_argument("--serving-budget-gib", type=float, default=16.0)
     ap.add_argument("--serving-max-active", type=int, default=2 << 20,
                     help="elements of running requests above which new requests wait (work-in-flight cap)")
-    ap.add_argument("--profile-case", choices=["c2", "c3"],
+    ap.add_argument("--profile-case", choices=["c2", "c3", "batch", "batch_per_order"],
                     help="run a fixed launch sequence for ncu (no timing, no autotuning): c2 = the workload "
-                         "above, c3 = the 1024 x 512 p = 3 O-grid (M 0.7, AoA 2 deg)")
+                         "above, c3 = the 1024 x 512 p = 3 O-grid (M 0.7, AoA 2 deg), batch / batch_per_order = "
+                         "the 256-instance batch as one mixed context / one context per order")
     ap.add_argument("--precision", choices=["fp64", "fp32", "fp32_compute", "tf32", "tf32x3"], default="fp64")
     ap.add_argument("--launch", default="128,2368,128,1,0",
                     help="edge threads, edge blocks, element threads, staged limiter detector, edge pass form "
@@ -804,6 +805,34 @@ def run_ours(args):
     return 0
 
 
+def run_profile_batch(args):
+    """The batching configuration's 256 instances for ncu captures, no autotuning: "batch" is the
+    mixed batch (one context, one stream, one launch per kernel of the step over both orders),
+    "batch_per_order" one batch per order on its own stream; --warmup + --steps steps."""
+    from dgm_in_rust_b200 import Batch
+    from dgm_in_rust_b200.workloads import batch_instances, instance_mesh
+    built = [(inst, *instance_mesh(inst)) for inst in batch_instances(args.batched_instances, seed=2024)]
+    if args.profile_case == "batch":
+        sets = [([inst.order for inst, _, _ in built], built)]
+    else:
+        sets = [(p, [b for b in built if b[0].order == p]) for p in (1, 2)]
+    batches = []
+    for order, items in sets:
+        b = Batch([m for _, m, _ in items], order, HCR, [CFL] * len(items), [1.0e30] * len(items),
+                  [10 ** 12] * len(items), limiter=True, precision=args.precision)
+        for i, (_, _, init) in enumerate(items):
+            b.set_initial(i, init)
+        batches.append(b)
+    for b in batches:
+        b.advance(args.warmup + args.steps)
+    status = [b.synchronize() for b in batches]
+    print(json.dumps({"profile_case": args.profile_case, "precision": args.precision, "instances": len(built),
+                      "contexts": len(batches), "status": status}), flush=True)
+    for b in batches:
+        b.close()
+    return 0 if not any(status) else 1
+
+
 def run_profile_case(args):
     """A deterministic launch sequence for ncu captures: the case's context (one k_weno_gram and
     one k_project_uniform launch), then --warmup + --steps time-march steps with the launch
@@ -816,6 +845,8 @@ def run_profile_case(args):
     from dgm_in_rust_b200.workloads import Instance, instance_mesh
     build()
     torch.cuda.set_device(0)
+    if args.profile_case in ("batch", "batch_per_order"):
+        return run_profile_batch(args)
     inst = {"c2": Instance(NI, NJ, MACH, AOA, ORDER), "c3": Instance(1024, 512, 0.7, 2.0, 3)}[args.profile_case]
     mesh, init = instance_mesh(inst)
     s = build_solver(mesh, inst.order, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, precision=args.precision)

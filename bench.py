@@ -76,8 +76,8 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "fp32", "fp32_compute", "tf32", "tf32x3"], default="fp64")
     ap.add_argument("--launch", default="128,2368,128,1,0",
                     help="edge threads, edge blocks, element threads, staged limiter detector, edge pass form "
-                         "(0 point, 1 lane pair, 2 staged), queue limiter schedule (profile case; the last two "
-                         "may be left out: 0)")
+                         "(0 point, 1 lane pair, 2 staged, 3 point at 64 registers), queue limiter schedule "
+                         "(profile case; the last two may be left out: 0)")
     return ap.parse_args()
 
 
@@ -856,7 +856,7 @@ def run_profile_case(args):
     sd.set_launch_config(e_t, e_b, l_t)
     sd.set_limiter_detector(bool(staged))
     sd.set_limiter_schedule(bool(queue))
-    sd.set_edge_form(("point", "pair", "staged")[pair])
+    sd.set_edge_form(("point", "pair", "staged", "point_r64")[pair])
     td.set_initial_on_device(init)
     td.advance(args.warmup + args.steps)
     td.synchronize()

@@ -81,7 +81,8 @@ struct dgm_ctx {
   int lim_staged = 0;            // limiter detector variant (dgm_set_limiter_variant / autotune)
   int lim_queue = 0;             // limiter schedule (dgm_set_limiter_schedule / autotune)
   int edge_pair = 0;             // edge pass form: 0 thread per (slot, point), 1 lane pair per slot,
-                                 // 2 lane per point with the slots' records staged in shared memory
+                                 // 2 lane per point with the slots' records staged in shared memory,
+                                 // 3 form 0 compiled for 64 registers
   float lim_us[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // last autotuned limiter times [detector][schedule]
   // launch configuration of the edge and element passes (dgm_set_launch_config / dgm_autotune):
   // edge_blocks = 0 launches one thread per (slot, Gauss point), else a grid-stride grid
@@ -220,7 +221,10 @@ struct Ops {
       const int64_t total = (c->n_int + c->n_bnd) * V::NG;
       const int64_t full = std::max<int64_t>(1, (total + threads - 1) / threads);
       const int blocks = (int)(c->edge_blocks > 0 ? std::min<int64_t>(c->edge_blocks, full) : full);
-      dgm::k_edge_flux<P, T, St><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, Fx(c->F));
+      if (c->edge_pair == 3)  // the point form at 64 registers
+        dgm::k_edge_flux_r64<P, T, St><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, Fx(c->F));
+      else
+        dgm::k_edge_flux<P, T, St><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), U, Fx(c->F));
     }
     CK(cudaGetLastError());
     return DGM_OK;
@@ -1847,7 +1851,7 @@ int32_t dgm_get_limiter_schedule(dgm_ctx* c, int32_t* queue, double* tuned_us) {
 
 int32_t dgm_set_edge_variant(dgm_ctx* c, int32_t pair) {
   if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
-  if (!c || pair < 0 || pair > 2) return DGM_BAD_ARG;
+  if (!c || pair < 0 || pair > 3) return DGM_BAD_ARG;
   if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
   CK(cudaStreamSynchronize(c->stream));
   c->edge_pair = pair;
@@ -1889,12 +1893,14 @@ int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
     return DGM_CUDA_ERROR;
   }
   const int sms = c->num_sms;
-  // (form, threads, blocks): per-point, lane-pair and staged edge passes, one work item per thread
-  // or a grid-stride grid of 4-16 blocks per SM (the staged form always runs 128-thread blocks)
+  // (form, threads, blocks): per-point (at two register budgets), lane-pair and staged edge
+  // passes, one work item per thread or a grid-stride grid of 4-16 blocks per SM (the staged form
+  // always runs 128-thread blocks)
   const int edge_cand[][3] = {{0, 256, 0},        {0, 128, 0},        {0, 64, 0},         {0, 256, 4 * sms},
                               {0, 256, 8 * sms},  {0, 128, 8 * sms},  {0, 128, 16 * sms}, {1, 256, 0},
                               {1, 128, 0},        {1, 64, 0},         {1, 128, 8 * sms},  {1, 128, 16 * sms},
-                              {2, 128, 0},        {2, 128, 8 * sms},  {2, 128, 16 * sms}};
+                              {2, 128, 0},        {2, 128, 8 * sms},  {2, 128, 16 * sms}, {3, 256, 0},
+                              {3, 128, 0},        {3, 256, 8 * sms},  {3, 128, 16 * sms}};
   const int elem_cand[] = {256, 128, 64};
   auto time_phase = [&](int phase, float* us) -> int {
     for (int w = 0; w < 2; ++w) {

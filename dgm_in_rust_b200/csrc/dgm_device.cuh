@@ -631,6 +631,15 @@ __global__ void __launch_bounds__(256, 3) k_edge_flux(const __grid_constant__ KP
   edge_flux_body<P, T, S>(kp, U, F, blockIdx.x, gridDim.x);
 }
 
+// The same kernel compiled for 4 blocks of 256 threads per SM (at most 64 registers, a few bytes
+// of spills) instead of 3: more warps in flight for the latency-bound gathers, more local-memory
+// traffic; the autotuner picks one of the two per context.
+template <int P, typename T, typename S = T>
+__global__ void __launch_bounds__(256, 4) k_edge_flux_r64(const __grid_constant__ KParams<P, T> kp,
+                                                          const S* __restrict__ U, T* __restrict__ F) {
+  edge_flux_body<P, T, S>(kp, U, F, blockIdx.x, gridDim.x);
+}
+
 // The same edge pass with two lanes per edge slot, one per side: each lane loads its element's
 // modes once, evaluates the traces at all NG points (the right side at the reversed points,
 // spatial_disc.rs:185), the pair swaps traces with shuffles, and the two lanes split the points

@@ -130,7 +130,7 @@ def initial_state(mesh: Mesh, basis: DubinerBasis, gauss_points: GaussPoints, hc
     return U
 
 
-EDGE_FORMS = ("point", "pair", "staged")  # dgm_set_edge_variant's 0, 1, 2
+EDGE_FORMS = ("point", "pair", "staged", "point_r64")  # dgm_set_edge_variant's 0, 1, 2, 3
 
 
 def _launch_config(L, ctx) -> dict:
@@ -331,9 +331,9 @@ class SpatialDisc:
 
     def set_edge_form(self, form) -> None:
         """Pick the edge pass's form: "point" (a thread per (slot, Gauss point)), "pair" (a lane pair
-        per edge slot, each side's state loaded once) or "staged" (a lane per point, the slots'
-        records copied to shared memory first); all give the same fluxes.  A bool picks "pair"
-        (True) or "point" (False)."""
+        per edge slot, each side's state loaded once), "staged" (a lane per point, the slots'
+        records copied to shared memory first) or "point_r64" (the point form compiled for 64
+        registers); all give the same fluxes.  A bool picks "pair" (True) or "point" (False)."""
         if isinstance(form, bool):
             form = "pair" if form else "point"
         if form not in EDGE_FORMS:

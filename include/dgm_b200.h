@@ -252,7 +252,8 @@ int32_t dgm_autotune(dgm_ctx* ctx, int32_t repeats, double* best_us /* [2] */);
  * Gauss point), 1 two lanes per slot, one per side, each loading its element once and evaluating
  * the traces at every point (fewer loads per slot), 2 one lane per (slot, point) with the warp's
  * slots' element records first copied to shared memory by coalesced loads (each record loaded
- * once per slot, all lanes busy; 128-thread blocks whatever the launch configuration says).
+ * once per slot, all lanes busy; 128-thread blocks whatever the launch configuration says), 3 form 0
+ * compiled for 4 blocks of 256 threads per SM (64 registers) instead of 3.
  * No counterpart in the reference. */
 int32_t dgm_set_edge_variant(dgm_ctx* ctx, int32_t pair);
 int32_t dgm_get_edge_variant(dgm_ctx* ctx);

@@ -1,9 +1,9 @@
 """Launch configuration and autotuner: the chosen grouping of edge slots and elements into blocks
-must not change any result (bitwise).  The three edge-pass forms (a thread per slot and point, a
-lane pair per slot, a lane per point over records staged in shared memory) evaluate the same
-expressions in the same order; the compiler's FMA contraction may still differ between the
-kernels in FP64 (measured: up to 1 ulp in a residual), so they agree bitwise in FP32 and to 1e-14
-relative in FP64."""
+must not change any result (bitwise).  The edge-pass forms (a thread per slot and point, at two
+register budgets; a lane pair per slot; a lane per point over records staged in shared memory)
+evaluate the same expressions in the same order; the compiler's FMA contraction may still differ
+between the kernels in FP64 (measured: up to 1 ulp in a residual), so they agree bitwise in FP32
+and to 1e-14 relative in FP64."""
 import numpy as np
 import pytest
 
@@ -44,7 +44,7 @@ def test_launch_config_does_not_change_results(built, order, precision):
     mesh, init = instance_mesh(Instance(40, 20, 0.8, 1.25, order))
     U0, t0 = _advance(mesh, init, order, precision, 6)
     for cfg in CONFIGS[1:]:
-        for form in ("point", "pair", "staged"):
+        for form in ("point", "pair", "staged", "point_r64"):
             U, t = _advance(mesh, init, order, precision, 6, config=cfg, form=form)
             if form != "point" and precision == "fp64":
                 assert abs(t - t0) <= 1e-14 * t0 and np.abs(U - U0).max() <= 1e-14 * np.abs(U0).max(), (cfg, form)
@@ -66,7 +66,7 @@ def test_launch_config_rejects_bad_values(built):
                                                 "limiter_detector": "compact", "limiter_schedule": "barrier",
                                                 "edge_form": "point"}
         sd = s.spatial_disc
-        assert sd._lib.dgm_set_edge_variant(sd.ctx, 3) == 7  # DGM_BAD_ARG
+        assert sd._lib.dgm_set_edge_variant(sd.ctx, 4) == 7  # DGM_BAD_ARG
         with pytest.raises(ValueError):
             sd.set_edge_form("tiles")
         assert sd._lib.dgm_set_limiter_variant(sd.ctx, 2) == 7  # DGM_BAD_ARG

@@ -61,7 +61,7 @@ struct dgm_ctx {
   unsigned char* t0 = nullptr;
   unsigned int* status = nullptr;
   int* work = nullptr;
-  int* wl1 = nullptr;    // limiter: cells the detection enlists for wave 1
+  int* wl1 = nullptr;    // limiter: cells the detection enlists for wave 1 (entries of kEntryInts ints)
   int* pend = nullptr;   // limiter: elements the detection leaves for later waves
   int* order = nullptr;  // limiter: the detection's visiting order of the warp batches (breadth-first)
   int* d_elem_rng = nullptr;   // [2 n] first element, element count of each instance's mesh
@@ -1093,7 +1093,7 @@ dgm_ctx* create(int n_inst, const dgm_mesh_desc* meshes, const dgm_slot_capacity
       (st = dev_alloc_bytes(c, &c->F, n_flux * flux_bytes(c))) ||
       (st = dev_alloc(c, &c->stage, (size_t)c->max_inst_ne * NEQ * c->nb)) ||
       (st = dev_alloc(c, &c->t0, (size_t)c->ne)) || (st = dev_alloc(c, &c->status, (size_t)c->ne)) ||
-      (st = dev_alloc(c, &c->work, (size_t)c->ne)) || (st = dev_alloc(c, &c->wl1, (size_t)c->ne)) ||
+      (st = dev_alloc(c, &c->work, (size_t)c->ne)) || (st = dev_alloc(c, &c->wl1, (size_t)c->ne * dgm::kEntryInts)) ||
       (st = dev_alloc(c, &c->pend, (size_t)c->ne)) || (st = dev_alloc(c, &c->d_diag, (size_t)n_inst * 8)))
     return fail(st);
   for (void* p : {c->U, c->U1, c->U2, c->R})

@@ -190,6 +190,32 @@ __device__ __forceinline__ void list_put(Control* ctl, int* __restrict__ list, i
   }
 }
 
+// Wave-1 worklist entries carry the element's faces and neighbours, so that the reconstruction
+// that takes the entry needs no further dependent load before the states:
+// list[8 i .. 8 i + 7] = {e, face[0..2], nbr[0..2], 0}.  Dropped and reported like list_put.
+constexpr int kEntryInts = 8;
+__device__ __forceinline__ void entry_put(Control* ctl, int* __restrict__ list, int i, int cap, int e,
+                                          const int (&f)[3], const int (&n)[3]) {
+  if (i < cap) {
+    int4* p = reinterpret_cast<int4*>(list + (size_t)kEntryInts * i);
+    p[0] = make_int4(e, f[0], f[1], f[2]);
+    p[1] = make_int4(n[0], n[1], n[2], 0);
+  } else if (atomicCAS(&ctl->status, 0, ST_LIST_OVERFLOW) == 0) {
+    ctl->err_where = i;
+  }
+}
+
+// Reads entry i of such a list into every lane of the warp (lanes 0-6 load one word each).
+__device__ __forceinline__ int entry_get(const int* __restrict__ list, int i, int lane, int (&f)[3], int (&n)[3]) {
+  const int v = lane < 7 ? __ldcg(&list[(size_t)kEntryInts * i + lane]) : 0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    f[k] = __shfl_sync(0xffffffffu, v, 1 + k);
+    n[k] = __shfl_sync(0xffffffffu, v, 4 + k);
+  }
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
 template <typename T>
 __device__ __forceinline__ T ld_state(const T* p) { return __ldcg(p); }
 
@@ -1626,7 +1652,15 @@ __device__ __forceinline__ void lim_detect_body(const KParams<P, T>& kp, const S
     int base = 0;
     if (lane == 0) base = atomicAdd(&ctl->wl1_count, __popc(em));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (enlist) list_put(ctl, wl1, base + __popc(em & below), m.ne, e);
+    if (enlist) {
+      int f[3], n[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        f[k] = m.face[k * m.ld + e];
+        n[k] = m.nbr[k * m.ld + e];
+      }
+      entry_put(ctl, wl1, base + __popc(em & below), m.ne, e, f, n);
+    }
   }
   const unsigned int wm = __ballot_sync(0xffffffffu, wait);
   if (wm) {
@@ -1637,8 +1671,9 @@ __device__ __forceinline__ void lim_detect_body(const KParams<P, T>& kp, const S
   }
 }
 
+// The compact detector at 6 blocks per SM (80 registers); the staged one keeps its registers.
 template <int P, typename T, bool STAGED, typename S = T>
-__global__ void __launch_bounds__(kDetectThreads) k_lim_detect(const __grid_constant__ KParams<P, T> kp,
+__global__ void __launch_bounds__(kDetectThreads, STAGED ? 1 : 6) k_lim_detect(const __grid_constant__ KParams<P, T> kp,
                                                                const S* __restrict__ U,
                                                                unsigned char* __restrict__ t0,
                                                                unsigned int* __restrict__ status,
@@ -1671,6 +1706,13 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
   int troubled_local = 0;
   int wave = 1;
   // reconstruction of one enlisted element by the whole warp
+  auto reconstruct_with = [&](int et, const int (&fwt)[3], const int (&nbt)[3]) {
+    const int rs = weno_reconstruct<P, T, S>(kp, U, et, fwt, nbt, lane, *scratch_w);
+    if (rs != ST_OK && lane == 0) {
+      const int inst = m.n_inst > 1 ? m.inst[et] : 0;
+      raise_status(ctl, &kp.ic[inst], rs, et);
+    }
+  };
   auto reconstruct = [&](int et) {
     int fwt[3], nbt[3];
 #pragma unroll
@@ -1678,17 +1720,14 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter(const __grid_con
       fwt[k] = m.face[k * m.ld + et];
       nbt[k] = m.nbr[k * m.ld + et];
     }
-    const int rs = weno_reconstruct<P, T, S>(kp, U, et, fwt, nbt, lane, *scratch_w);
-    if (rs != ST_OK && lane == 0) {
-      const int inst = m.n_inst > 1 ? m.inst[et] : 0;
-      raise_status(ctl, &kp.ic[inst], rs, et);
-    }
+    reconstruct_with(et, fwt, nbt);
   };
   if (flagged > 0) {  // else no element is limited: every block leaves at once
     // ---- wave 1: the cells enlisted by the detection (the list is complete) ----
     for (int i = gwarp; i < n_wl1; i += nwarps) {
-      const int et = __ldcg(&wl1[i]);
-      reconstruct(et);
+      int fwt[3], nbt[3];
+      const int et = entry_get(wl1, i, lane, fwt, nbt);
+      reconstruct_with(et, fwt, nbt);
       if (lane == 0) status[et] = (1u << 2) | 2u;
       ++troubled_local;
     }

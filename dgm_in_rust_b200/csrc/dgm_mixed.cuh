@@ -219,15 +219,17 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
   const int n1_all = n1[0] + n1[1] + n1[2], np_all = np[0] + np[1] + np[2];
   int troubled_local[3] = {0, 0, 0};
   int wave = 1;
-  auto reconstruct = [&](int gi, int et) {
+  // reconstruction of element et of group gi; faces and neighbours from its worklist entry
+  // (have_ids) or loaded here
+  auto reconstruct = [&](int gi, int et, bool have_ids, const int (&fin)[3], const int (&nin)[3]) {
     with_group(mp, gi, [&](const auto& kp, const GroupArgs<T, S>& g) {
       constexpr int P = OrderOf<std::decay_t<decltype(kp)>>::value;
       const MeshDev& m = kp.m;
       int fwt[3], nbt[3];
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        fwt[k] = m.face[k * m.ld + et];
-        nbt[k] = m.nbr[k * m.ld + et];
+        fwt[k] = have_ids ? fin[k] : m.face[k * m.ld + et];
+        nbt[k] = have_ids ? nin[k] : m.nbr[k * m.ld + et];
       }
       const int rs = weno_reconstruct<P, T, S>(kp, g.Uout, et, fwt, nbt, lane,
                                             *reinterpret_cast<WenoScratch<P>*>(s_warp[wib]));
@@ -247,9 +249,9 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
     for (int i = gwarp; i < n1_all; i += nwarps) {
       int gi;
       const int li = split(n1, i, gi);
-      int et = 0;
-      with_group(mp, gi, [&](const auto&, const GroupArgs<T, S>& g) { et = __ldcg(&g.wl1[li]); });
-      reconstruct(gi, et);
+      int et = 0, fwt[3], nbt[3];
+      with_group(mp, gi, [&](const auto&, const GroupArgs<T, S>& g) { et = entry_get(g.wl1, li, lane, fwt, nbt); });
+      reconstruct(gi, et, true, fwt, nbt);
       with_group(mp, gi, [&](const auto&, const GroupArgs<T, S>& g) {
         if (lane == 0) g.status[et] = (1u << 2) | 2u;
       });
@@ -316,7 +318,8 @@ __global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __gr
       for (int i = gwarp; i < n_work; i += nwarps) {
         const int entry = __ldcg(&work[i]);
         const int gi = entry >> 30, et = entry & ((1 << 30) - 1);
-        reconstruct(gi, et);
+        const int none[3] = {0, 0, 0};
+        reconstruct(gi, et, false, none, none);
         __threadfence();
         with_group(mp, gi, [&](const auto&, const GroupArgs<T, S>& g) {
           if (lane == 0) g.status[et] = ((unsigned int)wave << 2) | 2u;

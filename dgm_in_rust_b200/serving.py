@@ -118,7 +118,7 @@ def footprint_bytes(meshes: list, order: int, precision: str, limiter: bool = Tr
     state = 4 * NEQ * nb * ld * eb                                   # U, U1, U2, R
     flux = (n_int + n_bnd) * ng * 4 * eb                             # F
     stage = max_ne * NEQ * nb * 8                                    # FP64 staging
-    limiter_bytes = ne * (1 + 4 + 4 + 4 + 4)                         # t0, status, work, wl1, pend
+    limiter_bytes = ne * (1 + 4 + 4 + 32 + 4)                        # t0, status, work, wl1 entries, pend
     diag = n * 8 * 8
     gram = nb * (nb + 1) // 2 * ld * 8 if limiter else 0              # WENO Gram matrices
     return int(control + geometry + edges + offsets + state + flux + stage + limiter_bytes + diag + gram)

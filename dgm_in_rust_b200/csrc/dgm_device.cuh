@@ -1473,29 +1473,40 @@ __device__ __forceinline__ int weno_reconstruct(const KParams<P, T>& kp, Sto* __
   return ST_OK;
 }
 
-// Bounded grid barrier for the co-resident (cooperative) limiter kernels.  One arrival word:
-// thread 0 of every block adds 1, except block 0, which adds 2^31 - (nblocks - 1), so that a
+// Release add and acquire load at GPU scope (the PTX memory model's synchronisation pair).
+__device__ __forceinline__ unsigned int atom_add_release_gpu(unsigned int* p, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Bounded grid barrier for the co-resident (cooperative) limiter kernels: a sense-reversing
+// arrival word.  Thread 0 of every block adds 1, block 0 adds 2^31 - (nblocks - 1), so that a
 // barrier adds exactly 2^31 in all -- the top bit flips with the last arrival, whatever the order,
 // and the low bits return to their value (nothing to reset, no second word to publish).  A block
-// waits until the top bit differs from the one its own arrival saw.
+// waits until the top bit differs from the one its own arrival saw.  The arrival is a release
+// (the block's writes, ordered by __syncthreads, before it) and the polling an acquire (every
+// arrival's writes before the block's next reads): no separate fences.
 __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int nblocks) {
   __syncthreads();
   __shared__ int s_fail;
   if (threadIdx.x == 0) {
     s_fail = 0;
     const unsigned int inc = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
-    __threadfence();  // the block's writes (ordered by __syncthreads) before its arrival
-    const unsigned int seen = atomicAdd(&ctl->bar_word, inc);
-    volatile unsigned int* word = &ctl->bar_word;
+    const unsigned int seen = atom_add_release_gpu(&ctl->bar_word, inc);
     long long it = 0;
-    while (((seen ^ *word) & 0x80000000u) == 0u) {
+    while (((seen ^ ld_acquire_gpu(&ctl->bar_word)) & 0x80000000u) == 0u) {
       if (++it > (1ll << 25)) {  // ~ seconds: co-residency is guaranteed, so this is a fault
         if (atomicCAS(&ctl->status, 0, ST_TIMEOUT) == 0) ctl->err_where = -1;
         s_fail = 1;
         break;
       }
     }
-    __threadfence();  // the other blocks' writes before this block's next reads
   }
   __syncthreads();
   return s_fail == 0;

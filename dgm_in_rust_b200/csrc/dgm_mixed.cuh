@@ -198,8 +198,10 @@ struct MixedScratch {
 // group, so each group settles exactly as in its own pass.  The lead group's control block holds
 // the grid barrier and the wave counters; the element pass of the next stage resets every group's
 // counters.
+// Held at 3 blocks per SM (168 registers) when the batch has orders 1 and 2 only -- the occupancy
+// of the order-2 kernel; with order 3 (whose kernel alone needs 222 registers), 2 blocks per SM.
 template <typename T, int MASK, typename S = T>
-__global__ void __launch_bounds__(kLimiterWarps * 32) k_limiter_mixed(const __grid_constant__ Mixed<T, MASK, S> mp,
+__global__ void __launch_bounds__(kLimiterWarps * 32, (MASK & 4) ? 2 : 3) k_limiter_mixed(const __grid_constant__ Mixed<T, MASK, S> mp,
                                                                       int* __restrict__ work) {
   Control* ctl = lead_ctl(mp);
   constexpr size_t kWarpBytes = MixedScratch<MASK>::bytes;

@@ -184,6 +184,8 @@ def lib() -> ctypes.CDLL:
     L.dgm_instance_set_initial.argtypes = [vp, ctypes.c_int32] + [ctypes.c_double] * 4
     L.dgm_diagnostics.argtypes = [vp, ctypes.c_int32, P_D]
     L.dgm_enqueue_diagnostics.argtypes = [vp, ctypes.c_int32]
+    L.dgm_set_viscous.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, P_D]
+    L.dgm_get_viscous.argtypes = [vp]
     L.dgm_collected_diagnostics.argtypes = [vp, P_D]
     L.dgm_precision.argtypes = [vp]
     L.dgm_upload_solutions.argtypes = [vp, P_D]
@@ -237,7 +239,7 @@ def lib() -> ctypes.CDLL:
                  "dgm_set_limiter_variant", "dgm_get_limiter_variant", "dgm_set_limiter_schedule",
                  "dgm_get_limiter_schedule", "dgm_cell_fields", "dgm_set_edge_variant", "dgm_get_edge_variant",
                  "dgm_instance_replace", "dgm_instance_capacity", "dgm_enqueue_diagnostics",
-                 "dgm_collected_diagnostics"):
+                 "dgm_collected_diagnostics", "dgm_set_viscous", "dgm_get_viscous"):
         getattr(L, name).restype = ctypes.c_int32
     _lib = L
     return L

@@ -320,6 +320,14 @@ class DubinerBasis:
                     for c in range(o + 1):
                         a = o - c
                         self.dphis_cell_gps[i, b, key_index(a, c)] = _ref_deriv(b, a, c, xi, eta)
+        # compute_dphi_edge, basis_function.rs:152-193: the first derivatives (d/dxi, d/deta)
+        self.dphis_edge_gps = np.zeros((3, ng, nb, 2))
+        for e in range(3):
+            for i in range(ng):
+                xi, eta = float(g.edge_points[e, i, 0]), float(g.edge_points[e, i, 1])
+                for b in range(nb):
+                    self.dphis_edge_gps[e, i, b, 0] = _ref_deriv(b, 1, 0, xi, eta)
+                    self.dphis_edge_gps[e, i, b, 1] = _ref_deriv(b, 0, 1, xi, eta)
         # compute_mass_mat, basis_function.rs:194-203
         for b in range(nb):
             acc = 0.0

@@ -19,6 +19,7 @@
 #include "dgm_device.cuh"
 #include "dgm_mixed.cuh"
 #include "dgm_tc.cuh"
+#include "dgm_viscous.cuh"
 
 using dgm::Control;
 using dgm::InstCtl;
@@ -54,6 +55,10 @@ struct dgm_ctx {
   double hcr = 1.4;
   std::vector<HostInst> inst;
   std::vector<unsigned char> kparams;  // host image of KParams<P, T>
+  // Navier-Stokes residual (dgm_set_viscous): host image of NsParams<P>, the global lifts
+  int viscous = 0;
+  std::vector<unsigned char> nsparams;
+  double* ns_lift = nullptr;
   std::vector<double> proj_phi, proj_w, proj_mass;  // FP64 tables of the initial projection
   // device buffers (state arrays are of the storage type)
   void *U = nullptr, *U1 = nullptr, *U2 = nullptr, *R = nullptr, *F = nullptr;
@@ -193,6 +198,11 @@ KParams<P, T>& kp_of(dgm_ctx* c) {
   return *reinterpret_cast<KParams<P, T>*>(c->kparams.data());
 }
 
+template <int P>
+dgm::NsParams<P>& ns_of(dgm_ctx* c) {
+  return *reinterpret_cast<dgm::NsParams<P>*>(c->nsparams.data());
+}
+
 // ---------------------------------------------------------------------------------------------
 // Kernel launch helpers, one instantiation per (order, storage type).
 // ---------------------------------------------------------------------------------------------
@@ -204,7 +214,25 @@ struct Ops {
   static St* S(void* p) { return static_cast<St*>(p); }
   static T* Fx(void* p) { return static_cast<T*>(p); }
 
+  // The viscous residual's lift and edge passes (FP64 contexts only: dgm_set_viscous checks).
+  static int ns_edge(dgm_ctx* c, const St* U) {
+    if constexpr (std::is_same<T, double>::value && std::is_same<St, double>::value) {
+      const int64_t nt = c->ne * NEQ;
+      dgm::k_ns_lift<P><<<(int)std::max<int64_t>(1, (nt + 255) / 256), 256, 0, c->stream>>>(kp_of<P, T>(c),
+                                                                                           ns_of<P>(c), U);
+      CK(cudaGetLastError());
+      const int64_t np = (c->n_int + c->n_bnd) * V::NG;
+      dgm::k_edge_flux_ns<P><<<(int)std::max<int64_t>(1, (np + 127) / 128), 128, 0, c->stream>>>(
+          kp_of<P, T>(c), ns_of<P>(c), U, Fx(c->F));
+      CK(cudaGetLastError());
+      return DGM_OK;
+    } else {
+      return DGM_BAD_ARG;
+    }
+  }
+
   static int edge_flux(dgm_ctx* c, const St* U) {
+    if (c->viscous) return ns_edge(c, U);
     const int threads = c->edge_threads;
     if (c->edge_pair == 2) {  // a warp covers 32 / NG slots per iteration; fixed 128-thread blocks
       constexpr int spw = 32 / V::NG, tpb = dgm::kEdgeStagedThreads;
@@ -250,6 +278,16 @@ struct Ops {
 
   template <int MODE>
   static int element(dgm_ctx* c, const St* Uin, const St* Ubase, St* Uout, const St* Rin, St* Rout) {
+    if constexpr (std::is_same<T, double>::value && std::is_same<St, double>::value) {
+      if (c->viscous) {  // the element pass with the viscous volume term
+        const int threads = c->elem_threads, per_block = threads / 4;
+        const int blocks = (int)std::max<int64_t>(1, (c->ne + per_block - 1) / per_block);
+        dgm::k_element_ns<P, MODE><<<blocks, threads, 0, c->stream>>>(kp_of<P, T>(c), ns_of<P>(c), Uin, Ubase,
+                                                                      Fx(c->F), Uout, Rin, Rout);
+        CK(cudaGetLastError());
+        return DGM_OK;
+      }
+    }
     if constexpr (std::is_same<T, float>::value && std::is_same<St, float>::value) {
       if (c->tc_split == 1) return element_tc<MODE, 1>(c, Uin, Ubase, Uout, Rin, Rout);
       if (c->tc_split == 3) return element_tc<MODE, 3>(c, Uin, Ubase, Uout, Rin, Rout);
@@ -461,6 +499,26 @@ struct Ops {
 
   static int set_mesh(dgm_ctx* c, const MeshDev& md) {
     kp_of<P, T>(c).m = md;
+    return DGM_OK;
+  }
+
+  // NsParams<P> from the reference-space edge derivative table [3][NG][NB][2] and the flow
+  // parameters; the global-lift array is allocated once.
+  static int set_viscous(dgm_ctx* c, double prandtl_number, double gas_constant, const double* dphi_edge) {
+    c->nsparams.assign(sizeof(dgm::NsParams<P>), 0);
+    auto& ns = ns_of<P>(c);
+    for (int k = 0; k < 3; ++k)
+      for (int g = 0; g < V::NG; ++g)
+        for (int b = 0; b < V::NB; ++b)
+          for (int d = 0; d < 2; ++d) ns.dphi_edge[k][g][b][d] = dphi_edge[((k * V::NG + g) * V::NB + b) * 2 + d];
+    for (int b = 0; b < V::NB; ++b) ns.mass[b] = c->proj_mass[b];
+    ns.hp = c->hcr / prandtl_number;
+    ns.rgas = gas_constant;
+    if (!c->ns_lift) {
+      const int st = dev_alloc(c, &c->ns_lift, (size_t)c->ld * 2 * NEQ * V::NB);
+      if (st) return st;
+    }
+    ns.lift = c->ns_lift;
     return DGM_OK;
   }
 };
@@ -1861,6 +1919,27 @@ int32_t dgm_set_edge_variant(dgm_ctx* c, int32_t pair) {
 
 int32_t dgm_get_edge_variant(dgm_ctx* c) { return c ? c->edge_pair : -1; }
 
+int32_t dgm_set_viscous(dgm_ctx* c, int32_t enable, double prandtl_number, double gas_constant,
+                        const double* dphi_edge_ref) {
+  if (!c || c->mixed || (enable != 0 && enable != 1)) return DGM_BAD_ARG;
+  if (enable && (c->prec_mode != 0 || !dphi_edge_ref || !(prandtl_number > 0.0) || !(gas_constant > 0.0) ||
+                 !std::isfinite(prandtl_number) || !std::isfinite(gas_constant)))
+    return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  CK(cudaStreamSynchronize(c->stream));
+  if (enable) {
+    const int st = dispatch(c, [&](auto ops) {
+      return decltype(ops)::set_viscous(c, prandtl_number, gas_constant, dphi_edge_ref);
+    });
+    if (st) return st;
+  }
+  c->viscous = enable;
+  reset_graphs(c);
+  return DGM_OK;
+}
+
+int32_t dgm_get_viscous(dgm_ctx* c) { return c ? c->viscous : -1; }
+
 int32_t dgm_get_limiter_variant(dgm_ctx* c, int32_t* staged, double* tuned_us) {
   if (!c) return DGM_BAD_ARG;
   if (staged) *staged = c->lim_staged;
@@ -2005,7 +2084,7 @@ int32_t dgm_phase_launches_per_step(dgm_ctx* c, int32_t phase) {
 int32_t dgm_launches_per_step(dgm_ctx* c) {
   if (!c) return 0;
   return 1 /* step head: loop condition + time step */ + 1 /* step end */ +
-         3 * (2 + (c->limiter ? 2 /* detection, waves */ : 0));
+         3 * (2 + (c->viscous ? 1 /* global lifts */ : 0) + (c->limiter ? 2 /* detection, waves */ : 0));
 }
 
 int64_t dgm_error_location(dgm_ctx* c) {

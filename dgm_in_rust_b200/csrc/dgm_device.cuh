@@ -496,19 +496,12 @@ __device__ __forceinline__ double phys_deriv(const double (&r)[NK], double xx, d
 // [0, p nx, p ny, 0] (boundary_condition.rs:31-47); far field: characteristic upwinding between
 // the interior trace and the patch's free stream, then the physical normal flux of the blended
 // state (boundary_condition.rs:48-94).  (nx, ny) is the element's outward normal.
+// The far-field boundary state (boundary_condition.rs:64-73): the characteristic variables of the
+// interior trace lv where the wave leaves the domain (eigenvalue >= 0), of the free stream bq
+// (conserved) where it enters, mapped back to conserved variables.
 template <typename T>
-__device__ __forceinline__ void boundary_flux(const T lv[4], int info, T nx, T ny, const MeshDev& m, const Gas& gas,
-                                              T out[4]) {
+__device__ __forceinline__ void far_field_state(const T lv[4], T nx, T ny, const double4 bq, const Gas& gas, T q[4]) {
   const T gm1 = T(gas.gm1);
-  if (((info >> 2) & 1) == 0) {
-    const T pressure = gm1 * (lv[3] - T(0.5) * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
-    out[0] = T(0);
-    out[1] = pressure * nx;
-    out[2] = pressure * ny;
-    out[3] = T(0);
-    return;
-  }
-  const double4 bq = m.patch_q[info >> 3];
   const T bc[4] = {T(bq.x), T(bq.y), T(bq.z), T(bq.w)};
   const T u = lv[1] / lv[0];
   const T v = lv[2] / lv[0];
@@ -529,7 +522,6 @@ __device__ __forceinline__ void boundary_flux(const T lv[4], int info, T nx, T n
     }
     mix[i] = lam[i] >= T(0) ? alpha : beta;
   }
-  T q[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     T sum = T(0);
@@ -537,6 +529,22 @@ __device__ __forceinline__ void boundary_flux(const T lv[4], int info, T nx, T n
     for (int j = 0; j < 4; ++j) sum += Rm[i][j] * mix[j];
     q[i] = sum;
   }
+}
+
+template <typename T>
+__device__ __forceinline__ void boundary_flux(const T lv[4], int info, T nx, T ny, const MeshDev& m, const Gas& gas,
+                                              T out[4]) {
+  const T gm1 = T(gas.gm1);
+  if (((info >> 2) & 1) == 0) {
+    const T pressure = gm1 * (lv[3] - T(0.5) * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+    out[0] = T(0);
+    out[1] = pressure * nx;
+    out[2] = pressure * ny;
+    out[3] = T(0);
+    return;
+  }
+  T q[4];
+  far_field_state<T>(lv, nx, ny, m.patch_q[info >> 3], gas, q);
   const T un = q[1] / q[0];
   const T vv = q[2] / q[0];
   const T vn_new = un * nx + vv * ny;

@@ -340,6 +340,20 @@ class SpatialDisc:
             raise ValueError(f"edge form must be one of {EDGE_FORMS}")
         self._check(self._lib.dgm_set_edge_variant(self._ctx, EDGE_FORMS.index(form)), "set_edge_form")
 
+    def set_viscous(self, enable: bool = True, prandtl_number: float = 0.72, gas_constant: float = 287.0) -> None:
+        """Evaluate the Navier-Stokes residual (BR2 lifting) instead of the Euler one: the
+        reference's integrate_over_cell_ns / integrate_over_edges_ns / apply_bc_ns
+        (spatial_disc.rs:70-160,212-348, boundary_condition.rs:121-413), which its compute_residuals
+        keeps disabled (spatial_disc.rs:34-36).  FlowParameters::prandtl_number and gas_constant
+        (parameters.json).  FP64 contexts only."""
+        table = np.ascontiguousarray(self.basis.dphis_edge_gps, dtype=np.float64)
+        self._check(self._lib.dgm_set_viscous(self._ctx, 1 if enable else 0, float(prandtl_number),
+                                              float(gas_constant), _native.dptr(table)), "set_viscous")
+
+    @property
+    def viscous(self) -> bool:
+        return bool(self._lib.dgm_get_viscous(self._ctx) == 1)
+
     def set_limiter_detector(self, staged: bool) -> None:
         """Pick the limiter's KXRCF detector form: staged loads (fewer memory round trips, more
         registers) or compact; both give the same flags.  The autotuner picks one per context."""

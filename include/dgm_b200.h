@@ -257,6 +257,20 @@ int32_t dgm_autotune(dgm_ctx* ctx, int32_t repeats, double* best_us /* [2] */);
  * No counterpart in the reference. */
 int32_t dgm_set_edge_variant(dgm_ctx* ctx, int32_t pair);
 int32_t dgm_get_edge_variant(dgm_ctx* ctx);
+
+/* The Navier-Stokes residual (BR2 lifting) in place of the Euler one -- the reference's
+ * integrate_over_cell_ns / integrate_over_edges_ns / apply_bc_ns (src/spatial_disc.rs:70-160,
+ * 212-348, src/spatial_disc/boundary_condition.rs:121-413, src/spatial_disc/viscous.rs:6-64), which
+ * its compute_residuals keeps commented out (src/spatial_disc.rs:34-36) -- for every entry point
+ * that evaluates residuals (compute_residuals, rk3, time_march, advance).  FlowParameters::
+ * prandtl_number and gas_constant (parameters.json: 0.72, 287) and the reference-space first
+ * derivatives of the modes at the edge points, dphi_edge_ref[3][n_edge_gp][n_basis][2] (d/dxi,
+ * d/deta: the (1,0) and (0,1) keys of DubinerBasis::dphis_edge_gps, basis_function.rs:152-193).
+ * FP64 contexts only (precision 0), not mixed batches: DGM_BAD_ARG otherwise.  enable = 0 returns
+ * to the Euler residual.  Adds one launch per stage (the global lifts). */
+int32_t dgm_set_viscous(dgm_ctx* ctx, int32_t enable, double prandtl_number, double gas_constant,
+                        const double* dphi_edge_ref);
+int32_t dgm_get_viscous(dgm_ctx* ctx);
 /* The form of the limiter's detection launch (modified_kxrcf, weno.rs:7-85, on every element, one
  * lane each; same arithmetic in both): 0 compact (walks the faces in turn: fewer registers, more
  * lanes in flight), 1 staged (all loads of a round issued together: fewer memory round trips,

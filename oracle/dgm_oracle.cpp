@@ -335,6 +335,7 @@ struct Basis {
   std::vector<double> phi_cell;   // [nq][nb]          basis_function.rs:80-95
   std::vector<double> phi_edge;   // [3][ng][nb]       basis_function.rs:96-113
   std::vector<double> dphi_cell;  // [nq][nb][nkeys]   reference-space derivatives
+  std::vector<double> dphi_edge;  // [3][ng][nb][2]    d/dxi, d/deta at the edge points (basis_function.rs:152-193)
   std::vector<double> mass;       // [nb]              basis_function.rs:194-203
 };
 
@@ -374,6 +375,16 @@ void make_basis(int p, const Gauss& g, Basis& B) {
           B.dphi_cell[((size_t)i * nb + b) * B.nkeys + key_index(a, c)] = ref_deriv(b, a, c, xi, eta);
         }
   }
+  // compute_dphi_edge, basis_function.rs:152-193 (first derivatives, the keys the viscous terms use)
+  B.dphi_edge.assign((size_t)3 * ng * nb * 2, 0.0);
+  for (int e = 0; e < 3; ++e)
+    for (int i = 0; i < ng; ++i) {
+      const double xi = g.edge_pts[(e * ng + i) * 2], eta = g.edge_pts[(e * ng + i) * 2 + 1];
+      for (int b = 0; b < nb; ++b) {
+        B.dphi_edge[(((size_t)e * ng + i) * nb + b) * 2 + 0] = ref_deriv(b, 1, 0, xi, eta);
+        B.dphi_edge[(((size_t)e * ng + i) * nb + b) * 2 + 1] = ref_deriv(b, 0, 1, xi, eta);
+      }
+    }
   // compute_mass_mat, basis_function.rs:194-203
   for (int b = 0; b < nb; ++b)
     for (int i = 0; i < nq; ++i) {
@@ -869,6 +880,12 @@ struct Solver {
   FreeStream init{};
   int threads = 1;
   int limiter = 1;  // 1 = reference sequential in-place WENO, 0 = off
+  // Navier-Stokes (BR2) residual in place of the Euler one: the reference's integrate_over_cell_ns,
+  // integrate_over_edges_ns and apply_bc_ns (spatial_disc.rs:70-160,212-348,
+  // boundary_condition.rs:121-413), which it keeps disabled (spatial_disc.rs:34-36)
+  int viscous = 0;
+  double prandtl_number = 0.72;  // parameters.json
+  double gas_constant = 287.0;
   // time_march state (temporal_disc.rs:8-19)
   double current_time = 0.0;
   int64_t current_step = 0;
@@ -959,8 +976,11 @@ void boundary_trace(const Solver& s, int64_t d, const double* U, int g, double* 
   }
 }
 
+int compute_residuals_ns(Solver& s, double* R, const double* U);
+
 // compute_residuals, spatial_disc.rs:27-39
 int compute_residuals(Solver& s, double* R, const double* U) {
+  if (s.viscous) return compute_residuals_ns(s, R, U);
   const int nb = s.B.nb, ng = s.g.ng;
   // integrate_over_cell_euler (spatial_disc.rs:40-69)
   int st = fold_reduce(s, s.m.internal_elements, R, [&](int64_t e, double* acc) {
@@ -1070,6 +1090,415 @@ int compute_residuals(Solver& s, double* R, const double* U) {
   });
   if (st) return st;
   // divide_residual_by_mass_mat_diag, spatial_disc.rs:349-357
+  const int64_t ne = s.m.ne;
+  for (int64_t e = 0; e < ne; ++e)
+    for (int v = 0; v < NEQ; ++v)
+      for (int b = 0; b < nb; ++b) R[(e * NEQ + v) * nb + b] /= s.B.mass[b] * 0.5 * s.m.e_jac[e];
+  return ORC_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Navier-Stokes terms (BR2 lifting), kept disabled by the reference (spatial_disc.rs:34-36).
+// ------------------------------------------------------------------------------------------
+
+// compute_dynamic_viscosity, viscous.rs:6-12 (Sutherland's law)
+double dynamic_viscosity(double temperature) {
+  const double mu_ref = 1.716e-5;
+  const double sutherland_constant = 110.4;
+  const double t_ref = 273.15;
+  return mu_ref * std::pow(temperature / t_ref, 1.5) * (t_ref + sutherland_constant) /
+         (temperature + sutherland_constant);
+}
+
+// viscous_jacobian, viscous.rs:13-64: G[0..3] = g11, g12, g21, g22, each [4][4], times mu / rho.
+void viscous_jacobian(const Solver& s, const double* q, double mu, double G[4][4][4]) {
+  const double hcr = s.hcr, pr = s.prandtl_number;
+  const double u = q[1] / q[0];
+  const double v = q[2] / q[0];
+  const double e = q[3] / q[0];
+  for (int m = 0; m < 4; ++m)
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) G[m][i][j] = 0.0;
+  double(&g11)[4][4] = G[0];
+  double(&g12)[4][4] = G[1];
+  double(&g21)[4][4] = G[2];
+  double(&g22)[4][4] = G[3];
+  g11[1][0] = -4.0 / 3.0 * u;
+  g11[1][1] = 4.0 / 3.0;
+  g11[2][0] = -v;
+  g11[2][2] = 1.0;
+  g11[3][0] = -(4.0 / 3.0 * std::pow(u, 2.0) + std::pow(v, 2.0) + hcr / pr * (e - std::pow(u, 2.0) - std::pow(v, 2.0)));
+  g11[3][1] = (4.0 / 3.0 - hcr / pr) * u;
+  g11[3][2] = (1.0 - hcr / pr) * v;
+  g11[3][3] = hcr / pr;
+  g12[1][0] = 2.0 / 3.0 * v;
+  g12[1][2] = -2.0 / 3.0;
+  g12[2][0] = -u;
+  g12[2][1] = 1.0;
+  g12[3][0] = -1.0 / 3.0 * u * v;
+  g12[3][1] = v;
+  g12[3][2] = -2.0 / 3.0 * u;
+  g21[1][0] = -v;
+  g21[1][2] = 1.0;
+  g21[2][0] = 2.0 / 3.0 * u;
+  g21[2][1] = -2.0 / 3.0;
+  g21[3][0] = -1.0 / 3.0 * u * v;
+  g21[3][1] = -2.0 / 3.0 * v;
+  g21[3][2] = u;
+  g22[1][0] = -u;
+  g22[1][1] = 1.0;
+  g22[2][0] = -4.0 / 3.0 * v;
+  g22[2][2] = 4.0 / 3.0;
+  g22[3][0] = -(std::pow(u, 2.0) + 4.0 / 3.0 * std::pow(v, 2.0) + hcr / pr * (e - std::pow(u, 2.0) - std::pow(v, 2.0)));
+  g22[3][1] = (1.0 - hcr / pr) * u;
+  g22[3][2] = (4.0 / 3.0 - hcr / pr) * v;
+  g22[3][3] = hcr / pr;
+  const double scale = mu / q[0];  // g11 *= mu / q[0], ... (viscous.rs:58-61)
+  for (int m = 0; m < 4; ++m)
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) G[m][i][j] *= scale;
+}
+
+// The viscosity of a state (the `viscosity` blocks of spatial_disc.rs:125-129 and the other
+// NS sites): pressure, T = p / (R rho), Sutherland.
+double state_viscosity(const Solver& s, const double* q) {
+  const double pressure = (s.hcr - 1.0) * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+  const double temperature = pressure / (s.gas_constant * q[0]);
+  return dynamic_viscosity(temperature);
+}
+
+// Physical first derivative of mode b at point g of local edge k of an element (the
+// dphis_edge_gps of mesh.rs:115-127), kk = 0: d/dx, 1: d/dy.
+double phys_deriv_edge(const Basis& B, int ng, const double* dinv, int k, int g, int b, int kk) {
+  const double* r = &B.dphi_edge[(((size_t)k * ng + g) * B.nb + b) * 2];
+  return kk == 0 ? dinv[0] * r[0] + dinv[2] * r[1] : dinv[1] * r[0] + dinv[3] * r[1];
+}
+
+// fv, gv of spatial_disc.rs:131-146 and the other NS sites: G times (gradient + lift), with the
+// gradient of dofs and the lift evaluated by the callbacks for (ivar, ibasis).
+template <class DX, class DY, class LX, class LY>
+void viscous_flux(const double G[4][4][4], const double* dofs, int nb, DX dphi_dx, DY dphi_dy, LX lift_x, LY lift_y,
+                  double* fv, double* gv) {
+  for (int i = 0; i < 4; ++i) fv[i] = gv[i] = 0.0;
+  for (int iflux = 0; iflux < NEQ; ++iflux)
+    for (int ivar = 0; ivar < NEQ; ++ivar) {
+      double dsol_dx = 0.0, dsol_dy = 0.0, lx = 0.0, ly = 0.0;
+      for (int b = 0; b < nb; ++b) {
+        dsol_dx += dofs[ivar * nb + b] * dphi_dx(b);
+        dsol_dy += dofs[ivar * nb + b] * dphi_dy(b);
+        lx += lift_x(ivar, b);
+        ly += lift_y(ivar, b);
+      }
+      fv[iflux] += G[0][iflux][ivar] * (dsol_dx + lx) + G[1][iflux][ivar] * (dsol_dy + ly);
+      gv[iflux] += G[2][iflux][ivar] * (dsol_dx + lx) + G[3][iflux][ivar] * (dsol_dy + ly);
+    }
+}
+
+// The neighbour an element's lifting operator takes across its local edge k (spatial_disc.rs:86-93,
+// boundary_condition.rs:145-152), with the reference's test: the edge's first in-cell index equal
+// to k selects the edge's second element and the edge normal, else its first element and the
+// negated normal -- whichever side e is on.
+void lift_neighbour(const Solver& s, int64_t d, int k, int& iric, int64_t& irelem, double& nx, double& ny) {
+  if (s.m.d_icell[2 * d] == k) {
+    iric = (int)s.m.d_icell[2 * d + 1];
+    irelem = s.m.d_elem[2 * d + 1];
+    nx = s.m.d_normal[2 * d];
+    ny = s.m.d_normal[2 * d + 1];
+  } else {
+    iric = (int)s.m.d_icell[2 * d];
+    irelem = s.m.d_elem[2 * d];
+    nx = -s.m.d_normal[2 * d];
+    ny = -s.m.d_normal[2 * d + 1];
+  }
+}
+
+// The jump terms of variable ivar, mode ibasis across local edge k into lift[ivar][ibasis]
+// (spatial_disc.rs:95-108, boundary_condition.rs:156-167).
+void lift_edge_terms(const Solver& s, int64_t e, int k, const double* U, int ivar, int ibasis, double* lx, double* ly) {
+  const int nb = s.B.nb, ng = s.g.ng;
+  const int64_t d = s.m.e_edge[3 * e + k];
+  int iric;
+  int64_t irelem;
+  double nx, ny;
+  lift_neighbour(s, d, k, iric, irelem, nx, ny);
+  for (int g = 0; g < ng; ++g) {
+    double left_value = 0.0, right_value = 0.0;
+    for (int b = 0; b < nb; ++b) {
+      left_value += U[(e * NEQ + ivar) * nb + b] * s.B.phi_edge[(k * ng + g) * nb + b];
+      right_value += U[(irelem * NEQ + ivar) * nb + b] * s.B.phi_edge[(iric * ng + (ng - 1 - g)) * nb + b];
+    }
+    const double jump_x = (left_value - right_value) * nx;
+    const double jump_y = (left_value - right_value) * ny;
+    *lx -= 0.5 * jump_x * s.B.phi_edge[(k * ng + g) * nb + ibasis] * s.g.edge_w[g] * 0.5 * s.m.d_jac[d];
+    *ly -= 0.5 * jump_y * s.B.phi_edge[(k * ng + g) * nb + ibasis] * s.g.edge_w[g] * 0.5 * s.m.d_jac[d];
+  }
+}
+
+// The cell term with the element's global lift (spatial_disc.rs:114-155, boundary_condition.rs:373-407).
+void ns_volume(const Solver& s, int64_t e, const double* U, const double* glx, const double* gly, double* acc) {
+  const int nb = s.B.nb, nq = s.g.nq;
+  const double* dinv = &s.m.e_dinv[4 * e];
+  const double J = s.m.e_jac[e];
+  for (int q = 0; q < nq; ++q) {
+    double sol[4] = {0, 0, 0, 0};
+    for (int v = 0; v < NEQ; ++v)
+      for (int b = 0; b < nb; ++b) sol[v] += U[(e * NEQ + v) * nb + b] * s.B.phi_cell[q * nb + b];
+    double f[4], gg[4];
+    euler_flux(sol, s.hcr, f, gg);
+    double G[4][4][4];
+    viscous_jacobian(s, sol, state_viscosity(s, sol), G);
+    double fv[4], gv[4];
+    viscous_flux(
+        G, &U[e * NEQ * nb], nb, [&](int b) { return phys_deriv(s.B, dinv, q, b, 0); },
+        [&](int b) { return phys_deriv(s.B, dinv, q, b, 1); },
+        [&](int ivar, int b) { return glx[ivar * nb + b] * s.B.phi_cell[q * nb + b]; },
+        [&](int ivar, int b) { return gly[ivar * nb + b] * s.B.phi_cell[q * nb + b]; }, fv, gv);
+    for (int v = 0; v < NEQ; ++v)
+      for (int b = 0; b < nb; ++b) {
+        const double dx = phys_deriv(s.B, dinv, q, b, 0);
+        const double dy = phys_deriv(s.B, dinv, q, b, 1);
+        acc[(e * NEQ + v) * nb + b] += ((f[v] - fv[v]) * dx + (gg[v] - gv[v]) * dy) * s.g.cell_w[q] * 0.5 * J;
+      }
+  }
+}
+
+// compute_residuals with the Navier-Stokes terms (spatial_disc.rs:27-39 with the NS calls of
+// :34-36 in place of the Euler ones).
+int compute_residuals_ns(Solver& s, double* R, const double* U) {
+  const int nb = s.B.nb, ng = s.g.ng;
+  // integrate_over_cell_ns, spatial_disc.rs:70-160
+  int st = fold_reduce(s, s.m.internal_elements, R, [&](int64_t e, double* acc) {
+    std::vector<double> glx(NEQ * nb, 0.0), gly(NEQ * nb, 0.0);
+    for (int ivar = 0; ivar < NEQ; ++ivar)
+      for (int ibasis = 0; ibasis < nb; ++ibasis) {
+        for (int k = 0; k < 3; ++k) lift_edge_terms(s, e, k, U, ivar, ibasis, &glx[ivar * nb + ibasis], &gly[ivar * nb + ibasis]);
+        glx[ivar * nb + ibasis] /= s.B.mass[ibasis] * 0.5 * s.m.e_jac[e];
+        gly[ivar * nb + ibasis] /= s.B.mass[ibasis] * 0.5 * s.m.e_jac[e];
+      }
+    ns_volume(s, e, U, glx.data(), gly.data(), acc);
+    return (int)ORC_OK;
+  });
+  if (st) return st;
+  // integrate_over_edges_ns, spatial_disc.rs:212-348
+  st = fold_reduce(s, s.m.internal_edges, R, [&](int64_t d, double* acc) {
+    const int ilic = (int)s.m.d_icell[2 * d], iric = (int)s.m.d_icell[2 * d + 1];
+    const int64_t L = s.m.d_elem[2 * d], Rr = s.m.d_elem[2 * d + 1];
+    const double nx = s.m.d_normal[2 * d], ny = s.m.d_normal[2 * d + 1];
+    const double jd = s.m.d_jac[d];
+    const double* ldofs = &U[L * NEQ * nb];
+    const double* rdofs = &U[Rr * NEQ * nb];
+    std::vector<double> llx(NEQ * nb, 0.0), lly(NEQ * nb, 0.0), rlx(NEQ * nb, 0.0), rly(NEQ * nb, 0.0);
+    for (int ivar = 0; ivar < NEQ; ++ivar)
+      for (int ibasis = 0; ibasis < nb; ++ibasis) {
+        const int i = ivar * nb + ibasis;
+        for (int g = 0; g < ng; ++g) {
+          double left_value = 0.0, right_value = 0.0;
+          for (int b = 0; b < nb; ++b) {
+            left_value += ldofs[ivar * nb + b] * s.B.phi_edge[(ilic * ng + g) * nb + b];
+            right_value += rdofs[ivar * nb + b] * s.B.phi_edge[(iric * ng + (ng - 1 - g)) * nb + b];
+          }
+          const double jump_x = (left_value - right_value) * nx;
+          const double jump_y = (left_value - right_value) * ny;
+          llx[i] -= 0.5 * jump_x * s.B.phi_edge[(ilic * ng + g) * nb + ibasis] * s.g.edge_w[g] * 0.5 * jd;
+          lly[i] -= 0.5 * jump_y * s.B.phi_edge[(ilic * ng + g) * nb + ibasis] * s.g.edge_w[g] * 0.5 * jd;
+          rlx[i] += 0.5 * jump_x * s.B.phi_edge[(iric * ng + (ng - 1 - g)) * nb + ibasis] * s.g.edge_w[ng - 1 - g] * 0.5 * jd;
+          rly[i] += 0.5 * jump_y * s.B.phi_edge[(iric * ng + (ng - 1 - g)) * nb + ibasis] * s.g.edge_w[ng - 1 - g] * 0.5 * jd;
+        }
+        llx[i] /= s.B.mass[ibasis] * 0.5 * s.m.e_jac[L];
+        lly[i] /= s.B.mass[ibasis] * 0.5 * s.m.e_jac[L];
+        rlx[i] /= s.B.mass[ibasis] * 0.5 * s.m.e_jac[Rr];
+        rly[i] /= s.B.mass[ibasis] * 0.5 * s.m.e_jac[Rr];
+      }
+    const double* ldinv = &s.m.e_dinv[4 * L];
+    const double* rdinv = &s.m.e_dinv[4 * Rr];
+    for (int g = 0; g < ng; ++g) {
+      const int gr = ng - 1 - g;
+      double lv[4] = {0, 0, 0, 0}, rv[4] = {0, 0, 0, 0};
+      for (int v = 0; v < NEQ; ++v)
+        for (int b = 0; b < nb; ++b) {
+          lv[v] += ldofs[v * nb + b] * s.B.phi_edge[(ilic * ng + g) * nb + b];
+          rv[v] += rdofs[v * nb + b] * s.B.phi_edge[(iric * ng + gr) * nb + b];
+        }
+      double num_flux[4];
+      const int hs = hllc(lv, rv, nx, ny, s.hcr, num_flux);
+      if (hs != ORC_OK) return hs;
+      double num_visc[4] = {0, 0, 0, 0};
+      double G[4][4][4], fv[4], gv[4];
+      // left contribution (spatial_disc.rs:281-307): lifts scaled by 3
+      viscous_jacobian(s, lv, state_viscosity(s, lv), G);
+      viscous_flux(
+          G, ldofs, nb, [&](int b) { return phys_deriv_edge(s.B, ng, ldinv, ilic, g, b, 0); },
+          [&](int b) { return phys_deriv_edge(s.B, ng, ldinv, ilic, g, b, 1); },
+          [&](int ivar, int b) { return 3.0 * llx[ivar * nb + b] * s.B.phi_edge[(ilic * ng + g) * nb + b]; },
+          [&](int ivar, int b) { return 3.0 * lly[ivar * nb + b] * s.B.phi_edge[(ilic * ng + g) * nb + b]; }, fv, gv);
+      for (int v = 0; v < NEQ; ++v) num_visc[v] = num_visc[v] + 0.5 * (nx * fv[v] + ny * gv[v]);
+      // right contribution (spatial_disc.rs:309-335): lifts not scaled
+      viscous_jacobian(s, rv, state_viscosity(s, rv), G);
+      viscous_flux(
+          G, rdofs, nb, [&](int b) { return phys_deriv_edge(s.B, ng, rdinv, iric, gr, b, 0); },
+          [&](int b) { return phys_deriv_edge(s.B, ng, rdinv, iric, gr, b, 1); },
+          [&](int ivar, int b) { return rlx[ivar * nb + b] * s.B.phi_edge[(iric * ng + gr) * nb + b]; },
+          [&](int ivar, int b) { return rly[ivar * nb + b] * s.B.phi_edge[(iric * ng + gr) * nb + b]; }, fv, gv);
+      for (int v = 0; v < NEQ; ++v) num_visc[v] = num_visc[v] + 0.5 * (nx * fv[v] + ny * gv[v]);
+      for (int v = 0; v < NEQ; ++v)
+        for (int b = 0; b < nb; ++b) {
+          acc[(L * NEQ + v) * nb + b] -=
+              s.g.edge_w[g] * (num_flux[v] - num_visc[v]) * s.B.phi_edge[(ilic * ng + g) * nb + b] * 0.5 * jd;
+          acc[(Rr * NEQ + v) * nb + b] +=
+              s.g.edge_w[gr] * (num_flux[v] - num_visc[v]) * s.B.phi_edge[(iric * ng + gr) * nb + b] * 0.5 * jd;
+        }
+    }
+    return (int)ORC_OK;
+  });
+  if (st) return st;
+  // apply_bc_ns, boundary_condition.rs:121-413
+  st = fold_reduce(s, s.m.boundary_elements, R, [&](int64_t e, double* acc) {
+    std::vector<double> glx(NEQ * nb, 0.0), gly(NEQ * nb, 0.0);
+    const double J = s.m.e_jac[e];
+    const double* dofs = &U[e * NEQ * nb];
+    const double* dinv = &s.m.e_dinv[4 * e];
+    for (int k = 0; k < 3; ++k) {
+      const int64_t d = s.m.e_edge[3 * e + k];
+      const int64_t patch = s.m.d_patch[d];
+      if (patch == -1) {  // boundary_condition.rs:144-168
+        for (int ivar = 0; ivar < NEQ; ++ivar)
+          for (int ibasis = 0; ibasis < nb; ++ibasis)
+            lift_edge_terms(s, e, k, U, ivar, ibasis, &glx[ivar * nb + ibasis], &gly[ivar * nb + ibasis]);
+        continue;
+      }
+      double nx, ny;
+      if (s.m.e_vert[3 * e + k] == s.m.d_vert[2 * d]) {
+        nx = s.m.d_normal[2 * d];
+        ny = s.m.d_normal[2 * d + 1];
+      } else {
+        nx = -s.m.d_normal[2 * d];
+        ny = -s.m.d_normal[2 * d + 1];
+      }
+      const double jd = s.m.d_jac[d];
+      std::vector<double> llx(NEQ * nb, 0.0), lly(NEQ * nb, 0.0);
+      if (s.m.p_type[patch] == WALL) {  // boundary_condition.rs:181-246
+        for (int g = 0; g < ng; ++g) {
+          double lv[4];
+          boundary_trace(s, d, U, g, lv);
+          const double pressure = (s.hcr - 1.0) * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+          const double boundary_energy = pressure / (s.hcr - 1.0);
+          const double jx[4] = {0.0, lv[1] * nx, lv[2] * nx, (lv[3] - boundary_energy) * nx};
+          const double jy[4] = {0.0, lv[1] * ny, lv[2] * ny, (lv[3] - boundary_energy) * ny};
+          // the cell table and cell weights at index g, as the reference writes them (:193-200)
+          for (int b = 0; b < nb; ++b)
+            for (int v = 1; v < NEQ; ++v) {
+              llx[v * nb + b] -= 0.5 * jx[v] * s.B.phi_cell[g * nb + b] * s.g.cell_w[g] * 0.5 * J;
+              lly[v * nb + b] -= 0.5 * jy[v] * s.B.phi_cell[g * nb + b] * s.g.cell_w[g] * 0.5 * J;
+            }
+        }
+        for (int i = 0; i < NEQ * nb; ++i) {
+          glx[i] = glx[i] + llx[i];
+          gly[i] = gly[i] + lly[i];
+        }
+        for (int v = 1; v < NEQ; ++v)
+          for (int b = 0; b < nb; ++b) {
+            llx[v * nb + b] /= s.B.mass[b] * 0.5 * J;
+            lly[v * nb + b] /= s.B.mass[b] * 0.5 * J;
+          }
+        for (int g = 0; g < ng; ++g) {
+          double lv[4];
+          boundary_trace(s, d, U, g, lv);
+          const double pressure = (s.hcr - 1.0) * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+          const double inv[4] = {0.0, pressure * nx, pressure * ny, 0.0};
+          const double temperature = pressure / (s.gas_constant * lv[0]);
+          double G[4][4][4], fv[4], gv[4];
+          viscous_jacobian(s, lv, dynamic_viscosity(temperature), G);
+          viscous_flux(
+              G, dofs, nb, [&](int b) { return phys_deriv_edge(s.B, ng, dinv, k, g, b, 0); },
+              [&](int b) { return phys_deriv_edge(s.B, ng, dinv, k, g, b, 1); },
+              [&](int ivar, int b) { return 3.0 * llx[ivar * nb + b] * s.B.phi_edge[(k * ng + g) * nb + b]; },
+              [&](int ivar, int b) { return 3.0 * lly[ivar * nb + b] * s.B.phi_edge[(k * ng + g) * nb + b]; }, fv, gv);
+          for (int v = 0; v < NEQ; ++v) {
+            const double visc = nx * fv[v] + ny * gv[v];
+            for (int b = 0; b < nb; ++b)
+              acc[(e * NEQ + v) * nb + b] -= s.g.edge_w[g] * (inv[v] - visc) * s.B.phi_edge[(k * ng + g) * nb + b] * 0.5 * jd;
+          }
+        }
+      } else {  // far field, boundary_condition.rs:248-370
+        const double* bq = &s.m.p_q[4 * patch];
+        const double bc[4] = {bq[0], bq[0] * bq[1], bq[0] * bq[2],
+                              bq[3] / (s.hcr - 1.0) + 0.5 * bq[0] * (bq[1] * bq[1] + bq[2] * bq[2])};
+        std::vector<double> qn(ng * 4);
+        for (int g = 0; g < ng; ++g) {
+          double lv[4];
+          boundary_trace(s, d, U, g, lv);
+          const double u = lv[1] / lv[0];
+          const double v = lv[2] / lv[0];
+          const double p = (s.hcr - 1.0) * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+          const double c = std::sqrt(s.hcr * p / lv[0]);
+          const double vn = u * nx + v * ny;
+          double Lm[4][4], Rm[4][4];
+          eigenmatrix(lv, nx, ny, s.hcr, Lm, Rm);
+          const double lam[4] = {vn - c, vn, vn, vn + c};
+          double mix[4];
+          for (int i = 0; i < 4; ++i) {
+            double alpha = 0.0, beta = 0.0;
+            for (int j = 0; j < 4; ++j) {
+              alpha = alpha + Lm[i][j] * lv[j];
+              beta = beta + Lm[i][j] * bc[j];
+            }
+            mix[i] = lam[i] >= 0.0 ? alpha : beta;
+          }
+          double* q = &qn[g * 4];
+          for (int i = 0; i < 4; ++i) {
+            double sum = 0.0;
+            for (int j = 0; j < 4; ++j) sum = sum + Rm[i][j] * mix[j];
+            q[i] = sum;
+          }
+          for (int b = 0; b < nb; ++b)
+            for (int w = 0; w < NEQ; ++w) {
+              llx[w * nb + b] -= 0.5 * ((lv[w] - q[w]) * nx) * s.B.phi_edge[(k * ng + g) * nb + b] * s.g.edge_w[g] * 0.5 * jd;
+              lly[w * nb + b] -= 0.5 * ((lv[w] - q[w]) * ny) * s.B.phi_edge[(k * ng + g) * nb + b] * s.g.edge_w[g] * 0.5 * jd;
+            }
+        }
+        for (int i = 0; i < NEQ * nb; ++i) {
+          glx[i] = glx[i] + llx[i];
+          gly[i] = gly[i] + lly[i];
+        }
+        for (int w = 0; w < NEQ; ++w)
+          for (int b = 0; b < nb; ++b) {
+            llx[w * nb + b] /= s.B.mass[b] * 0.5 * J;
+            lly[w * nb + b] /= s.B.mass[b] * 0.5 * J;
+          }
+        for (int g = 0; g < ng; ++g) {
+          const double* q = &qn[g * 4];
+          const double u_new = q[1] / q[0];
+          const double v_new = q[2] / q[0];
+          const double vn_new = u_new * nx + v_new * ny;
+          const double p_new = (s.hcr - 1.0) * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+          const double h_new = q[3] + p_new;
+          const double inv[4] = {q[0] * vn_new, q[1] * vn_new + p_new * nx, q[2] * vn_new + p_new * ny,
+                                 h_new * vn_new};
+          double lv[4];
+          boundary_trace(s, d, U, g, lv);
+          double G[4][4][4], fv[4], gv[4];
+          viscous_jacobian(s, lv, state_viscosity(s, lv), G);
+          viscous_flux(
+              G, dofs, nb, [&](int b) { return phys_deriv_edge(s.B, ng, dinv, k, g, b, 0); },
+              [&](int b) { return phys_deriv_edge(s.B, ng, dinv, k, g, b, 1); },
+              [&](int ivar, int b) { return 3.0 * llx[ivar * nb + b] * s.B.phi_edge[(k * ng + g) * nb + b]; },
+              [&](int ivar, int b) { return 3.0 * lly[ivar * nb + b] * s.B.phi_edge[(k * ng + g) * nb + b]; }, fv, gv);
+          for (int v = 0; v < NEQ; ++v) {
+            const double visc = nx * fv[v] + ny * gv[v];
+            for (int b = 0; b < nb; ++b)
+              acc[(e * NEQ + v) * nb + b] -= s.g.edge_w[g] * (inv[v] - visc) * s.B.phi_edge[(k * ng + g) * nb + b] * 0.5 * jd;
+          }
+        }
+      }
+    }
+    for (int i = 0; i < NEQ * nb; ++i) {
+      glx[i] /= s.B.mass[i % nb] * 0.5 * J;
+      gly[i] /= s.B.mass[i % nb] * 0.5 * J;
+    }
+    ns_volume(s, e, U, glx.data(), gly.data(), acc);
+    return (int)ORC_OK;
+  });
+  if (st) return st;
   const int64_t ne = s.m.ne;
   for (int64_t e = 0; e < ne; ++e)
     for (int v = 0; v < NEQ; ++v)
@@ -1435,6 +1864,14 @@ void* orc_create_from_raw(const orc_raw_mesh* r, const orc_config* c, int32_t* s
 }
 
 void orc_destroy(void* h) { delete static_cast<Solver*>(h); }
+
+// The Navier-Stokes residual (the reference's disabled NS calls, spatial_disc.rs:34-36) on or off.
+void orc_set_viscous(void* h, int32_t enable, double prandtl_number, double gas_constant) {
+  auto* s = static_cast<Solver*>(h);
+  s->viscous = enable ? 1 : 0;
+  s->prandtl_number = prandtl_number;
+  s->gas_constant = gas_constant;
+}
 
 // sizes: ne, ned, nv, np, nb, nq, ng, n_internal_edges, n_internal_elements,
 // n_boundary_elements, nkeys, max_order

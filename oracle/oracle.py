@@ -97,6 +97,7 @@ def lib():
         L.orc_time_march.restype = ctypes.c_int32
         L.orc_reset_clock.argtypes = [vp]
         L.orc_set_threads.argtypes = [vp, ctypes.c_int32]
+        L.orc_set_viscous.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double]
         L.orc_hllc.argtypes = [P_D, P_D, ctypes.c_double, ctypes.c_double, ctypes.c_double, P_D]
         L.orc_hllc.restype = ctypes.c_int32
         L.orc_flux.argtypes = [P_D, ctypes.c_double, P_D, P_D]
@@ -270,3 +271,8 @@ class Oracle:
 
     def set_threads(self, n: int):
         self._L.orc_set_threads(self._h, int(n))
+
+    def set_viscous(self, enable: bool = True, prandtl_number: float = 0.72, gas_constant: float = 287.0):
+        """Navier-Stokes (BR2) residual in place of the Euler one: the reference's disabled
+        integrate_over_cell_ns / integrate_over_edges_ns / apply_bc_ns (spatial_disc.rs:34-36)."""
+        self._L.orc_set_viscous(self._h, 1 if enable else 0, float(prandtl_number), float(gas_constant))

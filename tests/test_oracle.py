@@ -241,3 +241,25 @@ def test_time_march_clamps_to_final_time():
     R = o.new_state()
     t, s = o.time_march(R, U)
     assert t == 2.5e-4 and 0 < s < 1000
+
+
+def test_viscous_residual_freestream_only_at_the_wall():
+    """The Navier-Stokes residual (the reference's disabled NS functions) of the uniform free
+    stream: zero jumps and gradients everywhere except the no-slip wall, so it equals the Euler
+    residual bit for bit on every element that does not touch the wall, and differs on those that
+    do (the wall's momentum jumps feed their lifts)."""
+    raw = naca0012_ogrid(16, 8)
+    o = orc.Oracle(raw=raw, order=2, freestream=FS)
+    U = o.initial_solution()
+    U[:, :, 0] = U[0, :, 0]  # exactly uniform: the projection's mode 0 and the higher modes
+    U[:, :, 1:] = 0.0        # carry element-to-element round-off
+    Re, Rn = o.new_state(), o.new_state()
+    o.compute_residuals(Re, U)
+    o.set_viscous(True, 0.72, 1e-3)
+    o.compute_residuals(Rn, U)
+    differs = np.nonzero(np.abs(Rn - Re).max(axis=(1, 2)) > 0.0)[0]
+    m = process_mesh(raw, freestream_quantity(FS[1], FS[0], FS[2], FS[3], 1.4), 1.4)
+    wall = [m.edge_elements[d, 0] for d in range(m.n_edges)
+            if m.edge_elements[d, 1] == -1 and m.patch_type[m.edge_patch[d]] == 0]
+    assert len(wall) == 16 and set(differs.tolist()) == set(int(e) for e in wall)
+    assert np.isfinite(Rn).all()

@@ -59,7 +59,9 @@ def parse():
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 p=3 measurement")
     ap.add_argument("--precision-steps", type=int, default=500)
     ap.add_argument("--precision-c2-steps", type=int, default=2000)
-    ap.add_argument("--only", choices=["batched", "precision", "serving"],
+    ap.add_argument("--no-viscous", action="store_true", help="skip the Navier-Stokes residual measurement")
+    ap.add_argument("--viscous-steps", type=int, default=200)
+    ap.add_argument("--only", choices=["batched", "precision", "serving", "viscous"],
                     help="run one secondary measurement alone and print its JSON (for profiling)")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-rates", default="20",
@@ -556,6 +558,56 @@ def run_precision(args, local):
 
 
 # ------------------------------------------------------------------------------------------
+# Navier-Stokes residual (the reference's disabled viscous terms) on the transonic workload
+# ------------------------------------------------------------------------------------------
+def run_viscous(args, local):
+    """The transonic workload's grid (256 x 128 O-grid, 65,536 triangles, p = 2, M 0.8, AoA 1.25
+    deg, limiter on, FP64) in the reference's dimensional free stream (rho 1, p 1e5: T = p / (R rho)
+    = 348 K, Sutherland viscosity 2.1e-5, Reynolds number ~1.4e7 per chord) with the Navier-Stokes
+    (BR2) residual at the reference's parameters (Prandtl 0.72, gas constant 287) against the Euler
+    residual: DOF-stage updates/s of each over --viscous-steps steps from the free stream (after 3
+    warm-up steps), CUDA events on the library stream, and the state difference the viscous terms
+    make."""
+    import torch
+    from dgm_in_rust_b200 import InitialSolution, build_solver, freestream_quantity, naca0012_ogrid, process_mesh
+    rho, p = 1.0, 1.0e5
+    mesh = process_mesh(naca0012_ogrid(NI, NJ), freestream_quantity(MACH, AOA, rho, p, HCR), HCR)
+    init = InitialSolution(rho, AOA, MACH, p)
+    dofs = mesh.n_elements * 4 * (ORDER + 1) * (ORDER + 2) // 2
+    K, W = args.viscous_steps, 3
+    out = {"workload": f"naca0012_ogrid_{NI}x{NJ}_p{ORDER}: {mesh.n_elements} triangles, M={MACH}, AoA={AOA}deg, "
+                       f"rho 1, p 1e5, limiter on, CFL {CFL}, FP64, free-stream start, {K} steps after {W}",
+           "prandtl_number": 0.72, "gas_constant": 287.0}
+    states = {}
+    for visc in (False, True):
+        s = build_solver(mesh, ORDER, HCR, CFL, 1.0e30, 10 ** 12, limiter=True, device=local)
+        sd, td = s.spatial_disc, s.temporal_disc
+        if visc:
+            sd.set_viscous(True, 0.72, 287.0)
+        td.set_initial_on_device(init)
+        td.advance(W)
+        td.synchronize()
+        st = torch.cuda.ExternalStream(sd._lib.dgm_stream(sd.ctx))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        td.advance(K)
+        b.record(st)
+        td.synchronize()
+        ms = a.elapsed_time(b)
+        U = sd.new_state()
+        td.download(U)
+        states[visc] = U
+        key = "navier_stokes" if visc else "euler"
+        out[key] = {"dof_stage_updates_per_s": dofs * 3 * K / (ms * 1e-3), "ms_per_step": ms / K,
+                    "launches_per_step": int(sd._lib.dgm_launches_per_step(sd.ctx))}
+        s.close()
+    out["ns_over_euler_time"] = out["navier_stokes"]["ms_per_step"] / out["euler"]["ms_per_step"]
+    diff = states[True] - states[False]
+    out["state_rel_l2_ns_vs_euler"] = float(np.linalg.norm(diff) / np.linalg.norm(states[False]))
+    return out
+
+
+# ------------------------------------------------------------------------------------------
 # Serving: Poisson request stream, continuous batching, vs FP64 one at a time
 # ------------------------------------------------------------------------------------------
 def run_serving(args, local):
@@ -773,6 +825,8 @@ def run_ours(args):
         line["precision"] = run_precision(args, local)
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving(args, local)
+    if world == 1 and not args.no_viscous:
+        line["viscous"] = run_viscous(args, local)
     # the metric's comparison and latencies, lifted from the secondary measurements
     if "batched" in line:
         b = line["batched"]
@@ -878,7 +932,8 @@ def main():
         from dgm_in_rust_b200.build import build
         build()
         torch.cuda.set_device(0)
-        fn = {"batched": run_batched, "precision": run_precision, "serving": run_serving}[args.only]
+        fn = {"batched": run_batched, "precision": run_precision, "serving": run_serving,
+              "viscous": run_viscous}[args.only]
         print(json.dumps({args.only: fn(args, 0)}), flush=True)
         return 0
     return run_ours(args)

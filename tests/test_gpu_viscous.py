@@ -119,3 +119,30 @@ def test_viscous_switch_and_refusals():
     assert m._lib.dgm_set_viscous(m.ctx, 1, PR, RGAS, table.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 7
     # DGM_BAD_ARG
     m.close()
+
+
+def test_viscous_reference_configuration():
+    """The reference's configured case (its airfoil.msh, p = 2, M 0.8, AoA 1.5 deg, rho 1, p 1e5,
+    CFL 0.1) with the NS terms at its parameters (Prandtl 0.72, gas constant 287: T = 348 K):
+    5 steps against the oracle at 1e-10, where the viscous terms move the state by ~3.5e-8."""
+    ref_fs = (1.5, 0.8, 1.0, 100000.0)
+    raw = airfoil_raw()
+    mesh = process_mesh(raw, freestream_quantity(ref_fs[1], ref_fs[0], ref_fs[2], ref_fs[3], 1.4), 1.4)
+    s = build_solver(mesh, 2, 1.4, 0.1, 1.0e30, 5)
+    o = Oracle(raw=raw, order=2, cfl=0.1, final_time=1.0e30, final_step=5, threads=4, freestream=ref_fs)
+    U0 = initial_state(mesh, s.basis, s.gauss_points, 1.4, InitialSolution(ref_fs[2], ref_fs[0], ref_fs[1], ref_fs[3]))
+    s.spatial_disc.set_viscous(True, 0.72, 287.0)
+    o.set_viscous(True, 0.72, 287.0)
+    Uo, Ro = U0.copy(), o.new_state()
+    to, so = o.time_march(Ro, Uo)
+    Ug, Rg = U0.copy(), s.spatial_disc.new_state()
+    s.temporal_disc.time_march(s.spatial_disc, Rg, Ug)
+    assert so == s.temporal_disc.current_step == 5
+    assert abs(s.temporal_disc.current_time - to) <= 1e-14 * to
+    assert rel_l2(Ug, Uo) < 1e-10
+    o.set_viscous(False)
+    Ue, Re = U0.copy(), o.new_state()
+    o.time_march(Re, Ue)
+    assert rel_l2(Uo, Ue) > 1e-8  # the viscous terms count
+    s.close()
+    o.close()

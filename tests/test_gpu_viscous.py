@@ -141,8 +141,9 @@ def test_viscous_reference_configuration():
     assert abs(s.temporal_disc.current_time - to) <= 1e-14 * to
     assert rel_l2(Ug, Uo) < 1e-10
     o.set_viscous(False)
+    o.reset_clock()
     Ue, Re = U0.copy(), o.new_state()
-    o.time_march(Re, Ue)
+    assert o.time_march(Re, Ue)[1] == 5
     assert rel_l2(Uo, Ue) > 1e-8  # the viscous terms count
     s.close()
     o.close()

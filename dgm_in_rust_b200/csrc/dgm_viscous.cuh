@@ -245,8 +245,8 @@ __global__ void __launch_bounds__(128) k_edge_flux_ns(const __grid_constant__ KP
     const double rxx = m.dinv[0 * ld + lr.y], rxy = m.dinv[1 * ld + lr.y], rex = m.dinv[2 * ld + lr.y],
                  rey = m.dinv[3 * ld + lr.y];
     double lv[4], rv[4], gxL[4], gyL[4], gxR[4], gyR[4];
-#pragma unroll
-    for (int w = 0; w < NEQ; ++w) {
+#pragma unroll 1
+    for (int w = 0; w < NEQ; ++w) {  // one variable at a time: keeps the two records out of registers
       // traces of variable w at every point of the edge (the jumps of the local lifts)
       double tl[NG], tr[NG];
 #pragma unroll

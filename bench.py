@@ -75,6 +75,8 @@ def parse():
                     help="run a fixed launch sequence for ncu (no timing, no autotuning): c2 = the workload "
                          "above, c3 = the 1024 x 512 p = 3 O-grid (M 0.7, AoA 2 deg), batch / batch_per_order = "
                          "the 256-instance batch as one mixed context / one context per order")
+    ap.add_argument("--profile-viscous", action="store_true",
+                    help="profile case with the Navier-Stokes residual (Prandtl 0.72, gas constant 287)")
     ap.add_argument("--precision", choices=["fp64", "fp32", "fp32_compute", "tf32", "tf32x3"], default="fp64")
     ap.add_argument("--launch", default="128,2368,128,1,0",
                     help="edge threads, edge blocks, element threads, staged limiter detector, edge pass form "
@@ -914,11 +916,14 @@ def run_profile_case(args):
     sd.set_limiter_detector(bool(staged))
     sd.set_limiter_schedule(bool(queue))
     sd.set_edge_form(("point", "pair", "staged", "point_r64")[pair])
+    if args.profile_viscous:
+        sd.set_viscous(True, 0.72, 287.0)
     td.set_initial_on_device(init)
     td.advance(args.warmup + args.steps)
     td.synchronize()
     troubled, _ = sd.limiter_stats()
-    print(json.dumps({"profile_case": args.profile_case, "precision": args.precision, "elements": mesh.n_elements,
+    print(json.dumps({"profile_case": args.profile_case, "precision": args.precision, "viscous": sd.viscous,
+                      "elements": mesh.n_elements,
                       "steps": td.current_step, "launch": sd.launch_config, "troubled_last_step": troubled}), flush=True)
     s.close()
     return 0

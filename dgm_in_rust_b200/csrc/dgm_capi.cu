@@ -221,8 +221,9 @@ struct Ops {
       dgm::k_ns_lift<P><<<(int)std::max<int64_t>(1, (nt + 255) / 256), 256, 0, c->stream>>>(kp_of<P, T>(c),
                                                                                            ns_of<P>(c), U);
       CK(cudaGetLastError());
-      const int64_t np = (c->n_int + c->n_bnd) * V::NG;
-      dgm::k_edge_flux_ns<P><<<(int)std::max<int64_t>(1, (np + 127) / 128), 128, 0, c->stream>>>(
+      const int64_t nt2 = (c->n_int + c->n_bnd) * 4;  // four lanes per edge slot
+      constexpr int tpb = dgm::kNsEdgeThreads;
+      dgm::k_edge_flux_ns<P><<<(int)std::max<int64_t>(1, (nt2 + tpb - 1) / tpb), tpb, 0, c->stream>>>(
           kp_of<P, T>(c), ns_of<P>(c), U, Fx(c->F));
       CK(cudaGetLastError());
       return DGM_OK;

@@ -8,10 +8,11 @@
 //                  the jumps across its faces (the neighbour chosen by the reference's in-cell index
 //                  test, spatial_disc.rs:86-93), plus on boundary faces the wall / far-field local
 //                  lifts (boundary_condition.rs:181-302) -- divided by the mass diagonal;
-//   k_edge_flux_ns a thread per (edge slot, Gauss point): HLLC minus the viscous flux of both
-//                  sides, each with its own gradient and its local lift (the left one scaled by 3,
-//                  the right one not, spatial_disc.rs:298-299,326-327), stored like the Euler
-//                  fluxes; boundary slots: the wall / far-field inviscid flux minus the viscous one;
+//   k_edge_flux_ns four lanes per edge slot (the lifts once per slot, a point per lane): HLLC minus
+//                  the viscous flux of both sides, each with its own gradient and its local lift
+//                  (the left one scaled by 3, the right one not, spatial_disc.rs:298-299,
+//                  326-327), stored like the Euler fluxes; boundary slots: the wall / far-field
+//                  inviscid flux minus the viscous one;
 //   k_element_ns   the Euler element pass with the volume term (F - Fv, G - Gv), the viscous
 //                  fluxes from the state's gradient plus the global lift at each cell point.
 //
@@ -206,7 +207,11 @@ __global__ void __launch_bounds__(256) k_ns_lift(const __grid_constant__ KParams
 }
 
 // ------------------------------------------------------------------------------------------
-// Edge pass: a thread per (edge slot, Gauss point).
+// Edge pass: four lanes per edge slot.  Lane w first evaluates, for variable w, the traces at
+// every point of the edge, the local lifts of every mode and the gradient plus lift at every point
+// (the work a point needs of all variables, done once per slot instead of once per point); the
+// four lanes then exchange them by shuffles, and lane g < NG evaluates HLLC and the viscous fluxes
+// at point g.  Every value is the same expression in the same order as in the reference's loops.
 // ------------------------------------------------------------------------------------------
 // Physical first derivatives of mode b at point g of local edge k (mesh.rs:115-127) with the
 // element's inverse Jacobian (dxi/dx, dxi/dy, deta/dx, deta/dy).
@@ -217,85 +222,114 @@ __device__ __forceinline__ void ns_dphi_edge(const NsParams<P>& ns, int k, int g
   dy = xy * ns.dphi_edge[k][g][b][0] + ey * ns.dphi_edge[k][g][b][1];
 }
 
+// The four lanes' values a[h] at point `me`: out[j] = lane j's a[me] (all lanes take part).
+template <int NG>
+__device__ __forceinline__ void ns_gather(unsigned int mask, const double (&a)[NG], int me, double out[4]) {
+#pragma unroll
+  for (int h = 0; h < NG; ++h)
+#pragma unroll
+    for (int j = 0; j < NEQ; ++j) {
+      const double v = __shfl_sync(mask, a[h], j, 4);
+      if (h == me) out[j] = v;
+    }
+}
+
+constexpr int kNsEdgeThreads = 128;  // 32 slots per block
+
 template <int P>
-__global__ void __launch_bounds__(128) k_edge_flux_ns(const __grid_constant__ KParams<P, double> kp,
-                                                      const __grid_constant__ NsParams<P> ns,
-                                                      const double* __restrict__ U, double* __restrict__ F) {
+__global__ void __launch_bounds__(kNsEdgeThreads) k_edge_flux_ns(const __grid_constant__ KParams<P, double> kp,
+                                                                 const __grid_constant__ NsParams<P> ns,
+                                                                 const double* __restrict__ U, double* __restrict__ F) {
   using V = Variant<P>;
   constexpr int NB = V::NB, NG = V::NG;
   const MeshDev& m = kp.m;
   const Gas& gas = kp.gas;
   const size_t ld = m.ld;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)(m.n_int + m.n_bnd) * NG) return;
-  const int s = (int)(t / NG), g = (int)(t - (long long)s * NG);
+  if ((t >> 2) >= (long long)(m.n_int + m.n_bnd)) return;  // the slot's four lanes together
+  const int s = (int)(t >> 2), w = (int)(t & 3);
+  const unsigned int mask = 0xFu << (threadIdx.x & 28);     // the slot's four lanes
   double out[4];
   if (s < m.n_int) {  // integrate_over_edges_ns, spatial_disc.rs:212-348
     const int2 lr = m.ie_lr[s];
     const int inst = m.n_inst > 1 ? m.inst[lr.x] : 0;
     if (!kp.ic[inst].active) return;
-    const int ic = m.ie_ic[s], ilic = ic & 3, iric = ic >> 2, gr = NG - 1 - g;
+    const int ic = m.ie_ic[s], ilic = ic & 3, iric = ic >> 2;
     const double4 geo = m.ie_geo[s];
     const double nx = geo.x, ny = geo.y, jd = geo.w;
-    const double* UL = U + (size_t)lr.x * NEQ * NB;
-    const double* UR = U + (size_t)lr.y * NEQ * NB;
+    const double* UL = U + (size_t)lr.x * NEQ * NB + w * NB;
+    const double* UR = U + (size_t)lr.y * NEQ * NB + w * NB;
     const double JL = m.jac[lr.x], JR = m.jac[lr.y];
     const double lxx = m.dinv[0 * ld + lr.x], lxy = m.dinv[1 * ld + lr.x], lex = m.dinv[2 * ld + lr.x],
                  ley = m.dinv[3 * ld + lr.x];
     const double rxx = m.dinv[0 * ld + lr.y], rxy = m.dinv[1 * ld + lr.y], rex = m.dinv[2 * ld + lr.y],
                  rey = m.dinv[3 * ld + lr.y];
-    double lv[4], rv[4], gxL[4], gyL[4], gxR[4], gyR[4];
-#pragma unroll 1
-    for (int w = 0; w < NEQ; ++w) {  // one variable at a time: keeps the two records out of registers
-      // traces of variable w at every point of the edge (the jumps of the local lifts)
-      double tl[NG], tr[NG];
+    // variable w: traces at every point (the jumps of the local lifts)
+    double tl[NG], tr[NG];
 #pragma unroll
-      for (int h = 0; h < NG; ++h) {
-        double a = 0.0, c = 0.0;
-#pragma unroll
-        for (int b = 0; b < NB; ++b) {
-          a += UL[w * NB + b] * kp.d.phi_edge[ilic][h][b];
-          c += UR[w * NB + b] * kp.d.phi_edge[iric][NG - 1 - h][b];
-        }
-        tl[h] = a;
-        tr[h] = c;
-      }
-      lv[w] = tl[g];
-      rv[w] = tr[g];
-      // gradient and local lift at this point, each side (spatial_disc.rs:290-300, 318-328)
-      double dxl = 0.0, dyl = 0.0, llx = 0.0, lly = 0.0, dxr = 0.0, dyr = 0.0, rlx = 0.0, rly = 0.0;
+    for (int h = 0; h < NG; ++h) {
+      double a = 0.0, c = 0.0;
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        double ax = 0.0, ay = 0.0, cx = 0.0, cy = 0.0;  // local lifts of mode b (:233-249)
+        a += UL[b] * kp.d.phi_edge[ilic][h][b];
+        c += UR[b] * kp.d.phi_edge[iric][NG - 1 - h][b];
+      }
+      tl[h] = a;
+      tr[h] = c;
+    }
+    // gradient and local lift of variable w at every point, each side (spatial_disc.rs:290-300,
+    // 318-328); the right side at the reversed point
+    double dxl[NG], dyl[NG], llx[NG], lly[NG], dxr[NG], dyr[NG], rlx[NG], rly[NG];
 #pragma unroll
-        for (int h = 0; h < NG; ++h) {
-          const double jump_x = (tl[h] - tr[h]) * nx, jump_y = (tl[h] - tr[h]) * ny;
-          ax -= 0.5 * jump_x * kp.d.phi_edge[ilic][h][b] * kp.d.edge_w[h] * 0.5 * jd;
-          ay -= 0.5 * jump_y * kp.d.phi_edge[ilic][h][b] * kp.d.edge_w[h] * 0.5 * jd;
-          cx += 0.5 * jump_x * kp.d.phi_edge[iric][NG - 1 - h][b] * kp.d.edge_w[NG - 1 - h] * 0.5 * jd;
-          cy += 0.5 * jump_y * kp.d.phi_edge[iric][NG - 1 - h][b] * kp.d.edge_w[NG - 1 - h] * 0.5 * jd;
-        }
-        ax /= ns.mass[b] * 0.5 * JL;
-        ay /= ns.mass[b] * 0.5 * JL;
-        cx /= ns.mass[b] * 0.5 * JR;
-        cy /= ns.mass[b] * 0.5 * JR;
+    for (int g = 0; g < NG; ++g) dxl[g] = dyl[g] = llx[g] = lly[g] = dxr[g] = dyr[g] = rlx[g] = rly[g] = 0.0;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      double ax = 0.0, ay = 0.0, cx = 0.0, cy = 0.0;  // local lifts of mode b (:233-249)
+#pragma unroll
+      for (int h = 0; h < NG; ++h) {
+        const double jump_x = (tl[h] - tr[h]) * nx, jump_y = (tl[h] - tr[h]) * ny;
+        ax -= 0.5 * jump_x * kp.d.phi_edge[ilic][h][b] * kp.d.edge_w[h] * 0.5 * jd;
+        ay -= 0.5 * jump_y * kp.d.phi_edge[ilic][h][b] * kp.d.edge_w[h] * 0.5 * jd;
+        cx += 0.5 * jump_x * kp.d.phi_edge[iric][NG - 1 - h][b] * kp.d.edge_w[NG - 1 - h] * 0.5 * jd;
+        cy += 0.5 * jump_y * kp.d.phi_edge[iric][NG - 1 - h][b] * kp.d.edge_w[NG - 1 - h] * 0.5 * jd;
+      }
+      ax /= ns.mass[b] * 0.5 * JL;
+      ay /= ns.mass[b] * 0.5 * JL;
+      cx /= ns.mass[b] * 0.5 * JR;
+      cy /= ns.mass[b] * 0.5 * JR;
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        const int gr = NG - 1 - g;
         double dpx, dpy;
         ns_dphi_edge<P>(ns, ilic, g, b, lxx, lxy, lex, ley, dpx, dpy);
-        dxl += UL[w * NB + b] * dpx;
-        dyl += UL[w * NB + b] * dpy;
-        llx += 3.0 * ax * kp.d.phi_edge[ilic][g][b];
-        lly += 3.0 * ay * kp.d.phi_edge[ilic][g][b];
+        dxl[g] += UL[b] * dpx;
+        dyl[g] += UL[b] * dpy;
+        llx[g] += 3.0 * ax * kp.d.phi_edge[ilic][g][b];
+        lly[g] += 3.0 * ay * kp.d.phi_edge[ilic][g][b];
         ns_dphi_edge<P>(ns, iric, gr, b, rxx, rxy, rex, rey, dpx, dpy);
-        dxr += UR[w * NB + b] * dpx;
-        dyr += UR[w * NB + b] * dpy;
-        rlx += cx * kp.d.phi_edge[iric][gr][b];
-        rly += cy * kp.d.phi_edge[iric][gr][b];
+        dxr[g] += UR[b] * dpx;
+        dyr[g] += UR[b] * dpy;
+        rlx[g] += cx * kp.d.phi_edge[iric][gr][b];
+        rly[g] += cy * kp.d.phi_edge[iric][gr][b];
       }
-      gxL[w] = dxl + llx;
-      gyL[w] = dyl + lly;
-      gxR[w] = dxr + rlx;
-      gyR[w] = dyr + rly;
     }
+    double gl_x[NG], gl_y[NG], gr_x[NG], gr_y[NG];
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+      gl_x[g] = dxl[g] + llx[g];
+      gl_y[g] = dyl[g] + lly[g];
+      gr_x[g] = dxr[g] + rlx[g];
+      gr_y[g] = dyr[g] + rly[g];
+    }
+    // lane g: every variable's values at point g
+    double lv[4], rv[4], gxL[4], gyL[4], gxR[4], gyR[4];
+    ns_gather<NG>(mask, tl, w, lv);
+    ns_gather<NG>(mask, tr, w, rv);
+    ns_gather<NG>(mask, gl_x, w, gxL);
+    ns_gather<NG>(mask, gl_y, w, gyL);
+    ns_gather<NG>(mask, gr_x, w, gxR);
+    ns_gather<NG>(mask, gr_y, w, gyR);
+    if (w >= NG) return;
     const int st = hllc<double>(lv, rv, nx, ny, gas, out);
     if (st != ST_OK) raise_status(kp.ctl, &kp.ic[inst], st, m.slot_ref[s]);
     const double muL = ns_viscosity(lv, gas, ns.rgas), muR = ns_viscosity(rv, gas, ns.rgas);
@@ -320,82 +354,105 @@ __global__ void __launch_bounds__(128) k_edge_flux_ns(const __grid_constant__ KP
     const double* Ue = U + (size_t)e * NEQ * NB;
     const double J = m.jac[e];
     const double xx = m.dinv[0 * ld + e], xy = m.dinv[1 * ld + e], ex = m.dinv[2 * ld + e], ey = m.dinv[3 * ld + e];
-    // traces (and far-field states) at every point of the face
+    // every variable's traces at every point (lane w evaluates variable w), and the far-field
+    // states there
+    double tw[NG];
+#pragma unroll
+    for (int h = 0; h < NG; ++h) {
+      double a = 0.0;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) a += Ue[w * NB + b] * kp.d.phi_edge[ic][h][b];
+      tw[h] = a;
+    }
     double tv[NG][4], qn[NG][4];
 #pragma unroll
     for (int h = 0; h < NG; ++h) {
 #pragma unroll
-      for (int v = 0; v < NEQ; ++v) {
-        double a = 0.0;
-#pragma unroll
-        for (int b = 0; b < NB; ++b) a += Ue[v * NB + b] * kp.d.phi_edge[ic][h][b];
-        tv[h][v] = a;
-      }
+      for (int j = 0; j < NEQ; ++j) tv[h][j] = __shfl_sync(mask, tw[h], j, 4);
       if (!wall) far_field_state<double>(tv[h], nx, ny, m.patch_q[info >> 3], gas, qn[h]);
     }
-    double gx[4], gy[4];
+    // variable w: local lift (wall :181-201, with the cell tables at the point index; far field
+    // :264-302), gradient plus 3 x lift at every point
+    double gxw[NG], gyw[NG], dx[NG], dy[NG], lx[NG], ly[NG];
 #pragma unroll
-    for (int w = 0; w < NEQ; ++w) {
-      double dx = 0.0, dy = 0.0, lx = 0.0, ly = 0.0;
+    for (int g = 0; g < NG; ++g) dx[g] = dy[g] = lx[g] = ly[g] = 0.0;
 #pragma unroll
-      for (int b = 0; b < NB; ++b) {
-        double ax = 0.0, ay = 0.0;  // local lift of mode b: wall (:181-201, cell tables), far field (:264-302)
-        if (!wall || w > 0) {
+    for (int b = 0; b < NB; ++b) {
+      double ax = 0.0, ay = 0.0;
+      if (!wall || w > 0) {
 #pragma unroll
-          for (int h = 0; h < NG; ++h) {
-            double comp;
-            if (wall) {
-              const double pressure =
-                  gas.gm1 * (tv[h][3] - 0.5 * (tv[h][1] * tv[h][1] + tv[h][2] * tv[h][2]) / tv[h][0]);
-              comp = w == 3 ? tv[h][3] - pressure / gas.gm1 : tv[h][w];
-              ax -= 0.5 * (comp * nx) * kp.t.phi_cell[h][b] * kp.d.cell_w[h] * 0.5 * J;
-              ay -= 0.5 * (comp * ny) * kp.t.phi_cell[h][b] * kp.d.cell_w[h] * 0.5 * J;
-            } else {
-              comp = tv[h][w] - qn[h][w];
-              ax -= 0.5 * (comp * nx) * kp.d.phi_edge[ic][h][b] * kp.d.edge_w[h] * 0.5 * jd;
-              ay -= 0.5 * (comp * ny) * kp.d.phi_edge[ic][h][b] * kp.d.edge_w[h] * 0.5 * jd;
-            }
+        for (int h = 0; h < NG; ++h) {
+          double comp;
+          if (wall) {
+            const double pressure =
+                gas.gm1 * (tv[h][3] - 0.5 * (tv[h][1] * tv[h][1] + tv[h][2] * tv[h][2]) / tv[h][0]);
+            comp = w == 3 ? tv[h][3] - pressure / gas.gm1 : tw[h];
+            ax -= 0.5 * (comp * nx) * kp.t.phi_cell[h][b] * kp.d.cell_w[h] * 0.5 * J;
+            ay -= 0.5 * (comp * ny) * kp.t.phi_cell[h][b] * kp.d.cell_w[h] * 0.5 * J;
+          } else {
+            const double qw = w == 0 ? qn[h][0] : w == 1 ? qn[h][1] : w == 2 ? qn[h][2] : qn[h][3];
+            comp = tw[h] - qw;
+            ax -= 0.5 * (comp * nx) * kp.d.phi_edge[ic][h][b] * kp.d.edge_w[h] * 0.5 * jd;
+            ay -= 0.5 * (comp * ny) * kp.d.phi_edge[ic][h][b] * kp.d.edge_w[h] * 0.5 * jd;
           }
-          ax /= ns.mass[b] * 0.5 * J;
-          ay /= ns.mass[b] * 0.5 * J;
         }
+        ax /= ns.mass[b] * 0.5 * J;
+        ay /= ns.mass[b] * 0.5 * J;
+      }
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
         double dpx, dpy;
         ns_dphi_edge<P>(ns, ic, g, b, xx, xy, ex, ey, dpx, dpy);
-        dx += Ue[w * NB + b] * dpx;
-        dy += Ue[w * NB + b] * dpy;
-        lx += 3.0 * ax * kp.d.phi_edge[ic][g][b];
-        ly += 3.0 * ay * kp.d.phi_edge[ic][g][b];
+        dx[g] += Ue[w * NB + b] * dpx;
+        dy[g] += Ue[w * NB + b] * dpy;
+        lx[g] += 3.0 * ax * kp.d.phi_edge[ic][g][b];
+        ly[g] += 3.0 * ay * kp.d.phi_edge[ic][g][b];
       }
-      gx[w] = dx + lx;
-      gy[w] = dy + ly;
     }
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+      gxw[g] = dx[g] + lx[g];
+      gyw[g] = dy[g] + ly[g];
+    }
+    double gx[4], gy[4];
+    ns_gather<NG>(mask, gxw, w, gx);
+    ns_gather<NG>(mask, gyw, w, gy);
+    if (w >= NG) return;
+    double tg[4], qg[4];  // the trace and far-field state at this lane's point
+#pragma unroll
+    for (int h = 0; h < NG; ++h)
+      if (h == w)
+#pragma unroll
+        for (int j = 0; j < NEQ; ++j) {
+          tg[j] = tv[h][j];
+          qg[j] = qn[h][j];
+        }
     double inv[4];
     if (wall) {
-      const double pressure = gas.gm1 * (tv[g][3] - 0.5 * (tv[g][1] * tv[g][1] + tv[g][2] * tv[g][2]) / tv[g][0]);
+      const double pressure = gas.gm1 * (tg[3] - 0.5 * (tg[1] * tg[1] + tg[2] * tg[2]) / tg[0]);
       inv[0] = 0.0;
       inv[1] = pressure * nx;
       inv[2] = pressure * ny;
       inv[3] = 0.0;
     } else {
-      const double* q = qn[g];
-      const double u_new = q[1] / q[0], v_new = q[2] / q[0];
+      const double u_new = qg[1] / qg[0], v_new = qg[2] / qg[0];
       const double vn_new = u_new * nx + v_new * ny;
-      const double p_new = gas.gm1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
-      const double h_new = q[3] + p_new;
-      inv[0] = q[0] * vn_new;
-      inv[1] = q[1] * vn_new + p_new * nx;
-      inv[2] = q[2] * vn_new + p_new * ny;
+      const double p_new = gas.gm1 * (qg[3] - 0.5 * (qg[1] * qg[1] + qg[2] * qg[2]) / qg[0]);
+      const double h_new = qg[3] + p_new;
+      inv[0] = qg[0] * vn_new;
+      inv[1] = qg[1] * vn_new + p_new * nx;
+      inv[2] = qg[2] * vn_new + p_new * ny;
       inv[3] = h_new * vn_new;
     }
-    const double mu = ns_viscosity(tv[g], gas, ns.rgas);
+    const double mu = ns_viscosity(tg, gas, ns.rgas);
 #pragma unroll
     for (int i = 0; i < NEQ; ++i) {
       double fv, gv;
-      ns_viscous_row(i, tv[g], mu, ns.hp, gx, gy, fv, gv);
+      ns_viscous_row(i, tg, mu, ns.hp, gx, gy, fv, gv);
       out[i] = (inv[i] - (nx * fv + ny * gv)) * geo.z;
     }
   }
-  store_flux<double>(F, (size_t)s, NG, g, out);
+  store_flux<double>(F, (size_t)s, NG, w, out);
 }
 
 // ------------------------------------------------------------------------------------------

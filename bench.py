@@ -488,6 +488,7 @@ def precision_case(inst, K, modes, local, label):
         sd.set_edge_form(cfg["edge_form"])
         sd.set_limiter_detector(cfg["limiter_detector"] == "staged")
         sd.set_limiter_schedule(cfg["limiter_schedule"] == "queue")
+        sd.set_limiter_grid(cfg["limiter_grid"] == "one_per_sm")
         td.set_initial_on_device(init)
         if prec == "fp64_perturbed":
             U0 = sd.new_state()

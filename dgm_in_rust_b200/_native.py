@@ -185,6 +185,8 @@ def lib() -> ctypes.CDLL:
     L.dgm_diagnostics.argtypes = [vp, ctypes.c_int32, P_D]
     L.dgm_enqueue_diagnostics.argtypes = [vp, ctypes.c_int32]
     L.dgm_set_viscous.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, P_D]
+    L.dgm_set_limiter_grid.argtypes = [vp, ctypes.c_int32]
+    L.dgm_get_limiter_grid.argtypes = [vp]
     L.dgm_get_viscous.argtypes = [vp]
     L.dgm_collected_diagnostics.argtypes = [vp, P_D]
     L.dgm_precision.argtypes = [vp]
@@ -239,7 +241,8 @@ def lib() -> ctypes.CDLL:
                  "dgm_set_limiter_variant", "dgm_get_limiter_variant", "dgm_set_limiter_schedule",
                  "dgm_get_limiter_schedule", "dgm_cell_fields", "dgm_set_edge_variant", "dgm_get_edge_variant",
                  "dgm_instance_replace", "dgm_instance_capacity", "dgm_enqueue_diagnostics",
-                 "dgm_collected_diagnostics", "dgm_set_viscous", "dgm_get_viscous"):
+                 "dgm_collected_diagnostics", "dgm_set_viscous", "dgm_get_viscous", "dgm_set_limiter_grid",
+                 "dgm_get_limiter_grid"):
         getattr(L, name).restype = ctypes.c_int32
     _lib = L
     return L

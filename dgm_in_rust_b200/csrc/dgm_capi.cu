@@ -83,6 +83,7 @@ struct dgm_ctx {
   std::vector<void*> allocs;
   int64_t bytes = 0;
   int coop_blocks[2] = {1, 1};   // co-resident blocks of the limiter's wave kernel [schedule]
+  int lim_one_per_sm = 0;        // wave kernel on one block per SM (cheaper grid barriers) instead of all
   int lim_staged = 0;            // limiter detector variant (dgm_set_limiter_variant / autotune)
   int lim_queue = 0;             // limiter schedule (dgm_set_limiter_schedule / autotune)
   int edge_pair = 0;             // edge pass form: 0 thread per (slot, point), 1 lane pair per slot,
@@ -313,7 +314,8 @@ struct Ops {
                                                                                     c->status, c->wl1, c->pend, c->order);
     CK(cudaGetLastError());
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(c->coop_blocks[c->lim_queue]);
+    const int full = c->coop_blocks[c->lim_queue];
+    cfg.gridDim = dim3(c->lim_one_per_sm ? std::min(full, c->num_sms) : full);
     cfg.blockDim = dim3(dgm::kLimiterWarps * 32);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = c->stream;
@@ -1889,6 +1891,18 @@ static int set_schedule(dgm_ctx* c, int queue) {
   return DGM_OK;
 }
 
+int32_t dgm_set_limiter_grid(dgm_ctx* c, int32_t one_per_sm) {
+  if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
+  if (!c || (one_per_sm != 0 && one_per_sm != 1)) return DGM_BAD_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return DGM_CUDA_ERROR;
+  CK(cudaStreamSynchronize(c->stream));
+  c->lim_one_per_sm = one_per_sm;
+  reset_graphs(c);
+  return DGM_OK;
+}
+
+int32_t dgm_get_limiter_grid(dgm_ctx* c) { return c ? c->lim_one_per_sm : -1; }
+
 int32_t dgm_set_limiter_schedule(dgm_ctx* c, int32_t queue) {
   if (c && c->mixed) return DGM_BAD_ARG;  // per-order settings and single-mesh calls
   if (!c || (queue != 0 && queue != 1)) return DGM_BAD_ARG;
@@ -2033,15 +2047,24 @@ int32_t dgm_autotune(dgm_ctx* c, int32_t repeats, double* best_us) {
     return DGM_OK;
   };
   if (c->limiter) {
-    int bv = 0, bq = 0;
+    // detector form x schedule x wave-kernel grid (all co-resident blocks, or one per SM)
+    int bv = 0, bq = 0, bg = 0;
+    float best = 1e30f;
     for (int v = 0; v < 2 && !st; ++v)
       for (int q = 0; q < 2 && !st; ++q) {
-        c->lim_staged = v;
-        st = set_schedule(c, q);
-        if (!st) st = time_limiter(&c->lim_us[v][q]);
-        if (!st && c->lim_us[v][q] < c->lim_us[bv][bq]) bv = v, bq = q;
+        c->lim_us[v][q] = 1e30f;
+        for (int gsz = 0; gsz < 2 && !st; ++gsz) {
+          c->lim_staged = v;
+          c->lim_one_per_sm = gsz;
+          st = set_schedule(c, q);
+          float us = 0.f;
+          if (!st) st = time_limiter(&us);
+          if (!st && us < c->lim_us[v][q]) c->lim_us[v][q] = us;
+          if (!st && us < best) best = us, bv = v, bq = q, bg = gsz;
+        }
       }
     c->lim_staged = bv;
+    c->lim_one_per_sm = bg;
     if (!st) st = set_schedule(c, bq);
   }
   for (auto& cand : edge_cand) {

@@ -142,7 +142,8 @@ def _launch_config(L, ctx) -> dict:
     return {"edge_threads": cfg[0], "edge_blocks": cfg[1], "element_threads": cfg[2],
             "limiter_detector": "staged" if staged.value else "compact",
             "limiter_schedule": "queue" if queue.value else "barrier",
-            "edge_form": EDGE_FORMS[L.dgm_get_edge_variant(ctx)]}
+            "edge_form": EDGE_FORMS[L.dgm_get_edge_variant(ctx)],
+            "limiter_grid": "one_per_sm" if L.dgm_get_limiter_grid(ctx) == 1 else "full"}
 
 
 def _autotune(L, ctx, repeats: int) -> dict:
@@ -353,6 +354,11 @@ class SpatialDisc:
     @property
     def viscous(self) -> bool:
         return bool(self._lib.dgm_get_viscous(self._ctx) == 1)
+
+    def set_limiter_grid(self, one_per_sm: bool) -> None:
+        """Run the limiter's cooperative wave kernel on one block per SM (cheaper grid barriers)
+        or on every co-resident block (more warps for the reconstructions); same results."""
+        self._check(self._lib.dgm_set_limiter_grid(self._ctx, 1 if one_per_sm else 0), "set_limiter_grid")
 
     def set_limiter_detector(self, staged: bool) -> None:
         """Pick the limiter's KXRCF detector form: staged loads (fewer memory round trips, more

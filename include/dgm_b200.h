@@ -279,6 +279,12 @@ int32_t dgm_set_limiter_variant(dgm_ctx* ctx, int32_t staged);
 /* Current form, and the limiter times the last dgm_autotune measured for forms 0 and 1 at their
  * faster schedule (us; either pointer may be NULL). */
 int32_t dgm_get_limiter_variant(dgm_ctx* ctx, int32_t* staged, double* tuned_us /* [2] */);
+/* The grid of the limiter's cooperative wave kernel: 0 every co-resident block (the most warps
+ * for the reconstructions), 1 one block per SM (fewer arrivals at each grid barrier: cheaper
+ * waves when a wave holds few cells).  Same results.  The autotuner picks one.  No counterpart in
+ * the reference. */
+int32_t dgm_set_limiter_grid(dgm_ctx* ctx, int32_t one_per_sm);
+int32_t dgm_get_limiter_grid(dgm_ctx* ctx);
 /* The schedule of the limiter's wave launch from wave 2 on (same results bit for bit): 0 barrier
  * (each wave scans the elements still waiting for a lower-index neighbour, passes a grid barrier,
  * then reconstructs the troubled elements it enlisted), 1 queue (warps that have finished the scan

@@ -64,13 +64,14 @@ def test_launch_config_rejects_bad_values(built):
                 s.spatial_disc.set_launch_config(*bad)
         assert s.spatial_disc.launch_config == {"edge_threads": 256, "edge_blocks": 0, "element_threads": 256,
                                                 "limiter_detector": "compact", "limiter_schedule": "barrier",
-                                                "edge_form": "point"}
+                                                "edge_form": "point", "limiter_grid": "full"}
         sd = s.spatial_disc
         assert sd._lib.dgm_set_edge_variant(sd.ctx, 4) == 7  # DGM_BAD_ARG
         with pytest.raises(ValueError):
             sd.set_edge_form("tiles")
         assert sd._lib.dgm_set_limiter_variant(sd.ctx, 2) == 7  # DGM_BAD_ARG
         assert sd._lib.dgm_set_limiter_schedule(sd.ctx, 2) == 7
+        assert sd._lib.dgm_set_limiter_grid(sd.ctx, 2) == 7
     finally:
         s.close()
 
@@ -101,17 +102,21 @@ def test_batch_autotune_keeps_results(built):
 @pytest.mark.parametrize("order", [1, 2, 3])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_limiter_detector_forms_agree(built, order, precision):
-    """The staged and compact KXRCF detectors, each under the barrier and the queue schedule,
-    flag the same cells, limit a perturbed state identically and give the same time steps."""
+    """The staged and compact KXRCF detectors, each under the barrier and the queue schedule and
+    on either wave-kernel grid, flag the same cells, limit a perturbed state identically and give
+    the same time steps."""
     mesh, init = instance_mesh(Instance(40, 20, 0.8, 1.25, order))
     rng = np.random.default_rng(order)
     out = []
-    for staged, queue in ((False, False), (True, False), (False, True), (True, True)):
+    for staged, queue, one_per_sm in ((False, False, False), (True, False, False), (False, True, False),
+                                      (True, True, False), (False, False, True), (True, True, True)):
         s = build_solver(mesh, order, 1.4, 0.1, 1.0e30, 6, precision=precision)
         try:
             sd, td = s.spatial_disc, s.temporal_disc
             sd.set_limiter_detector(staged)
             sd.set_limiter_schedule(queue)
+            sd.set_limiter_grid(one_per_sm)
+            assert sd.launch_config["limiter_grid"] == ("one_per_sm" if one_per_sm else "full")
             assert sd.launch_config["limiter_detector"] == ("staged" if staged else "compact")
             assert sd.launch_config["limiter_schedule"] == ("queue" if queue else "barrier")
             td.set_initial_on_device(init)

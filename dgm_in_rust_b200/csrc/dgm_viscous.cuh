@@ -98,6 +98,52 @@ __device__ __forceinline__ void ns_viscous_row(int i, const double q[4], double 
   }
 }
 
+// The local lift of variable w on boundary slot sb (boundary_condition.rs:181-302): the wall's
+// momentum and energy jumps with the cell tables at the point index, the far field's jumps to the
+// characteristic state with the edge tables.
+template <int P>
+__device__ __noinline__ void ns_boundary_lift(const KParams<P, double>& kp, const double* __restrict__ Ue, int sb,
+                                              int w, double J, double (&llx)[Variant<P>::NB],
+                                              double (&lly)[Variant<P>::NB]) {
+  using V = Variant<P>;
+  constexpr int NB = V::NB, NG = V::NG;
+  const MeshDev& m = kp.m;
+  const int info = m.be_info[sb];
+  const int ic = info & 3;
+  const double4 geo = m.be_geo[sb];
+  const bool wall = ((info >> 2) & 1) == 0;
+  for (int b = 0; b < NB; ++b) llx[b] = lly[b] = 0.0;
+  if (wall && w == 0) return;
+  for (int g = 0; g < NG; ++g) {
+    double lv[4];
+    for (int v = 0; v < NEQ; ++v) {
+      double a = 0.0;
+      for (int b = 0; b < NB; ++b) a += Ue[v * NB + b] * kp.d.phi_edge[ic][g][b];
+      lv[v] = a;
+    }
+    double comp;
+    if (wall) {  // boundary_condition.rs:183-201: momentum and energy jumps, cell tables at g
+      const double pressure = kp.gas.gm1 * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
+      const double boundary_energy = pressure / kp.gas.gm1;
+      comp = w == 1 ? lv[1] : w == 2 ? lv[2] : lv[3] - boundary_energy;
+    } else {  // boundary_condition.rs:264-289
+      double q[4];
+      far_field_state<double>(lv, geo.x, geo.y, m.patch_q[info >> 3], kp.gas, q);
+      comp = lv[w] - q[w];
+    }
+    const double jx = comp * geo.x, jy = comp * geo.y;
+    for (int b = 0; b < NB; ++b) {
+      if (wall) {
+        llx[b] -= 0.5 * jx * kp.t.phi_cell[g][b] * kp.d.cell_w[g] * 0.5 * J;
+        lly[b] -= 0.5 * jy * kp.t.phi_cell[g][b] * kp.d.cell_w[g] * 0.5 * J;
+      } else {
+        llx[b] -= 0.5 * jx * kp.d.phi_edge[ic][g][b] * kp.d.edge_w[g] * 0.5 * geo.w;
+        lly[b] -= 0.5 * jy * kp.d.phi_edge[ic][g][b] * kp.d.edge_w[g] * 0.5 * geo.w;
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Global lifts: a thread per (element, variable).
 // ------------------------------------------------------------------------------------------
@@ -148,49 +194,10 @@ __global__ void __launch_bounds__(256) k_ns_lift(const __grid_constant__ KParams
         }
       }
     } else {
-      // boundary face: its local lift, added whole (global_lift + local_lift)
-      const int sb = slot - m.n_int;
-      const int info = m.be_info[sb];
-      const int ic = info & 3;
-      const double4 geo = m.be_geo[sb];
-      const bool wall = ((info >> 2) & 1) == 0;
+      // boundary face: its local lift, added whole (global_lift + local_lift); out of line, so
+      // that the rare far-field arithmetic does not hold registers in the common path
       double llx[NB], lly[NB];
-#pragma unroll
-      for (int b = 0; b < NB; ++b) llx[b] = lly[b] = 0.0;
-      if (!wall || w > 0) {
-#pragma unroll
-        for (int g = 0; g < NG; ++g) {
-          double lv[4];
-#pragma unroll
-          for (int v = 0; v < NEQ; ++v) {
-            double a = 0.0;
-#pragma unroll
-            for (int b = 0; b < NB; ++b) a += Ue[v * NB + b] * kp.d.phi_edge[ic][g][b];
-            lv[v] = a;
-          }
-          double comp;
-          if (wall) {  // boundary_condition.rs:183-201: momentum and energy jumps, cell tables at g
-            const double pressure = kp.gas.gm1 * (lv[3] - 0.5 * (lv[1] * lv[1] + lv[2] * lv[2]) / lv[0]);
-            const double boundary_energy = pressure / kp.gas.gm1;
-            comp = w == 1 ? lv[1] : w == 2 ? lv[2] : lv[3] - boundary_energy;
-          } else {  // boundary_condition.rs:264-289
-            double q[4];
-            far_field_state<double>(lv, geo.x, geo.y, m.patch_q[info >> 3], kp.gas, q);
-            comp = lv[w] - q[w];
-          }
-          const double jx = comp * geo.x, jy = comp * geo.y;
-#pragma unroll
-          for (int b = 0; b < NB; ++b) {
-            if (wall) {
-              llx[b] -= 0.5 * jx * kp.t.phi_cell[g][b] * kp.d.cell_w[g] * 0.5 * J;
-              lly[b] -= 0.5 * jy * kp.t.phi_cell[g][b] * kp.d.cell_w[g] * 0.5 * J;
-            } else {
-              llx[b] -= 0.5 * jx * kp.d.phi_edge[ic][g][b] * kp.d.edge_w[g] * 0.5 * geo.w;
-              lly[b] -= 0.5 * jy * kp.d.phi_edge[ic][g][b] * kp.d.edge_w[g] * 0.5 * geo.w;
-            }
-          }
-        }
-      }
+      ns_boundary_lift<P>(kp, Ue, slot - m.n_int, w, J, llx, lly);
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
         lx[b] = lx[b] + llx[b];

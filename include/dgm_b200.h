@@ -243,10 +243,10 @@ int32_t dgm_launch_phase(dgm_ctx* ctx, int32_t phase);
  * not depend on it.  No counterpart in the reference. */
 int32_t dgm_set_launch_config(dgm_ctx* ctx, int32_t edge_threads, int32_t edge_blocks, int32_t element_threads);
 int32_t dgm_get_launch_config(dgm_ctx* ctx, int32_t* config /* [3] as above */);
-/* Autotuner: times each candidate configuration of the edge pass (both forms) and the element
- * pass, and both forms of the limiter's KXRCF detector, on the resident state (repeats launches each, CUDA events)
- * and keeps the fastest; best_us (may be NULL) receives the chosen edge and element times in
- * microseconds.  Call after a state is uploaded. */
+/* Autotuner: times each candidate configuration of the edge pass (every form) and the element
+ * pass, and the limiter's detector forms, schedules and wave-kernel grids, on the resident state
+ * (repeats launches each, CUDA events) and keeps the fastest; best_us (may be NULL) receives the
+ * chosen edge and element times in microseconds.  Call after a state is uploaded. */
 int32_t dgm_autotune(dgm_ctx* ctx, int32_t repeats, double* best_us /* [2] */);
 /* The edge pass's form (same arithmetic, bitwise identical results): 0 one thread per (edge slot,
  * Gauss point), 1 two lanes per slot, one per side, each loading its element once and evaluating

@@ -242,7 +242,7 @@ struct Ops {
       const int64_t full = std::max<int64_t>(1, (warps * 32 + tpb - 1) / tpb);
       const int blocks = (int)(c->edge_blocks > 0 ? std::min<int64_t>(c->edge_blocks, full) : full);
       dgm::k_edge_flux_staged<P, T, St><<<blocks, tpb, 0, c->stream>>>(kp_of<P, T>(c), U, Fx(c->F));
-    } else if (c->edge_pair) {  // a warp covers 16 slots per iteration
+    } else if (c->edge_pair == 1) {  // a warp covers 16 slots per iteration
       const int64_t warps = (c->n_int + c->n_bnd + 15) / 16;
       const int64_t full = std::max<int64_t>(1, (warps * 32 + threads - 1) / threads);
       const int blocks = (int)(c->edge_blocks > 0 ? std::min<int64_t>(c->edge_blocks, full) : full);
